@@ -1,0 +1,148 @@
+/*
+ * necgpu -- C-ABI of the sm_100a kernels behind the NEC2++ thin-wire hot path.
+ *
+ * The host library (libnecpp_b200.so, which also exports the libnecpp.h API)
+ * calls these at the three points where NEC2++ runs its hot path:
+ *
+ *   nec_context::structure_segment_loading  (src/nec_context.cpp:1523-1558)
+ *       cmset (fill, 2077-2204) + factrs (LU, src/matrix_algebra.cpp:319-338)
+ *       -> necgpu_set_structure, necgpu_fill, necgpu_factor
+ *   nec_context::netwk_compute_currents     (src/nec_context.cpp:4850-4935)
+ *       solves (src/matrix_algebra.cpp:351-503) +
+ *       c_geometry::get_current_coefficients (src/c_geometry.cpp:3299-3387)
+ *       -> necgpu_solve
+ *   nec_context::excitation_compute_far_field (src/nec_context.cpp:1761-1790)
+ *       ffld (6639-6888) inside nec_radiation_pattern::analyze
+ *       (src/nec_radiation_pattern.cpp:209-450)
+ *       -> necgpu_pattern
+ *
+ * Plain pointers and sizes only.  Every function returns 0 on success and a
+ * non-zero NECGPU_* status on failure; necgpu_last_error() gives the text.
+ * There is no CPU fallback: without a usable CUDA device necgpu_create fails.
+ */
+#ifndef NECGPU_H
+#define NECGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum necgpu_status {
+  NECGPU_OK = 0,
+  NECGPU_ERR_CUDA = 1,        /* a CUDA call failed */
+  NECGPU_ERR_ARG = 2,         /* bad argument or call order */
+  NECGPU_ERR_SINGULAR = 3,    /* zero pivot met in the factorisation */
+  NECGPU_ERR_NONFINITE = 4,   /* NaN / Inf in the matrix or solution */
+  NECGPU_ERR_REFINE = 5,      /* iterative refinement did not converge */
+  NECGPU_ERR_UNSUPPORTED = 6, /* a kernel path this build does not provide */
+  NECGPU_ERR_NO_DEVICE = 7
+};
+
+enum necgpu_precision {
+  NECGPU_FP64 = 0,  /* complex128 fill, LU and solve */
+  NECGPU_MIXED = 1  /* complex64 LU (tensor-core trailing update) + FP64 refinement */
+};
+
+enum necgpu_ground {
+  NECGPU_GROUND_NONE = 0,
+  NECGPU_GROUND_PERFECT = 1,
+  NECGPU_GROUND_REFLECTION = 2, /* finite ground, reflection-coefficient approximation */
+  NECGPU_GROUND_SOMMERFELD = 3  /* finite ground, Sommerfeld/Norton (Norton branch) */
+};
+
+/* One structure at one frequency.  Lengths are in wavelengths, as after
+ * c_geometry::frequency_scale.  Basis tables are the per-source-segment lists
+ * of c_geometry::trio (src/c_geometry.cpp:2982-3100) in CSR form with
+ * 0-based basis indices. */
+typedef struct necgpu_structure {
+  int64_t n;
+  const double *x, *y, *z, *length, *radius, *cab, *sab, *salp;
+  const int32_t* trio_ptr; /* n+1 */
+  const int32_t* trio_basis;
+  const double *trio_a, *trio_b, *trio_c;
+  const int32_t* ek_ind1; /* extended-kernel end flags per source segment (or NULL) */
+  const int32_t* ek_ind2;
+  double rkh;   /* far-pair threshold in wavelengths (KH card) */
+  int32_t use_exk;
+  int32_t ground; /* necgpu_ground */
+  double zrati_re, zrati_im; /* 1/sqrt(eps_c) */
+  double frati_re, frati_im; /* image scale factor */
+  double eta;   /* wave impedance of the medium, sqrt(mu/eps) (src/electromag.cpp:31-35) */
+} necgpu_structure;
+
+typedef struct necgpu_engine necgpu_engine;
+
+/* Replaces: nothing in the reference (the reference has no device state);
+ * owned per nec_context and released by nec_delete (src/libNEC.cpp:40-42). */
+int necgpu_create(necgpu_engine** out, int device);
+int necgpu_destroy(necgpu_engine* e);
+const char* necgpu_last_error(const necgpu_engine* e);
+
+/* Use the given cudaStream_t (as void*) for all work; NULL = the engine's own
+ * stream. */
+int necgpu_set_stream(necgpu_engine* e, void* stream);
+
+/* Upload one structure (host arrays, copied). */
+int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s);
+
+/* Replaces cmset (src/nec_context.cpp:2077-2204) for wires: fills Z on the
+ * device, row-major, Z[obs*n + basis] = field at obs due to basis (the
+ * reference's cm layout). */
+int necgpu_fill(necgpu_engine* e);
+
+/* Replaces factrs/lu_decompose (src/matrix_algebra.cpp:217-266, 319-338):
+ * LU with partial pivoting of the filled Z in the requested precision. */
+int necgpu_factor(necgpu_engine* e, int precision);
+
+/* Replaces solves/solve (src/matrix_algebra.cpp:271-307, 351-503) and
+ * get_current_coefficients (src/c_geometry.cpp:3299-3387).  rhs: n complex
+ * (interleaved re,im) applied field; cur: n complex segment-centre currents
+ * (the reference's current_vector after the call); abc: if not NULL, 6*n
+ * doubles air,aii,bir,bii,cir,cii.  Mixed precision refines the solution in
+ * FP64 against the FP64 Z until the relative residual drops below tol. */
+int necgpu_solve(necgpu_engine* e, const double* rhs, double* cur, double* abc);
+
+/* Replaces the ffld loop of nec_radiation_pattern::analyze
+ * (src/nec_context.cpp:6639-6888, src/nec_radiation_pattern.cpp:281-283):
+ * far field of the last solution at n_dir directions (radians).
+ * eth/eph: n_dir complex each.  ksymp/ground describe the image (the ground
+ * of necgpu_structure is used). */
+int necgpu_pattern(necgpu_engine* e, int n_dir, const double* theta,
+                   const double* phi, double* eth, double* eph);
+
+/* Refinement controls for NECGPU_MIXED (defaults: 1e-13, 30). */
+int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter);
+
+/* Diagnostics of the last necgpu_solve / necgpu_factor. */
+typedef struct necgpu_stats {
+  int refine_iters;
+  double refine_residual;   /* final ||b - Z x|| / ||b|| (FP64) */
+  double ms_fill, ms_factor, ms_solve, ms_pattern; /* last timings (0 if not timed) */
+  int64_t launches;         /* kernels launched by the engine since create */
+} necgpu_stats;
+int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out);
+int necgpu_enable_timing(necgpu_engine* e, int on);
+
+/* Device-resident access for benchmarks and tests: pointers into the engine's
+ * own device buffers (valid until the next set_structure / destroy). */
+int necgpu_device_z(necgpu_engine* e, void** z_fp64, int64_t* ld);
+/* Copy the filled (unfactored) Z to the host: n*n complex, out[basis + obs*n],
+ * the layout of the reference's cm after cmset.  Only valid between
+ * necgpu_fill and necgpu_factor(NECGPU_FP64) (which factors in place). */
+int necgpu_copy_z(necgpu_engine* e, double* host_out);
+
+/* Benchmark support: keep one right-hand side and one direction list
+ * resident, then run fill -> factor -> solve -> coefficients -> far field
+ * entirely on the device (no host transfers; one status read at the end). */
+int necgpu_set_resident(necgpu_engine* e, const double* rhs, int n_dir, const double* theta,
+                        const double* phi);
+int necgpu_step_resident(necgpu_engine* e, int precision);
+/* Copy results of the last resident step (cur: n complex, eth/eph: n_dir complex). */
+int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NECGPU_H */

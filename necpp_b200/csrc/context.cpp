@@ -1,0 +1,885 @@
+// Card state machine, excitation, network-free solve and far-field epilogue.
+// Follows nec_context (src/nec_context.cpp, line ranges per function); the
+// fill, factor, solve and far-field sum run on the GPU via necgpu.h.
+#include "context.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+
+#include "../../include/necgpu.h"
+#include "nec_constants.h"
+#include "nec_error.h"
+
+namespace necb {
+
+Medium& medium() {
+  static Medium m;
+  return m;
+}
+
+namespace {
+void check(necgpu_engine* e, int st) {
+  if (st != NECGPU_OK) fail("GPU: ", necgpu_last_error(e));
+}
+}  // namespace
+
+Context::Context() {}
+Context::~Context() {
+  if (eng_) necgpu_destroy(eng_);
+}
+
+necgpu_engine* Context::engine() {
+  if (!eng_) {
+    int dev = 0;
+    if (const char* s = std::getenv("NECPP_B200_DEVICE")) dev = std::atoi(s);
+    necgpu_engine* e = nullptr;
+    int st = necgpu_create(&e, dev);
+    if (st != NECGPU_OK) {
+      std::string msg = e ? necgpu_last_error(e) : "no CUDA device";
+      if (e) necgpu_destroy(e);
+      fail("GPU: ", msg);
+    }
+    eng_ = e;
+  }
+  return eng_;
+}
+
+// calc_prepare, src/nec_context.cpp:123-165
+void Context::calc_prepare() {
+  iflow = 1;
+  state_ = MEM;
+  rkh = 1.;
+  use_exk = false;
+  ex_type = 0;
+  m_near = -1;
+  ifar = -1;
+  freq_mhz = speed_of_light() / 1.0e6;
+  zrati = cd(1.0, 0.0);
+  ksymp = 1;
+  nradl = 0;
+  iperf = 0;
+  epsr = 0;
+  sig = 0;
+  nfrq = 1;
+  iptflg = -2;
+  iptflq = -1;
+  iped = 0;
+}
+
+void Context::reset_to_structure_loading() {
+  if (state_ != MEM) state_ = STRUCT;
+}
+void Context::reset_to_excitation_setup() {
+  if (state_ != MEM && state_ != STRUCT) state_ = EXSETUP;
+}
+
+void Context::geometry_complete(int gpflag) {
+  geo_.complete(gpflag);
+  calc_prepare();
+}
+
+// fr_card, src/nec_context.cpp:406-420
+void Context::fr_card(int in_ifrq, int in_nfrq, double in_freq, double in_del) {
+  ifrq = in_ifrq;
+  nfrq = in_nfrq == 0 ? 1 : in_nfrq;
+  freq_mhz = in_freq;
+  delfrq = in_del;
+  if (iped == 1) zpnorm = 0.0;
+  state_ = MEM;
+  iflow = 1;
+}
+
+// gn_card / nec_ground::parse_gn, src/nec_context.cpp:486-499,
+// src/nec_ground.cpp:75-120
+void Context::gn_card(int itmp1, int itmp2, double t1, double t2, double t3,
+                      double t4, double t5, double t6) {
+  (void)t3;
+  (void)t4;
+  (void)t5;
+  (void)t6;
+  if (itmp1 == -1) {
+    ksymp = 1;
+    nradl = 0;
+    iperf = 0;
+  } else {
+    if (itmp1 < 0 || itmp1 > 2) fail("GN: unknown ground type ", itmp1);
+    iperf = itmp1;
+    nradl = itmp2;
+    ksymp = 2;
+    epsr = t1;
+    sig = t2;
+    if (nradl != 0) {
+      if (iperf == 2)
+        fail("RADIAL WIRE G.S. APPROXIMATION MAY NOT BE USED WITH SOMMERFELD GROUND OPTION");
+      fail("GN: radial-wire ground screen is not part of the B200 hot path");
+    }
+    if (iperf == 0) {
+      if (epsr == 0.0) fail("GROUND DIELECTRIC CONSTANT IS ZERO");
+      if (sig == 0.0) fail("GROUND CONDUCTIVITY IS ZERO");
+    }
+  }
+  iflow = 4;
+  reset_to_structure_loading();
+}
+
+// ex_card, src/nec_context.cpp:521-608
+void Context::ex_card(int type, int i2, int i3, int i4, double f1, double f2,
+                      double f3, double f4, double f5, double f6) {
+  if (!geo_.completed) fail("EX card before geometry_complete");
+  if (type < 0 || type > 5) fail("EX: unknown excitation type ", type);
+  if (type == 5) fail("EX 5 (voltage discontinuity source) is not part of the B200 hot path");
+  if (iflow != 5) {
+    src_seg.clear();
+    src_volt.clear();
+    iped = 0;
+    iflow = 5;
+    reset_to_excitation_setup();
+  }
+  masym = i4 / 10;
+  ex_type = type;
+  if (type == 0) {
+    int64_t seg = geo_.segment_number(i2, i3);
+    if (seg > geo_.n)
+      fail("CHECK DATA, PARAMETER SPECIFYING EXCITATION SOURCE SEGMENT [", seg, "] IS TOO LARGE");
+    cd v(f1, f2);
+    if (std::abs(v) < 1.e-20) v = cd(1.0, 0.0);
+    src_seg.push_back(seg);
+    src_volt.push_back(v);
+    iped = i4 - masym * 10;
+    zpnorm = f3;
+    if (iped == 1 && zpnorm > 0.0) iped = 2;
+    return;
+  }
+  nthi = i2;
+  nphi = i3;
+  xpr1 = f1;
+  xpr2 = f2;
+  xpr3 = f3;
+  xpr4 = f4;
+  xpr5 = f5;
+  xpr6 = f6;
+  src_seg.clear();
+  src_volt.clear();
+  thetis = xpr1;
+  phiss = xpr2;
+}
+
+// xq_card, src/nec_context.cpp:709-743
+void Context::xq_card(int mode) {
+  if ((iflow == 10 && mode == 0) || (nfrq == 1 && mode == 0 && iflow > 7)) return;
+  if (mode == 0) {
+    iflow = (iflow > 7) ? 11 : 7;
+  } else {
+    ifar = 0;
+    rfld = 0.;
+    ipd = 0;
+    iavp = 0;
+    rp_norm = 0;
+    rp_fmt = 0;
+    nth = 91;
+    nph = 1;
+    thets = 0.0;
+    phis = 0.0;
+    dth = 1.0;
+    dph = 0.0;
+    if (mode == 2) phis = 90.0;
+    if (mode == 3) {
+      nph = 2;
+      dph = 90.0;
+    }
+  }
+  simulate(true);
+}
+
+// rp_card, src/nec_context.cpp:828-869
+void Context::rp_card(int mode, int n_theta, int n_phi, int fmt, int norm, int d,
+                      int a, double th0, double ph0, double in_dth, double in_dph,
+                      double radial, double gain_norm) {
+  if (mode != 0) fail("RP mode ", mode, " (ground-wave / cliff patterns) is not part of the B200 hot path");
+  ifar = mode;
+  nth = n_theta == 0 ? 1 : n_theta;
+  nph = n_phi == 0 ? 1 : n_phi;
+  rp_fmt = fmt != 0 ? 1 : 0;
+  rp_norm = norm;
+  ipd = d != 0 ? 1 : 0;
+  iavp = a;
+  if (nth < 2 || nph < 2 || ifar == 1) iavp = 0;
+  thets = th0;
+  phis = ph0;
+  dth = in_dth;
+  dph = in_dph;
+  rfld = radial;
+  gnor = gain_norm;
+  iflow = 10;
+  simulate(true);
+}
+
+void Context::kh_card(double r) {
+  rkh = r;
+  reset_to_structure_loading();
+  iflow = 1;
+}
+
+void Context::ek_card(int flag) {
+  use_exk = (-1 != flag);
+  reset_to_structure_loading();
+  iflow = 1;
+}
+
+void Context::pt_card(int a, int b, int c, int d) {
+  iptflg = a;
+  iptag = b;
+  iptagf = c;
+  iptagt = d;
+  if (c == 0 && iptflg != -1) iptflg = -2;
+  if (d == 0) iptagt = iptagf;
+}
+
+void Context::pq_card(int a, int b, int c, int d) {
+  iptflq = a;
+  iptaq = b;
+  iptaqf = c;
+  iptaqt = d;
+  if (c == 0 && iptflq != -1) iptflq = -2;
+  if (d == 0) iptaqt = iptaqf;
+}
+
+void Context::medium_parameters(double permittivity, double permeability) {
+  medium().permittivity = permittivity;
+  medium().permeability = permeability;
+}
+
+// simulate, src/nec_context.cpp:1031-1160.  The processing state the call
+// starts from decides how much is recomputed; for every frequency of an FR
+// sweep the structure is rescaled, refilled and refactored.
+void Context::simulate(bool far_field_flag) {
+  if (!geo_.completed) fail("simulation requested before geometry_complete");
+  const int igox = (far_field_flag && state_ == NEAR) ? FAR : state_;
+  int mhz = 1;
+  bool in_freq_loop = false;
+  do {
+    if (igox <= MEM) {
+      if (!in_freq_loop) {
+        mhz = 1;
+        in_freq_loop = true;
+      }
+      if (mhz != 1) {
+        if (ifrq == 1)
+          freq_mhz *= delfrq;
+        else
+          freq_mhz += delfrq;
+      }
+      wavelength_ = wavelength_of(1.0e6 * freq_mhz);
+      geo_.frequency_scale(freq_mhz);
+      state_ = STRUCT;
+    }
+    if (igox <= STRUCT) {
+      structure_loading();
+      state_ = EXSETUP;
+    }
+    if (igox <= EXSETUP) {
+      nthic = 1;
+      nphic = 1;
+      inc = 1;
+    }
+    int ret = excitation_loop(igox, mhz);
+    if (ret == FREQ_CONT) continue;
+    if (ret == CARD_CONT) return;
+    nphic = 1;
+    xpr2 = phiss;
+    if (mhz == nfrq) ifar = -1;
+    if (nfrq == 1) return;
+    nfrq = 1;
+    mhz = 1;
+  } while (++mhz <= nfrq);
+}
+
+// excitation_loop, src/nec_context.cpp:1793-1857
+int Context::excitation_loop(int state_in, int mhz) {
+  while (true) {
+    if (state_in < EXLOOP) {
+      int ret = excitation_inner(mhz);
+      if (ret == INNER_CONT) continue;
+      if (ret != PHASE_DONE) return ret;
+    }
+    if (state_in < NEAR) state_ = NEAR;
+    // near fields (NE/NH) are not part of the hot path: m_near stays -1
+    far_field();
+    if (ex_type == 0 || ex_type == 4 || ex_type == 5) {
+      if (mhz == nfrq) ifar = -1;
+      if (nfrq != 1) return FREQ_CONT;
+      return CARD_CONT;
+    }
+    nthic++;
+    inc++;
+    xpr1 += xpr4;
+    if (nthic <= nthi) continue;
+    nthic = 1;
+    xpr1 = thetis;
+    xpr2 += xpr5;
+    nphic++;
+    if (nphic > nphi) {
+      if (nfrq != 1) return FREQ_CONT;
+      return PRINT_NORM;
+    }
+  }
+}
+
+// excitation_process_inner, src/nec_context.cpp:1622-1738 (no networks, no
+// loads, no coupling).
+int Context::excitation_inner(int mhz) {
+  (void)mhz;
+  network_solve();
+  if (iptflg < -2 || iptflg > 3) iptflg = -1;
+  if (iptflq < -2 || iptflq > 0) iptflq = -1;
+  if (ex_type != 1 && ex_type != 2 && ex_type != 3 && (iptflg == 2 || iptflg == 3)) iptflg = -1;
+  structure_power_loss = 0.0;
+  if (iptflg != -1 || iptflq != -1) {
+    if ((iptflg < 1 || iptflg == 3 || ((iptflg == 1 || iptflg == 2) && inc <= 1)) ||
+        (iptflg == -1 && iptflq != -1)) {
+      if (iptflg != 3) {
+        StructureCurrents sc;
+        sc.freq_hz = freq_mhz * 1.0e6;
+        sc.current.resize(geo_.n);
+        for (int64_t i = 0; i < geo_.n; i++) sc.current[i] = solution[i] * wavelength_;
+        currents.push_back(std::move(sc));
+      }
+    }
+  }
+  state_ = EXLOOP;
+  if (iflow == 7) {
+    if (ex_type >= 1 && ex_type <= 3) {
+      nthic++;
+      inc++;
+      xpr1 += xpr4;
+      if (nthic <= nthi) return INNER_CONT;
+      nthic = 1;
+      xpr1 = thetis;
+      xpr2 = xpr2 + xpr5;
+      nphic++;
+      if (nphic <= nphi) return INNER_CONT;
+      return PRINT_NORM;
+    }
+    if (nfrq != 1) return FREQ_CONT;
+    return CARD_CONT;
+  }
+  return PHASE_DONE;
+}
+
+// nec_ground::calculate_antenna_environment, src/nec_ground.cpp:177-219
+void Context::antenna_environment() {
+  if (ksymp != 2) return;
+  frati = cd(1.0, 0.0);
+  if (iperf == 1) return;
+  double lambda = wavelength_of(freq_mhz * 1.0e6);
+  if (sig < 0.) sig = -sig / (impedance_over_2pi() * lambda);
+  epsc = cd(epsr, -sig * lambda * impedance_over_2pi());
+  zrati = 1.0 / std::sqrt(epsc);
+  if (iperf == 2) frati = (epsc - 1.0) / (epsc + 1.0);
+}
+
+// structure_segment_loading, src/nec_context.cpp:1523-1558: ground
+// environment, then fill and factor on the GPU.
+void Context::structure_loading() {
+  antenna_environment();
+  const int64_t n = geo_.n;
+  geo_.prepare_basis();
+
+  std::vector<int32_t> tptr(n + 1), tbasis;
+  std::vector<double> ta, tb, tc;
+  tbasis.reserve(3 * n);
+  ta.reserve(3 * n);
+  tb.reserve(3 * n);
+  tc.reserve(3 * n);
+  std::vector<BasisEntry> entries;
+  tptr[0] = 0;
+  for (int64_t j = 0; j < n; j++) {
+    geo_.trio((int)(j + 1), entries);
+    for (auto& e : entries) {
+      tbasis.push_back(e.basis - 1);
+      ta.push_back(e.a);
+      tb.push_back(e.b);
+      tc.push_back(e.c);
+    }
+    tptr[j + 1] = (int32_t)tbasis.size();
+  }
+
+  // extended thin-wire kernel end flags, cmww src/nec_context.cpp:2533-2594
+  std::vector<int32_t> ind1(n, 0), ind2(n, 0);
+  if (use_exk) {
+    for (int64_t jj = 0; jj < n; jj++) {
+      const int jx = (int)jj + 1;
+      const double cabj = geo_.cab[jj], sabj = geo_.sab[jj];
+      int ipr = geo_.icon1[jj];
+      int i1 = 2;
+      int iprx = std::abs(ipr) - 1;
+      if (ipr > kPatchConnection)
+        i1 = 0;
+      else if (ipr == 0)
+        i1 = 1;
+      else if (ipr == jx && cabj * cabj + sabj * sabj <= 1.e-8)
+        i1 = 0;
+      else if (ipr > 0 && geo_.icon2[iprx] == jx)
+        i1 = geo_.test_ek_approximation((int)jj, ipr - 1);
+      else if (ipr < 0 && geo_.icon1[iprx] == -jx)
+        i1 = geo_.test_ek_approximation((int)jj, -ipr - 1);
+      ind1[jj] = i1;
+
+      ipr = geo_.icon2[jj];
+      int i2;
+      if (ipr > kPatchConnection)
+        i2 = 2;
+      else if (ipr == 0)
+        i2 = 1;
+      else if (ipr < 0) {
+        int ix = -ipr - 1;
+        i2 = (-geo_.icon2[ix] != jx) ? 2 : geo_.test_ek_approximation((int)jj, ix);
+      } else if (ipr != jx) {
+        int ix = ipr - 1;
+        i2 = (geo_.icon1[ix] != jx) ? 2 : geo_.test_ek_approximation((int)jj, ix);
+      } else {
+        i2 = (cabj * cabj + sabj * sabj > 1.e-8) ? 2 : 0;
+      }
+      ind2[jj] = i2;
+    }
+  }
+
+  necgpu_structure s{};
+  s.n = n;
+  s.x = geo_.x.data();
+  s.y = geo_.y.data();
+  s.z = geo_.z.data();
+  s.length = geo_.length.data();
+  s.radius = geo_.radius.data();
+  s.cab = geo_.cab.data();
+  s.sab = geo_.sab.data();
+  s.salp = geo_.salp.data();
+  s.trio_ptr = tptr.data();
+  s.trio_basis = tbasis.data();
+  s.trio_a = ta.data();
+  s.trio_b = tb.data();
+  s.trio_c = tc.data();
+  s.ek_ind1 = ind1.data();
+  s.ek_ind2 = ind2.data();
+  s.rkh = rkh;
+  s.use_exk = use_exk ? 1 : 0;
+  if (ksymp != 2)
+    s.ground = NECGPU_GROUND_NONE;
+  else if (iperf == 1)
+    s.ground = NECGPU_GROUND_PERFECT;
+  else if (iperf == 0)
+    s.ground = NECGPU_GROUND_REFLECTION;
+  else
+    s.ground = NECGPU_GROUND_SOMMERFELD;
+  s.zrati_re = zrati.real();
+  s.zrati_im = zrati.imag();
+  s.frati_re = frati.real();
+  s.frati_im = frati.imag();
+  s.eta = impedance();
+
+  necgpu_engine* e = engine();
+  check(e, necgpu_set_structure(e, &s));
+  check(e, necgpu_fill(e));
+  check(e, necgpu_factor(e, precision_));
+  have_factor_ = true;
+}
+
+// etmns and its helpers, src/nec_context.cpp:3193-3550 (wires only).
+void Context::build_rhs(std::vector<cd>& e) {
+  const int64_t n = geo_.n;
+  e.assign(n, cd(0, 0));
+  double p1 = 0, p2 = 0, p3 = 0, p4 = 0, p5 = 0, p6 = 0;
+  if (ex_type != 0 && ex_type != 5) {
+    p5 = degrees_to_rad(xpr5);
+    p4 = degrees_to_rad(xpr4);
+    if (ex_type == 4) {
+      p1 = xpr1 / wavelength_;
+      p2 = xpr2 / wavelength_;
+      p3 = xpr3 / wavelength_;
+      p6 = xpr6 / (wavelength_ * wavelength_);
+    } else {
+      p1 = degrees_to_rad(xpr1);
+      p2 = degrees_to_rad(xpr2);
+      p3 = degrees_to_rad(xpr3);
+      p6 = xpr6;
+    }
+  }
+  const double amp = (xpr7 != 0.0) ? xpr7 : 1.0;
+  const auto& g = geo_;
+
+  if (ex_type == 0) {
+    for (size_t k = 0; k < src_seg.size(); k++) {
+      int64_t s = src_seg[k] - 1;
+      e[s] = -src_volt[k] / (g.length[s] * wavelength_);
+    }
+    return;
+  }
+  if (ex_type == 4) {  // elementary current source, 3387-3486
+    double cosp4 = std::cos(p4);
+    double wx = cosp4 * std::cos(p5), wy = cosp4 * std::sin(p5), wz = std::sin(p4);
+    double ds = p6 * impedance_over_2pi();
+    for (int64_t i = 0; i < n; i++) {
+      double pxl = g.x[i] - p1, pyl = g.y[i] - p2, pzl = g.z[i] - p3;
+      double rs = pxl * pxl + pyl * pyl + pzl * pzl;
+      if (rs < 1.0e-30) continue;
+      double r = std::sqrt(rs);
+      pxl = pxl / r;
+      pyl = pyl / r;
+      pzl = pzl / r;
+      double cth = pxl * wx + pyl * wy + pzl * wz;
+      double sth = std::sqrt(1.0 - cth * cth);
+      double qx = pxl - wx * cth, qy = pyl - wy * cth, qz = pzl - wz * cth;
+      double arg = std::sqrt(qx * qx + qy * qy + qz * qz);
+      if (arg >= 1.e-30) {
+        qx = qx / arg;
+        qy = qy / arg;
+        qz = qz / arg;
+      } else {
+        qx = 1.0;
+        qy = 0.0;
+        qz = 0.0;
+      }
+      arg = kTwoPi * r;
+      cd tt1(std::cos(arg), -std::sin(arg));
+      cd tt2 = cd(1.0, -1.0 / arg) / rs;
+      cd er = ds * tt1 * tt2 * cth;
+      cd et = 0.5 * ds * tt1 * (cd(0.0, 1.0) * kTwoPi / r + tt2) * sth;
+      cd ezh = er * cth - et * sth;
+      cd erh = er * sth + et * cth;
+      cd cx = ezh * wx + erh * qx, cy = ezh * wy + erh * qy, cz = ezh * wz + erh * qz;
+      e[i] = -(cx * g.cab[i] + cy * g.sab[i] + cz * g.salp[i]);
+    }
+    return;
+  }
+  // plane waves, 3505-3550
+  double cth = std::cos(p1), sth = std::sin(p1);
+  double cph = std::cos(p2), sph = std::sin(p2);
+  double cet = std::cos(p3), set = std::sin(p3);
+  double pxl = cth * cph * cet - sph * set;
+  double pyl = cth * sph * cet + cph * set;
+  double pzl = -sth * cet;
+  double wx = -sth * cph, wy = -sth * sph, wz = -cth;
+  double qx = wy * pzl - wz * pyl;
+  double qy = wz * pxl - wx * pzl;
+  double qz = wx * pyl - wy * pxl;
+  cd rrv, rrh;
+  if (ksymp == 2) {
+    if (iperf == 1) {
+      rrv = -cd(1.0, 0.0);
+      rrh = -cd(1.0, 0.0);
+    } else {
+      rrv = std::sqrt(1.0 - zrati * zrati * sth * sth);
+      rrh = zrati * cth;
+      rrh = (rrh - rrv) / (rrh + rrv);
+      rrv = zrati * rrv;
+      rrv = -(cth - rrv) / (cth + rrv);
+    }
+  }
+  if (ex_type == 1) {  // 3213-3291
+    for (int64_t i = 0; i < n; i++) {
+      double arg = -kTwoPi * (wx * g.x[i] + wy * g.y[i] + wz * g.z[i]);
+      cd ea(std::cos(arg), std::sin(arg));
+      e[i] = -(pxl * g.cab[i] + pyl * g.sab[i] + pzl * g.salp[i]) * ea * amp;
+    }
+    if (ksymp == 2) {
+      cd tt1 = (pyl * cph - pxl * sph) * (rrh - rrv);
+      cd cx = rrv * pxl - tt1 * sph;
+      cd cy = rrv * pyl + tt1 * cph;
+      cd cz = -rrv * pzl;
+      for (int64_t i = 0; i < n; i++) {
+        double arg = -kTwoPi * (wx * g.x[i] + wy * g.y[i] - wz * g.z[i]);
+        cd ea(std::cos(arg), std::sin(arg));
+        e[i] -= (cx * g.cab[i] + cy * g.sab[i] + cz * g.salp[i]) * ea * amp;
+      }
+    }
+    return;
+  }
+  // elliptic, 3294-3385
+  cd tt1 = -(cd(0.0, 1.0)) * p6;
+  if (ex_type == 3) tt1 = -tt1;
+  cd cx = pxl + tt1 * qx, cy = pyl + tt1 * qy, cz = pzl + tt1 * qz;
+  for (int64_t i = 0; i < n; i++) {
+    double arg = -kTwoPi * (wx * g.x[i] + wy * g.y[i] + wz * g.z[i]);
+    cd ea(std::cos(arg), std::sin(arg));
+    e[i] = -(cx * g.cab[i] + cy * g.sab[i] + cz * g.salp[i]) * ea * amp;
+  }
+  if (ksymp == 2) {
+    cd tt2 = (cy * cph - cx * sph) * (rrh - rrv);
+    cd ccx = rrv * cx - tt2 * sph;
+    cd ccy = rrv * cy + tt2 * cph;
+    cd ccz = -rrv * cz;
+    for (int64_t i = 0; i < n; i++) {
+      double arg = -kTwoPi * (wx * g.x[i] + wy * g.y[i] - wz * g.z[i]);
+      cd ea(std::cos(arg), std::sin(arg));
+      e[i] -= (ccx * g.cab[i] + ccy * g.sab[i] + ccz * g.salp[i]) * ea * amp;
+    }
+  }
+}
+
+// netwk without networks (src/nec_context.cpp:4494-5065): solve, currents,
+// antenna input parameters of the voltage sources.
+void Context::network_solve() {
+  input_power = 0.0;
+  network_power_loss = 0.0;
+  const int64_t n = geo_.n;
+  std::vector<cd> rhs;
+  build_rhs(rhs);
+  solution.assign(n, cd(0, 0));
+  abc.assign(6 * n, 0.0);
+  necgpu_engine* e = engine();
+  check(e, necgpu_solve(e, reinterpret_cast<const double*>(rhs.data()),
+                        reinterpret_cast<double*>(solution.data()), abc.data()));
+  necgpu_stats st{};
+  necgpu_get_stats(e, &st);
+  last_refine_residual = st.refine_residual;
+  last_refine_iters = st.refine_iters;
+
+  if (src_seg.empty()) return;
+  AntennaInput ai;
+  ai.freq_hz = freq_mhz * 1.0e6;
+  for (size_t k = 0; k < src_seg.size(); k++) {
+    int64_t s = src_seg[k] - 1;
+    cd voltage = src_volt[k];
+    cd current = solution[s] * wavelength_;
+    cd admittance = current / voltage;
+    cd imp = voltage / current;
+    double power = 0.5 * std::real(voltage * std::conj(current));
+    input_power += power;
+    ai.tag.push_back(geo_.tags[s]);
+    ai.seg.push_back((int)(s + 1));
+    ai.voltage.push_back(voltage);
+    ai.current.push_back(current);
+    ai.impedance.push_back(imp);
+    ai.admittance.push_back(admittance);
+    ai.power.push_back(power);
+  }
+  inputs.push_back(std::move(ai));
+}
+
+// excitation_compute_far_field + nec_radiation_pattern::analyze,
+// src/nec_context.cpp:1761-1790, src/nec_radiation_pattern.cpp:209-450.
+// The direction grid is stepped exactly as the reference steps it; the field
+// sum runs on the GPU; gains and polarisation are evaluated here.
+void Context::far_field() {
+  if (ifar == -1) return;
+  const bool ground = (ksymp == 2);
+  RadiationPattern rp;
+  rp.freq_hz = freq_mhz * 1.0e6;
+  rp.nth = nth;
+  rp.nph = nph;
+  rp.th0 = thets;
+  rp.ph0 = phis;
+  rp.dth = dth;
+  rp.dph = dph;
+  const size_t cells = (size_t)nth * nph;
+  rp.gain.assign(cells, 0.0);
+  rp.gain_vert.assign(cells, 0.0);
+  rp.gain_horiz.assign(cells, 0.0);
+  rp.gain_tot.assign(cells, 0.0);
+  rp.gain_rhcp.assign(cells, 0.0);
+  rp.gain_lhcp.assign(cells, 0.0);
+  rp.axial_ratio.assign(cells, 0.0);
+  rp.tilt.assign(cells, 0.0);
+  rp.avg_scale.assign(cells, 0.0);
+  rp.sense.assign(cells, 0);
+  rp.e_theta.assign(cells, cd(0, 0));
+  rp.e_phi.assign(cells, cd(0, 0));
+
+  double gcon, gcop;
+  const double pinr_in = input_power, pnlr = network_power_loss;
+  double pinr = pinr_in;
+  if (ex_type == 0 || ex_type == 5) {
+    gcop = wavelength_ * wavelength_ * 2.0 * kPi / (impedance() * pinr);
+    double prad = pinr - structure_power_loss - pnlr;
+    gcon = gcop;
+    if (ipd != 0) gcon = gcon * pinr / prad;
+  } else if (ex_type == 4) {
+    pinr = 394.51 * xpr6 * xpr6 * wavelength_ * wavelength_;
+    gcop = wavelength_ * wavelength_ * 2. * kPi / (impedance() * pinr);
+    double prad = pinr - structure_power_loss - pnlr;
+    gcon = gcop;
+    if (ipd != 0) gcon = gcon * pinr / prad;
+  } else {
+    gcon = 4. * kPi / (1.0 + xpr6 * xpr6);
+    gcop = gcon;
+  }
+  double exrm = 0., exra = 0.;
+  if (rfld >= 1.0e-20) {
+    exrm = 1. / rfld;
+    exra = rfld / wavelength_;
+    exra = -360. * (exra - std::floor(exra));
+  }
+
+  // direction list, stepped as in analyze (accumulated degrees)
+  std::vector<double> tha_list, pha_list;
+  std::vector<int> cell_list;
+  {
+    double phi = phis - dph;
+    for (int kph = 0; kph < nph; kph++) {
+      phi += dph;
+      double pha = degrees_to_rad(phi);
+      double thet = thets - dth;
+      for (int kth = 0; kth < nth; kth++) {
+        thet += dth;
+        if (ground && thet > 90.01) continue;
+        tha_list.push_back(degrees_to_rad(thet));
+        pha_list.push_back(pha);
+        cell_list.push_back(kth + kph * nth);
+      }
+    }
+  }
+  const int ndir = (int)tha_list.size();
+  std::vector<cd> eth(ndir), eph(ndir);
+  if (ndir > 0) {
+    necgpu_engine* e = engine();
+    check(e, necgpu_pattern(e, ndir, tha_list.data(), pha_list.data(),
+                            reinterpret_cast<double*>(eth.data()),
+                            reinterpret_cast<double*>(eph.data())));
+  }
+
+  double pint = 0.0;
+  const double delta_phi_rad = degrees_to_rad(dph);
+  const double tmp2 = 0.5 * degrees_to_rad(dth);
+  for (int d = 0; d < ndir; d++) {
+    const int cell = cell_list[d];
+    const int kth = cell % nth, kph = cell / nth;
+    const double tha = tha_list[d];
+    double ethm2 = std::norm(eth[d]);
+    double ethm = std::sqrt(ethm2);
+    double etha = rad_to_degrees(std::arg(eth[d]));
+    double ephm2 = std::norm(eph[d]);
+    double ephm = std::sqrt(ephm2);
+    double epha = rad_to_degrees(std::arg(eph[d]));
+    double tilta, emajr2, eminr2, axrat;
+    int sense;
+    if (ethm2 <= 1.0e-20 && ephm2 <= 1.0e-20) {
+      tilta = 0.;
+      emajr2 = 0.;
+      eminr2 = 0.;
+      axrat = 0.;
+      sense = 3;
+    } else {
+      double dfaz = epha - etha;
+      double dfaz2 = (epha >= 0.) ? dfaz - 360. : dfaz + 360.;
+      if (std::fabs(dfaz) > std::fabs(dfaz2)) dfaz = dfaz2;
+      double cdfaz = std::cos(degrees_to_rad(dfaz));
+      double tstor1 = ethm2 - ephm2;
+      double tstor2 = 2. * ephm * ethm * cdfaz;
+      tilta = .5 * std::atan2(tstor2, tstor1);
+      double stilta = std::sin(tilta);
+      tstor1 = tstor1 * stilta * stilta;
+      tstor2 = tstor2 * stilta * std::cos(tilta);
+      emajr2 = -tstor1 + tstor2 + ethm2;
+      eminr2 = tstor1 - tstor2 + ephm2;
+      if (eminr2 < 0.) eminr2 = 0.;
+      axrat = std::sqrt(eminr2 / emajr2);
+      tilta = rad_to_degrees(tilta);
+      if (axrat <= 1.0e-5)
+        sense = 0;  // linear
+      else if (dfaz <= 0.)
+        sense = 1;  // right
+      else
+        sense = 2;  // left
+    }
+    double gnmj = db10(gcon * emajr2);
+    double gnmn = db10(gcon * eminr2);
+    double gnv = db10(gcon * ethm2);
+    double gnh = db10(gcon * ephm2);
+    double gtot = db10(gcon * (ethm2 + ephm2));
+    double g;
+    switch (rp_norm) {
+      case 0: g = gtot; break;
+      case 1: g = gnmj; break;
+      case 2: g = gnmn; break;
+      case 3: g = gnv; break;
+      case 4: g = gnh; break;
+      case 5: g = gtot; break;
+      default: fail("Unknown Gain Normalization Encountered.");
+    }
+    rp.gain[cell] = g;
+    if (iavp != 0) {
+      double tstor1 = gcop * (ethm2 + ephm2);
+      double tmp3 = tha - tmp2, tmp4 = tha + tmp2;
+      if (kth == 0)
+        tmp3 = tha;
+      else if (kth == nth - 1)
+        tmp4 = tha;
+      double da = std::fabs(delta_phi_rad * (std::cos(tmp3) - std::cos(tmp4)));
+      if (kph == 0 || kph == nph - 1) da *= .5;
+      pint += tstor1 * da;
+      if (iavp == 2) continue;
+    }
+    if (rp_fmt != 1) {
+      rp.gain_vert[cell] = gnmj;
+      rp.gain_horiz[cell] = gnmn;
+    } else {
+      rp.gain_vert[cell] = gnv;
+      rp.gain_horiz[cell] = gnh;
+    }
+    ethm *= wavelength_;
+    ephm *= wavelength_;
+    if (rfld >= 1.0e-20) {
+      ethm = ethm * exrm;
+      etha = etha + exra;
+      ephm = ephm * exrm;
+      epha = epha + exra;
+    }
+    rp.e_theta[cell] = std::polar(ethm, degrees_to_rad(etha));
+    rp.e_phi[cell] = std::polar(ephm, degrees_to_rad(epha));
+    rp.gain_tot[cell] = gtot;
+    {
+      double a = axrat;
+      if (sense == 1) a = -a;
+      double gain = from_db10(gtot);
+      double lhcp_f = (1 + 2 * a + a * a) / (2 * (1 + a * a));
+      double rhcp_f = (1 - 2 * a + a * a) / (2 * (1 + a * a));
+      rp.gain_rhcp[cell] = db10(gain * rhcp_f);
+      rp.gain_lhcp[cell] = db10(gain * lhcp_f);
+    }
+    rp.axial_ratio[cell] = axrat;
+    rp.tilt[cell] = tilta;
+    rp.sense[cell] = sense;
+    rp.avg_scale[cell] = (std::sin(tha) * (nth - 1) / nth) + 1.0 / nth;
+  }
+  if (iavp != 0) {
+    double th0r = degrees_to_rad(thets);
+    double th_range = degrees_to_rad(dth) * static_cast<double>(nth - 1);
+    double ph_range = degrees_to_rad(dph) * static_cast<double>(nph - 1);
+    double total = th0r + th_range;
+    double solid = std::fabs(ph_range * (std::cos(th0r) - std::cos(total)));
+    rp.average_power_gain = pint / solid;
+    rp.average_power_solid_angle = solid / kPi;
+  }
+  rp.max_gain = *std::max_element(rp.gain.begin(), rp.gain.end());
+  patterns.push_back(std::move(rp));
+}
+
+// statistics of nec_radiation_pattern.h:246-320; matrices are walked row
+// (theta) outer, column (phi) inner as the reference's loops do.
+double RadiationPattern::stat_max(const std::vector<double>& v) const {
+  return *std::max_element(v.begin(), v.end());
+}
+double RadiationPattern::stat_min(const std::vector<double>& v) const {
+  return *std::min_element(v.begin(), v.end());
+}
+double RadiationPattern::stat_mean(const std::vector<double>& v) const {
+  double sum = 0.0;
+  for (int i = 0; i < nth; i++)
+    for (int j = 0; j < nph; j++) sum += v[i + j * nth] * avg_scale[i + j * nth];
+  int64_t len = (int64_t)nth * nph;
+  return sum / (double(len * 2) / kPi);
+}
+double RadiationPattern::stat_sd(const std::vector<double>& v) const {
+  double mean = stat_mean(v);
+  double sum = 0.0;
+  for (int i = 0; i < nth; i++)
+    for (int j = 0; j < nph; j++) {
+      double diff = v[i + j * nth] - mean;
+      sum += diff * diff * avg_scale[i + j * nth];
+    }
+  int64_t len = (int64_t)nth * nph;
+  return std::sqrt(sum / (double(len * 2) / kPi));
+}
+
+}  // namespace necb

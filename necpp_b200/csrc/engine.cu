@@ -1,0 +1,853 @@
+// necgpu engine: device buffers, kernel orchestration and the C-ABI of
+// include/necgpu.h.  One engine per nec_context; all work goes to one
+// stream.  There is no CPU fallback: every compute step is a kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/necgpu.h"
+#include "fill.cuh"
+#include "lu.cuh"
+#include "pattern.cuh"
+#include "solve.cuh"
+
+using namespace necb;
+
+namespace {
+constexpr int kNB = 64;  // LU panel width
+}
+
+struct necgpu_engine {
+  int device = 0;
+  int nsm = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  int64_t n = 0, ld = 0;
+  int64_t launches = 0;
+  bool timing = false;
+  necgpu_stats stats{};
+
+  FieldParams P{};
+  int ground = 0, use_exk = 0;
+  double* d_seg = nullptr;  // 8n: x y z s b cab sab salp
+  int32_t* d_ind = nullptr; // 2n
+  int32_t *d_tile_ptr = nullptr, *d_tsrc = nullptr, *d_tsrc_eptr = nullptr;
+  uint8_t* d_ecol = nullptr;
+  double* d_ecoef = nullptr;  // 3*ne
+  int64_t ne = 0;
+  int ntiles = 0;
+  int32_t *d_cptr = nullptr, *d_cbasis = nullptr;
+  double* d_ccoef = nullptr;
+  int64_t nc = 0;
+
+  double2* Z64 = nullptr;
+  float2* Z32 = nullptr;
+  int factored = -1;  // precision of the factors held, -1 none
+  bool filled = false;
+  int* d_piv = nullptr;
+  int* d_perm = nullptr;
+
+  double* d_cand_val = nullptr;
+  float* d_cand_valf = nullptr;
+  int* d_cand_row = nullptr;
+  double2* d_cand_rows = nullptr;  // sized for FP64 (also used as float2)
+  double2* d_rowc = nullptr;
+  unsigned* d_counter = nullptr;
+  int* d_status = nullptr;  // [4]
+
+  double2 *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_cur = nullptr;
+  double2 *d_w1 = nullptr, *d_w2 = nullptr;  // factor-precision work (sized FP64)
+  double* d_abc = nullptr;
+  double* d_rn2 = nullptr;
+  int pat_cap = 0;
+  double *d_theta = nullptr, *d_phi = nullptr;
+  double2 *d_eth = nullptr, *d_eph = nullptr;
+  int res_ndir = 0;  // resident pattern directions (bench)
+  bool res_rhs = false;
+
+  double refine_tol = 1e-13;
+  int refine_max = 30;
+  bool have_solution = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int fail(necgpu_engine* e, int code, const std::string& msg) {
+  e->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                         \
+  do {                                                                                         \
+    cudaError_t _st = (call);                                                                  \
+    if (_st != cudaSuccess)                                                                    \
+      return fail(e, NECGPU_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_st));   \
+  } while (0)
+
+#define LAUNCHED()                                                                             \
+  do {                                                                                         \
+    e->launches++;                                                                             \
+    cudaError_t _st = cudaGetLastError();                                                      \
+    if (_st != cudaSuccess)                                                                    \
+      return fail(e, NECGPU_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(_st)); \
+  } while (0)
+
+#define TRY(x)           \
+  do {                   \
+    int _r = (x);        \
+    if (_r) return _r;   \
+  } while (0)
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+template <typename T>
+int dalloc(necgpu_engine* e, T*& p, size_t count) {
+  dfree(p);
+  if (count == 0) count = 1;
+  cudaError_t st = cudaMalloc((void**)&p, count * sizeof(T));
+  if (st != cudaSuccess) {
+    p = nullptr;
+    return fail(e, NECGPU_ERR_CUDA,
+                std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) + "): " + cudaGetErrorString(st));
+  }
+  return 0;
+}
+
+template <typename T>
+int upload(necgpu_engine* e, T*& p, const T* h, size_t count) {
+  TRY(dalloc(e, p, count));
+  if (count) CUDA_TRY(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, e->stream));
+  return 0;
+}
+
+void free_all(necgpu_engine* e) {
+  dfree(e->d_seg);
+  dfree(e->d_ind);
+  dfree(e->d_tile_ptr);
+  dfree(e->d_tsrc);
+  dfree(e->d_tsrc_eptr);
+  dfree(e->d_ecol);
+  dfree(e->d_ecoef);
+  dfree(e->d_cptr);
+  dfree(e->d_cbasis);
+  dfree(e->d_ccoef);
+  dfree(e->Z64);
+  dfree(e->Z32);
+  dfree(e->d_piv);
+  dfree(e->d_perm);
+  dfree(e->d_cand_val);
+  dfree(e->d_cand_valf);
+  dfree(e->d_cand_row);
+  dfree(e->d_cand_rows);
+  dfree(e->d_rowc);
+  dfree(e->d_counter);
+  dfree(e->d_b);
+  dfree(e->d_x);
+  dfree(e->d_r);
+  dfree(e->d_cur);
+  dfree(e->d_w1);
+  dfree(e->d_w2);
+  dfree(e->d_abc);
+  dfree(e->d_rn2);
+  dfree(e->d_theta);
+  dfree(e->d_phi);
+  dfree(e->d_eth);
+  dfree(e->d_eph);
+  e->pat_cap = 0;
+  e->res_ndir = 0;
+  e->res_rhs = false;
+  e->n = 0;
+  e->factored = -1;
+  e->filled = false;
+}
+
+int sync_status(necgpu_engine* e, int* out) {
+  int h[4];
+  CUDA_TRY(cudaMemcpyAsync(h, e->d_status, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  *out = h[0];
+  return 0;
+}
+
+void tick(necgpu_engine* e) {
+  if (e->timing) cudaEventRecord(e->ev0, e->stream);
+}
+double tock(necgpu_engine* e) {
+  if (!e->timing) return 0.0;
+  cudaEventRecord(e->ev1, e->stream);
+  cudaEventSynchronize(e->ev1);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+  return ms;
+}
+
+// ---------------- fill ----------------
+template <int G, bool X>
+int launch_fill_t(necgpu_engine* e, const FillArgs& a) {
+  dim3 grid((unsigned)((e->n + kFillTI - 1) / kFillTI), (unsigned)e->ntiles);
+  fill_kernel<G, X><<<grid, kFillTI, 0, e->stream>>>(a);
+  LAUNCHED();
+  return 0;
+}
+
+int run_fill(necgpu_engine* e, bool want64, bool want32) {
+  if (e->n <= 0) return fail(e, NECGPU_ERR_ARG, "fill: no structure set");
+  const int64_t n = e->n;
+  if (want64 && !e->Z64) TRY(dalloc(e, e->Z64, (size_t)n * e->ld));
+  if (want32 && !e->Z32) TRY(dalloc(e, e->Z32, (size_t)n * e->ld));
+  FillArgs a{};
+  a.n = n;
+  a.ld = e->ld;
+  a.x = e->d_seg;
+  a.y = e->d_seg + n;
+  a.z = e->d_seg + 2 * n;
+  a.s = e->d_seg + 3 * n;
+  a.b = e->d_seg + 4 * n;
+  a.cab = e->d_seg + 5 * n;
+  a.sab = e->d_seg + 6 * n;
+  a.salp = e->d_seg + 7 * n;
+  a.ind1 = e->d_ind;
+  a.ind2 = e->d_ind + n;
+  a.tile_src_ptr = e->d_tile_ptr;
+  a.tsrc = e->d_tsrc;
+  a.tsrc_eptr = e->d_tsrc_eptr;
+  a.ecol = e->d_ecol;
+  a.ea = e->d_ecoef;
+  a.eb = e->d_ecoef + e->ne;
+  a.ec = e->d_ecoef + 2 * e->ne;
+  a.P = e->P;
+  a.Z64 = want64 ? e->Z64 : nullptr;
+  a.Z32 = want32 ? e->Z32 : nullptr;
+  a.status = e->d_status;
+  const bool x = e->use_exk != 0;
+  switch (e->ground) {
+    case kGroundNone: return x ? launch_fill_t<kGroundNone, true>(e, a) : launch_fill_t<kGroundNone, false>(e, a);
+    case kGroundPerfect: return x ? launch_fill_t<kGroundPerfect, true>(e, a) : launch_fill_t<kGroundPerfect, false>(e, a);
+    case kGroundReflection:
+      return x ? launch_fill_t<kGroundReflection, true>(e, a) : launch_fill_t<kGroundReflection, false>(e, a);
+    default: return x ? launch_fill_t<kGroundSommerfeld, true>(e, a) : launch_fill_t<kGroundSommerfeld, false>(e, a);
+  }
+}
+
+// ---------------- LU ----------------
+template <typename R>
+int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
+  using T = typename cvec<R>::T;
+  const int64_t n = e->n, ld = e->ld;
+  if (!e->d_piv) TRY(dalloc(e, e->d_piv, (size_t)n));
+  const int Pmax = e->nsm;
+  if (!e->d_cand_val) TRY(dalloc(e, e->d_cand_val, 2 * (size_t)Pmax));
+  if (!e->d_cand_valf) TRY(dalloc(e, e->d_cand_valf, 2 * (size_t)Pmax));
+  if (!e->d_cand_row) TRY(dalloc(e, e->d_cand_row, 2 * (size_t)Pmax));
+  if (!e->d_cand_rows) TRY(dalloc(e, e->d_cand_rows, 2 * (size_t)Pmax * kNB));
+  if (!e->d_rowc) TRY(dalloc(e, e->d_rowc, 2 * (size_t)kNB));
+  if (!e->d_counter) TRY(dalloc(e, e->d_counter, 1));
+
+  constexpr size_t kSmemLimit = 200 * 1024;
+  const size_t row_bytes = kNB * sizeof(T);
+  const int rpc_max = (int)((kSmemLimit - 2 * row_bytes) / row_bytes);
+  CUDA_TRY(cudaFuncSetAttribute(panel_kernel<R, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSmemLimit));
+  const size_t trsm_smem = (size_t)(kNB * kNB + kNB * 32) * sizeof(T);
+  CUDA_TRY(cudaFuncSetAttribute(trsm_kernel<T, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm_smem));
+
+  PanelArgs<R> pa{};
+  pa.M = M;
+  pa.ld = ld;
+  pa.n = n;
+  pa.piv = e->d_piv;
+  pa.cand_val = std::is_same<R, double>::value ? (R*)e->d_cand_val : (R*)e->d_cand_valf;
+  pa.cand_row = e->d_cand_row;
+  pa.cand_rows = (T*)e->d_cand_rows;
+  pa.rowc = (T*)e->d_rowc;
+  pa.counter = e->d_counter;
+  pa.status = e->d_status;
+
+  for (int64_t k0 = 0; k0 < n; k0 += kNB) {
+    const int kb = (int)std::min<int64_t>(kNB, n - k0);
+    const int64_t m = n - k0;
+    int P = (int)std::min<int64_t>(Pmax, (m + 15) / 16);
+    P = std::max(P, 1);
+    int rpc = (int)((m + P - 1) / P);
+    if (rpc > rpc_max) return fail(e, NECGPU_ERR_UNSUPPORTED, "LU: panel does not fit in shared memory");
+    P = (int)((m + rpc - 1) / rpc);
+    pa.k0 = k0;
+    pa.kb = kb;
+    pa.rpc = rpc;
+    const size_t smem = (size_t)rpc * row_bytes + 2 * row_bytes;
+    CUDA_TRY(cudaMemsetAsync(e->d_counter, 0, sizeof(unsigned), e->stream));
+    void* args[] = {&pa};
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)panel_kernel<R, kNB>, dim3(P), dim3(kPanelThreads),
+                                         args, smem, e->stream));
+    LAUNCHED();
+    if (n > kb) {
+      laswp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv);
+      LAUNCHED();
+    }
+    const int64_t rest = n - k0 - kb;
+    if (rest > 0) {
+      trsm_kernel<T, kNB><<<(unsigned)((rest + 31) / 32), 256, trsm_smem, e->stream>>>(M, ld, n, k0, kb);
+      LAUNCHED();
+      dim3 g((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
+      gemm_sub_kernel<R><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb, ld,
+                                                  M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb);
+      LAUNCHED();
+    }
+  }
+  // permutation of the right-hand side from the interchange sequence
+  std::vector<int> piv(n), perm(n);
+  CUDA_TRY(cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  int st = 0;
+  TRY(sync_status(e, &st));
+  for (int64_t i = 0; i < n; i++) perm[i] = (int)i;
+  for (int64_t k = 0; k < n; k++) {
+    int p = piv[k];
+    if (p < 0 || p >= n) return fail(e, NECGPU_ERR_NONFINITE, "LU: invalid pivot index");
+    std::swap(perm[k], perm[p]);
+  }
+  TRY(upload(e, e->d_perm, perm.data(), perm.size()));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (st & kLuStatBarrierTimeout) return fail(e, NECGPU_ERR_CUDA, "LU: panel barrier timed out");
+  if (st & kLuStatNonFinite) return fail(e, NECGPU_ERR_NONFINITE, "LU: NaN/Inf in the matrix");
+  if (st & kLuStatSingular) return fail(e, NECGPU_ERR_SINGULAR, "LU: singular matrix (zero pivot)");
+  return 0;
+}
+
+// ---------------- triangular solves ----------------
+// x (factor precision, in d_w1) = U^-1 L^-1 P b
+template <typename R>
+int run_trsv(necgpu_engine* e, const typename cvec<R>::T* M, typename cvec<R>::T* rhs,
+             typename cvec<R>::T* sol) {
+  using T = typename cvec<R>::T;
+  const int64_t n = e->n, ld = e->ld;
+  const int nblk = (int)((n + kTrsvB - 1) / kTrsvB);
+  constexpr size_t dsm = trsv_diag_smem<T>();
+  CUDA_TRY(cudaFuncSetAttribute(trsv_diag_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+  CUDA_TRY(cudaFuncSetAttribute(trsv_diag_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+  for (int k = 0; k < nblk; k++) {
+    const int64_t b0 = (int64_t)k * kTrsvB;
+    trsv_diag_kernel<T, true><<<1, 64, dsm, e->stream>>>(M, ld, n, b0, rhs, sol);
+    LAUNCHED();
+    const int64_t r0 = b0 + kTrsvB;
+    if (r0 < n) {
+      unsigned g = (unsigned)std::min<int64_t>((n - r0 + 7) / 8, 4 * e->nsm);
+      trsv_update_kernel<T><<<g, 256, 0, e->stream>>>(M, ld, n, b0, r0, n, sol, rhs);
+      LAUNCHED();
+    }
+  }
+  // backward: sol holds y; reuse rhs as the running right-hand side
+  CUDA_TRY(cudaMemcpyAsync(rhs, sol, n * sizeof(T), cudaMemcpyDeviceToDevice, e->stream));
+  for (int k = nblk - 1; k >= 0; k--) {
+    const int64_t b0 = (int64_t)k * kTrsvB;
+    trsv_diag_kernel<T, false><<<1, 64, dsm, e->stream>>>(M, ld, n, b0, rhs, sol);
+    LAUNCHED();
+    if (b0 > 0) {
+      unsigned g = (unsigned)std::min<int64_t>((b0 + 7) / 8, 4 * e->nsm);
+      trsv_update_kernel<T><<<g, 256, 0, e->stream>>>(M, ld, n, b0, 0, b0, sol, rhs);
+      LAUNCHED();
+    }
+  }
+  return 0;
+}
+
+int ensure_vectors(necgpu_engine* e) {
+  const int64_t n = e->n;
+  if (!e->d_b) TRY(dalloc(e, e->d_b, n));
+  if (!e->d_x) TRY(dalloc(e, e->d_x, n));
+  if (!e->d_r) TRY(dalloc(e, e->d_r, n));
+  if (!e->d_cur) TRY(dalloc(e, e->d_cur, n));
+  if (!e->d_w1) TRY(dalloc(e, e->d_w1, n));
+  if (!e->d_w2) TRY(dalloc(e, e->d_w2, n));
+  if (!e->d_abc) TRY(dalloc(e, e->d_abc, 6 * (size_t)n));
+  if (!e->d_rn2) TRY(dalloc(e, e->d_rn2, 2));
+  return 0;
+}
+
+// Solve Z x = b (d_b) into d_x (FP64) with the held factors; then the
+// current coefficients into d_abc / d_cur.
+int run_solve(necgpu_engine* e, bool sync_checks) {
+  const int64_t n = e->n;
+  const unsigned g1 = (unsigned)((n + 255) / 256);
+  e->stats.refine_iters = 0;
+  e->stats.refine_residual = 0.0;
+  if (e->factored == NECGPU_FP64) {
+    permute_kernel<double2, double2><<<g1, 256, 0, e->stream>>>(e->d_b, e->d_perm, e->d_w1, n);
+    LAUNCHED();
+    TRY(run_trsv<double>(e, e->Z64, e->d_w1, e->d_x));
+  } else if (e->factored == NECGPU_MIXED) {
+    // x = 0, r = b; repeat: d = LU32^-1 r, x += d, r = b - Z64 x
+    float2* w1 = reinterpret_cast<float2*>(e->d_w1);
+    float2* w2 = reinterpret_cast<float2*>(e->d_w2);
+    CUDA_TRY(cudaMemsetAsync(e->d_x, 0, n * sizeof(double2), e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->d_r, e->d_b, n * sizeof(double2), cudaMemcpyDeviceToDevice, e->stream));
+    // ||b||
+    double bn2 = 0.0;
+    {
+      std::vector<double2> hb(n);
+      CUDA_TRY(cudaMemcpyAsync(hb.data(), e->d_b, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+      CUDA_TRY(cudaStreamSynchronize(e->stream));
+      for (auto& v : hb) bn2 += v.x * v.x + v.y * v.y;
+    }
+    const double bn = std::sqrt(bn2);
+    double prev = 1e300, rel = 1.0;
+    int it = 0;
+    const unsigned gr = (unsigned)std::min<int64_t>((n + 7) / 8, 8 * e->nsm);
+    for (; it <= e->refine_max; it++) {
+      permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(e->d_r, e->d_perm, w1, n);
+      LAUNCHED();
+      TRY(run_trsv<float>(e, e->Z32, w1, w2));
+      axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(e->d_x, w2, n);
+      LAUNCHED();
+      CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
+      residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, e->d_x, e->d_b, e->d_r, e->d_rn2);
+      LAUNCHED();
+      double rn2 = 0;
+      CUDA_TRY(cudaMemcpyAsync(&rn2, e->d_rn2, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+      CUDA_TRY(cudaStreamSynchronize(e->stream));
+      rel = bn > 0 ? std::sqrt(rn2) / bn : 0.0;
+      if (!std::isfinite(rel)) return fail(e, NECGPU_ERR_NONFINITE, "refinement: non-finite residual");
+      if (rel <= e->refine_tol) {
+        it++;
+        break;
+      }
+      if (rel > 0.5 * prev) {  // stagnated at the FP64 floor (or diverging)
+        it++;
+        break;
+      }
+      prev = rel;
+    }
+    e->stats.refine_iters = it;
+    e->stats.refine_residual = rel;
+    if (rel > 1e-6) return fail(e, NECGPU_ERR_REFINE, "refinement did not converge");
+  } else {
+    return fail(e, NECGPU_ERR_ARG, "solve: no factorisation held");
+  }
+  coeff_kernel<<<g1, 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc,
+                                          e->d_ccoef + 2 * e->nc, e->d_x, e->d_abc, e->d_cur);
+  LAUNCHED();
+  if (sync_checks) CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->have_solution = true;
+  return 0;
+}
+
+int run_pattern(necgpu_engine* e, int ndir) {
+  PatternArgs a{};
+  const int64_t n = e->n;
+  a.n = n;
+  a.ndir = ndir;
+  a.theta = e->d_theta;
+  a.phi = e->d_phi;
+  a.x = e->d_seg;
+  a.y = e->d_seg + n;
+  a.z = e->d_seg + 2 * n;
+  a.s = e->d_seg + 3 * n;
+  a.cab = e->d_seg + 5 * n;
+  a.sab = e->d_seg + 6 * n;
+  a.salp = e->d_seg + 7 * n;
+  a.abc = e->d_abc;
+  a.ksymp = (e->ground == kGroundNone) ? 1 : 2;
+  a.perfect = (e->ground == kGroundPerfect) ? 1 : 0;
+  a.zrati = e->P.zrati;
+  a.eta = e->P.eta;
+  a.eth = e->d_eth;
+  a.eph = e->d_eph;
+  pattern_kernel<<<(unsigned)((ndir + kPatDirs - 1) / kPatDirs), kPatDirs * 32, 0, e->stream>>>(a);
+  LAUNCHED();
+  return 0;
+}
+
+int ensure_pattern(necgpu_engine* e, int ndir) {
+  if (ndir <= e->pat_cap) return 0;
+  TRY(dalloc(e, e->d_theta, ndir));
+  TRY(dalloc(e, e->d_phi, ndir));
+  TRY(dalloc(e, e->d_eth, ndir));
+  TRY(dalloc(e, e->d_eph, ndir));
+  e->pat_cap = ndir;
+  return 0;
+}
+
+int run_factor(necgpu_engine* e, int precision) {
+  if (!e->filled) return fail(e, NECGPU_ERR_ARG, "factor: matrix not filled");
+  if (precision == NECGPU_FP64) {
+    TRY(run_lu<double>(e, e->Z64));
+    e->filled = false;  // Z64 now holds the factors
+  } else if (precision == NECGPU_MIXED) {
+    if (!e->Z32) TRY(dalloc(e, e->Z32, (size_t)e->n * e->ld));
+    demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld);
+    LAUNCHED();
+    TRY(run_lu<float>(e, e->Z32));
+  } else {
+    return fail(e, NECGPU_ERR_ARG, "factor: unknown precision");
+  }
+  e->factored = precision;
+  return 0;
+}
+
+int fill_checked(necgpu_engine* e, bool want32) {
+  CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+  TRY(run_fill(e, true, want32));
+  e->filled = true;
+  e->factored = -1;
+  return 0;
+}
+
+}  // namespace
+
+// ======================= C-ABI =======================
+extern "C" {
+
+int necgpu_create(necgpu_engine** out, int device) {
+  if (!out) return NECGPU_ERR_ARG;
+  auto* e = new necgpu_engine();
+  *out = e;
+  int count = 0;
+  cudaError_t st = cudaGetDeviceCount(&count);
+  if (st != cudaSuccess || count == 0)
+    return fail(e, NECGPU_ERR_NO_DEVICE,
+                std::string("no CUDA device: ") + (st != cudaSuccess ? cudaGetErrorString(st) : "count=0"));
+  if (device < 0 || device >= count) return fail(e, NECGPU_ERR_ARG, "device index out of range");
+  e->device = device;
+  CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) return fail(e, NECGPU_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+  if (!prop.cooperativeLaunch) return fail(e, NECGPU_ERR_NO_DEVICE, "device lacks cooperative launch");
+  e->nsm = prop.multiProcessorCount;
+  CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+  e->own_stream = true;
+  CUDA_TRY(cudaEventCreate(&e->ev0));
+  CUDA_TRY(cudaEventCreate(&e->ev1));
+  CUDA_TRY(cudaMalloc((void**)&e->d_status, 4 * sizeof(int)));
+  CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+  return NECGPU_OK;
+}
+
+int necgpu_destroy(necgpu_engine* e) {
+  if (!e) return NECGPU_OK;
+  if (e->stream) {
+    cudaSetDevice(e->device);
+    cudaStreamSynchronize(e->stream);
+  }
+  free_all(e);
+  dfree(e->d_status);
+  if (e->ev0) cudaEventDestroy(e->ev0);
+  if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+  return NECGPU_OK;
+}
+
+const char* necgpu_last_error(const necgpu_engine* e) { return e ? e->err.c_str() : "null engine"; }
+
+int necgpu_set_stream(necgpu_engine* e, void* stream) {
+  if (!e) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  if (e->stream) CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (stream == nullptr) {
+    if (!e->own_stream) {
+      CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+      e->own_stream = true;
+    }
+    return NECGPU_OK;
+  }
+  if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
+  e->stream = (cudaStream_t)stream;
+  e->own_stream = false;
+  return NECGPU_OK;
+}
+
+int necgpu_enable_timing(necgpu_engine* e, int on) {
+  if (!e) return NECGPU_ERR_ARG;
+  e->timing = on != 0;
+  return NECGPU_OK;
+}
+
+int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter) {
+  if (!e || !(tol > 0) || max_iter < 0) return NECGPU_ERR_ARG;
+  e->refine_tol = tol;
+  e->refine_max = max_iter;
+  return NECGPU_OK;
+}
+
+int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out) {
+  if (!e || !out) return NECGPU_ERR_ARG;
+  *out = e->stats;
+  out->launches = e->launches;
+  return NECGPU_OK;
+}
+
+int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (!s || s->n < 2) return fail(e, NECGPU_ERR_ARG, "set_structure: need at least 2 segments");
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int64_t n = s->n;
+  if (n > (int64_t)1 << 28) return fail(e, NECGPU_ERR_ARG, "set_structure: too many segments");
+  if (s->ground < 0 || s->ground > 3) return fail(e, NECGPU_ERR_ARG, "set_structure: bad ground type");
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (n != e->n) free_all(e);
+  e->n = n;
+  e->ld = n;
+  e->ground = s->ground;
+  e->use_exk = s->use_exk;
+  e->P.rkh = s->rkh;
+  e->P.eta = s->eta;
+  e->P.zrati = mk(s->zrati_re, s->zrati_im);
+  e->P.frati = mk(s->frati_re, s->frati_im);
+  e->P.u = e->P.zrati;
+  e->P.u2 = e->P.zrati * e->P.zrati;
+  e->factored = -1;
+  e->filled = false;
+  e->have_solution = false;
+  dfree(e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
+
+  std::vector<double> seg(8 * n);
+  for (int64_t i = 0; i < n; i++) {
+    seg[i] = s->x[i];
+    seg[n + i] = s->y[i];
+    seg[2 * n + i] = s->z[i];
+    seg[3 * n + i] = s->length[i];
+    seg[4 * n + i] = s->radius[i];
+    seg[5 * n + i] = s->cab[i];
+    seg[6 * n + i] = s->sab[i];
+    seg[7 * n + i] = s->salp[i];
+  }
+  std::vector<int32_t> ind(2 * n, 0);
+  if (s->ek_ind1 && s->ek_ind2)
+    for (int64_t i = 0; i < n; i++) {
+      ind[i] = s->ek_ind1[i];
+      ind[n + i] = s->ek_ind2[i];
+    }
+
+  const int32_t* tp = s->trio_ptr;
+  if (tp[0] != 0) return fail(e, NECGPU_ERR_ARG, "set_structure: trio_ptr[0] != 0");
+  for (int64_t j = 0; j < n; j++)
+    if (tp[j + 1] < tp[j]) return fail(e, NECGPU_ERR_ARG, "set_structure: trio_ptr not ascending");
+  const int64_t ntrio = tp[n];
+  for (int64_t k = 0; k < ntrio; k++)
+    if (s->trio_basis[k] < 0 || s->trio_basis[k] >= n)
+      return fail(e, NECGPU_ERR_ARG, "set_structure: basis index out of range");
+
+  // column tiles: for every tile, the distinct contributing sources
+  // (ascending) and their (column, a, b, c) entries
+  const int ntiles = (int)((n + kFillTB - 1) / kFillTB);
+  e->ntiles = ntiles;
+  struct Ent {
+    int32_t j;
+    uint8_t col;
+    double a, b, c;
+  };
+  std::vector<std::vector<Ent>> tiles(ntiles);
+  for (int64_t j = 0; j < n; j++)
+    for (int32_t k = tp[j]; k < tp[j + 1]; k++) {
+      int32_t bas = s->trio_basis[k];
+      tiles[bas / kFillTB].push_back(
+          Ent{(int32_t)j, (uint8_t)(bas % kFillTB), s->trio_a[k], s->trio_b[k], s->trio_c[k]});
+    }
+  std::vector<int32_t> tile_ptr(ntiles + 1), tsrc, tsrc_eptr;
+  std::vector<uint8_t> ecol;
+  std::vector<double> ea, eb, ec;
+  for (int t = 0; t < ntiles; t++) {
+    auto& v = tiles[t];  // pushed in ascending source order
+    tile_ptr[t] = (int32_t)tsrc.size();
+    size_t k = 0;
+    while (k < v.size()) {
+      const int32_t j = v[k].j;
+      tsrc.push_back(j);
+      tsrc_eptr.push_back((int32_t)ecol.size());
+      while (k < v.size() && v[k].j == j) {
+        ecol.push_back(v[k].col);
+        ea.push_back(v[k].a);
+        eb.push_back(v[k].b);
+        ec.push_back(v[k].c);
+        k++;
+      }
+    }
+  }
+  tile_ptr[ntiles] = (int32_t)tsrc.size();
+  tsrc_eptr.push_back((int32_t)ecol.size());
+  e->ne = (int64_t)ecol.size();
+  std::vector<double> ecoef(3 * std::max<int64_t>(e->ne, 1));
+  std::copy(ea.begin(), ea.end(), ecoef.begin());
+  std::copy(eb.begin(), eb.end(), ecoef.begin() + e->ne);
+  std::copy(ec.begin(), ec.end(), ecoef.begin() + 2 * e->ne);
+
+  // per segment: basis functions with support on it, ascending basis
+  e->nc = ntrio;
+  std::vector<int32_t> cptr(n + 1), cbasis(std::max<int64_t>(ntrio, 1));
+  std::vector<double> ccoef(3 * std::max<int64_t>(ntrio, 1));
+  {
+    std::vector<int> order;
+    for (int64_t j = 0; j < n; j++) {
+      order.clear();
+      for (int32_t k = tp[j]; k < tp[j + 1]; k++) order.push_back(k);
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int p, int q) { return s->trio_basis[p] < s->trio_basis[q]; });
+      cptr[j] = tp[j];
+      for (size_t q = 0; q < order.size(); q++) {
+        const int k = order[q];
+        cbasis[tp[j] + q] = s->trio_basis[k];
+        ccoef[tp[j] + q] = s->trio_a[k];
+        ccoef[ntrio + tp[j] + q] = s->trio_b[k];
+        ccoef[2 * ntrio + tp[j] + q] = s->trio_c[k];
+      }
+    }
+    cptr[n] = tp[n];
+  }
+
+  TRY(upload(e, e->d_seg, seg.data(), seg.size()));
+  TRY(upload(e, e->d_ind, ind.data(), ind.size()));
+  TRY(upload(e, e->d_tile_ptr, tile_ptr.data(), tile_ptr.size()));
+  TRY(upload(e, e->d_tsrc, tsrc.data(), std::max<size_t>(tsrc.size(), 1)));
+  TRY(upload(e, e->d_tsrc_eptr, tsrc_eptr.data(), tsrc_eptr.size()));
+  TRY(upload(e, e->d_ecol, ecol.data(), std::max<size_t>(ecol.size(), 1)));
+  TRY(upload(e, e->d_ecoef, ecoef.data(), ecoef.size()));
+  TRY(upload(e, e->d_cptr, cptr.data(), cptr.size()));
+  TRY(upload(e, e->d_cbasis, cbasis.data(), cbasis.size()));
+  TRY(upload(e, e->d_ccoef, ccoef.data(), ccoef.size()));
+  TRY(ensure_vectors(e));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));  // host staging freed on return
+  return NECGPU_OK;
+}
+
+int necgpu_fill(necgpu_engine* e) {
+  if (!e) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  tick(e);
+  TRY(fill_checked(e, false));
+  e->stats.ms_fill = tock(e);
+  int st = 0;
+  TRY(sync_status(e, &st));
+  if (st & kStatSommerfeldTab)
+    return fail(e, NECGPU_ERR_UNSUPPORTED,
+                "fill: a segment pair lies within 0.95 wavelength of its ground image; the "
+                "Sommerfeld table-interpolation path is not part of this build");
+  if (st & kStatIterCap) return fail(e, NECGPU_ERR_NONFINITE, "fill: quadrature did not terminate (non-finite geometry?)");
+  return NECGPU_OK;
+}
+
+int necgpu_factor(necgpu_engine* e, int precision) {
+  if (!e) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+  tick(e);
+  TRY(run_factor(e, precision));
+  e->stats.ms_factor = tock(e);
+  return NECGPU_OK;
+}
+
+int necgpu_solve(necgpu_engine* e, const double* rhs, double* cur, double* abc) {
+  if (!e || !rhs || !cur) return e ? fail(e, NECGPU_ERR_ARG, "solve: null argument") : NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int64_t n = e->n;
+  CUDA_TRY(cudaMemcpyAsync(e->d_b, rhs, n * sizeof(double2), cudaMemcpyHostToDevice, e->stream));
+  tick(e);
+  TRY(run_solve(e, false));
+  e->stats.ms_solve = tock(e);
+  CUDA_TRY(cudaMemcpyAsync(cur, e->d_cur, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  if (abc) CUDA_TRY(cudaMemcpyAsync(abc, e->d_abc, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  for (int64_t i = 0; i < 2 * n; i++)
+    if (!std::isfinite(cur[i])) return fail(e, NECGPU_ERR_NONFINITE, "solve: non-finite current");
+  return NECGPU_OK;
+}
+
+int necgpu_pattern(necgpu_engine* e, int ndir, const double* theta, const double* phi, double* eth,
+                   double* eph) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (ndir <= 0 || !theta || !phi || !eth || !eph) return fail(e, NECGPU_ERR_ARG, "pattern: bad arguments");
+  if (!e->have_solution) return fail(e, NECGPU_ERR_ARG, "pattern: no solution");
+  CUDA_TRY(cudaSetDevice(e->device));
+  TRY(ensure_pattern(e, ndir));
+  CUDA_TRY(cudaMemcpyAsync(e->d_theta, theta, ndir * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_phi, phi, ndir * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  tick(e);
+  TRY(run_pattern(e, ndir));
+  e->stats.ms_pattern = tock(e);
+  CUDA_TRY(cudaMemcpyAsync(eth, e->d_eth, ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(eph, e->d_eph, ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->res_ndir = 0;  // the resident direction list was overwritten
+  return NECGPU_OK;
+}
+
+int necgpu_device_z(necgpu_engine* e, void** z, int64_t* ld) {
+  if (!e || !z || !ld) return NECGPU_ERR_ARG;
+  *z = e->Z64;
+  *ld = e->ld;
+  return NECGPU_OK;
+}
+
+int necgpu_copy_z(necgpu_engine* e, double* out) {
+  if (!e || !out) return NECGPU_ERR_ARG;
+  if (!e->filled || !e->Z64) return fail(e, NECGPU_ERR_ARG, "copy_z: no unfactored matrix held");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaMemcpyAsync(out, e->Z64, (size_t)e->n * e->ld * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return NECGPU_OK;
+}
+
+int necgpu_set_resident(necgpu_engine* e, const double* rhs, int ndir, const double* theta,
+                        const double* phi) {
+  if (!e || !rhs || ndir < 0) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaMemcpyAsync(e->d_b, rhs, e->n * sizeof(double2), cudaMemcpyHostToDevice, e->stream));
+  if (ndir > 0) {
+    TRY(ensure_pattern(e, ndir));
+    CUDA_TRY(cudaMemcpyAsync(e->d_theta, theta, ndir * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->d_phi, phi, ndir * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->res_ndir = ndir;
+  e->res_rhs = true;
+  return NECGPU_OK;
+}
+
+// One full pass on resident inputs: fill -> factor -> solve -> coefficients
+// -> far field.  The only host interaction is the pivot download inside the
+// factorisation and the refinement's residual norms (mixed precision).
+int necgpu_step_resident(necgpu_engine* e, int precision) {
+  if (!e || !e->res_rhs) return e ? fail(e, NECGPU_ERR_ARG, "step: no resident inputs") : NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  tick(e);
+  TRY(fill_checked(e, false));
+  e->stats.ms_fill = tock(e);
+  tick(e);
+  TRY(run_factor(e, precision));
+  e->stats.ms_factor = tock(e);
+  tick(e);
+  TRY(run_solve(e, false));
+  e->stats.ms_solve = tock(e);
+  tick(e);
+  if (e->res_ndir > 0) TRY(run_pattern(e, e->res_ndir));
+  e->stats.ms_pattern = tock(e);
+  int st = 0;
+  TRY(sync_status(e, &st));
+  if (st & (kStatSommerfeldTab | kStatIterCap)) return fail(e, NECGPU_ERR_UNSUPPORTED, "step: fill status");
+  return NECGPU_OK;
+}
+
+int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph) {
+  if (!e) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  if (cur) CUDA_TRY(cudaMemcpyAsync(cur, e->d_cur, e->n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  if (eth && e->res_ndir > 0)
+    CUDA_TRY(cudaMemcpyAsync(eth, e->d_eth, e->res_ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  if (eph && e->res_ndir > 0)
+    CUDA_TRY(cudaMemcpyAsync(eph, e->d_eph, e->res_ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return NECGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,888 @@
+// Thin-wire geometry, connection tables and basis-function tables.
+// Algorithms follow NEC2++ src/c_geometry.cpp (line ranges cited per
+// function); the code is organised around per-segment precomputed terms
+// instead of the reference's recomputation inside every sbf/tbf call.
+#include "geometry.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <numeric>
+
+#include "nec_constants.h"
+#include "nec_error.h"
+
+namespace necb {
+
+namespace {
+
+struct V3 {
+  double x, y, z;
+};
+inline V3 sub(const V3& a, const V3& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+// Euclidean norm, summed x, y, z in order then sqrt (the order of a
+// fixed-size 3-vector reduction).
+inline double norm3(const V3& v) { return std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z); }
+inline double norm_l1(const V3& v) { return std::fabs(v.x) + std::fabs(v.y) + std::fabs(v.z); }
+
+}  // namespace
+
+void Geometry::grow(int64_t new_n) {
+  tags.resize(new_n);
+  x.resize(new_n);
+  y.resize(new_n);
+  z.resize(new_n);
+  x2.resize(new_n);
+  y2.resize(new_n);
+  z2.resize(new_n);
+  radius.resize(new_n);
+}
+
+// Straight or tapered wire: c_geometry.cpp:614-696.
+void Geometry::wire(int tag, int nseg, double xw1, double yw1, double zw1,
+                    double xw2, double yw2, double zw2, double rad, double rdel,
+                    double rrad) {
+  if (completed) fail("GEOMETRY ALREADY COMPLETE");
+  int64_t istart = n;
+  n += nseg;
+  np = n;
+  ipsym = 0;
+  if (nseg < 1) return;
+  grow(n);
+
+  double dx = xw2 - xw1, dy = yw2 - yw1, dz = zw2 - zw1;
+  double delz, rd;
+  if (std::fabs(rdel - 1.0) >= 1.0e-6) {
+    delz = norm3({dx, dy, dz});
+    dx /= delz;
+    dy /= delz;
+    dz /= delz;
+    delz = delz * (1. - rdel) / (1. - std::pow(rdel, nseg));
+    rd = rdel;
+  } else {
+    double fns = nseg;
+    dx /= fns;
+    dy /= fns;
+    dz /= fns;
+    delz = 1.0;
+    rd = 1.0;
+  }
+  double radz = rad;
+  double sx = xw1, sy = yw1, sz = zw1;
+  for (int64_t i = istart; i < n; i++) {
+    tags[i] = tag;
+    double ex = sx + dx * delz, ey = sy + dy * delz, ez = sz + dz * delz;
+    x[i] = sx;
+    y[i] = sy;
+    z[i] = sz;
+    x2[i] = ex;
+    y2[i] = ey;
+    z2[i] = ez;
+    radius[i] = radz;
+    delz = delz * rd;
+    radz = radz * rrad;
+    sx = ex;
+    sy = ey;
+    sz = ez;
+  }
+  x2[n - 1] = xw2;
+  y2[n - 1] = yw2;
+  z2[n - 1] = zw2;
+}
+
+// Helix / spiral: c_geometry.cpp:698-826 (the printout is not reproduced).
+void Geometry::helix(int tag, int nseg, double s, double hl, double a1,
+                     double b1, double a2, double b2, double rad) {
+  if (completed) fail("GEOMETRY ALREADY COMPLETE");
+  if (nseg < 1) fail("HELIX: segment count must be >= 1");
+  int64_t ist = n;
+  n += nseg;
+  np = n;
+  ipsym = 0;
+  double zinc = std::fabs(hl / nseg);
+  grow(n);
+
+  if (hl == 0.) {  // flat spiral
+    double phi = 0.;
+    double dphi = 2. * kPi / s;
+    double da = (a1 - a2) / nseg;
+    double db = (b1 - b2) / nseg;
+    for (int64_t i = ist; i < n; i++) {
+      radius[i] = rad;
+      tags[i] = tag;
+      z[i] = 0.;
+      z2[i] = 0.;
+      x[i] = a1 * std::cos(phi);
+      y[i] = b1 * std::sin(phi);
+      a1 -= da;
+      b1 -= db;
+      phi += dphi;
+      x2[i] = a1 * std::cos(phi);
+      y2[i] = b1 * std::sin(phi);
+    }
+    return;
+  }
+
+  z[ist] = 0.;
+  for (int64_t i = ist; i < n; i++) {
+    radius[i] = rad;
+    tags[i] = tag;
+    if (i != ist) z[i] = z[i - 1] + zinc;
+    z2[i] = z[i] + zinc;
+    if (a2 == a1) {
+      if (b1 == 0.) b1 = a1;
+      x[i] = a1 * std::cos(2. * kPi * z[i] / s);
+      y[i] = b1 * std::sin(2. * kPi * z[i] / s);
+      x2[i] = a1 * std::cos(2. * kPi * z2[i] / s);
+      y2[i] = b1 * std::sin(2. * kPi * z2[i] / s);
+    } else {
+      if (b2 == 0.) b2 = a2;
+      x[i] = (a1 + (a2 - a1) * z[i] / std::fabs(hl)) * std::cos(2. * kPi * z[i] / s);
+      y[i] = (b1 + (b2 - b1) * z[i] / std::fabs(hl)) * std::sin(2. * kPi * z[i] / s);
+      x2[i] = (a1 + (a2 - a1) * z2[i] / std::fabs(hl)) * std::cos(2. * kPi * z2[i] / s);
+      y2[i] = (b1 + (b2 - b1) * z2[i] / std::fabs(hl)) * std::sin(2. * kPi * z2[i] / s);
+    }
+    if (hl < 0.) {  // left-handed
+      y[i] = -y[i];
+      y2[i] = -y2[i];
+    }
+  }
+}
+
+int64_t Geometry::segment_number(int tag, int m) const {
+  if (m <= 0)
+    fail("CHECK DATA, PARAMETER SPECIFYING SEGMENT POSITION IN A GROUP OF "
+         "EQUAL TAGS MUST NOT BE ZERO");
+  if (tag == 0) return m;
+  int64_t count = 0;
+  for (int64_t i = 0; i < n; i++)
+    if (tags[i] == tag && ++count == m) return i + 1;
+  fail("NO SEGMENT HAS AN ITAG OF ", tag);
+}
+
+// GM card: rotate by (rox, roy, roz) radians then shift; nrpt copies with
+// tag increment itgi, starting at the first segment of tag its
+// (c_geometry.cpp:830-980; patches are not part of this build).
+void Geometry::move(double rox, double roy, double roz, double xs, double ys,
+                    double zs, int its, int nrpt, int itgi) {
+  if (completed) fail("GEOMETRY ALREADY COMPLETE");
+  if (std::fabs(rox) + std::fabs(roy) > 1.0e-10) ipsym = ipsym * 3;
+  double sps = std::sin(rox), cps = std::cos(rox);
+  double sth = std::sin(roy), cth = std::cos(roy);
+  double sph = std::sin(roz), cph = std::cos(roz);
+  double xx = cph * cth;
+  double xy = cph * sth * sps - sph * cps;
+  double xz = cph * sth * cps + sph * sps;
+  double yx = sph * cth;
+  double yy = sph * sth * sps + cph * cps;
+  double yz = sph * sth * cps - cph * sps;
+  double zx = -sth;
+  double zy = cth * sps;
+  double zz = cth * cps;
+  int64_t nrp = (nrpt == 0) ? 1 : nrpt;
+  int64_t ix = 1;
+  if (n > 0) {
+    int64_t i1 = segment_number(its, 1);
+    if (i1 < 1) i1 = 1;
+    ix = i1;
+    int64_t k;
+    if (nrpt == 0) {
+      k = i1 - 1;
+    } else {
+      k = n;
+      grow(n + (n + 1 - i1) * nrpt);
+    }
+    for (int64_t ir = 0; ir < nrp; ir++) {
+      for (int64_t i = i1 - 1; i < n; i++) {
+        double xi = x[i], yi = y[i], zi = z[i];
+        x[k] = xi * xx + yi * xy + zi * xz + xs;
+        y[k] = xi * yx + yi * yy + zi * yz + ys;
+        z[k] = xi * zx + yi * zy + zi * zz + zs;
+        xi = x2[i];
+        yi = y2[i];
+        zi = z2[i];
+        x2[k] = xi * xx + yi * xy + zi * xz + xs;
+        y2[k] = xi * yx + yi * yy + zi * yz + ys;
+        z2[k] = xi * zx + yi * zy + zi * zz + zs;
+        radius[k] = radius[i];
+        tags[k] = tags[i];
+        if (tags[i] != 0) tags[k] = tags[i] + itgi;
+        k++;
+      }
+      i1 = n + 1;
+      n = k;
+    }
+  }
+  if (nrpt == 0 && ix == 1) return;
+  np = n;
+  ipsym = 0;
+}
+
+void Geometry::scale(double f) {
+  if (completed) fail("GEOMETRY ALREADY COMPLETE");
+  for (int64_t i = 0; i < n; i++) {
+    x[i] *= f;
+    y[i] *= f;
+    z[i] *= f;
+    x2[i] *= f;
+    y2[i] *= f;
+    z2[i] *= f;
+    radius[i] *= f;
+  }
+}
+
+// Connection search, c_geometry.cpp:1705-1916 (wire part).  For every end of
+// every segment, the other segments are scanned starting after the segment
+// itself, wrapping round; the first end within SMIN * length (L1 distance)
+// wins.  The sign of the stored index says whether the touching end is of
+// the same kind (negative) or the opposite kind (positive).
+void Geometry::build_connections(int ignd) {
+  if (ignd != 0) {
+    if (ipsym == 2) np = 2 * np;
+    if (std::abs(ipsym) > 2) np = n;
+    if (np > n) fail("ERROR: NP > N IN c_geometry::build_connections()");
+    if (np == n) ipsym = 0;
+  }
+  icon1.assign(n, 0);
+  icon2.assign(n, 0);
+  for (int64_t i = 0; i < n; i++) {
+    int64_t iz = i + 1;
+    double zi1 = z[i], zi2 = z2[i];
+    V3 v1{x[i], y[i], z[i]}, v2{x2[i], y2[i], z2[i]};
+    double slen = norm3(sub(v2, v1)) * kSmin;
+
+    bool on_ground = false;
+    if (ignd > 0) {
+      if (zi1 <= -slen) fail("GEOMETRY DATA ERROR--SEGMENT ", iz, "EXTENDS BELOW GROUND");
+      if (zi1 <= slen) {
+        icon1[i] = (int)iz;
+        z[i] = 0.;
+        on_ground = true;
+      }
+    }
+    if (!on_ground) {
+      int64_t ic = i;
+      bool found = false;
+      for (int64_t j = 1; j < n; j++) {
+        if (++ic >= n) ic = 0;
+        if (norm_l1(sub(v1, V3{x[ic], y[ic], z[ic]})) <= slen) {
+          icon1[i] = -(int)(ic + 1);
+          found = true;
+          break;
+        }
+        if (norm_l1(sub(v1, V3{x2[ic], y2[ic], z2[ic]})) <= slen) {
+          icon1[i] = (int)(ic + 1);
+          found = true;
+          break;
+        }
+      }
+      if (!found) icon1[i] = 0;
+    }
+
+    if (ignd > 0 || on_ground) {
+      if (zi2 <= -slen) fail("GEOMETRY DATA ERROR--SEGMENT ", iz, "EXTENDS BELOW GROUND");
+      if (zi2 <= slen) {
+        if (icon1[i] == iz) fail("GEOMETRY DATA ERROR--SEGMENT ", iz, "LIES IN GROUND PLANE");
+        icon2[i] = (int)iz;
+        z2[i] = 0.;
+        continue;
+      }
+    }
+    v1 = V3{x[i], y[i], z[i]};
+    v2 = V3{x2[i], y2[i], z2[i]};
+    int64_t ic = i;
+    bool found = false;
+    for (int64_t j = 1; j < n; j++) {
+      if (++ic >= n) ic = 0;
+      if (norm_l1(sub(v2, V3{x[ic], y[ic], z[ic]})) <= slen) {
+        icon2[i] = (int)(ic + 1);
+        found = true;
+        break;
+      }
+      if (norm_l1(sub(v2, V3{x2[ic], y2[ic], z2[ic]})) <= slen) {
+        icon2[i] = -(int)(ic + 1);
+        found = true;
+        break;
+      }
+    }
+    if (!found) icon2[i] = 0;
+  }
+  if (np == 0) fail("connect_segments Geometry has zero wires and zero patches.");
+  if (n / np != 1 && ipsym == 0) fail("ERROR: IPSYM=0 IN build_connections()");
+}
+
+// Junction averaging, c_geometry.cpp:1918-2075.  Starting from each end of
+// each segment, the ring of ends joined there is walked through icon1/icon2;
+// the walk is abandoned when it meets a lower-numbered segment (that segment
+// already averaged the junction).  Otherwise all ends on the ring are moved
+// to the mean of their positions, summed in walk order.
+void Geometry::resolve_junctions() {
+  std::vector<int64_t> ring(8);
+  for (int64_t j = 0; j < n; j++) {
+    const int64_t jx = j + 1;
+    int iend = -1, jend = -1;
+    int64_t ix = icon1[j];
+    int64_t ic = 1;
+    ring[0] = -jx;
+    double xa = x[j], ya = y[j], za = z[j];
+    while (true) {
+      if (ix != 0 && ix != jx && ix <= n) {
+        bool jump = false;
+        do {
+          if (ix == 0) fail("CONNECT - SEGMENT CONNECTION ERROR FOR SEGMENT: ", ix);
+          if (ix < 0)
+            ix = -ix;
+          else
+            jend = -jend;
+          jump = false;
+          if (ix == jx) break;
+          if (ix < jx) {
+            jump = true;
+            break;
+          }
+          ic++;
+          if ((int64_t)ring.size() < ic) ring.resize(ic * 2);
+          ring[ic - 1] = ix * jend;
+          int64_t ixx = ix - 1;
+          if (ixx < 0 || ixx >= n) fail("CONNECT - SEGMENT CONNECTION ERROR (bad index): ", ix);
+          if (jend != 1) {
+            xa = xa + x[ixx];
+            ya = ya + y[ixx];
+            za = za + z[ixx];
+            ix = icon1[ixx];
+          } else {
+            xa = xa + x2[ixx];
+            ya = ya + y2[ixx];
+            za = za + z2[ixx];
+            ix = icon2[ixx];
+          }
+        } while (ix != 0);
+
+        if (jump && iend == 1) break;
+        if (jump) {
+          iend = 1;
+          jend = 1;
+          ix = icon2[j];
+          ic = 1;
+          ring[0] = jx;
+          xa = x2[j];
+          ya = y2[j];
+          za = z2[j];
+          continue;
+        }
+        double sep = static_cast<double>(ic);
+        xa = xa / sep;
+        ya = ya / sep;
+        za = za / sep;
+        for (int64_t i = 0; i < ic; i++) {
+          int64_t e = ring[i];
+          if (e <= 0) {
+            int64_t ixx = -e - 1;
+            if (ixx < 0 || ixx >= n) fail("CONNECT - JUNCTION INDEX ERROR: ", -e);
+            x[ixx] = xa;
+            y[ixx] = ya;
+            z[ixx] = za;
+          } else {
+            int64_t ixx = e - 1;
+            if (ixx < 0 || ixx >= n) fail("CONNECT - JUNCTION INDEX ERROR: ", e);
+            x2[ixx] = xa;
+            y2[ixx] = ya;
+            z2[ixx] = za;
+          }
+        }
+      }
+      if (iend == 1) break;
+      iend = 1;
+      jend = 1;
+      ix = icon2[j];
+      ic = 1;
+      ring[0] = jx;
+      xa = x2[j];
+      ya = y2[j];
+      za = z2[j];
+    }
+  }
+}
+
+// Segment-overlap rule, c_geometry.cpp:1405-1703: a segment centre lying
+// inside the volume of a segment it does not share exactly one node with is
+// an error (fatal by default).  Nodes are the classes of segment ends in
+// contact (L1 distance within the larger of the two ends' thresholds).
+void Geometry::check_overlaps() {
+  if (!check_overlaps_ || n < 2) return;
+  struct End {
+    V3 p;
+    int64_t idx;
+    double thr;
+  };
+  struct View {
+    int64_t idx;
+    V3 a, b, c;  // end one, end two, centre
+    double r;
+    int tag;
+  };
+  std::vector<End> ends;
+  std::vector<View> views;
+  ends.reserve(2 * n);
+  views.reserve(n);
+  for (int64_t i = 0; i < n; i++) {
+    V3 c{x[i], y[i], z[i]};
+    double h = 0.5 * length[i];
+    V3 ha{cab[i] * h, sab[i] * h, salp[i] * h};
+    V3 a = sub(c, ha);
+    V3 b{c.x + ha.x, c.y + ha.y, c.z + ha.z};
+    views.push_back(View{i, a, b, c, radius[i], tags[i]});
+    double thr = norm3(sub(b, a)) * kSmin;
+    ends.push_back(End{a, 2 * i, thr});
+    ends.push_back(End{b, 2 * i + 1, thr});
+  }
+  auto axis_of = [](auto& items) {
+    V3 lo = items[0].p, hi = lo;
+    for (size_t i = 1; i < items.size(); i++) {
+      lo = V3{std::min(lo.x, items[i].p.x), std::min(lo.y, items[i].p.y), std::min(lo.z, items[i].p.z)};
+      hi = V3{std::max(hi.x, items[i].p.x), std::max(hi.y, items[i].p.y), std::max(hi.z, items[i].p.z)};
+    }
+    double e[3] = {hi.x - lo.x, hi.y - lo.y, hi.z - lo.z};
+    int ax = 0;
+    for (int k = 1; k < 3; k++)
+      if (e[k] > e[ax]) ax = k;
+    return ax;
+  };
+  auto coord = [](const V3& v, int ax) { return ax == 0 ? v.x : (ax == 1 ? v.y : v.z); };
+
+  // node classes (union-find over ends)
+  std::vector<int64_t> parent(2 * n);
+  std::iota(parent.begin(), parent.end(), 0);
+  auto root = [&](int64_t e) {
+    while (parent[e] != e) {
+      parent[e] = parent[parent[e]];
+      e = parent[e];
+    }
+    return e;
+  };
+  double thr_max = 0.0;
+  for (auto& e : ends) thr_max = std::max(thr_max, e.thr);
+  {
+    int ax = axis_of(ends);
+    std::stable_sort(ends.begin(), ends.end(), [&](const End& l, const End& r) {
+      return coord(l.p, ax) < coord(r.p, ax);
+    });
+    for (size_t a = 0; a < ends.size(); a++)
+      for (size_t p = a + 1; p < ends.size() && coord(ends[p].p, ax) - coord(ends[a].p, ax) <= thr_max; p++) {
+        double t = std::max(ends[a].thr, ends[p].thr);
+        if (norm_l1(sub(ends[a].p, ends[p].p)) <= t) parent[root(ends[p].idx)] = root(ends[a].idx);
+      }
+  }
+  std::vector<std::pair<int64_t, int64_t>> nodes(n);
+  for (int64_t i = 0; i < n; i++) nodes[i] = {root(2 * i), root(2 * i + 1)};
+  auto one_node = [&](int64_t s, int64_t t) {
+    auto& A = nodes[s];
+    auto& B = nodes[t];
+    int shared = int(A.first == B.first || A.first == B.second) + int(A.second == B.first || A.second == B.second);
+    return shared == 1;
+  };
+  // distance from a point to a segment axis, clamped to the segment
+  auto axis_distance = [](const View& w, const V3& q) {
+    double a0x = w.a.x, a0y = w.a.y, a0z = w.a.z, a1x = w.b.x, a1y = w.b.y, a1z = w.b.z;
+    double sq = (a1x - a0x) * (a1x - a0x) + (a1y - a0y) * (a1y - a0y) + (a1z - a0z) * (a1z - a0z);
+    if (sq == 0.0) fail("nec_wire::axis_distance(): zero-length wire");
+    double sa = (a1x * q.x + a1y * q.y + a1z * q.z - a0x * a1x - a0x * q.x - a0y * a1y - a0y * q.y -
+                 a0z * a1z - a0z * q.z + a0x * a0x + a0y * a0y + a0z * a0z) / sq;
+    if (sa < 0) sa = 0.0;
+    if (sa > 1.0) sa = 1.0;
+    V3 pt{a0x + (a1x - a0x) * sa, a0y + (a1y - a0y) * sa, a0z + (a1z - a0z) * sa};
+    return norm3(sub(pt, q));
+  };
+  double reach = 0.0;
+  for (auto& v : views) reach = std::max(reach, 0.5 * norm3(sub(v.b, v.a)) + v.r);
+  // views carry their centre in .c; sort along the widest axis of the centres
+  struct P {
+    V3 p;
+  };
+  std::vector<P> cen(views.size());
+  for (size_t i = 0; i < views.size(); i++) cen[i].p = views[i].c;
+  int ax = axis_of(cen);
+  std::stable_sort(views.begin(), views.end(), [&](const View& l, const View& r) {
+    return coord(l.c, ax) < coord(r.c, ax);
+  });
+  for (size_t a = 0; a < views.size(); a++)
+    for (size_t p = a + 1; p < views.size() && coord(views[p].c, ax) - coord(views[a].c, ax) <= reach; p++) {
+      if (one_node(views[a].idx, views[p].idx)) continue;
+      const View* pairs[2][2] = {{&views[a], &views[p]}, {&views[p], &views[a]}};
+      for (auto& pr : pairs) {
+        const View& inside = *pr[0];
+        const View& container = *pr[1];
+        double d = axis_distance(container, inside.c);
+        if (d > container.r) continue;
+        if (overlap_fatal_) {
+          char buf[256];
+          snprintf(buf, sizeof(buf),
+                   "GEOMETRY DATA ERROR -- SEGMENT #%lld (TAG ID #%d) MIDPOINT LIES WITHIN "
+                   "SEGMENT #%lld (TAG ID #%d) AT DISTANCE %.5f RADIUS %.5f",
+                   (long long)(inside.idx + 1), inside.tag, (long long)(container.idx + 1),
+                   container.tag, d, container.r);
+          throw nec_error(buf);
+        }
+      }
+    }
+}
+
+// geometry_complete, c_geometry.cpp:454-612 (wire part).
+void Geometry::complete(int gpflag) {
+  if (completed) fail("GEOMETRY ALREADY COMPLETE");
+  if (np == 0) fail("Geometry has no wires or patches.");
+  if (n <= 1)
+    fail("GEOMETRY HAS ONE OR FEWER SEGMENTS and no patches. Please send bug "
+         "report. This causes an error that we're trying to fix.");
+  build_connections(gpflag);
+  resolve_junctions();
+
+  length.resize(n);
+  cab.resize(n);
+  sab.resize(n);
+  salp.resize(n);
+  for (int64_t i = 0; i < n; i++) {
+    double xw1 = x2[i] - x[i];
+    double yw1 = y2[i] - y[i];
+    double zw1 = z2[i] - z[i];
+    x[i] = (x[i] + x2[i]) * .5;
+    y[i] = (y[i] + y2[i]) * .5;
+    z[i] = (z[i] + z2[i]) * .5;
+    double xw2 = xw1 * xw1 + yw1 * yw1 + zw1 * zw1;
+    double yw2 = std::sqrt(xw2);
+    yw2 = (xw2 / yw2 + yw2) * .5;
+    length[i] = yw2;
+    cab[i] = xw1 / yw2;
+    sab[i] = yw1 / yw2;
+    xw2 = zw1 / yw2;
+    if (xw2 > 1.) xw2 = 1.;
+    if (xw2 < -1.) xw2 = -1.;
+    salp[i] = xw2;
+    if (length[i] <= 1.e-20 || radius[i] <= 0.) fail("SEGMENT DATA ERROR");
+  }
+  check_overlaps();
+  x_m_.assign(x.begin(), x.begin() + n);
+  y_m_.assign(y.begin(), y.begin() + n);
+  z_m_.assign(z.begin(), z.begin() + n);
+  si_m_.assign(length.begin(), length.begin() + n);
+  bi_m_.assign(radius.begin(), radius.begin() + n);
+  completed = true;
+}
+
+// Scale to wavelengths, c_geometry.cpp:3389-3418.
+void Geometry::frequency_scale(double freq_mhz) {
+  double fr = (1.0e6 * freq_mhz) / speed_of_light();
+  for (int64_t i = 0; i < n; i++) {
+    x[i] = x_m_[i] * fr;
+    y[i] = y_m_[i] * fr;
+    z[i] = z_m_[i] * fr;
+    length[i] = si_m_[i] * fr;
+    radius[i] = bi_m_[i] * fr;
+  }
+}
+
+// Per-segment terms used by sbf/tbf (c_geometry.cpp:2798-2812, 3132-3146,
+// 2871-2886).  Two "1 - cos(2d)" forms appear in the reference and round
+// differently: segments reached through a connection use 1 - cdh^2 + sdh^2,
+// the segment a basis function is centred on uses 1 - (cdh^2 - sdh^2).
+void Geometry::prepare_basis() {
+  terms_.resize(n);
+  for (int64_t i = 0; i < n; i++) {
+    SegTerms& t = terms_[i];
+    double d = kPi * length[i];
+    t.sdh = std::sin(d);
+    t.cdh = std::cos(d);
+    t.sd = 2.0 * t.sdh * t.cdh;
+    t.cd = t.cdh * t.cdh - t.sdh * t.sdh;
+    if (d <= 0.015) {
+      double omc = 4. * d * d;
+      omc = ((1.3888889e-3 * omc - 4.1666666667e-2) * omc + .5) * omc;
+      t.omc_link = omc;
+      t.omc_self = omc;
+    } else {
+      t.omc_link = 1. - t.cdh * t.cdh + t.sdh * t.sdh;
+      t.omc_self = 1. - t.cd;
+    }
+    t.aj = 1. / (std::log(1. / (kPi * radius[i])) - .577215664);
+    double qp = kPi * radius[i];
+    double xxi = qp * qp;
+    t.xxi = qp * (1. - .5 * xxi) / (1. - xxi);
+  }
+}
+
+// sbf, c_geometry.cpp:3102-3297.
+void Geometry::sbf(int i, int is, double* aa, double* bb, double* cc) const {
+  *aa = 0.;
+  *bb = 0.;
+  *cc = 0.;
+  int june = 0, count = 0, njun1 = 0;
+  double pp = 0., pm = 0.;
+  const int ix = i - 1;
+  int jcox = icon1[ix];
+  if (jcox > kPatchConnection) jcox = i;
+  int jend = -1, iend = -1;
+  double sig = -1.;
+  do {
+    if (jcox != 0) {
+      if (jcox < 0)
+        jcox = -jcox;
+      else {
+        sig = -sig;
+        jend = -jend;
+      }
+      const int jcoxx = jcox - 1;
+      count++;
+      const SegTerms& t = terms_[jcoxx];
+      pp -= t.omc_link / t.sd * t.aj;
+      if (jcox == is) {
+        *aa = t.aj / t.sd * sig;
+        *bb = t.aj / (2. * t.cdh);
+        *cc = -t.aj / (2. * t.sdh) * sig;
+        june = iend;
+      }
+      if (jcox != i) {
+        jcox = (jend != 1) ? icon1[jcoxx] : icon2[jcoxx];
+        if (std::abs(jcox) != i) {
+          if (jcox == 0) fail("SBF - SEGMENT CONNECTION ERROR FOR SEGMENT ", i);
+          continue;
+        }
+      } else if (jcox == is) {
+        *bb = -*bb;
+      }
+      if (iend == 1) break;
+    }
+    pm = -pp;
+    pp = 0.;
+    njun1 = count;
+    jcox = icon2[ix];
+    if (jcox > kPatchConnection) jcox = i;
+    jend = 1;
+    iend = 1;
+    sig = -1.;
+  } while (jcox != 0);
+
+  const int njun2 = count - njun1;
+  const SegTerms& t = terms_[ix];
+  const double sdh = t.sdh, cdh = t.cdh, sd = t.sd, cd = t.cd, omc = t.omc_self;
+  const double ap = t.aj, aj = t.aj, xxi = t.xxi;
+  if (njun1 == 0) {
+    if (njun2 == 0) {
+      *aa = -1.;
+      *cc = 1. / (cdh - xxi * sdh);
+      return;
+    }
+    double qp = -(omc + xxi * sd) / (sd * (ap + xxi * pp) + cd * (xxi * ap - pp));
+    if (june == 1) {
+      *aa = -*aa * qp;
+      *bb = *bb * qp;
+      *cc = -*cc * qp;
+      if (i != is) return;
+    }
+    *aa -= 1.;
+    double d = cd - xxi * sd;
+    *bb += (sdh + ap * qp * (cdh - xxi * sdh)) / d;
+    *cc += (cdh + ap * qp * (sdh + xxi * cdh)) / d;
+    return;
+  }
+  if (njun2 == 0) {
+    double qm = (omc + xxi * sd) / (sd * (aj - xxi * pm) + cd * (pm + xxi * aj));
+    if (june == -1) {
+      *aa = *aa * qm;
+      *bb = *bb * qm;
+      *cc = *cc * qm;
+      if (i != is) return;
+    }
+    *aa -= 1.;
+    double d = cd - xxi * sd;
+    *bb += (aj * qm * (cdh - xxi * sdh) - sdh) / d;
+    *cc += (cdh - aj * qm * (sdh + xxi * cdh)) / d;
+    return;
+  }
+  double qp = sd * (pm * pp + aj * ap) + cd * (pm * ap - pp * aj);
+  double qm = (ap * omc - pp * sd) / qp;
+  qp = -(aj * omc + pm * sd) / qp;
+  if (june != 0) {
+    if (june < 0) {
+      *aa = *aa * qm;
+      *bb = *bb * qm;
+      *cc = *cc * qm;
+    } else {
+      *aa = -*aa * qp;
+      *bb = *bb * qp;
+      *cc = -*cc * qp;
+    }
+    if (i != is) return;
+  }
+  *aa -= 1.;
+  *bb += (aj * qm + ap * qp) * sdh / sd;
+  *cc += (aj * qm - ap * qp) * cdh / sd;
+}
+
+// trio, c_geometry.cpp:2982-3100: every basis function with support on
+// source segment j, the segment's own basis function last.
+void Geometry::trio(int j, std::vector<BasisEntry>& out) const {
+  out.clear();
+  BasisEntry e;
+  const int jx = j - 1;
+  int jend = 0, iend = 0;
+  int jcox = icon1[jx];
+  if (jcox <= kPatchConnection) {
+    jend = -1;
+    iend = -1;
+  }
+  if (jcox == 0 || jcox > kPatchConnection) {
+    jcox = icon2[jx];
+    if (jcox <= kPatchConnection) {
+      jend = 1;
+      iend = 1;
+    }
+    if (jcox == 0 || jcox > kPatchConnection) {
+      sbf(j, j, &e.a, &e.b, &e.c);
+      e.basis = j;
+      out.push_back(e);
+      return;
+    }
+  }
+  do {
+    if (jcox < 0)
+      jcox = -jcox;
+    else
+      jend = -jend;
+    const int jcoxx = jcox - 1;
+    if (jcox != j) {
+      sbf(jcox, j, &e.a, &e.b, &e.c);
+      e.basis = jcox;
+      out.push_back(e);
+      jcox = (jend != 1) ? icon1[jcoxx] : icon2[jcoxx];
+      if (jcox == 0) fail("TRIO - SEGMENT CONNENTION ERROR FOR SEGMENT ", j);
+      continue;
+    }
+    if (iend == 1) break;
+    jcox = icon2[jx];
+    if (jcox > kPatchConnection) break;
+    jend = 1;
+    iend = 1;
+  } while (jcox != 0);
+  sbf(j, j, &e.a, &e.b, &e.c);
+  e.basis = j;
+  out.push_back(e);
+}
+
+// tbf, c_geometry.cpp:2763-2980: the basis function centred on segment i
+// over every segment it covers (connected ends first, segment i last).
+// Entries carry the covered segment in .basis.
+void Geometry::tbf(int i, int icap, std::vector<BasisEntry>& out) const {
+  out.clear();
+  double pp = 0.0, pm = 0.0;
+  int njun1 = 0;
+  const int ix = i - 1;
+  int jcox = icon1[ix];
+  if (jcox > kPatchConnection) jcox = i;
+  int jend = -1, iend = -1;
+  double sig = -1.0;
+  do {
+    if (jcox != 0) {
+      if (jcox < 0)
+        jcox = -jcox;
+      else {
+        sig = -sig;
+        jend = -jend;
+      }
+      const int jcoxx = jcox - 1;
+      const SegTerms& t = terms_[jcoxx];
+      pp = pp - t.omc_link / t.sd * t.aj;
+      BasisEntry e;
+      e.basis = jcox;
+      e.a = t.aj / t.sd * sig;
+      e.b = t.aj / (2. * t.cdh);
+      e.c = -t.aj / (2. * t.sdh) * sig;
+      out.push_back(e);
+      if (jcox != i) {
+        jcox = (jend == 1) ? icon2[jcoxx] : icon1[jcoxx];
+        if (std::abs(jcox) != i) {
+          if (jcox != 0) continue;
+          fail("TBF - SEGMENT CONNECTION ERROR FOR SEGMENT ", i);
+        }
+      } else {
+        out.back().b = -out.back().b;
+      }
+      if (iend == 1) break;
+    }
+    pm = -pp;
+    pp = 0.;
+    njun1 = (int)out.size();
+    jcox = icon2[ix];
+    if (jcox > kPatchConnection) jcox = i;
+    jend = 1;
+    iend = 1;
+    sig = -1.;
+  } while (jcox != 0);
+
+  const int jsno = (int)out.size();
+  const int njun2 = jsno - njun1;
+  const SegTerms& t = terms_[ix];
+  const double sdh = t.sdh, cdh = t.cdh, sd = t.sd, cd = t.cd, omc = t.omc_self;
+  const double ap = t.aj, aj = t.aj;
+  const double xxi = (icap == 0) ? 0. : t.xxi;
+  BasisEntry self;
+  self.basis = i;
+  self.a = -1.;
+  if (njun1 == 0) {
+    if (njun2 == 0) {
+      self.b = 0.;
+      self.c = 1. / (cdh - xxi * sdh);
+      out.push_back(self);
+      return;
+    }
+    double qp = -(omc + xxi * sd) / (sd * (ap + xxi * pp) + cd * (xxi * ap - pp));
+    double d = cd - xxi * sd;
+    self.b = (sdh + ap * qp * (cdh - xxi * sdh)) / d;
+    self.c = (cdh + ap * qp * (sdh + xxi * cdh)) / d;
+    for (int k = 0; k < njun2; k++) {
+      out[k].a = -out[k].a * qp;
+      out[k].b = out[k].b * qp;
+      out[k].c = -out[k].c * qp;
+    }
+    out.push_back(self);
+    return;
+  }
+  if (njun2 == 0) {
+    double qm = (omc + xxi * sd) / (sd * (aj - xxi * pm) + cd * (pm + xxi * aj));
+    double d = cd - xxi * sd;
+    self.b = (aj * qm * (cdh - xxi * sdh) - sdh) / d;
+    self.c = (cdh - aj * qm * (sdh + xxi * cdh)) / d;
+    for (int k = 0; k < njun1; k++) {
+      out[k].a = out[k].a * qm;
+      out[k].b = out[k].b * qm;
+      out[k].c = out[k].c * qm;
+    }
+    out.push_back(self);
+    return;
+  }
+  double qp = sd * (pm * pp + aj * ap) + cd * (pm * ap - pp * aj);
+  double qm = (ap * omc - pp * sd) / qp;
+  qp = -(aj * omc + pm * sd) / qp;
+  self.b = (aj * qm + ap * qp) * sdh / sd;
+  self.c = (aj * qm - ap * qp) * cdh / sd;
+  for (int k = 0; k < njun1; k++) {
+    out[k].a = out[k].a * qm;
+    out[k].b = out[k].b * qm;
+    out[k].c = out[k].c * qm;
+  }
+  for (int k = njun1; k < jsno; k++) {
+    out[k].a = -out[k].a * qp;
+    out[k].b = out[k].b * qp;
+    out[k].c = -out[k].c * qp;
+  }
+  out.push_back(self);
+}
+
+// c_geometry.cpp:3449-3458.
+int Geometry::test_ek_approximation(int seg1, int seg2) const {
+  double ratio = radius[seg2] / radius[seg1];
+  double xi = std::fabs(cab[seg1] * cab[seg2] + sab[seg1] * sab[seg2] + salp[seg1] * salp[seg2]);
+  if (xi < 0.999999 || std::fabs(ratio - 1.0) > 1.e-6) return 2;
+  return 0;
+}
+
+}  // namespace necb

@@ -1,0 +1,188 @@
+// Triangular solves on the row-major LU factors (replaces solve,
+// src/matrix_algebra.cpp:271-307), the FP64 residual of the mixed-precision
+// refinement, and the basis-to-segment current coefficients (replaces
+// c_geometry::get_current_coefficients, src/c_geometry.cpp:3299-3387).
+//
+// The triangular solves are blocked by TB rows: a one-CTA kernel solves the
+// diagonal block (column-oriented, lanes over rows), then a row-parallel
+// kernel (one warp per row, coalesced along the row) subtracts the block's
+// contribution from every remaining row.
+#pragma once
+#include <cstdint>
+
+#include "lu.cuh"
+
+namespace necb {
+
+constexpr int kTrsvB = 64;
+template <typename T>
+constexpr size_t trsv_diag_smem() {
+  return sizeof(T) * (kTrsvB * (kTrsvB + 1) + kTrsvB);
+}
+
+// Diagonal block of L (unit) or U: x = T_blk^-1 rhs_blk.  64 threads.
+template <typename T, bool LOWER>
+__global__ void __launch_bounds__(64) trsv_diag_kernel(const T* M, int64_t ld, int64_t n, int64_t b0,
+                                                       const T* rhs, T* sol) {
+  // dynamic shared memory: D[kTrsvB][kTrsvB + 1] then x[kTrsvB]
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*D)[kTrsvB + 1] = reinterpret_cast<T(*)[kTrsvB + 1]>(smem_raw);
+  T* x = reinterpret_cast<T*>(smem_raw) + kTrsvB * (kTrsvB + 1);
+  const int t = threadIdx.x;
+  const int bs = (int)min((int64_t)kTrsvB, n - b0);
+  for (int idx = t; idx < bs * bs; idx += 64) {
+    int r = idx / bs, q = idx - r * bs;
+    D[r][q] = M[(b0 + r) * ld + b0 + q];
+  }
+  if (t < bs) x[t] = rhs[b0 + t];
+  __syncthreads();
+  if (LOWER) {
+    for (int q = 0; q < bs - 1; q++) {
+      T xq = x[q];
+      if (t > q && t < bs) {
+        T l = D[t][q];
+        T a = x[t];
+        a.x -= l.x * xq.x - l.y * xq.y;
+        a.y -= l.x * xq.y + l.y * xq.x;
+        x[t] = a;
+      }
+      __syncthreads();
+    }
+  } else {
+    for (int q = bs - 1; q >= 0; q--) {
+      if (t == q) x[q] = cdiv(x[q], D[q][q]);
+      __syncthreads();
+      T xq = x[q];
+      if (t < q) {
+        T u = D[t][q];
+        T a = x[t];
+        a.x -= u.x * xq.x - u.y * xq.y;
+        a.y -= u.x * xq.y + u.y * xq.x;
+        x[t] = a;
+      }
+      __syncthreads();
+    }
+  }
+  if (t < bs) sol[b0 + t] = x[t];
+}
+
+// rhs[r] -= sum_{q in block} M[r][q] sol[q] for rows r in [r0, r1).
+template <typename T>
+__global__ void __launch_bounds__(256) trsv_update_kernel(const T* M, int64_t ld, int64_t n, int64_t b0,
+                                                          int64_t r0, int64_t r1, const T* sol, T* rhs) {
+  __shared__ T xs[kTrsvB];
+  const int bs = (int)min((int64_t)kTrsvB, n - b0);
+  if (threadIdx.x < bs) xs[threadIdx.x] = sol[b0 + threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t r = r0 + (int64_t)blockIdx.x * 8 + warp; r < r1; r += (int64_t)gridDim.x * 8) {
+    decltype(xs[0].x) sr = 0, si = 0;
+    for (int q = lane; q < bs; q += 32) {
+      T a = M[r * ld + b0 + q];
+      T v = xs[q];
+      sr += a.x * v.x - a.y * v.y;
+      si += a.x * v.y + a.y * v.x;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sr += __shfl_down_sync(0xffffffffu, sr, off);
+      si += __shfl_down_sync(0xffffffffu, si, off);
+    }
+    if (lane == 0) {
+      T a = rhs[r];
+      a.x -= sr;
+      a.y -= si;
+      rhs[r] = a;
+    }
+  }
+}
+
+// y[i] = src[perm[i]] converted to the factor precision.
+template <typename TO, typename TI>
+__global__ void permute_kernel(const TI* src, const int* perm, TO* dst, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    TI v = src[perm[i]];
+    TO o;
+    o.x = v.x;
+    o.y = v.y;
+    dst[i] = o;
+  }
+}
+
+// x += d (d in the factor precision)
+template <typename TD>
+__global__ void axpy_kernel(double2* x, const TD* d, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    x[i].x += (double)d[i].x;
+    x[i].y += (double)d[i].y;
+  }
+}
+
+// r = b - Z x (FP64), one warp per row; accumulates ||r||^2 into *rn2.
+__global__ void __launch_bounds__(256) residual_kernel(const double2* Z, int64_t ld, int64_t n,
+                                                       const double2* x, const double2* b,
+                                                       double2* r, double* rn2) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double part = 0.0;
+  for (int64_t row = (int64_t)blockIdx.x * 8 + warp; row < n; row += (int64_t)gridDim.x * 8) {
+    const double2* zr = Z + row * ld;
+    double sr = 0, si = 0;
+    for (int64_t q = lane; q < n; q += 32) {
+      double2 a = zr[q];
+      double2 v = x[q];
+      sr += a.x * v.x - a.y * v.y;
+      si += a.x * v.y + a.y * v.x;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      sr += __shfl_down_sync(0xffffffffu, sr, off);
+      si += __shfl_down_sync(0xffffffffu, si, off);
+    }
+    if (lane == 0) {
+      double2 bb = b[row];
+      double2 o = make_double2(bb.x - sr, bb.y - si);
+      r[row] = o;
+      part += o.x * o.x + o.y * o.y;
+    }
+  }
+  if (lane == 0) atomicAdd(rn2, part);
+}
+
+// Current coefficients: for each segment j, sum over the basis functions
+// with support on j in ascending basis order (the reference's accumulation
+// order), then the segment-centre current (air+cir, aii+cii).
+__global__ void coeff_kernel(int64_t n, const int32_t* ptr, const int32_t* basis,
+                             const double* a, const double* b, const double* c,
+                             const double2* sol, double* abc, double2* cur) {
+  int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  double air = 0, aii = 0, bir = 0, bii = 0, cir = 0, cii = 0;
+  for (int e = ptr[j]; e < ptr[j + 1]; e++) {
+    double2 s = sol[basis[e]];
+    double ax = a[e], bx = b[e], cx = c[e];
+    air += ax * s.x;
+    aii += ax * s.y;
+    bir += bx * s.x;
+    bii += bx * s.y;
+    cir += cx * s.x;
+    cii += cx * s.y;
+  }
+  abc[0 * n + j] = air;
+  abc[1 * n + j] = aii;
+  abc[2 * n + j] = bir;
+  abc[3 * n + j] = bii;
+  abc[4 * n + j] = cir;
+  abc[5 * n + j] = cii;
+  cur[j] = make_double2(air + cir, aii + cii);
+}
+
+// FP64 -> FP32 copy of a row-major matrix
+__global__ void demote_kernel(const double2* src, float2* dst, int64_t count) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (; i < count; i += stride) dst[i] = make_float2((float)src[i].x, (float)src[i].y);
+}
+
+}  // namespace necb
