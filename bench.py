@@ -1,0 +1,424 @@
+#!/usr/bin/env python3
+"""Solves/s of the NEC2++ thin-wire hot path on one B200 (or N replicas).
+
+A step is one pass of the hot path -- interaction-matrix fill, dense complex
+LU, solve (with FP64 refinement in mixed precision), current coefficients and
+the 91 x 72 far-field pattern -- for the 8 x 8 axial-mode helix array
+(11,520 segments, dense complex Z of 11,520^2, 1 GHz, 64 feeds with seeded
+phases).  Synthetic seeded geometry; no dataset.
+
+  value   mixed-precision solves/s with all inputs resident in HBM
+          (structure tables, right-hand side, direction list), all ranks
+  fp64    the same step in plain complex128 (reported beside it)
+  e2e     solves/s through the NEC2++ C API with host buffers: create the
+          context, build the geometry, cards, nec_rp_card (fill, factor,
+          solve, pattern), read Zin and gains, delete -- every byte moved
+          between host and device inside the timed region
+  cpu_baseline  the reference's own CPU implementation (oracle/_ref),
+          timed on a bounded sample of the same workload
+
+``--impl reference`` times the reference's CPU path alone (rank 0).
+Under torchrun each rank runs an independent replica (no collective on the
+data path); value is the total over ranks and the step time the max.
+"""
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "Solves/s at N=11520, mixed vs FP64 on B200 at ≤1e-6 Zin err; grad/fwd cost"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--k", type=int, default=8, help="helix array is k x k (k=8: N=11520)")
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fp64", action="store_true")
+    return p.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d, "measured"
+    return FALLBACK_PEAKS, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() in ("active", "1", "yes"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference CPU path
+def reference_sample(k_sample, seed, omp):
+    """Time the reference (oracle/_ref) on the k_sample x k_sample helix array
+    and extrapolate to the 8 x 8 array: fill and pattern scale as N^2, the LU
+    as N^3 (its dense O(N^3) factorisation dominates)."""
+    from oracle.refwrap import RefAPI
+    from necpp_b200 import workloads as W
+    ref = RefAPI(omp=omp)
+    ctx = ref.nec_create()
+    t0 = time.perf_counter()
+    n = W.helix_array(ref, ctx, k=k_sample, seed=seed)
+    t_total = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ref.fill(ctx)  # the reference's cmset again, alone
+    t_fill = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ref.nec_rp_card(ctx, *W.PATTERN_91x72)  # far field only (factors held)
+    t_pat = time.perf_counter() - t0
+    ref.nec_delete(ctx)
+    t_lu = max(t_total - t_fill - t_pat, 0.0)
+    scale = 8.0 / k_sample
+    t_full = t_fill * scale ** 2 + t_pat * scale ** 2 + t_lu * scale ** 3
+    return {"n_sample": n, "t_sample_s": t_total, "t_fill_s": t_fill, "t_lu_s": t_lu,
+            "t_pattern_s": t_pat, "t_extrapolated_s": t_full}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    from oracle import refwrap
+    omp = refwrap.available(omp=True)
+    k_sample = 4
+    for _ in range(args.warmup):
+        reference_sample(2, args.seed, omp)
+    ts = []
+    last = None
+    for _ in range(args.steps):
+        last = reference_sample(k_sample, args.seed, omp)
+        ts.append(last["t_extrapolated_s"])
+    t = statistics.mean(ts)
+    v = 1.0 / t
+    sample = ("%dx%d helix array (N=%d) solved per step with the reference's CPU path; "
+              "extrapolated to 8x8 (N=11520) with fill/pattern ~N^2, LU ~N^3"
+              % (k_sample, k_sample, last["n_sample"]))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "helix_array_8x8 N=11520 1GHz seed=%d, 91x72 pattern" % args.seed,
+                   "precision": "fp64 (Eigen PartialPivLU)"},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores if omp else 1,
+                         "kind": "reference", "sample": sample,
+                         "threads": "Eigen OpenMP build" if omp else "single thread"},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "detail": last,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- B200 path
+class Stats(C.Structure):
+    _fields_ = [("refine_iters", C.c_int), ("refine_residual", C.c_double),
+                ("ms_fill", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
+                ("ms_pattern", C.c_double), ("launches", C.c_int64), ("h2d_bytes", C.c_int64),
+                ("d2h_bytes", C.c_int64), ("k_ms", C.c_double * 9), ("k_launches", C.c_int64 * 9),
+                ("k_flops", C.c_double * 9)]
+
+
+K_NAMES = ["fill", "lu_panel", "lu_laswp", "lu_trsm", "lu_gemm", "trsv", "refine_residual",
+           "pattern", "other"]
+# roofline class of each kernel: (bound, unit of the recorded work)
+K_BOUND = {"fill": ("compute", "pair evaluations"), "lu_gemm": ("tensor", "flops"),
+           "lu_panel": ("latency", "flops"), "lu_trsm": ("compute", "flops"),
+           "trsv": ("hbm", "bytes"), "refine_residual": ("hbm", "bytes"),
+           "pattern": ("compute", "terms"), "lu_laswp": ("hbm", "bytes"), "other": ("hbm", "bytes")}
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    os.environ["NECPP_B200_DEVICE"] = str(local)
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    import necpp_b200 as nb
+    from necpp_b200 import workloads as W
+    L = nb.lib
+    L.nec_gpu_engine.restype = C.c_void_p
+    L.nec_gpu_engine.argtypes = [C.c_void_p]
+    for nm in ("necgpu_set_stream",):
+        getattr(L, nm).argtypes = [C.c_void_p, C.c_void_p]
+    L.necgpu_step_resident.argtypes = [C.c_void_p, C.c_int]
+    L.necgpu_reuse_last_inputs.argtypes = [C.c_void_p]
+    L.necgpu_enable_timing.argtypes = [C.c_void_p, C.c_int]
+    L.necgpu_reset_kernel_stats.argtypes = [C.c_void_p]
+    L.necgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    L.necgpu_last_error.restype = C.c_char_p
+    L.necgpu_last_error.argtypes = [C.c_void_p]
+    L.necgpu_read_resident.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+
+    class API:
+        def __getattr__(self, k):
+            return getattr(nb, k)
+
+        def helix(self, ctx, *a):
+            return nb.nec_helix(ctx, *a)
+
+    api = API()
+    stream = torch.cuda.Stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def check(eng, rc):
+        if rc != 0:
+            raise RuntimeError(L.necgpu_last_error(eng).decode())
+
+    def prepare(precision):
+        ctx = nb.nec_create()
+        nb.nec_set_precision(ctx, precision)
+        W.helix_array(api, ctx, k=args.k, seed=args.seed)
+        eng = L.nec_gpu_engine(ctx)
+        check(eng, L.necgpu_set_stream(eng, C.c_void_p(stream.cuda_stream)))
+        check(eng, L.necgpu_reuse_last_inputs(eng))
+        return ctx, eng
+
+    def zin_all(ctx):
+        nfeed = args.k * args.k
+        return np.array([complex(nb.nec_impedance_real_indexed(ctx, 0, f),
+                                 nb.nec_impedance_imag_indexed(ctx, 0, f)) for f in range(nfeed)])
+
+    def timed(eng, precision, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            check(eng, L.necgpu_step_resident(eng, precision))
+        st0 = Stats()
+        L.necgpu_get_stats(eng, C.byref(st0))
+        check(eng, L.necgpu_enable_timing(eng, 2))
+        L.necgpu_reset_kernel_stats(eng)
+        barrier()
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            check(eng, L.necgpu_step_resident(eng, precision))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        ms = e0.elapsed_time(e1) / steps
+        st = Stats()
+        L.necgpu_get_stats(eng, C.byref(st))
+        L.necgpu_enable_timing(eng, 0)
+        return ms, st, st.launches - st0.launches, clocks
+
+    peaks, peak_src = load_peaks()
+    out = {}
+
+    # ---- mixed precision, resident inputs
+    ctx_m, eng_m = prepare(1)
+    z_mixed = zin_all(ctx_m)
+    iters, resid = nb.last_refinement(ctx_m)
+    sampler = ClockSampler(local)
+    ms_m, st_m, launches_m, clocks = timed(eng_m, 1, args.steps, args.warmup, sampler)
+    ms_m_max = max_over_ranks(ms_m)
+
+    # ---- plain FP64
+    ms_f_max, z_fp64 = None, None
+    if not args.no_fp64:
+        ctx_f, eng_f = prepare(0)
+        z_fp64 = zin_all(ctx_f)
+        fsteps = max(1, min(args.steps, 5))
+        ms_f, st_f, _, _ = timed(eng_f, 0, fsteps, min(args.warmup, 3))
+        ms_f_max = max_over_ranks(ms_f)
+        out["fp64_kernels_ms_per_step"] = {K_NAMES[i]: st_f.k_ms[i] / fsteps for i in range(9) if st_f.k_launches[i]}
+        nb.nec_delete(ctx_f)
+
+    # ---- end to end through the C API (host buffers)
+    e2e_ms = []
+    h2d = d2h = 0
+    for s in range(args.e2e_steps + 1):
+        barrier()
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        ctx = nb.nec_create()
+        nb.nec_set_precision(ctx, 1)
+        W.helix_array(api, ctx, k=args.k, seed=args.seed)
+        z = zin_all(ctx)
+        g = nb.nec_gain_max(ctx, 0)
+        eng = L.nec_gpu_engine(ctx)
+        st = Stats()
+        L.necgpu_get_stats(eng, C.byref(st))
+        nb.nec_delete(ctx)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        if s > 0:  # the first pass is warm-up
+            e2e_ms.append(a0.elapsed_time(a1))
+            h2d, d2h = st.h2d_bytes, st.d2h_bytes
+        if not np.all(np.isfinite(z)) or not math.isfinite(g):
+            raise RuntimeError("e2e produced non-finite results")
+    e2e_ms_max = max_over_ranks(statistics.mean(e2e_ms))
+
+    # ---- roofline of the dominant kernel of the mixed step
+    shares = {K_NAMES[i]: st_m.k_ms[i] for i in range(9) if st_m.k_launches[i]}
+    tot = sum(shares.values()) or 1.0
+    dom = max(shares, key=shares.get)
+    di = K_NAMES.index(dom)
+    avg_ms = st_m.k_ms[di] / st_m.k_launches[di]
+    work = st_m.k_flops[di] / st_m.k_launches[di]
+    bound, unit_kind = K_BOUND[dom]
+    traffic = None
+    tfile = os.path.join(HERE, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get(dom)
+    if bound == "hbm":
+        achieved = work / (avg_ms * 1e-3) / 1e9
+        peak, unit = peaks["hbm_gbs"], "GB/s"
+    else:
+        achieved = work / (avg_ms * 1e-3) / 1e12
+        peak, unit = peaks["bf16_tflops_sustained"], "TFLOP/s"
+    roofline = {"kernel": dom, "bound": "hbm" if bound == "hbm" else "tensor", "achieved": achieved,
+                "peak": peak, "unit": unit, "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_src + (" bf16 dense sustained" if unit != "GB/s" else " copy"),
+                "avg_launch_ms": avg_ms, "work_per_launch": work, "work_unit": unit_kind,
+                "launches_per_step": st_m.k_launches[di] / args.steps,
+                "share": {k: round(v / tot, 4) for k, v in sorted(shares.items(), key=lambda kv: -kv[1])},
+                "ms_per_step_by_kernel": {k: v / args.steps for k, v in shares.items()}}
+
+    value = world * 1000.0 / ms_m_max
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_m_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 LU + c128 fill/refinement", "data": "synthetic",
+        "config": {"workload": "helix_array_%dx%d N=%d 1GHz seed=%d, 91x72 pattern"
+                   % (args.k, args.k, args.k * args.k * 180, args.seed),
+                   "precision": "mixed", "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (Z: 16 N^2 = %.2f GB rewritten every step)"
+                   % (16 * (args.k * args.k * 180) ** 2 / 1e9)},
+        "gpu_launches": int(launches_m / args.steps * args.steps),
+        "clocks": clocks,
+        "refine": {"iters": iters, "residual": resid},
+        "e2e": {"value": world * 1000.0 / e2e_ms_max, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": roofline,
+    }
+    if ms_f_max is not None:
+        line["fp64"] = {"value": world * 1000.0 / ms_f_max, "ms_per_step": ms_f_max}
+        line["mixed_vs_fp64"] = ms_f_max / ms_m_max
+        rel = np.abs(z_mixed - z_fp64) / np.abs(z_fp64)
+        line["zin_rel_err_mixed_vs_fp64"] = float(np.max(rel))
+    line.update(out)
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refwrap
+        if refwrap.available():
+            r = reference_sample(4, args.seed, omp=False)
+            line["cpu_baseline"] = {
+                "value": 1.0 / r["t_extrapolated_s"], "unit": "solves/s", "cores": 1, "kind": "reference",
+                "sample": "4x4 helix array (N=%d) with the reference's single-thread CPU path "
+                          "(%.1f s); extrapolated to N=11520 with fill/pattern ~N^2, LU ~N^3" % (r["n_sample"], r["t_sample_s"]),
+                "detail": r}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": 0, "kind": "reference",
+                                    "sample": "oracle/_ref not built on this host"}
+    nb.nec_delete(ctx_m)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

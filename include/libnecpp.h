@@ -157,6 +157,9 @@ long nec_get_segments(nec_context* in_context, double* x, double* y, double* z, 
    last frequency run; writes up to cap entries, returns the count. */
 long nec_get_trio(nec_context* in_context, int j, int* jco, double* ax, double* bx,
                   double* cx, long cap);
+/* The context's GPU engine (include/necgpu.h), created on first use; NULL
+   with nec_error_message() set when no usable device exists. */
+void* nec_gpu_engine(nec_context* in_context);
 /* Refinement diagnostics of the last solve (mixed precision). */
 long nec_last_refinement(nec_context* in_context, int* iters, double* residual);
 /* Complex far field E_theta / E_phi (V/m x wavelength, as stored by the

@@ -116,14 +116,40 @@ int necgpu_pattern(necgpu_engine* e, int n_dir, const double* theta,
 int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter);
 
 /* Diagnostics of the last necgpu_solve / necgpu_factor. */
+enum necgpu_kernel_class {
+  NECGPU_K_FILL = 0,
+  NECGPU_K_PANEL = 1,   /* LU panel factorisation */
+  NECGPU_K_LASWP = 2,   /* row interchanges */
+  NECGPU_K_TRSM = 3,    /* U12 = L11^-1 A12 */
+  NECGPU_K_GEMM = 4,    /* trailing update A22 -= L21 U12 */
+  NECGPU_K_TRSV = 5,    /* triangular solves */
+  NECGPU_K_RESID = 6,   /* FP64 refinement residual */
+  NECGPU_K_PATTERN = 7, /* far-field sum */
+  NECGPU_K_OTHER = 8,
+  NECGPU_K_COUNT = 9
+};
+
 typedef struct necgpu_stats {
   int refine_iters;
   double refine_residual;   /* final ||b - Z x|| / ||b|| (FP64) */
   double ms_fill, ms_factor, ms_solve, ms_pattern; /* last timings (0 if not timed) */
   int64_t launches;         /* kernels launched by the engine since create */
+  int64_t h2d_bytes, d2h_bytes; /* host<->device bytes copied since create */
+  /* per kernel class, accumulated while kernel timing is on: CUDA-event time
+     of every launch (ms), launch count, algorithmic flops of the launches */
+  double k_ms[NECGPU_K_COUNT];
+  int64_t k_launches[NECGPU_K_COUNT];
+  double k_flops[NECGPU_K_COUNT];
 } necgpu_stats;
 int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out);
+/* 1: time each stage (fill / factor / solve / pattern) with CUDA events.
+   2: additionally time every kernel launch by class (events around each
+      launch on the engine's stream; accumulated into k_ms / k_launches). */
 int necgpu_enable_timing(necgpu_engine* e, int on);
+int necgpu_reset_kernel_stats(necgpu_engine* e);
+/* Make the last right-hand side and direction list passed to necgpu_solve /
+   necgpu_pattern the resident inputs of necgpu_step_resident. */
+int necgpu_reuse_last_inputs(necgpu_engine* e);
 
 /* Device-resident access for benchmarks and tests: pointers into the engine's
  * own device buffers (valid until the next set_structure / destroy). */

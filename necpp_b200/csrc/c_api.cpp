@@ -260,6 +260,16 @@ long nec_get_trio(nec_context* c, int j, int* jco, double* ax, double* bx, doubl
   }
 }
 
+void* nec_gpu_engine(nec_context* c) {
+  if (!c) return nullptr;
+  try {
+    return (void*)c->engine();
+  } catch (const std::exception& ex) {
+    g_err = ex.what();
+    return nullptr;
+  }
+}
+
 long nec_last_refinement(nec_context* c, int* iters, double* residual) {
   if (!c) return 1;
   *iters = c->last_refine_iters;

@@ -75,6 +75,17 @@ struct necgpu_engine {
   int refine_max = 30;
   bool have_solution = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int timing_level = 0;
+  // per-launch kernel timing (level 2): event pairs pending until a sync
+  struct PendingK {
+    int cls, ev;
+    double flops;
+  };
+  std::vector<cudaEvent_t> kev;
+  int kev_used = 0;
+  std::vector<PendingK> kpend;
+  int last_ndir = 0;     // directions of the last necgpu_pattern call
+  bool last_rhs = false; // d_b holds the last right-hand side
 };
 
 namespace {
@@ -105,6 +116,47 @@ int fail(necgpu_engine* e, int code, const std::string& msg) {
     if (_r) return _r;   \
   } while (0)
 
+// Per-launch timing: an event pair on the launching stream around each
+// kernel of a class, resolved after the next stream synchronisation.
+int kbegin(necgpu_engine* e) {
+  if (e->timing_level < 2) return -1;
+  while ((int)e->kev.size() < e->kev_used + 2) {
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return -1;
+    e->kev.push_back(ev);
+  }
+  const int i = e->kev_used;
+  e->kev_used += 2;
+  cudaEventRecord(e->kev[i], e->stream);
+  return i;
+}
+void kend(necgpu_engine* e, int i, int cls, double flops) {
+  if (i < 0) return;
+  cudaEventRecord(e->kev[i + 1], e->stream);
+  e->kpend.push_back({cls, i, flops});
+}
+void kflush(necgpu_engine* e) {  // call after the stream has synchronised
+  for (auto& p : e->kpend) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e->kev[p.ev], e->kev[p.ev + 1]) == cudaSuccess) {
+      e->stats.k_ms[p.cls] += ms;
+      e->stats.k_launches[p.cls] += 1;
+      e->stats.k_flops[p.cls] += p.flops;
+    }
+  }
+  e->kpend.clear();
+  e->kev_used = 0;
+}
+
+// launch a kernel of class cls (algorithmic work 'flops') and check it
+#define KLAUNCH(cls, flops, ...)        \
+  do {                                  \
+    const int _kt = kbegin(e);          \
+    __VA_ARGS__;                        \
+    kend(e, _kt, (cls), (flops));       \
+    LAUNCHED();                         \
+  } while (0)
+
 template <typename T>
 void dfree(T*& p) {
   if (p) cudaFree((void*)p);
@@ -128,6 +180,7 @@ template <typename T>
 int upload(necgpu_engine* e, T*& p, const T* h, size_t count) {
   TRY(dalloc(e, p, count));
   if (count) CUDA_TRY(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, e->stream));
+  e->stats.h2d_bytes += count * sizeof(T);
   return 0;
 }
 
@@ -172,10 +225,14 @@ void free_all(necgpu_engine* e) {
   e->filled = false;
 }
 
+void kflush(necgpu_engine* e);
+
 int sync_status(necgpu_engine* e, int* out) {
   int h[4];
   CUDA_TRY(cudaMemcpyAsync(h, e->d_status, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->stats.d2h_bytes += sizeof(h);
+  kflush(e);
   *out = h[0];
   return 0;
 }
@@ -196,8 +253,9 @@ double tock(necgpu_engine* e) {
 template <int G, bool X>
 int launch_fill_t(necgpu_engine* e, const FillArgs& a) {
   dim3 grid((unsigned)((e->n + kFillTI - 1) / kFillTI), (unsigned)e->ntiles);
-  fill_kernel<G, X><<<grid, kFillTI, 0, e->stream>>>(a);
-  LAUNCHED();
+  // work units of the fill: one per (observation, source) pair
+  KLAUNCH(NECGPU_K_FILL, (double)e->n * (double)e->n,
+          fill_kernel<G, X><<<grid, kFillTI, 0, e->stream>>>(a));
   return 0;
 }
 
@@ -289,26 +347,32 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
     const size_t smem = (size_t)rpc * row_bytes + 2 * row_bytes;
     CUDA_TRY(cudaMemsetAsync(e->d_counter, 0, sizeof(unsigned), e->stream));
     void* args[] = {&pa};
-    CUDA_TRY(cudaLaunchCooperativeKernel((const void*)panel_kernel<R, kNB>, dim3(P), dim3(kPanelThreads),
-                                         args, smem, e->stream));
-    LAUNCHED();
-    if (n > kb) {
-      laswp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv);
+    {
+      // panel: m x kb unblocked LU, ~8 m kb^2 / 2 real flops
+      const int kt = kbegin(e);
+      CUDA_TRY(cudaLaunchCooperativeKernel((const void*)panel_kernel<R, kNB>, dim3(P), dim3(kPanelThreads),
+                                           args, smem, e->stream));
+      kend(e, kt, NECGPU_K_PANEL, 4.0 * (double)m * kb * kb);
       LAUNCHED();
     }
+    if (n > kb)
+      KLAUNCH(NECGPU_K_LASWP, 0.0,
+              laswp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
     const int64_t rest = n - k0 - kb;
     if (rest > 0) {
-      trsm_kernel<T, kNB><<<(unsigned)((rest + 31) / 32), 256, trsm_smem, e->stream>>>(M, ld, n, k0, kb);
-      LAUNCHED();
+      KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * rest,
+              trsm_kernel<T, kNB><<<(unsigned)((rest + 31) / 32), 256, trsm_smem, e->stream>>>(M, ld, n, k0, kb));
       dim3 g((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
-      gemm_sub_kernel<R><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb, ld,
-                                                  M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb);
-      LAUNCHED();
+      // complex multiply-add = 8 real flops
+      KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
+              gemm_sub_kernel<R><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb,
+                                                           ld, M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb));
     }
   }
   // permutation of the right-hand side from the interchange sequence
   std::vector<int> piv(n), perm(n);
   CUDA_TRY(cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  e->stats.d2h_bytes += n * sizeof(int);
   int st = 0;
   TRY(sync_status(e, &st));
   for (int64_t i = 0; i < n; i++) perm[i] = (int)i;
@@ -336,27 +400,28 @@ int run_trsv(necgpu_engine* e, const typename cvec<R>::T* M, typename cvec<R>::T
   constexpr size_t dsm = trsv_diag_smem<T>();
   CUDA_TRY(cudaFuncSetAttribute(trsv_diag_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
   CUDA_TRY(cudaFuncSetAttribute(trsv_diag_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+  // the 'flops' recorded for the solves are the bytes of factor read
   for (int k = 0; k < nblk; k++) {
     const int64_t b0 = (int64_t)k * kTrsvB;
-    trsv_diag_kernel<T, true><<<1, 64, dsm, e->stream>>>(M, ld, n, b0, rhs, sol);
-    LAUNCHED();
+    KLAUNCH(NECGPU_K_TRSV, (double)kTrsvB * kTrsvB * sizeof(T),
+            trsv_diag_kernel<T, true><<<1, 64, dsm, e->stream>>>(M, ld, n, b0, rhs, sol));
     const int64_t r0 = b0 + kTrsvB;
     if (r0 < n) {
       unsigned g = (unsigned)std::min<int64_t>((n - r0 + 7) / 8, 4 * e->nsm);
-      trsv_update_kernel<T><<<g, 256, 0, e->stream>>>(M, ld, n, b0, r0, n, sol, rhs);
-      LAUNCHED();
+      KLAUNCH(NECGPU_K_TRSV, (double)(n - r0) * kTrsvB * sizeof(T),
+              trsv_update_kernel<T><<<g, 256, 0, e->stream>>>(M, ld, n, b0, r0, n, sol, rhs));
     }
   }
   // backward: sol holds y; reuse rhs as the running right-hand side
   CUDA_TRY(cudaMemcpyAsync(rhs, sol, n * sizeof(T), cudaMemcpyDeviceToDevice, e->stream));
   for (int k = nblk - 1; k >= 0; k--) {
     const int64_t b0 = (int64_t)k * kTrsvB;
-    trsv_diag_kernel<T, false><<<1, 64, dsm, e->stream>>>(M, ld, n, b0, rhs, sol);
-    LAUNCHED();
+    KLAUNCH(NECGPU_K_TRSV, (double)kTrsvB * kTrsvB * sizeof(T),
+            trsv_diag_kernel<T, false><<<1, 64, dsm, e->stream>>>(M, ld, n, b0, rhs, sol));
     if (b0 > 0) {
       unsigned g = (unsigned)std::min<int64_t>((b0 + 7) / 8, 4 * e->nsm);
-      trsv_update_kernel<T><<<g, 256, 0, e->stream>>>(M, ld, n, b0, 0, b0, sol, rhs);
-      LAUNCHED();
+      KLAUNCH(NECGPU_K_TRSV, (double)b0 * kTrsvB * sizeof(T),
+              trsv_update_kernel<T><<<g, 256, 0, e->stream>>>(M, ld, n, b0, 0, b0, sol, rhs));
     }
   }
   return 0;
@@ -383,8 +448,8 @@ int run_solve(necgpu_engine* e, bool sync_checks) {
   e->stats.refine_iters = 0;
   e->stats.refine_residual = 0.0;
   if (e->factored == NECGPU_FP64) {
-    permute_kernel<double2, double2><<<g1, 256, 0, e->stream>>>(e->d_b, e->d_perm, e->d_w1, n);
-    LAUNCHED();
+    KLAUNCH(NECGPU_K_OTHER, 0.0,
+            permute_kernel<double2, double2><<<g1, 256, 0, e->stream>>>(e->d_b, e->d_perm, e->d_w1, n));
     TRY(run_trsv<double>(e, e->Z64, e->d_w1, e->d_x));
   } else if (e->factored == NECGPU_MIXED) {
     // x = 0, r = b; repeat: d = LU32^-1 r, x += d, r = b - Z64 x
@@ -392,31 +457,27 @@ int run_solve(necgpu_engine* e, bool sync_checks) {
     float2* w2 = reinterpret_cast<float2*>(e->d_w2);
     CUDA_TRY(cudaMemsetAsync(e->d_x, 0, n * sizeof(double2), e->stream));
     CUDA_TRY(cudaMemcpyAsync(e->d_r, e->d_b, n * sizeof(double2), cudaMemcpyDeviceToDevice, e->stream));
-    // ||b||
-    double bn2 = 0.0;
-    {
-      std::vector<double2> hb(n);
-      CUDA_TRY(cudaMemcpyAsync(hb.data(), e->d_b, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
-      CUDA_TRY(cudaStreamSynchronize(e->stream));
-      for (auto& v : hb) bn2 += v.x * v.x + v.y * v.y;
-    }
-    const double bn = std::sqrt(bn2);
-    double prev = 1e300, rel = 1.0;
-    int it = 0;
+    // ||b||^2 on the device (d_rn2[1])
     const unsigned gr = (unsigned)std::min<int64_t>((n + 7) / 8, 8 * e->nsm);
+    CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, 2 * sizeof(double), e->stream));
+    KLAUNCH(NECGPU_K_OTHER, 0.0, norm2_kernel<<<g1, 256, 0, e->stream>>>(e->d_b, n, e->d_rn2 + 1));
+    double prev = 1e300, rel = 1.0, bn = 0.0;
+    int it = 0;
     for (; it <= e->refine_max; it++) {
-      permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(e->d_r, e->d_perm, w1, n);
-      LAUNCHED();
+      KLAUNCH(NECGPU_K_OTHER, 0.0, permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(e->d_r, e->d_perm, w1, n));
       TRY(run_trsv<float>(e, e->Z32, w1, w2));
-      axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(e->d_x, w2, n);
-      LAUNCHED();
+      KLAUNCH(NECGPU_K_OTHER, 0.0, axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(e->d_x, w2, n));
       CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
-      residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, e->d_x, e->d_b, e->d_r, e->d_rn2);
-      LAUNCHED();
-      double rn2 = 0;
-      CUDA_TRY(cudaMemcpyAsync(&rn2, e->d_rn2, sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+      // bytes of FP64 Z read by the residual
+      KLAUNCH(NECGPU_K_RESID, (double)n * n * sizeof(double2),
+              residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, e->d_x, e->d_b, e->d_r, e->d_rn2));
+      double rn2[2] = {0, 0};
+      CUDA_TRY(cudaMemcpyAsync(rn2, e->d_rn2, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
       CUDA_TRY(cudaStreamSynchronize(e->stream));
-      rel = bn > 0 ? std::sqrt(rn2) / bn : 0.0;
+      e->stats.d2h_bytes += 2 * sizeof(double);
+      kflush(e);
+      bn = std::sqrt(rn2[1]);
+      rel = bn > 0 ? std::sqrt(rn2[0]) / bn : 0.0;
       if (!std::isfinite(rel)) return fail(e, NECGPU_ERR_NONFINITE, "refinement: non-finite residual");
       if (rel <= e->refine_tol) {
         it++;
@@ -434,9 +495,9 @@ int run_solve(necgpu_engine* e, bool sync_checks) {
   } else {
     return fail(e, NECGPU_ERR_ARG, "solve: no factorisation held");
   }
-  coeff_kernel<<<g1, 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc,
-                                          e->d_ccoef + 2 * e->nc, e->d_x, e->d_abc, e->d_cur);
-  LAUNCHED();
+  KLAUNCH(NECGPU_K_OTHER, 0.0,
+          coeff_kernel<<<g1, 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc,
+                                                  e->d_ccoef + 2 * e->nc, e->d_x, e->d_abc, e->d_cur));
   if (sync_checks) CUDA_TRY(cudaStreamSynchronize(e->stream));
   e->have_solution = true;
   return 0;
@@ -463,8 +524,9 @@ int run_pattern(necgpu_engine* e, int ndir) {
   a.eta = e->P.eta;
   a.eth = e->d_eth;
   a.eph = e->d_eph;
-  pattern_kernel<<<(unsigned)((ndir + kPatDirs - 1) / kPatDirs), kPatDirs * 32, 0, e->stream>>>(a);
-  LAUNCHED();
+  // work units: one per (direction, segment, image) term
+  KLAUNCH(NECGPU_K_PATTERN, (double)ndir * n * a.ksymp,
+          pattern_kernel<<<(unsigned)((ndir + kPatDirs - 1) / kPatDirs), kPatDirs * 32, 0, e->stream>>>(a));
   return 0;
 }
 
@@ -485,8 +547,7 @@ int run_factor(necgpu_engine* e, int precision) {
     e->filled = false;  // Z64 now holds the factors
   } else if (precision == NECGPU_MIXED) {
     if (!e->Z32) TRY(dalloc(e, e->Z32, (size_t)e->n * e->ld));
-    demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld);
-    LAUNCHED();
+    KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld));
     TRY(run_lu<float>(e, e->Z32));
   } else {
     return fail(e, NECGPU_ERR_ARG, "factor: unknown precision");
@@ -571,6 +632,25 @@ int necgpu_set_stream(necgpu_engine* e, void* stream) {
 int necgpu_enable_timing(necgpu_engine* e, int on) {
   if (!e) return NECGPU_ERR_ARG;
   e->timing = on != 0;
+  e->timing_level = on;
+  return NECGPU_OK;
+}
+
+int necgpu_reset_kernel_stats(necgpu_engine* e) {
+  if (!e) return NECGPU_ERR_ARG;
+  for (int k = 0; k < NECGPU_K_COUNT; k++) {
+    e->stats.k_ms[k] = 0;
+    e->stats.k_launches[k] = 0;
+    e->stats.k_flops[k] = 0;
+  }
+  return NECGPU_OK;
+}
+
+int necgpu_reuse_last_inputs(necgpu_engine* e) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (!e->last_rhs) return fail(e, NECGPU_ERR_ARG, "reuse_last_inputs: no solve has run");
+  e->res_rhs = true;
+  e->res_ndir = e->last_ndir;
   return NECGPU_OK;
 }
 
@@ -752,12 +832,19 @@ int necgpu_solve(necgpu_engine* e, const double* rhs, double* cur, double* abc) 
   CUDA_TRY(cudaSetDevice(e->device));
   const int64_t n = e->n;
   CUDA_TRY(cudaMemcpyAsync(e->d_b, rhs, n * sizeof(double2), cudaMemcpyHostToDevice, e->stream));
+  e->stats.h2d_bytes += n * sizeof(double2);
+  e->last_rhs = true;
   tick(e);
   TRY(run_solve(e, false));
   e->stats.ms_solve = tock(e);
   CUDA_TRY(cudaMemcpyAsync(cur, e->d_cur, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
-  if (abc) CUDA_TRY(cudaMemcpyAsync(abc, e->d_abc, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+  e->stats.d2h_bytes += n * sizeof(double2);
+  if (abc) {
+    CUDA_TRY(cudaMemcpyAsync(abc, e->d_abc, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    e->stats.d2h_bytes += 6 * n * sizeof(double);
+  }
   CUDA_TRY(cudaStreamSynchronize(e->stream));
+  kflush(e);
   for (int64_t i = 0; i < 2 * n; i++)
     if (!std::isfinite(cur[i])) return fail(e, NECGPU_ERR_NONFINITE, "solve: non-finite current");
   return NECGPU_OK;
@@ -772,13 +859,17 @@ int necgpu_pattern(necgpu_engine* e, int ndir, const double* theta, const double
   TRY(ensure_pattern(e, ndir));
   CUDA_TRY(cudaMemcpyAsync(e->d_theta, theta, ndir * sizeof(double), cudaMemcpyHostToDevice, e->stream));
   CUDA_TRY(cudaMemcpyAsync(e->d_phi, phi, ndir * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  e->stats.h2d_bytes += 2 * ndir * sizeof(double);
   tick(e);
   TRY(run_pattern(e, ndir));
   e->stats.ms_pattern = tock(e);
   CUDA_TRY(cudaMemcpyAsync(eth, e->d_eth, ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
   CUDA_TRY(cudaMemcpyAsync(eph, e->d_eph, ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  e->stats.d2h_bytes += 2 * ndir * sizeof(double2);
   CUDA_TRY(cudaStreamSynchronize(e->stream));
-  e->res_ndir = 0;  // the resident direction list was overwritten
+  kflush(e);
+  e->last_ndir = ndir;
+  if (e->res_ndir > 0) e->res_ndir = ndir;  // the resident direction list was overwritten
   return NECGPU_OK;
 }
 

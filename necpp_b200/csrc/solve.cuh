@@ -178,6 +178,16 @@ __global__ void coeff_kernel(int64_t n, const int32_t* ptr, const int32_t* basis
   cur[j] = make_double2(air + cir, aii + cii);
 }
 
+// *out += ||v||^2
+__global__ void norm2_kernel(const double2* v, int64_t n, double* out) {
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    s += v[i].x * v[i].x + v[i].y * v[i].y;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
 // FP64 -> FP32 copy of a row-major matrix
 __global__ void demote_kernel(const double2* src, float2* dst, int64_t count) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
