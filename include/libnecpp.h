@@ -157,6 +157,20 @@ long nec_get_segments(nec_context* in_context, double* x, double* y, double* z, 
    last frequency run; writes up to cap entries, returns the count. */
 long nec_get_trio(nec_context* in_context, int j, int* jco, double* ax, double* bx,
                   double* cx, long cap);
+/* Build, on the host only, the structure tables the GPU receives at
+   freq_mhz: scaling, ground constants, trio basis tables, extended-kernel
+   flags (for inspection and for driving include/necgpu.h directly). */
+long nec_prepare_structure(nec_context* in_context, double freq_mhz);
+/* Copy those tables out: seg (8n: x y z length radius cab sab salp, in
+   wavelengths), tptr (n+1), tbasis (nt, 0-based), tabc (3nt: a b c),
+   ind (2n: EK end flags), params (8: rkh, use_exk, ground, zrati re/im,
+   frati re/im, eta).  Any pointer may be NULL; returns nt or -1. */
+long nec_get_structure(nec_context* in_context, double* seg, int* tptr, int* tbasis, double* tabc,
+                       int* ind, double* params);
+/* Applied-field right-hand side of the current excitation at the prepared
+   frequency (nec_context::etmns, src/nec_context.cpp:3488-3550): n complex,
+   interleaved; host only. */
+long nec_get_rhs(nec_context* in_context, double* out);
 /* The context's GPU engine (include/necgpu.h), created on first use; NULL
    with nec_error_message() set when no usable device exists. */
 void* nec_gpu_engine(nec_context* in_context);

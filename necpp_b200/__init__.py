@@ -93,9 +93,11 @@ _sig("nec_get_currents", _l, [_p, _i, _dp, _l])
 _sig("nec_get_segments", _l, [_p] + [_dp] * 8 + [_ip] * 3)
 _sig("nec_get_trio", _l, [_p, _i, _ip, _dp, _dp, _dp, _l])
 _sig("nec_last_refinement", _l, [_p, _ip, _dp])
+_sig("nec_prepare_structure", _l, [_p, _d])
+_sig("nec_get_structure", _l, [_p, _dp, _ip, _ip, _dp, _ip, _dp])
+_sig("nec_gpu_engine", _p, [_p])
+_sig("nec_get_rhs", _l, [_p, _dp])
 _sig("nec_get_pattern_fields", _l, [_p, _i, _dp, _dp, _l])
-
-_EXPORTS = [n for n in dir(lib) if False]
 
 
 def _wrap(name):
@@ -179,6 +181,36 @@ def pattern_fields(nec, index, n_cells):
     return eth[0::2] + 1j * eth[1::2], eph[0::2] + 1j * eph[1::2]
 
 
+def structure(nec, freq_mhz=None):
+    """The structure tables the GPU receives (wavelengths): dict with n, seg
+    (8n), tptr, tbasis, tabc (3nt), ind (2n), params (8).  With freq_mhz the
+    tables are (re)built on the host at that frequency first."""
+    if freq_mhz is not None and lib.nec_prepare_structure(nec, freq_mhz) != 0:
+        raise RuntimeError(nec_error_message())
+    n = lib.nec_segment_count(nec)
+    nt = lib.nec_get_structure(nec, None, None, None, None, None, None)
+    if nt < 0:
+        raise RuntimeError("no structure tables built")
+    st = {"n": n, "seg": _np.zeros(8 * n), "tptr": _np.zeros(n + 1, dtype=_np.int32),
+          "tbasis": _np.zeros(max(nt, 1), dtype=_np.int32), "tabc": _np.zeros(3 * max(nt, 1)),
+          "ind": _np.zeros(2 * n, dtype=_np.int32), "params": _np.zeros(8)}
+    lib.nec_get_structure(nec, _dptr(st["seg"]), _iptr(st["tptr"]), _iptr(st["tbasis"]), _dptr(st["tabc"]),
+                          _iptr(st["ind"]), _dptr(st["params"]))
+    st["tbasis"] = st["tbasis"][:nt]
+    st["tabc"] = st["tabc"][:3 * nt].copy()
+    return st
+
+
+def rhs(nec):
+    """Applied-field vector (complex, n) of the current excitation at the
+    frequency of the last structure()/nec_prepare_structure call."""
+    n = lib.nec_segment_count(nec)
+    out = _np.zeros(2 * n)
+    if lib.nec_get_rhs(nec, _dptr(out)) != 0:
+        raise RuntimeError(nec_error_message())
+    return out[0::2] + 1j * out[1::2]
+
+
 def last_refinement(nec):
     it = _C.c_int(0)
     res = _C.c_double(0)
@@ -187,4 +219,4 @@ def last_refinement(nec):
 
 
 __all__ = _PUBLIC + ["nec_error_message", "segments", "trio", "currents", "pattern_fields",
-                     "last_refinement", "lib"]
+                     "last_refinement", "structure", "rhs", "lib"]

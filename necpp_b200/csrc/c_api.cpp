@@ -260,6 +260,55 @@ long nec_get_trio(nec_context* c, int j, int* jco, double* ax, double* bx, doubl
   }
 }
 
+long nec_prepare_structure(nec_context* c, double freq_mhz) { NEC_TRY(c->prepare_structure(freq_mhz)); }
+
+long nec_get_structure(nec_context* c, double* seg, int* tptr, int* tbasis, double* tabc, int* ind,
+                       double* params) {
+  if (!c || c->tables.tptr.empty()) return -1;
+  auto& g = c->geometry();
+  auto& t = c->tables;
+  const int64_t n = g.n, nt = (int64_t)t.tbasis.size();
+  if (seg)
+    for (int64_t i = 0; i < n; i++) {
+      seg[i] = g.x[i];
+      seg[n + i] = g.y[i];
+      seg[2 * n + i] = g.z[i];
+      seg[3 * n + i] = g.length[i];
+      seg[4 * n + i] = g.radius[i];
+      seg[5 * n + i] = g.cab[i];
+      seg[6 * n + i] = g.sab[i];
+      seg[7 * n + i] = g.salp[i];
+    }
+  if (tptr) std::memcpy(tptr, t.tptr.data(), sizeof(int) * (n + 1));
+  if (tbasis) std::memcpy(tbasis, t.tbasis.data(), sizeof(int) * nt);
+  if (tabc) {
+    std::memcpy(tabc, t.ta.data(), sizeof(double) * nt);
+    std::memcpy(tabc + nt, t.tb.data(), sizeof(double) * nt);
+    std::memcpy(tabc + 2 * nt, t.tc.data(), sizeof(double) * nt);
+  }
+  if (ind) {
+    std::memcpy(ind, t.ind1.data(), sizeof(int) * n);
+    std::memcpy(ind + n, t.ind2.data(), sizeof(int) * n);
+  }
+  if (params) {
+    params[0] = t.rkh;
+    params[1] = t.use_exk;
+    params[2] = t.ground;
+    params[3] = t.zr_re;
+    params[4] = t.zr_im;
+    params[5] = t.fr_re;
+    params[6] = t.fr_im;
+    params[7] = t.eta;
+  }
+  return (long)nt;
+}
+
+long nec_get_rhs(nec_context* c, double* out) {
+  NEC_TRY(if (c->tables.tptr.empty()) necb::fail("structure not prepared");
+          std::vector<necb::cd> e; c->rhs(e);
+          std::memcpy(out, e.data(), sizeof(double) * 2 * e.size()));
+}
+
 void* nec_gpu_engine(nec_context* c) {
   if (!c) return nullptr;
   try {

@@ -379,15 +379,29 @@ void Context::antenna_environment() {
   if (iperf == 2) frati = (epsc - 1.0) / (epsc + 1.0);
 }
 
-// structure_segment_loading, src/nec_context.cpp:1523-1558: ground
-// environment, then fill and factor on the GPU.
-void Context::structure_loading() {
+void Context::prepare_structure(double freq) {
+  if (!geo_.completed) fail("geometry not complete");
+  freq_mhz = freq;
+  wavelength_ = wavelength_of(1.0e6 * freq_mhz);
+  geo_.frequency_scale(freq_mhz);
+  build_tables();
+}
+
+// Ground environment, basis tables (trio per source segment) and the
+// extended-kernel end flags at the current scaling.
+void Context::build_tables() {
   antenna_environment();
   const int64_t n = geo_.n;
   geo_.prepare_basis();
 
-  std::vector<int32_t> tptr(n + 1), tbasis;
-  std::vector<double> ta, tb, tc;
+  std::vector<int32_t>& tptr = tables.tptr;
+  std::vector<int32_t>& tbasis = tables.tbasis;
+  std::vector<double>&ta = tables.ta, &tb = tables.tb, &tc = tables.tc;
+  tptr.assign(n + 1, 0);
+  tbasis.clear();
+  ta.clear();
+  tb.clear();
+  tc.clear();
   tbasis.reserve(3 * n);
   ta.reserve(3 * n);
   tb.reserve(3 * n);
@@ -406,7 +420,10 @@ void Context::structure_loading() {
   }
 
   // extended thin-wire kernel end flags, cmww src/nec_context.cpp:2533-2594
-  std::vector<int32_t> ind1(n, 0), ind2(n, 0);
+  std::vector<int32_t>& ind1 = tables.ind1;
+  std::vector<int32_t>& ind2 = tables.ind2;
+  ind1.assign(n, 0);
+  ind2.assign(n, 0);
   if (use_exk) {
     for (int64_t jj = 0; jj < n; jj++) {
       const int jx = (int)jj + 1;
@@ -444,7 +461,28 @@ void Context::structure_loading() {
       ind2[jj] = i2;
     }
   }
+  if (ksymp != 2)
+    tables.ground = NECGPU_GROUND_NONE;
+  else if (iperf == 1)
+    tables.ground = NECGPU_GROUND_PERFECT;
+  else if (iperf == 0)
+    tables.ground = NECGPU_GROUND_REFLECTION;
+  else
+    tables.ground = NECGPU_GROUND_SOMMERFELD;
+  tables.zr_re = zrati.real();
+  tables.zr_im = zrati.imag();
+  tables.fr_re = frati.real();
+  tables.fr_im = frati.imag();
+  tables.eta = impedance();
+  tables.rkh = rkh;
+  tables.use_exk = use_exk ? 1 : 0;
+}
 
+// structure_segment_loading, src/nec_context.cpp:1523-1558: ground
+// environment and tables, then fill and factor on the GPU.
+void Context::structure_loading() {
+  build_tables();
+  const int64_t n = geo_.n;
   necgpu_structure s{};
   s.n = n;
   s.x = geo_.x.data();
@@ -455,28 +493,21 @@ void Context::structure_loading() {
   s.cab = geo_.cab.data();
   s.sab = geo_.sab.data();
   s.salp = geo_.salp.data();
-  s.trio_ptr = tptr.data();
-  s.trio_basis = tbasis.data();
-  s.trio_a = ta.data();
-  s.trio_b = tb.data();
-  s.trio_c = tc.data();
-  s.ek_ind1 = ind1.data();
-  s.ek_ind2 = ind2.data();
-  s.rkh = rkh;
-  s.use_exk = use_exk ? 1 : 0;
-  if (ksymp != 2)
-    s.ground = NECGPU_GROUND_NONE;
-  else if (iperf == 1)
-    s.ground = NECGPU_GROUND_PERFECT;
-  else if (iperf == 0)
-    s.ground = NECGPU_GROUND_REFLECTION;
-  else
-    s.ground = NECGPU_GROUND_SOMMERFELD;
-  s.zrati_re = zrati.real();
-  s.zrati_im = zrati.imag();
-  s.frati_re = frati.real();
-  s.frati_im = frati.imag();
-  s.eta = impedance();
+  s.trio_ptr = tables.tptr.data();
+  s.trio_basis = tables.tbasis.data();
+  s.trio_a = tables.ta.data();
+  s.trio_b = tables.tb.data();
+  s.trio_c = tables.tc.data();
+  s.ek_ind1 = tables.ind1.data();
+  s.ek_ind2 = tables.ind2.data();
+  s.rkh = tables.rkh;
+  s.use_exk = tables.use_exk;
+  s.ground = tables.ground;
+  s.zrati_re = tables.zr_re;
+  s.zrati_im = tables.zr_im;
+  s.frati_re = tables.fr_re;
+  s.frati_im = tables.fr_im;
+  s.eta = tables.eta;
 
   necgpu_engine* e = engine();
   check(e, necgpu_set_structure(e, &s));

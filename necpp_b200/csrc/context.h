@@ -86,7 +86,22 @@ class Context {
 
   necgpu_engine* engine();
 
+  // Structure tables handed to the GPU at the current frequency (host only):
+  // scale to freq_mhz, ground environment, basis tables, EK flags.
+  void prepare_structure(double freq_mhz);
+  // Applied-field vector of the current excitation at the prepared
+  // frequency (etmns), host only.
+  void rhs(std::vector<cd>& e) { build_rhs(e); }
+  struct Tables {
+    std::vector<int32_t> tptr, tbasis, ind1, ind2;
+    std::vector<double> ta, tb, tc;
+    int ground = 0;
+    double zr_re = 1, zr_im = 0, fr_re = 1, fr_im = 0, eta = 0, rkh = 1;
+    int use_exk = 0;
+  } tables;
+
  private:
+  void build_tables();
   enum State { MEM = 1, STRUCT = 2, EXSETUP = 3, EXLOOP = 4, NEAR = 5, FAR = 6 };
   enum Ret { PRINT_NORM = 0, FREQ_CONT = 1, CARD_CONT = 2, INNER_CONT = 3, PHASE_DONE = 4 };
 

@@ -1,0 +1,779 @@
+/*
+ * mom_oracle.c -- CPU restatement of the NEC2++ thin-wire hot path.
+ * TEST INFRASTRUCTURE ONLY (see mom_oracle.h).
+ *
+ * Each function follows the reference routine named beside it
+ * (NEC2++ src/nec_context.cpp unless another file is named).
+ */
+#include "mom_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef double complex cx;
+
+static const double PI = 3.1415926536;     /* math_util.h:72-74 */
+static const double TWO_PI = 2.0 * 3.1415926536;
+static const double C1 = 4.771341189;      /* j*4.771341189, 3055 */
+
+enum { ST_STEP = 1, ST_TABLE = 4 };
+
+/* c_evlcom.cpp:845-868 */
+static void test2(double f1r, double f2r, double* tr, double f1i, double f2i, double* ti) {
+  double den = fabs(f2r), t = fabs(f2i);
+  if (den < t) den = t;
+  if (den < 1.0e-37) {
+    *tr = 0.0;
+    *ti = 0.0;
+    return;
+  }
+  *tr = fabs((f1r - f2r) / den);
+  *ti = fabs((f1i - f2i) / den);
+}
+
+typedef struct {
+  double zpk, rkb2;
+  int ija;
+} gfstate;
+
+/* gf, 3553-3578 */
+static void gf(const gfstate* g, double zk, double* co, double* si) {
+  double zdk = zk - g->zpk;
+  double rk = sqrt(g->rkb2 + zdk * zdk);
+  *si = sin(rk) / rk;
+  if (g->ija) {
+    *co = cos(rk) / rk;
+    return;
+  }
+  if (rk >= .2) {
+    *co = (cos(rk) - 1.0) / rk;
+    return;
+  }
+  double rks = rk * rk;
+  *co = ((-1.38888889e-3 * rks + 4.16666667e-2) * rks - 0.5) * rk;
+}
+
+/* intx, 4135-4300: variable-interval Romberg integration */
+static void intx(const gfstate* g, double el1, double el2, double b, int ij, double* sgr,
+                 double* sgi, int* st) {
+  const int nx = 1, nma = 65536, nts = 4;
+  const double rx = 1.0e-4;
+  double z = el1, ze = el2;
+  if (ij == 0) ze = 0.;
+  double s = ze - z;
+  double fnm = nma;
+  double ep = s / (10. * fnm);
+  double zend = ze - ep;
+  double sr = 0., si = 0.;
+  int ns = nx, nt = 0, flag = 1;
+  double g1r, g1i, g2r = 0, g2i = 0, g3r = 0, g3i = 0, g4r, g4i, g5r = 0, g5i = 0, dz = 0, dzot = 0;
+  gf(g, z, &g1r, &g1i);
+  for (;;) {
+    if (flag) {
+      double fns = ns;
+      dz = s / fns;
+      double zp = z + dz;
+      if (zp > ze) {
+        dz = ze - z;
+        if (fabs(dz) <= ep) break;
+      }
+      dzot = dz * .5;
+      gf(g, z + dzot, &g3r, &g3i);
+      gf(g, z + dz, &g5r, &g5i);
+    }
+    double t00r = (g1r + g5r) * dzot, t00i = (g1i + g5i) * dzot;
+    double t01r = (t00r + dz * g3r) * 0.5, t01i = (t00i + dz * g3i) * 0.5;
+    double t10r = (4.0 * t01r - t00r) / 3.0, t10i = (4.0 * t01i - t00i) / 3.0;
+    double te1r, te1i;
+    test2(t01r, t10r, &te1r, t01i, t10i, &te1i);
+    if (te1i <= rx && te1r <= rx) {
+      sr = sr + t10r;
+      si = si + t10i;
+      nt += 2;
+      z += dz;
+      if (z >= zend) break;
+      g1r = g5r;
+      g1i = g5i;
+      if (nt >= nts && ns > nx) {
+        ns = ns / 2;
+        nt = 1;
+      }
+      flag = 1;
+      continue;
+    }
+    gf(g, z + dz * 0.25, &g2r, &g2i);
+    gf(g, z + dz * 0.75, &g4r, &g4i);
+    double t02r = (t01r + dzot * (g2r + g4r)) * 0.5, t02i = (t01i + dzot * (g2i + g4i)) * 0.5;
+    double t11r = (4.0 * t02r - t01r) / 3.0, t11i = (4.0 * t02i - t01i) / 3.0;
+    double t20r = (16.0 * t11r - t10r) / 15.0, t20i = (16.0 * t11i - t10i) / 15.0;
+    double te2r, te2i;
+    test2(t11r, t20r, &te2r, t11i, t20i, &te2i);
+    if (te2i > rx || te2r > rx) {
+      nt = 0;
+      if (ns >= nma) {
+        *st |= ST_STEP;
+      } else {
+        ns = ns * 2;
+        double fns = ns;
+        dz = s / fns;
+        dzot = dz * 0.5;
+        g5r = g3r;
+        g5i = g3i;
+        g3r = g2r;
+        g3i = g2i;
+        flag = 0;
+        continue;
+      }
+    }
+    sr = sr + t20r;
+    si = si + t20i;
+    nt++;
+    z += dz;
+    if (z >= zend) break;
+    g1r = g5r;
+    g1i = g5i;
+    if (nt >= nts && ns > nx) {
+      ns = ns / 2;
+      nt = 1;
+    }
+    flag = 1;
+  }
+  if (ij == 0) {
+    sr = 2. * (sr + log((sqrt(b * b + s * s) + s) / b));
+    si = 2. * si;
+  }
+  *sgr = sr;
+  *sgi = si;
+}
+
+/* gx, 3605-3620 */
+static void gx(double zz, double rh, double xk, cx* gz, cx* gzp) {
+  double r2 = zz * zz + rh * rh;
+  double r = sqrt(r2);
+  double rkz = xk * r;
+  cx temp = cos(rkz) - sin(rkz) * I;
+  temp = CMPLX(creal(temp) / r, cimag(temp) / r);
+  *gz = temp;
+  cx a = -CMPLX(1.0, rkz);
+  cx p = a * temp;
+  *gzp = CMPLX(creal(p) / r2, cimag(p) / r2);
+}
+
+static inline cx rmul(double s, cx a) { return CMPLX(s * creal(a), s * cimag(a)); }
+static inline cx rdiv(cx a, double s) { return CMPLX(creal(a) / s, cimag(a) / s); }
+
+/* gxx, 3623-3676 */
+static void gxx(double zz, double rh, double a, double a2, double xk, int ira, cx* g1, cx* g1p,
+                cx* g2, cx* g2p, cx* g3, cx* gzp) {
+  double r2 = zz * zz + rh * rh;
+  double r = sqrt(r2);
+  double r4 = r2 * r2;
+  double rk = xk * r;
+  double rk2 = rk * rk;
+  double rh2 = rh * rh;
+  double t1 = .25 * a2 * rh2 / r4;
+  double t2 = .5 * a2 / r2;
+  cx c1 = CMPLX(1.0, rk);
+  cx c2 = rmul(3., c1) - rk2;
+  cx c3 = rmul(rk2, CMPLX(6.0, rk)) - rmul(15., c1);
+  cx gz = rdiv(CMPLX(cos(rk), -sin(rk)), r);
+  *g2 = gz * (1. + rmul(t1, c2));
+  *g1 = *g2 - rmul(t2, c1) * gz;
+  gz = rdiv(gz, r2);
+  *g2p = gz * (rmul(t1, c3) - c1);
+  *gzp = rmul(t2, c2) * gz;
+  *g3 = *g2p + *gzp;
+  *g1p = rmul(zz, *g3);
+  if (ira != 1) {
+    *g3 = rmul(rh, *g3 + *gzp);
+    *gzp = rmul(-zz, c1) * gz;
+    if (rh <= 1.0e-10) {
+      *g2 = 0.;
+      *g2p = 0.;
+      return;
+    }
+    *g2 = rdiv(*g2, rh);
+    *g2p = rdiv(rmul(zz, *g2p), rh);
+    return;
+  }
+  t2 = .5 * a;
+  *g2 = rmul(-t2, c1) * gz;
+  *g2p = rdiv(rmul(t2, gz) * c2, r2);
+  *g3 = rmul(rh2, *g2p) - rmul(a, gz) * c1;
+  *g2p = rmul(zz, *g2p);
+  *gzp = rmul(-zz, c1) * gz;
+}
+
+/* eksc, 3051-3104 */
+static void eksc(double s, double z, double rh, double xk, int ij, cx* ezs, cx* ers, cx* ezc,
+                 cx* erc, cx* ezk, cx* erk, int* st) {
+  const cx K = CMPLX(0.0, C1);
+  gfstate g;
+  g.ija = ij;
+  g.zpk = xk * z;
+  double rhk = xk * rh;
+  g.rkb2 = rhk * rhk;
+  double sh = .5 * s;
+  double shk = xk * sh;
+  double ss = sin(shk), cs = cos(shk);
+  double z2a = sh - z;
+  double z1a = -(sh + z);
+  cx gz1, gz2, gp1, gp2;
+  gx(z1a, rh, xk, &gz1, &gp1);
+  gx(z2a, rh, xk, &gz2, &gp2);
+  cx gzp1 = rmul(z1a, gp1), gzp2 = rmul(z2a, gp2);
+  *ezs = K * (rmul(xk, rmul(cs, gz2 - gz1)) - rmul(ss, gzp2 + gzp1));
+  *ezc = -K * (rmul(xk, rmul(ss, gz2 + gz1)) + rmul(cs, gzp2 - gzp1));
+  *erk = rmul(rh, K * (gp2 - gp1));
+  double cint, sint;
+  intx(&g, -shk, shk, rhk, ij, &cint, &sint, st);
+  *ezk = -K * (gzp2 - gzp1 + rmul(xk * xk, CMPLX(cint, -sint)));
+  if (rh >= 1.0e-10) {
+    gzp1 = rmul(z1a, gzp1);
+    gzp2 = rmul(z2a, gzp2);
+    *ers = rdiv(-K * (rmul(ss, gzp2 + gzp1 + gz2 + gz1) - rmul(xk, rmul(cs, rmul(z2a, gz2) - rmul(z1a, gz1)))), rh);
+    *erc = rdiv(-K * (rmul(cs, gzp2 - gzp1 + gz2 - gz1) + rmul(xk, rmul(ss, rmul(z2a, gz2) + rmul(z1a, gz1)))), rh);
+    return;
+  }
+  *ers = 0.;
+  *erc = 0.;
+}
+
+/* ekscx, 3108-3188 */
+static void ekscx(double bx, double s, double z, double rhx, double xk, int ij, int inx1, int inx2,
+                  cx* ezs, cx* ers, cx* ezc, cx* erc, cx* ezk, cx* erk, int* st) {
+  const cx K = CMPLX(0.0, C1);
+  double b, rh;
+  int ira;
+  if (rhx >= bx) {
+    rh = rhx;
+    b = bx;
+    ira = 0;
+  } else {
+    rh = bx;
+    b = rhx;
+    ira = 1;
+  }
+  double sh = .5 * s;
+  gfstate g;
+  g.ija = ij;
+  g.zpk = xk * z;
+  double rhk = xk * rh;
+  g.rkb2 = rhk * rhk;
+  double shk = xk * sh;
+  double ss = sin(shk), cs = cos(shk);
+  double z2a = sh - z, z1a = -(sh + z);
+  double a2 = b * b;
+  cx gz1, gz2, gzp1, gzp2, gr1, gr2, grp1, grp2, grk1, grk2, gzz1, gzz2;
+  if (inx1 != 2) {
+    gxx(z1a, rh, b, a2, xk, ira, &gz1, &gzp1, &gr1, &grp1, &grk1, &gzz1);
+  } else {
+    gx(z1a, rhx, xk, &gz1, &grk1);
+    gzp1 = rmul(z1a, grk1);
+    gr1 = rdiv(gz1, rhx);
+    grp1 = rdiv(gzp1, rhx);
+    grk1 = rmul(rhx, grk1);
+    gzz1 = 0.;
+  }
+  if (inx2 != 2) {
+    gxx(z2a, rh, b, a2, xk, ira, &gz2, &gzp2, &gr2, &grp2, &grk2, &gzz2);
+  } else {
+    gx(z2a, rhx, xk, &gz2, &grk2);
+    gzp2 = rmul(z2a, grk2);
+    gr2 = rdiv(gz2, rhx);
+    grp2 = rdiv(gzp2, rhx);
+    grk2 = rmul(rhx, grk2);
+    gzz2 = 0.;
+  }
+  *ezs = K * (rmul(xk, rmul(cs, gz2 - gz1)) - rmul(ss, gzp2 + gzp1));
+  *ezc = -K * (rmul(xk, rmul(ss, gz2 + gz1)) + rmul(cs, gzp2 - gzp1));
+  *ers = -K * (rmul(ss, rmul(z2a, grp2) + rmul(z1a, grp1) + gr2 + gr1) -
+               rmul(xk, rmul(cs, rmul(z2a, gr2) - rmul(z1a, gr1))));
+  *erc = -K * (rmul(cs, rmul(z2a, grp2) - rmul(z1a, grp1) + gr2 - gr1) +
+               rmul(xk, rmul(ss, rmul(z2a, gr2) + rmul(z1a, gr1))));
+  *erk = K * (grk2 - grk1);
+  double cint, sint;
+  intx(&g, -shk, shk, rhk, ij, &cint, &sint, st);
+  double bk = b * xk;
+  double bk2 = bk * bk * .25;
+  *ezk = -K * (gzp2 - gzp1 + rmul(xk * xk * (1. - bk2), CMPLX(cint, -sint)) - rmul(bk2, gzz2 - gzz1));
+}
+
+typedef struct {
+  double x, y, z, s, b, cab, sab, salp;
+  int ind1, ind2;
+} src_t;
+
+/* efld_compute, 2777-2843: fields e[0..8] of one source (direct or image) */
+static double efld_compute(const mo_structure* S, const src_t* J, double xij, double yij, double ai,
+                           double salpr, double zij, int ijx, cx e[9], int* st) {
+  double cabj = J->cab, sabj = J->sab;
+  cx tezs = 0, ters = 0, tezc, terc, tezk, terk;
+  double zp = xij * cabj + yij * sabj + zij * salpr;
+  double rhox = xij - cabj * zp, rhoy = yij - sabj * zp, rhoz = zij - salpr * zp;
+  double rh = sqrt(rhox * rhox + rhoy * rhoy + rhoz * rhoz + ai * ai);
+  if (rh <= 1.e-10) {
+    rhox = 0.0;
+    rhoy = 0.0;
+    rhoz = 0.0;
+  } else {
+    rhox /= rh;
+    rhoy /= rh;
+    rhoz /= rh;
+  }
+  double r = sqrt(zp * zp + rh * rh);
+  if (r >= S->rkh) {
+    double rmag = TWO_PI * r;
+    double cth = zp / r;
+    double px = rh / r;
+    cx e0 = CMPLX(cos(rmag), -sin(rmag));
+    double py = TWO_PI * r * r;
+    cx e1 = rdiv(rmul(S->eta * cth, e0) * CMPLX(1.0, -1.0 / rmag), py);
+    cx e2 = rdiv(rmul(S->eta * px, e0) * CMPLX(1.0, rmag - 1.0 / rmag), 2. * py);
+    tezk = rmul(cth, e1) - rmul(px, e2);
+    terk = rmul(px, e1) + rmul(cth, e2);
+    double sf = sin(PI * J->s) / PI;
+    tezc = rmul(sf, tezk);
+    terc = rmul(sf, terk);
+    tezk = rmul(J->s, tezk);
+    terk = rmul(J->s, terk);
+    e[3] = 0.;
+    e[4] = 0.;
+    e[5] = 0.;
+  } else {
+    if (!S->use_exk)
+      eksc(J->s, zp, rh, TWO_PI, ijx, &tezs, &ters, &tezc, &terc, &tezk, &terk, st);
+    else
+      ekscx(J->b, J->s, zp, rh, TWO_PI, ijx, J->ind1, J->ind2, &tezs, &ters, &tezc, &terc, &tezk,
+            &terk, st);
+    e[3] = rmul(cabj, tezs) + rmul(rhox, ters);
+    e[4] = rmul(sabj, tezs) + rmul(rhoy, ters);
+    e[5] = rmul(salpr, tezs) + rmul(rhoz, ters);
+  }
+  e[0] = rmul(cabj, tezk) + rmul(rhox, terk);
+  e[1] = rmul(sabj, tezk) + rmul(rhoy, terk);
+  e[2] = rmul(salpr, tezk) + rmul(rhoz, terk);
+  e[6] = rmul(cabj, tezc) + rmul(rhox, terc);
+  e[7] = rmul(sabj, tezc) + rmul(rhoy, terc);
+  e[8] = rmul(salpr, tezc) + rmul(rhoz, terc);
+  return r;
+}
+
+/* fbar, c_ggrid.cpp:291-350 */
+static cx fbar(cx p) {
+  const double sp = sqrt(PI);
+  const double tosp = 2.0 / sp;
+  cx z = I * csqrt(p);
+  if (cabs(z) <= 3.) {
+    cx zs = z * z, sum = z, pw = z;
+    for (int i = 1; i <= 100; i++) {
+      pw = -pw * zs / (double)i;
+      cx term = pw / (2. * i + 1.);
+      sum = sum + term;
+      double tms = creal(term) * creal(term) + cimag(term) * cimag(term);
+      double sms = creal(sum) * creal(sum) + cimag(sum) * cimag(sum);
+      if (tms / sms < 1.E-12) break;
+    }
+    return 1. - (1. - sum * tosp) * z * cexp(zs) * sp;
+  }
+  int minus = 0;
+  if (creal(z) < 0.) {
+    minus = 1;
+    z = -z;
+  }
+  cx zs = .5 / (z * z), sum = 0., term = 1.;
+  for (int i = 1; i <= 6; i++) {
+    term = -term * (2. * i - 1.) * zs;
+    sum += term;
+  }
+  if (minus) sum -= 2.0 * sp * z * cexp(z * z);
+  return -sum;
+}
+
+/* gwave, c_ggrid.cpp:351-432 (r1 = zmh = 1, xx1 = 0 as set by sflds) */
+static void gwave(double r2, double zph, cx xx2, cx u, cx u2, double eta, cx* erv, cx* ezv,
+                  cx* erh, cx* ezh, cx* eph) {
+  const cx C4 = CMPLX(0.0, eta / 2.0);
+  const double r1 = 1.0, zmh = 1.0;
+  const cx xx1 = 0.;
+  double sppp = zmh / r1, sppp2 = sppp * sppp, cppp2 = 1. - sppp2;
+  if (cppp2 < 1.0e-20) cppp2 = 1.0e-20;
+  double cppp = sqrt(cppp2);
+  double spp = zph / r2, spp2 = spp * spp, cpp2 = 1. - spp2;
+  if (cpp2 < 1.0e-20) cpp2 = 1.0e-20;
+  double cpp = sqrt(cpp2);
+  const cx tpj = CMPLX(0.0, TWO_PI);
+  cx rk1 = -tpj * r1, rk2 = -tpj * r2;
+  cx t1 = 1. - u2 * cpp2, t2 = csqrt(t1);
+  cx t3 = (1. - 1. / rk1) / rk1, t4 = (1. - 1. / rk2) / rk2;
+  cx p1 = rk2 * u2 * t1 / (2. * cpp2);
+  cx rv = (spp - u * t2) / (spp + u * t2);
+  cx omr = 1. - rv;
+  cx w = 1. / omr;
+  w = CMPLX(4.0, 0.0) * p1 * w * w;
+  cx f = fbar(w);
+  cx q1 = rk2 * t1 / (2. * u2 * cpp2);
+  cx rh = (t2 - u * spp) / (t2 + u * spp);
+  cx v = 1. / (1. + rh);
+  v = CMPLX(4.0, 0.0) * q1 * v * v;
+  cx g = fbar(v);
+  cx xr1 = xx1 / r1, xr2 = xx2 / r2;
+  cx x1 = cppp2 * xr1, x2 = rv * cpp2 * xr2, x3 = omr * cpp2 * f * xr2;
+  cx x4 = u * t2 * spp * 2. * xr2 / rk2;
+  cx x5 = xr1 * t3 * (1. - 3. * sppp2), x6 = xr2 * t4 * (1. - 3. * spp2);
+  *ezv = (x1 + x2 + x3 - x4 - x5 - x6) * (-C4);
+  x1 = sppp * cppp * xr1;
+  x2 = rv * spp * cpp * xr2;
+  x3 = cpp * omr * u * t2 * f * xr2;
+  x4 = spp * cpp * omr * xr2 / rk2;
+  x5 = 3. * sppp * cppp * t3 * xr1;
+  x6 = cpp * u * t2 * omr * xr2 / rk2 * .5;
+  cx x7 = 3. * spp * cpp * t4 * xr2;
+  *erv = -(x1 + x2 - x3 + x4 - x5 + x6 - x7) * (-C4);
+  *ezh = -(x1 - x2 + x3 - x4 - x5 - x6 + x7) * (-C4);
+  x1 = sppp2 * xr1;
+  x2 = rv * spp2 * xr2;
+  x4 = u2 * t1 * omr * f * xr2;
+  x5 = t3 * (1. - 3. * cppp2) * xr1;
+  x6 = t4 * (1. - 3. * cpp2) * (1. - u2 * (1. + rv) - u2 * omr * f) * xr2;
+  x7 = u2 * cpp2 * omr * (1. - 1. / rk2) * (f * (u2 * t1 - spp2 - 1. / rk2) + 1. / rk2) * xr2;
+  *erh = (x1 - x2 - x4 - x5 + x6 + x7) * (-C4);
+  x1 = xr1;
+  x2 = rh * xr2;
+  x3 = (rh + 1.) * g * xr2;
+  x4 = t3 * xr1;
+  x5 = t4 * (1. - u2 * (1. + rv) - u2 * omr * f) * xr2;
+  x6 = .5 * u2 * omr * (f * (u2 * t1 - spp2 - 1. / rk2) + 1. / rk2) * xr2 / rk2;
+  *eph = -(x1 - x2 + x3 - x4 + x5 + x6) * (-C4);
+}
+
+/* efld, 2845-3045 + projection of cmww, 2617-2619 */
+static void pair(const mo_structure* S, const src_t* J, int64_t i, int ij, cx* etk, cx* ets, cx* etc,
+                 int* st) {
+  double xi = S->x[i], yi = S->y[i], zi = S->z[i], ai = S->b[i];
+  cx e[9];
+  double xij = xi - J->x, yij = yi - J->y;
+  efld_compute(S, J, xij, yij, ai, J->salp, zi - J->z, ij, e, st);
+  cx ex[9];
+  memcpy(ex, e, sizeof(ex));
+  const cx zrati = CMPLX(S->zrati_re, S->zrati_im), frati = CMPLX(S->frati_re, S->frati_im);
+  if (S->ground != 0) {
+    double zij = zi + J->z;
+    double r = efld_compute(S, J, xij, yij, ai, -J->salp, zij, 1, e, st);
+    if (S->ground == 2) {
+      cx zratx = zrati;
+      double xymag = sqrt(xij * xij + yij * yij);
+      double px, py, cth;
+      cx zrsin;
+      if (xymag <= 1.0e-6) {
+        px = 0.;
+        py = 0.;
+        cth = 1.;
+        zrsin = 1.;
+      } else {
+        px = -yij / xymag;
+        py = xij / xymag;
+        cth = zij / r;
+        zrsin = csqrt(1.0 - zratx * zratx * (1.0 - cth * cth));
+      }
+      cx refs = (cth - zratx * zrsin) / (cth + zratx * zrsin);
+      cx refps = -(zratx * cth - zrsin) / (zratx * cth + zrsin);
+      refps = refps - refs;
+      for (int k = 0; k < 9; k += 3) {
+        cx epy = rmul(px, e[k]) + rmul(py, e[k + 1]);
+        cx epx = rmul(px, epy);
+        epy = rmul(py, epy);
+        e[k] = refs * e[k] + refps * epx;
+        e[k + 1] = refs * e[k + 1] + refps * epy;
+        e[k + 2] = refs * e[k + 2];
+      }
+    }
+    for (int k = 0; k < 9; k++) ex[k] -= e[k] * frati;
+  }
+  if (S->ground == 3) {
+    double cabj = J->cab, sabj = J->sab, salpj = J->salp;
+    double sn = sqrt(cabj * cabj + sabj * sabj), xsn, ysn;
+    if (sn >= 1.0e-5) {
+      xsn = cabj / sn;
+      ysn = sabj / sn;
+    } else {
+      sn = 0.0;
+      xsn = 1.0;
+      ysn = 0.0;
+    }
+    double zij = zi + J->z, salpr = -salpj;
+    double rhox = sabj * zij - salpr * yij, rhoy = salpr * xij - cabj * zij, rhoz = cabj * yij - sabj * xij;
+    double rh = sqrt(rhox * rhox + rhoy * rhoy + rhoz * rhoz), xo, yo, zo;
+    if (rh <= 1.e-10) {
+      xo = xi - ai * ysn;
+      yo = yi + ai * xsn;
+      zo = zi;
+    } else {
+      rh = ai / sqrt(rh);
+      if (rhoz < 0.0) rh = -rh;
+      xo = xi + rh * rhox;
+      yo = yi + rh * rhoy;
+      zo = zi + rh * rhoz;
+    }
+    double r = xij * xij + yij * yij + zij * zij;
+    if (r <= .95) {
+      *st |= ST_TABLE;
+      for (int k = 0; k < 9; k++) e[k] = 0.;
+    } else {
+      /* sflds(0), isnor = 2: 6024-6098 */
+      double xt = J->x + 0. * cabj, yt = J->y + 0. * sabj, zt = J->z + 0. * salpj;
+      double rhx = xo - xt, rhy = yo - yt, rhs = rhx * rhx + rhy * rhy, rho = sqrt(rhs), phx, phy;
+      if (rho <= 0.0) {
+        rhx = 1.0;
+        rhy = 0.0;
+        phx = 0.0;
+        phy = 1.0;
+      } else {
+        rhx = rhx / rho;
+        rhy = rhy / rho;
+        phx = -rhy;
+        phy = rhx;
+      }
+      double cph = rhx * xsn + rhy * ysn, sph = rhy * xsn - rhx * ysn;
+      if (fabs(cph) < 1.0e-10) cph = 0.0;
+      if (fabs(sph) < 1.0e-10) sph = 0.0;
+      double zph = zo + zt, zphs = zph * zph, r2s = rhs + zphs, r2 = sqrt(r2s), rk = r2 * TWO_PI;
+      cx xx2 = CMPLX(cos(rk), -sin(rk));
+      cx erv, ezv, erh, ezh, eph;
+      gwave(r2, zph, xx2, zrati, zrati * zrati, S->eta, &erv, &ezv, &erh, &ezh, &eph);
+      const cx K = CMPLX(0.0, C1);
+      cx et = -K * frati * xx2 / (r2s * r2);
+      cx er = 2. * et * CMPLX(1.0, rk);
+      et = et * CMPLX(1.0 - rk * rk, rk);
+      cx hrv = (er + et) * rho * zph / r2s;
+      cx hzv = (zphs * er - rhs * et) / r2s;
+      cx hrh = (rhs * er - zphs * et) / r2s;
+      erv = erv - hrv;
+      ezv = ezv - hzv;
+      erh = erh + hrh;
+      ezh = ezh + hrv;
+      eph = eph + et;
+      erv = erv * salpj;
+      ezv = ezv * salpj;
+      erh = erh * sn * cph;
+      ezh = ezh * sn * cph;
+      eph = eph * sn * sph;
+      erh = erv + erh;
+      e[0] = (erh * rhx + eph * phx) * J->s;
+      e[1] = (erh * rhy + eph * phy) * J->s;
+      e[2] = (ezv + ezh) * J->s;
+      e[3] = e[4] = e[5] = 0.;
+      double sfac = PI * J->s;
+      sfac = sin(sfac) / sfac;
+      e[6] = e[0] * sfac;
+      e[7] = e[1] * sfac;
+      e[8] = e[2] * sfac;
+      double zp = xij * cabj + yij * sabj + zij * salpr;
+      rh = r - zp * zp;
+      double dmin = (rh <= 1.e-10) ? 0.0 : sqrt(rh / (rh + ai * ai));
+      if (dmin <= .95) {
+        double px = 1. - dmin;
+        for (int k = 0; k < 9; k += 3) {
+          cx t = (e[k] * cabj + e[k + 1] * sabj + e[k + 2] * salpr) * px;
+          e[k] = dmin * e[k] + t * cabj;
+          e[k + 1] = dmin * e[k + 1] + t * sabj;
+          e[k + 2] = dmin * e[k + 2] + t * salpr;
+        }
+      }
+    }
+    for (int k = 0; k < 9; k++) ex[k] = ex[k] + e[k];
+  }
+  double cabi = S->cab[i], sabi = S->sab[i], salpi = S->salp[i];
+  *etk = rmul(cabi, ex[0]) + rmul(sabi, ex[1]) + rmul(salpi, ex[2]);
+  *ets = rmul(cabi, ex[3]) + rmul(sabi, ex[4]) + rmul(salpi, ex[5]);
+  *etc = rmul(cabi, ex[6]) + rmul(sabi, ex[7]) + rmul(salpi, ex[8]);
+}
+
+/* cmset/cmww, 2077-2204, 2514-2650: for each source j, scatter-add into the
+   basis columns of trio(j), obs rows ascending. */
+int mo_fill(const mo_structure* S, double* zout) {
+  const int64_t n = S->n;
+  cx* z = (cx*)zout;
+  memset(z, 0, sizeof(cx) * n * n);
+  int st = 0;
+  for (int64_t j = 0; j < n; j++) {
+    src_t J = {S->x[j], S->y[j], S->z[j], S->s[j], S->b[j], S->cab[j], S->sab[j], S->salp[j],
+               S->ind1 ? S->ind1[j] : 0, S->ind2 ? S->ind2[j] : 0};
+    for (int64_t i = 0; i < n; i++) {
+      cx etk, ets, etc;
+      pair(S, &J, i, i != j, &etk, &ets, &etc, &st);
+      for (int32_t k = S->trio_ptr[j]; k < S->trio_ptr[j + 1]; k++) {
+        int64_t b = S->trio_basis[k];
+        z[i * n + b] += rmul(S->trio_a[k], etk) + rmul(S->trio_b[k], ets) + rmul(S->trio_c[k], etc);
+      }
+    }
+  }
+  return st;
+}
+
+/* LU with partial pivoting (row interchanges, largest modulus). */
+int mo_lu(int64_t n, double* a_, int32_t* piv) {
+  cx* a = (cx*)a_;
+  int bad = 0;
+  for (int64_t k = 0; k < n; k++) {
+    int64_t p = k;
+    double best = -1.0;
+    for (int64_t r = k; r < n; r++) {
+      cx v = a[r * n + k];
+      double m = creal(v) * creal(v) + cimag(v) * cimag(v);
+      if (m > best) {
+        best = m;
+        p = r;
+      }
+    }
+    piv[k] = (int32_t)p;
+    if (best == 0.0) {
+      bad = 1;
+      continue;
+    }
+    if (p != k)
+      for (int64_t c = 0; c < n; c++) {
+        cx t = a[k * n + c];
+        a[k * n + c] = a[p * n + c];
+        a[p * n + c] = t;
+      }
+    cx pv = a[k * n + k];
+    for (int64_t r = k + 1; r < n; r++) {
+      cx l = a[r * n + k] / pv;
+      a[r * n + k] = l;
+      for (int64_t c = k + 1; c < n; c++) a[r * n + c] -= l * a[k * n + c];
+    }
+  }
+  return bad;
+}
+
+void mo_solve(int64_t n, const double* lu_, const int32_t* piv, double* b_) {
+  const cx* a = (const cx*)lu_;
+  cx* b = (cx*)b_;
+  for (int64_t k = 0; k < n; k++) {
+    int64_t p = piv[k];
+    if (p != k) {
+      cx t = b[k];
+      b[k] = b[p];
+      b[p] = t;
+    }
+  }
+  for (int64_t i = 0; i < n; i++)
+    for (int64_t j = 0; j < i; j++) b[i] -= a[i * n + j] * b[j];
+  for (int64_t i = n - 1; i >= 0; i--) {
+    cx s = 0.;
+    for (int64_t j = i + 1; j < n; j++) s += a[i * n + j] * b[j];
+    b[i] = (b[i] - s) / a[i * n + i];
+  }
+}
+
+/* get_current_coefficients, c_geometry.cpp:3299-3387: for each segment the
+   basis functions with support on it, in ascending basis order. */
+void mo_coefficients(const mo_structure* S, const double* x_, double* abc, double* cur) {
+  const int64_t n = S->n;
+  const cx* x = (const cx*)x_;
+  double *air = abc, *aii = abc + n, *bir = abc + 2 * n, *bii = abc + 3 * n, *cir = abc + 4 * n,
+         *cii = abc + 5 * n;
+  memset(abc, 0, sizeof(double) * 6 * n);
+  /* walk basis i ascending; add into the segments it covers */
+  int64_t nt = S->trio_ptr[n];
+  int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (nt > 0 ? nt : 1));
+  int64_t* seg_of = (int64_t*)malloc(sizeof(int64_t) * (nt > 0 ? nt : 1));
+  for (int64_t j = 0; j < n; j++)
+    for (int32_t k = S->trio_ptr[j]; k < S->trio_ptr[j + 1]; k++) seg_of[k] = j;
+  /* counting sort of entries by basis index (stable) */
+  int64_t* cnt = (int64_t*)calloc(n + 1, sizeof(int64_t));
+  for (int64_t k = 0; k < nt; k++) cnt[S->trio_basis[k] + 1]++;
+  for (int64_t i = 0; i < n; i++) cnt[i + 1] += cnt[i];
+  for (int64_t k = 0; k < nt; k++) order[cnt[S->trio_basis[k]]++] = k;
+  for (int64_t q = 0; q < nt; q++) {
+    int64_t k = order[q];
+    int64_t i = S->trio_basis[k], j = seg_of[k];
+    double ar = creal(x[i]), ai = cimag(x[i]);
+    air[j] += S->trio_a[k] * ar;
+    aii[j] += S->trio_a[k] * ai;
+    bir[j] += S->trio_b[k] * ar;
+    bii[j] += S->trio_b[k] * ai;
+    cir[j] += S->trio_c[k] * ar;
+    cii[j] += S->trio_c[k] * ai;
+  }
+  for (int64_t j = 0; j < n; j++) {
+    cur[2 * j] = air[j] + cir[j];
+    cur[2 * j + 1] = aii[j] + cii[j];
+  }
+  free(order);
+  free(seg_of);
+  free(cnt);
+}
+
+/* ffld, 6639-6888 (wires; free space or infinite-ground image) */
+void mo_ffld(const mo_structure* S, const double* abc, double thet, double phi, double* eth_,
+             double* eph_) {
+  const int64_t n = S->n;
+  const double *air = abc, *aii = abc + n, *bir = abc + 2 * n, *bii = abc + 3 * n, *cir = abc + 4 * n,
+               *cii = abc + 5 * n;
+  const cx CONST3 = CMPLX(0.0, -S->eta / (4.0 * PI));
+  const cx zrati = CMPLX(S->zrati_re, S->zrati_im);
+  double phx = -sin(phi), phy = cos(phi), roz = cos(thet);
+  double thx = roz * phy, thy = -roz * phx, thz = -sin(thet);
+  double rox = -thz * phy, roy = thz * phx;
+  int ksymp = S->ground ? 2 : 1;
+  cx cix = 0, ciy = 0, ciz = 0, ccx = 0, ccy = 0, ccz = 0, rrv = 0, rrh = 0;
+  for (int k = 0; k < ksymp; k++) {
+    if (k != 0) {
+      if (S->ground == 1) {
+        rrv = -1.;
+        rrh = -1.;
+      } else {
+        cx zrsin = csqrt(1. - zrati * zrati * thz * thz);
+        rrv = -(roz - zrati * zrsin) / (roz + zrati * zrsin);
+        rrh = (zrati * roz - zrsin) / (zrati * roz + zrsin);
+      }
+      roz = -roz;
+      ccx = cix;
+      ccy = ciy;
+      ccz = ciz;
+    }
+    cix = 0;
+    ciy = 0;
+    ciz = 0;
+    for (int64_t i = 0; i < n; i++) {
+      double omega = -(rox * S->cab[i] + roy * S->sab[i] + roz * S->salp[i]);
+      double el = PI * S->s[i];
+      double sill = omega * el, top = el + sill, bot = el - sill, a, too, boo;
+      if (fabs(omega) >= 1.0e-7)
+        a = 2. * sin(sill) / omega;
+      else
+        a = (2. - omega * omega * el * el / 3.) * el;
+      if (fabs(top) >= 1.0e-7)
+        too = sin(top) / top;
+      else
+        too = 1. - top * top / 6.;
+      if (fabs(bot) >= 1.0e-7)
+        boo = sin(bot) / bot;
+      else
+        boo = 1. - bot * bot / 6.;
+      double b = el * (boo - too), c = el * (boo + too);
+      double rr = a * air[i] + b * bii[i] + c * cir[i];
+      double ri = a * aii[i] - b * bir[i] + c * cii[i];
+      double arg = TWO_PI * (S->x[i] * rox + S->y[i] * roy + S->z[i] * roz);
+      cx exa = CMPLX(cos(arg), sin(arg)) * CMPLX(rr, ri);
+      cix = cix + rmul(S->cab[i], exa);
+      ciy = ciy + rmul(S->sab[i], exa);
+      ciz = ciz + rmul(S->salp[i], exa);
+    }
+    if (k == 0) continue;
+    cx cdp = (rmul(phx, cix) + rmul(phy, ciy)) * (rrh - rrv);
+    cix = ccx + cix * rrv + rmul(phx, cdp);
+    ciy = ccy + ciy * rrv + rmul(phy, cdp);
+    ciz = ccz - ciz * rrv;
+  }
+  cx eth = (rmul(thx, cix) + rmul(thy, ciy) + rmul(thz, ciz)) * CONST3;
+  cx eph = (rmul(phx, cix) + rmul(phy, ciy)) * CONST3;
+  eth_[0] = creal(eth);
+  eth_[1] = cimag(eth);
+  eph_[0] = creal(eph);
+  eph_[1] = cimag(eph);
+}

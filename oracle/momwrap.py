@@ -1,0 +1,103 @@
+"""ctypes wrapper of oracle/liboracle.so (the C restatement of the hot path).
+
+Test infrastructure: only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "liboracle.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class MoStructure(C.Structure):
+    _fields_ = [("n", C.c_int64)] + [(k, _dp) for k in ("x", "y", "z", "s", "b", "cab", "sab", "salp")] + [
+        ("trio_ptr", _ip), ("trio_basis", _ip), ("trio_a", _dp), ("trio_b", _dp), ("trio_c", _dp),
+        ("ind1", _ip), ("ind2", _ip), ("rkh", C.c_double), ("use_exk", C.c_int), ("ground", C.c_int),
+        ("zrati_re", C.c_double), ("zrati_im", C.c_double), ("frati_re", C.c_double),
+        ("frati_im", C.c_double), ("eta", C.c_double)]
+
+
+def build():
+    """Compile liboracle.so (gcc, no contraction) if missing or stale."""
+    src = [os.path.join(HERE, f) for f in ("mom_oracle.c", "mom_oracle.h")]
+    if not os.path.exists(SO) or any(os.path.getmtime(s) > os.path.getmtime(SO) for s in src):
+        cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+        subprocess.run([cc, "-std=c11", "-O2", "-fPIC", "-shared", "-fno-fast-math", "-ffp-contract=off",
+                        "-o", SO, os.path.join(HERE, "mom_oracle.c"), "-lm"], check=True)
+    return SO
+
+
+class Oracle:
+    def __init__(self):
+        build()
+        L = C.CDLL(SO)
+        L.mo_fill.argtypes = [C.POINTER(MoStructure), _dp]
+        L.mo_fill.restype = C.c_int
+        L.mo_lu.argtypes = [C.c_int64, _dp, _ip]
+        L.mo_lu.restype = C.c_int
+        L.mo_solve.argtypes = [C.c_int64, _dp, _ip, _dp]
+        L.mo_coefficients.argtypes = [C.POINTER(MoStructure), _dp, _dp, _dp]
+        L.mo_ffld.argtypes = [C.POINTER(MoStructure), _dp, C.c_double, C.c_double, _dp, _dp]
+        self.L = L
+
+    def structure(self, st):
+        """st: dict from tests.helpers.export_structure (kept alive by the caller)."""
+        s = MoStructure()
+        s.n = st["n"]
+        seg = st["seg"]
+        n = st["n"]
+        for k, name in enumerate(("x", "y", "z", "s", "b", "cab", "sab", "salp")):
+            setattr(s, name, seg[k * n:(k + 1) * n].ctypes.data_as(_dp))
+        s.trio_ptr = st["tptr"].ctypes.data_as(_ip)
+        s.trio_basis = st["tbasis"].ctypes.data_as(_ip)
+        nt = len(st["tbasis"])
+        s.trio_a = st["tabc"][:nt].ctypes.data_as(_dp)
+        s.trio_b = st["tabc"][nt:2 * nt].ctypes.data_as(_dp)
+        s.trio_c = st["tabc"][2 * nt:].ctypes.data_as(_dp)
+        s.ind1 = st["ind"][:n].ctypes.data_as(_ip)
+        s.ind2 = st["ind"][n:].ctypes.data_as(_ip)
+        p = st["params"]
+        s.rkh, s.use_exk, s.ground = p[0], int(p[1]), int(p[2])
+        s.zrati_re, s.zrati_im, s.frati_re, s.frati_im, s.eta = p[3], p[4], p[5], p[6], p[7]
+        return s
+
+    def fill(self, st):
+        s = self.structure(st)
+        n = st["n"]
+        z = np.zeros(2 * n * n)
+        status = self.L.mo_fill(C.byref(s), z.ctypes.data_as(_dp))
+        return (z[0::2] + 1j * z[1::2]).reshape(n, n), status
+
+    def solve(self, z, rhs):
+        n = z.shape[0]
+        a = np.ascontiguousarray(z, dtype=np.complex128).copy()
+        piv = np.zeros(n, dtype=np.int32)
+        bad = self.L.mo_lu(n, a.view(np.float64).ctypes.data_as(_dp), piv.ctypes.data_as(_ip))
+        b = np.ascontiguousarray(rhs, dtype=np.complex128).copy()
+        self.L.mo_solve(n, a.view(np.float64).ctypes.data_as(_dp), piv.ctypes.data_as(_ip),
+                        b.view(np.float64).ctypes.data_as(_dp))
+        return b, bad
+
+    def coefficients(self, st, x):
+        s = self.structure(st)
+        n = st["n"]
+        xx = np.ascontiguousarray(x, dtype=np.complex128)
+        abc = np.zeros(6 * n)
+        cur = np.zeros(2 * n)
+        self.L.mo_coefficients(C.byref(s), xx.view(np.float64).ctypes.data_as(_dp),
+                               abc.ctypes.data_as(_dp), cur.ctypes.data_as(_dp))
+        return abc, cur[0::2] + 1j * cur[1::2]
+
+    def ffld(self, st, abc, thet, phi):
+        s = self.structure(st)
+        a, b = np.zeros(2), np.zeros(2)
+        self.L.mo_ffld(C.byref(s), abc.ctypes.data_as(_dp), thet, phi, a.ctypes.data_as(_dp),
+                       b.ctypes.data_as(_dp))
+        return complex(a[0], a[1]), complex(b[0], b[1])

@@ -1,0 +1,108 @@
+"""Parity cases: NEC2++ C-API call sequences run identically against this
+library and the reference build.  Each case is (builder, description); a
+builder takes (api, ctx) and returns the frequency (MHz) of its last run.
+"""
+import numpy as np
+
+from necpp_b200 import workloads as W
+
+
+def _ex1(api, ctx):
+    # reference testharness/python/test_examples.py:27-31 (example 1, unloaded part)
+    api.nec_wire(ctx, 0, 7, 0., 0., .75, 0., 0., 1.25, .001, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 1)
+    api.nec_ex_card(ctx, 0, 0, 4, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_xq_card(ctx, 0)
+    return None
+
+
+def _ex3_perfect(api, ctx):
+    # test_examples.py:110-121 (example 3: EK, perfect ground)
+    api.nec_wire(ctx, 0, 9, 0., 0.0, 2.0, 0.0, 0.0, 7.0, 0.03, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 1)
+    api.nec_ek_card(ctx, 0)
+    api.nec_fr_card(ctx, 0, 1, 30., 0)
+    api.nec_ex_card(ctx, 0, 0, 5, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_gn_card(ctx, 1, 0, 0, 0, 0, 0, 0, 0)
+    api.nec_rp_card(ctx, 0, 10, 2, 1, 3, 0, 1, 0.0, 0.0, 10.0, 90.0, 0, 0)
+    return 30.0
+
+
+def _ex3_finite(api, ctx):
+    # test_examples.py:123-128 (example 3 continued: reflection-coefficient ground)
+    _ex3_perfect(api, ctx)
+    api.nec_gn_card(ctx, 0, 0, 6.0, 1.000E-03, 0, 0, 0, 0)
+    api.nec_rp_card(ctx, 0, 10, 2, 1, 3, 0, 1, 0.0, 0.0, 10.0, 90.0, 0, 0)
+    return 30.0
+
+
+def _dipole(api, ctx):
+    W.dipole(api, ctx)
+    return 150.0
+
+
+def _helix1(api, ctx):
+    W.helix_array(api, ctx, k=1, seed=1)
+    return 1000.0
+
+
+def _helix2(api, ctx):
+    W.helix_array(api, ctx, k=2, seed=2)
+    return 1000.0
+
+
+def _mesh_small(api, ctx):
+    W.wire_mesh(api, ctx, nwires=11, nseg=10, side=1.0,
+                pattern=(0, 19, 8, 1, 0, 0, 0, 0.0, 0.0, 10.0, 45.0, 0.0, 0.0))
+    return 150.0
+
+
+def _yagi(seed, nfreq=3):
+    def build(api, ctx):
+        p = W.yagi_params(np.random.default_rng(seed))
+        W.yagi(api, ctx, p, nfreq=nfreq, pattern=(0, 19, 8, 1, 0, 0, 0, 0.0, 0.0, 10.0, 45.0, 0.0, 0.0))
+        return 140.0 + (nfreq - 1) * 20.0 / 31.0
+    return build
+
+
+def _yagi_ground(api, ctx):
+    W.yagi_ground(api, ctx, seed=5)
+    return 145.0
+
+
+def _yagi_ek_perfect(api, ctx):
+    p = W.yagi_params(np.random.default_rng(7), n_elements=4, nseg=15)
+    W.yagi(api, ctx, p, height=2.0, nfreq=1, f0=145.0, df=0.0, ground=(1, 0, 0, 0, 0, 0, 0, 0),
+           pattern=(0, 10, 4, 1, 0, 0, 1, 0.0, 0.0, 10.0, 90.0, 0.0, 0.0))
+    return 145.0
+
+
+def _plane_wave_reflection(api, ctx):
+    p = W.yagi_params(np.random.default_rng(11), n_elements=3, nseg=13)
+    half, xs, rad, segs = p
+    for e in range(len(half)):
+        api.nec_wire(ctx, e + 1, int(segs[e]), float(xs[e]), 0.0, 3.0 - float(half[e]), float(xs[e]), 0.0,
+                     3.0 + float(half[e]), float(rad[e]), 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 0)
+    api.nec_gn_card(ctx, 0, 0, 10.0, 0.01, 0, 0, 0, 0)
+    api.nec_fr_card(ctx, 0, 1, 145.0, 0.0)
+    api.nec_ex_card(ctx, 1, 2, 2, 0, 60.0, 0.0, 30.0, 15.0, 90.0, 0.0)
+    api.nec_rp_card(ctx, 0, 10, 4, 1, 0, 0, 0, 0.0, 0.0, 10.0, 90.0, 0.0, 0.0)
+    return 145.0
+
+
+# name: (builder, pattern grid (n_theta, n_phi) or None)
+CASES = {
+    "ex1": (_ex1, None),
+    "ex3_perfect": (_ex3_perfect, (10, 2)),
+    "ex3_finite": (_ex3_finite, (10, 2)),
+    "dipole": (_dipole, (91, 72)),
+    "helix1": (_helix1, (91, 72)),
+    "helix2": (_helix2, (91, 72)),
+    "mesh_small": (_mesh_small, (19, 8)),
+    "yagi_s1": (_yagi(1), (19, 8)),
+    "yagi_s2": (_yagi(2), (19, 8)),
+    "yagi_ground": (_yagi_ground, (1, 1)),
+    "yagi_ek_perfect": (_yagi_ek_perfect, (10, 4)),
+    "plane_wave_reflection": (_plane_wave_reflection, (10, 4)),
+}

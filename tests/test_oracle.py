@@ -1,0 +1,143 @@
+"""The oracle (oracle/mom_oracle.c, a CPU restatement of the reference's
+algorithm) pinned against the reference: its fill, solve, current
+coefficients and far field against the golden fixtures the reference
+produced (tests/golden/), and the published full-precision values of the
+reference's own tests (testharness/python/test_examples.py)."""
+import math
+
+import numpy as np
+import pytest
+
+from cases import CASES
+from conftest import golden
+from helpers import host_case
+
+NAMES = list(CASES)
+ETA = math.sqrt((4.0 * 3.1415926536 * 1.0e-7) / 8.854e-12)
+
+
+def _zcheck(g, Z):
+    if "Z" in g:
+        ref = g["Z"]
+        return np.max(np.abs(Z - ref)) / np.max(np.abs(ref)), np.mean(Z == ref)
+    idx = g["Z_idx"]
+    vals = Z[idx[:, 0], idx[:, 1]]
+    d = np.abs(vals - g["Z_val"]) / np.max(np.abs(g["Z_diag"]))
+    dd = np.abs(np.diag(Z) - g["Z_diag"]) / np.max(np.abs(g["Z_diag"]))
+    return max(d.max(), dd.max()), np.mean(vals == g["Z_val"])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_oracle_fill_matches_reference(nb, oracle, name):
+    ctx, st, _, _ = host_case(nb, CASES[name][0])
+    Z, status = oracle.fill(st)
+    assert status == 0
+    err, exact = _zcheck(golden(name), Z)
+    assert err <= 1e-14, err
+    assert exact >= 0.999, exact  # the restatement rounds as the reference does
+    nb.nec_delete(ctx)
+
+
+def _solve_case(nb, oracle, name):
+    ctx, st, rhs, api = host_case(nb, CASES[name][0])
+    Z, _ = oracle.fill(st)
+    x, bad = oracle.solve(Z, rhs)
+    assert bad == 0
+    abc, cur = oracle.coefficients(st, x)
+    return ctx, st, rhs, abc, cur
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if n != "plane_wave_reflection"])
+def test_oracle_solution_matches_reference(nb, oracle, name):
+    """LU + solve + current coefficients of the oracle against the
+    reference's current_vector and coefficients of its last solve."""
+    ctx, st, rhs, abc, cur = _solve_case(nb, oracle, name)
+    g = golden(name)
+    scale = np.max(np.abs(g["current_vector"]))
+    assert np.max(np.abs(cur - g["current_vector"])) / scale <= 1e-10
+    assert np.max(np.abs(abc.reshape(6, -1) - g["abc"])) / np.max(np.abs(g["abc"])) <= 1e-10
+    nb.nec_delete(ctx)
+
+
+def _zin(g, nb, st, rhs, cur):
+    # voltage sources: e[seg] = -V / (s * lambda)  ->  V = -e * s * lambda
+    lam = float(g["wavelength"])
+    n = st["n"]
+    s = st["seg"][3 * n:4 * n]
+    feeds = np.nonzero(rhs)[0]
+    v = -rhs[feeds] * s[feeds] * lam
+    return v / (cur[feeds] * lam), v, feeds
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if n not in ("mesh_small", "plane_wave_reflection")])
+def test_oracle_zin_matches_reference(nb, oracle, name):
+    ctx, st, rhs, abc, cur = _solve_case(nb, oracle, name)
+    g = golden(name)
+    zin, _, _ = _zin(g, nb, st, rhs, cur)
+    ref = g["zin"][-1]
+    ref = ref[~np.isnan(ref)]
+    assert np.max(np.abs(zin - ref) / np.abs(ref)) <= 1e-10
+    nb.nec_delete(ctx)
+
+
+def _gains(oracle, st, abc, lam, power, grid, th0=0.0, dth=10.0, ph0=0.0, dph=90.0, ground=False):
+    nth, nph = grid
+    gcon = lam * lam * 2.0 * 3.1415926536 / (ETA * power)
+    rad = (2 * 3.1415926536) / 360.0
+    out = np.full((nth, nph), np.nan)
+    for p in range(nph):
+        for t in range(nth):
+            th = th0 + dth * t
+            if ground and th > 90.01:
+                continue
+            eth, eph = oracle.ffld(st, abc, th * rad, (ph0 + dph * p) * rad)
+            x = gcon * (abs(eth) ** 2 + abs(eph) ** 2)
+            out[t, p] = -999.99 if x < 1e-20 else 10 * math.log10(x)  # db10, math_util.h:134-139
+    return out
+
+
+def test_published_example1_zin(nb, oracle):
+    """test_examples.py:35-36: Zin = 82.69792906662622 + j46.30603888063429."""
+    ctx, st, rhs, abc, cur = _solve_case(nb, oracle, "ex1")
+    zin, _, _ = _zin(golden("ex1"), nb, st, rhs, cur)
+    want = complex(82.69792906662622, 46.30603888063429)
+    assert abs(zin[0] - want) / abs(want) <= 1e-12
+    nb.nec_delete(ctx)
+
+
+@pytest.mark.parametrize("name,zin_want,gmax_want,places", [
+    # test_examples.py:119-121 (EK, perfect ground) and 126-128 (finite ground)
+    ("ex3_perfect", complex(83.7552291016712, 45.32205265591289), 8.393875976328134, 12),
+    ("ex3_finite", complex(86.415, 47.822), 1.44837, 3),
+])
+def test_published_example3(nb, oracle, name, zin_want, gmax_want, places):
+    ctx, st, rhs, abc, cur = _solve_case(nb, oracle, name)
+    g = golden(name)
+    zin, v, feeds = _zin(g, nb, st, rhs, cur)
+    lam = float(g["wavelength"])
+    power = float(np.sum(0.5 * np.real(v * np.conj(cur[feeds] * lam))))
+    gains = _gains(oracle, st, abc, lam, power, (10, 2), ground=True)
+    if places >= 12:
+        assert abs(zin[0] - zin_want) / abs(zin_want) <= 1e-12
+        assert abs(np.nanmax(gains) - gmax_want) <= 1e-10
+    else:
+        assert abs(zin[0].real - zin_want.real) < 10 ** -places * 0.5 * 10
+        assert abs(zin[0].imag - zin_want.imag) < 10 ** -places * 0.5 * 10
+        assert abs(np.nanmax(gains) - gmax_want) < 10 ** -places * 0.5 * 10
+    nb.nec_delete(ctx)
+
+
+def test_oracle_far_field_matches_reference(nb, oracle, ref):
+    """Direct comparison of the far-field sum with the reference's ffld."""
+    from necpp_b200 import workloads as W
+    ctx, st, rhs, abc, cur = _solve_case(nb, oracle, "yagi_ek_perfect")
+    rc = ref.nec_create()
+    CASES["yagi_ek_perfect"][0](ref, rc)
+    rng = np.random.default_rng(0)
+    for th, ph in rng.uniform(0, 1.5, size=(8, 2)):
+        a = oracle.ffld(st, abc, th, ph * 4)
+        b = ref.ffld(rc, th, ph * 4)
+        assert abs(a[0] - b[0]) <= 1e-11 * (abs(b[0]) + 1e-30)
+        assert abs(a[1] - b[1]) <= 1e-11 * (abs(b[1]) + 1e-30) + 1e-14
+    ref.nec_delete(rc)
+    nb.nec_delete(ctx)
