@@ -188,7 +188,7 @@ class Stats(C.Structure):
                 ("ms_fill", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
                 ("ms_pattern", C.c_double), ("launches", C.c_int64), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64), ("k_ms", C.c_double * 9), ("k_launches", C.c_int64 * 9),
-                ("k_flops", C.c_double * 9)]
+                ("k_flops", C.c_double * 9), ("pivoting", C.c_int)]
 
 
 K_NAMES = ["fill", "lu_panel", "lu_laswp", "lu_trsm", "lu_gemm", "trsv", "refine_residual",
@@ -318,7 +318,7 @@ def run_b200(args):
     # ---- end to end through the C API (host buffers)
     e2e_ms = []
     h2d = d2h = 0
-    for s in range(args.e2e_steps + 1):
+    for s in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         barrier()
         torch.cuda.synchronize()
         a0 = torch.cuda.Event(enable_timing=True)
@@ -340,7 +340,7 @@ def run_b200(args):
             h2d, d2h = st.h2d_bytes, st.d2h_bytes
         if not np.all(np.isfinite(z)) or not math.isfinite(g):
             raise RuntimeError("e2e produced non-finite results")
-    e2e_ms_max = max_over_ranks(statistics.mean(e2e_ms))
+    e2e_ms_max = max_over_ranks(statistics.mean(e2e_ms)) if e2e_ms else float("nan")
 
     # ---- roofline of the dominant kernel of the mixed step
     shares = {K_NAMES[i]: st_m.k_ms[i] for i in range(9) if st_m.k_launches[i]}

@@ -114,6 +114,12 @@ int necgpu_pattern(necgpu_engine* e, int n_dir, const double* theta,
 
 /* Refinement controls for NECGPU_MIXED (defaults: 1e-13, 30). */
 int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter);
+/* Pivoting of the NECGPU_MIXED factorisation.  1 (default): pivots chosen
+ * inside each 64-row diagonal block; the FP64 refinement absorbs the extra
+ * growth, and a refinement that stalls above 1e-10 (or a zero pivot in a
+ * block) refactors with 0: partial pivoting over the whole column, the
+ * reference's choice.  NECGPU_FP64 always uses partial pivoting. */
+int necgpu_set_pivoting(necgpu_engine* e, int mode);
 
 /* Diagnostics of the last necgpu_solve / necgpu_factor. */
 enum necgpu_kernel_class {
@@ -140,6 +146,9 @@ typedef struct necgpu_stats {
   double k_ms[NECGPU_K_COUNT];
   int64_t k_launches[NECGPU_K_COUNT];
   double k_flops[NECGPU_K_COUNT];
+  /* pivoting of the last mixed factorisation: 0 partial (whole column),
+     1 block-local (64-row diagonal block; refined in FP64, falls back to 0) */
+  int pivoting;
 } necgpu_stats;
 int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out);
 /* 1: time each stage (fill / factor / solve / pattern) with CUDA events.
@@ -167,6 +176,12 @@ int necgpu_set_resident(necgpu_engine* e, const double* rhs, int n_dir, const do
 int necgpu_step_resident(necgpu_engine* e, int precision);
 /* Copy results of the last resident step (cur: n complex, eth/eph: n_dir complex). */
 int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph);
+
+/* Diagnostic: apply one complex64 update C -= A B (m x n, inner kb) to a
+ * seeded random matrix with the tensor-core kernel and with the CUDA-core
+ * FP32 kernel; report max |difference| and max |reference| over C. */
+int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, double* max_abs_diff,
+                         double* max_abs_ref);
 
 #ifdef __cplusplus
 }

@@ -6,12 +6,15 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
+#include <type_traits>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/necgpu.h"
 #include "fill.cuh"
+#include "gemm_tc.cuh"
 #include "lu.cuh"
 #include "pattern.cuh"
 #include "solve.cuh"
@@ -86,7 +89,43 @@ struct necgpu_engine {
   std::vector<PendingK> kpend;
   int last_ndir = 0;     // directions of the last necgpu_pattern call
   bool last_rhs = false; // d_b holds the last right-hand side
+  // triangular solves: persistent sweeps (flags per 64-row block, epoch per sweep)
+  bool sweep_trsv = true;
+  int* d_flags = nullptr;
+  int flag_epoch = 0;
+  // tensor-core trailing update of the FP32 LU: packed BF16 operands with
+  // tensor maps over the whole buffers (built once per size)
+  bool use_tc = true;
+  __nv_bfloat16 *d_Ap = nullptr, *d_Bp = nullptr;
+  int64_t tc_rows = 0;
+  int tc_kdim = 0;
+  CUtensorMap tmA{}, tmB{};
+  // mixed path: block-local pivoting first, full partial pivoting as fallback
+  bool prefer_blockpiv = true;
+  bool blockpiv = false;
 };
+
+namespace {
+// relative FP64 residual above which block-local pivoting is abandoned
+constexpr double kRefineFallback = 1e-10;
+}
+
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+}  // namespace
 
 namespace {
 
@@ -217,6 +256,10 @@ void free_all(necgpu_engine* e) {
   dfree(e->d_phi);
   dfree(e->d_eth);
   dfree(e->d_eph);
+  dfree(e->d_flags);
+  dfree(e->d_Ap);
+  dfree(e->d_Bp);
+  e->tc_rows = 0;
   e->pat_cap = 0;
   e->res_ndir = 0;
   e->res_rhs = false;
@@ -298,6 +341,83 @@ int run_fill(necgpu_engine* e, bool want64, bool want32) {
   }
 }
 
+// ---------------- tensor-core trailing update ----------------
+int ensure_tc(necgpu_engine* e, int kdim, int64_t rows) {
+  if (e->d_Ap && e->tc_rows >= rows && e->tc_kdim == kdim) return 0;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  TRY(dalloc(e, e->d_Ap, (size_t)rows * kdim));
+  TRY(dalloc(e, e->d_Bp, (size_t)2 * rows * kdim));
+  auto make = [&](CUtensorMap* map, void* base, int64_t nrows, uint32_t box_rows) -> int {
+    cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)nrows};
+    cuuint64_t strides[1] = {(cuuint64_t)kdim * 2};
+    cuuint32_t box[2] = {(cuuint32_t)tc::BK, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  };
+  TRY(make(&e->tmA, e->d_Ap, rows, tc::BM));
+  TRY(make(&e->tmB, e->d_Bp, 2 * rows, tc::BN));
+  CUDA_TRY(cudaFuncSetAttribute(tc::gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+  e->tc_rows = rows;
+  e->tc_kdim = kdim;
+  return 0;
+}
+
+// C (m x n) -= A (m x kb) B (kb x n), complex64 row-major with leading
+// dimension ld, on the tensor cores.  m, n <= e->n (packed-buffer size).
+int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, int64_t ld, int64_t m, int64_t n,
+                int kb) {
+  const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
+  const int kdim = 6 * kbp;
+  TRY(ensure_tc(e, kdim, std::max(e->n, std::max(m, n))));
+  const int64_t cnt = m * kbp;
+  KLAUNCH(NECGPU_K_OTHER, 0.0,
+          tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, e->d_Ap));
+  dim3 g((unsigned)((n + 31) / 32), (unsigned)(kbp / 64));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, e->d_Bp));
+  const int m_tiles = (int)((m + tc::BM - 1) / tc::BM);
+  const int n_tiles = (int)((2 * n + tc::BN - 1) / tc::BN);
+  const int grid = std::max(1, std::min(m_tiles * n_tiles, e->nsm));
+  KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)m * n * kb,
+          tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, e->stream>>>(e->tmA, e->tmB, C, ld, (int)m, (int)n,
+                                                                              kdim, e->d_status));
+  return 0;
+}
+
+// trailing update of the FP32 LU for the panel at k0 of width kb
+int tc_update(necgpu_engine* e, float2* M, int64_t k0, int kb) {
+  const int64_t ld = e->ld, r0 = k0 + kb, rest = e->n - r0;
+  return tc_gemm_sub(e, M + r0 * ld + k0, M + k0 * ld + r0, M + r0 * ld + r0, ld, rest, rest, kb);
+}
+
+__global__ void fill_random_kernel(float2* p, int64_t count, uint32_t seed) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint32_t h = (uint32_t)i * 2654435761u ^ seed;
+  h ^= h >> 16;
+  h *= 0x7feb352du;
+  h ^= h >> 15;
+  h *= 0x846ca68bu;
+  h ^= h >> 16;
+  uint32_t g = h * 1664525u + 1013904223u;
+  p[i] = make_float2((h & 0xffffff) / 16777216.0f - 0.5f, (g & 0xffffff) / 16777216.0f - 0.5f);
+}
+
+__global__ void max_diff_kernel(const float2* a, const float2* b, int64_t ld, int64_t m, int64_t n, float* out) {
+  float mx = 0.f, ref = 0.f;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m * n; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = i / n, c = i - r * n;
+    float2 x = a[r * ld + c], y = b[r * ld + c];
+    mx = fmaxf(mx, fmaxf(fabsf(x.x - y.x), fabsf(x.y - y.y)));
+    ref = fmaxf(ref, fmaxf(fabsf(y.x), fabsf(y.y)));
+  }
+  atomicMax((int*)out, __float_as_int(mx));
+  atomicMax((int*)out + 1, __float_as_int(ref));
+}
+
 // ---------------- LU ----------------
 template <typename R>
 int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
@@ -362,11 +482,20 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
     if (rest > 0) {
       KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * rest,
               trsm_kernel<T, kNB><<<(unsigned)((rest + 31) / 32), 256, trsm_smem, e->stream>>>(M, ld, n, k0, kb));
-      dim3 g((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
-      // complex multiply-add = 8 real flops
-      KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
-              gemm_sub_kernel<R><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb,
-                                                           ld, M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb));
+      bool done = false;
+      if constexpr (std::is_same<R, float>::value) {
+        if (e->use_tc) {
+          TRY(tc_update(e, M, k0, kb));
+          done = true;
+        }
+      }
+      if (!done) {
+        dim3 g((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
+        // complex multiply-add = 8 real flops
+        KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
+                gemm_sub_kernel<R><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb,
+                                                             ld, M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb));
+      }
     }
   }
   // permutation of the right-hand side from the interchange sequence
@@ -384,8 +513,63 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
   TRY(upload(e, e->d_perm, perm.data(), perm.size()));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   if (st & kLuStatBarrierTimeout) return fail(e, NECGPU_ERR_CUDA, "LU: panel barrier timed out");
+  if (st & tc::kStatTimeout) return fail(e, NECGPU_ERR_CUDA, "LU: tensor-core update pipeline timed out");
   if (st & kLuStatNonFinite) return fail(e, NECGPU_ERR_NONFINITE, "LU: NaN/Inf in the matrix");
   if (st & kLuStatSingular) return fail(e, NECGPU_ERR_SINGULAR, "LU: singular matrix (zero pivot)");
+  return 0;
+}
+
+// FP32 LU with block-local pivoting (mixed path): no grid-wide reductions;
+// the panel is one CTA on the diagonal block plus row-parallel kernels.
+int run_lu_blockpiv(necgpu_engine* e, float2* M) {
+  using T = float2;
+  const int64_t n = e->n, ld = e->ld;
+  if (!e->d_piv) TRY(dalloc(e, e->d_piv, (size_t)n));
+  const size_t trsm_smem = (size_t)(kNB * kNB + kNB * 32) * sizeof(T);
+  CUDA_TRY(cudaFuncSetAttribute(trsm_kernel<T, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+  const size_t right_smem = (size_t)(kNB + 128) * (kNB + 1) * sizeof(T);
+  CUDA_TRY(cudaFuncSetAttribute(trsm_right_kernel<T, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)right_smem));
+  for (int64_t k0 = 0; k0 < n; k0 += kNB) {
+    const int kb = (int)std::min<int64_t>(kNB, n - k0);
+    KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * kb / 3.0,
+            diag_lu_kernel<T, kNB><<<1, kNB, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_status));
+    if (n > kb)
+      KLAUNCH(NECGPU_K_LASWP, 0.0,
+              laswp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
+    const int64_t rest = n - k0 - kb;
+    if (rest > 0) {
+      KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * rest,
+              trsm_right_kernel<T, kNB><<<(unsigned)((rest + 127) / 128), 128, right_smem, e->stream>>>(M, ld, n, k0,
+                                                                                                         kb));
+      KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * rest,
+              trsm_kernel<T, kNB><<<(unsigned)((rest + 31) / 32), 256, trsm_smem, e->stream>>>(M, ld, n, k0, kb));
+      if (e->use_tc) {
+        TRY(tc_update(e, M, k0, kb));
+      } else {
+        dim3 g((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
+        KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
+                gemm_sub_kernel<float><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb,
+                                                                 ld, M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb));
+      }
+    }
+  }
+  std::vector<int> piv(n), perm(n);
+  CUDA_TRY(cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+  e->stats.d2h_bytes += n * sizeof(int);
+  int st = 0;
+  TRY(sync_status(e, &st));
+  for (int64_t i = 0; i < n; i++) perm[i] = (int)i;
+  for (int64_t k = 0; k < n; k++) {
+    int p = piv[k];
+    if (p < 0 || p >= n) return fail(e, NECGPU_ERR_NONFINITE, "LU: invalid pivot index");
+    std::swap(perm[k], perm[p]);
+  }
+  TRY(upload(e, e->d_perm, perm.data(), perm.size()));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (st & tc::kStatTimeout) return fail(e, NECGPU_ERR_CUDA, "LU: tensor-core update pipeline timed out");
+  if (st & kLuStatNonFinite) return fail(e, NECGPU_ERR_NONFINITE, "LU: NaN/Inf in the matrix");
+  if (st & kLuStatSingular) return fail(e, NECGPU_ERR_SINGULAR, "LU: zero pivot in a diagonal block");
   return 0;
 }
 
@@ -398,6 +582,36 @@ int run_trsv(necgpu_engine* e, const typename cvec<R>::T* M, typename cvec<R>::T
   const int64_t n = e->n, ld = e->ld;
   const int nblk = (int)((n + kTrsvB - 1) / kTrsvB);
   constexpr size_t dsm = trsv_diag_smem<T>();
+  if (e->sweep_trsv) {
+    // persistent sweeps: one cooperative launch per triangle
+    if (!e->d_flags) {
+      TRY(dalloc(e, e->d_flags, (size_t)nblk));
+      CUDA_TRY(cudaMemsetAsync(e->d_flags, 0, nblk * sizeof(int), e->stream));
+      e->flag_epoch = 0;
+    }
+    CUDA_TRY(cudaFuncSetAttribute(trsv_sweep_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    CUDA_TRY(cudaFuncSetAttribute(trsv_sweep_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trsv_sweep_kernel<T, true>, kSweepThreads, dsm));
+    const int grid = std::max(1, std::min(nblk, per_sm * e->nsm));
+    const double tri_bytes = 0.5 * (double)n * (double)n * sizeof(T);
+    for (int pass = 0; pass < 2; pass++) {
+      int epoch = ++e->flag_epoch;
+      const T* src = pass == 0 ? rhs : sol;
+      T* dst = pass == 0 ? sol : rhs;
+      void* args[] = {(void*)&M, (void*)&ld, (void*)&n, (void*)&src, (void*)&dst, (void*)&e->d_flags, (void*)&epoch,
+                      (void*)&e->d_status};
+      const int kt = kbegin(e);
+      CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)trsv_sweep_kernel<T, true>
+                                                     : (const void*)trsv_sweep_kernel<T, false>,
+                                           dim3(grid), dim3(kSweepThreads), args, dsm, e->stream));
+      kend(e, kt, NECGPU_K_TRSV, tri_bytes);
+      LAUNCHED();
+    }
+    // the backward pass wrote the solution into rhs; return it in sol
+    CUDA_TRY(cudaMemcpyAsync(sol, rhs, n * sizeof(T), cudaMemcpyDeviceToDevice, e->stream));
+    return 0;
+  }
   CUDA_TRY(cudaFuncSetAttribute(trsv_diag_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
   CUDA_TRY(cudaFuncSetAttribute(trsv_diag_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
   // the 'flops' recorded for the solves are the bytes of factor read
@@ -440,6 +654,69 @@ int ensure_vectors(necgpu_engine* e) {
   return 0;
 }
 
+// Mixed-precision factorisation of the FP64 matrix: demote to complex64, then
+// LU with block-local pivoting (blockpiv) or full partial pivoting.
+int factor_mixed(necgpu_engine* e, bool blockpiv) {
+  if (!e->Z32) TRY(dalloc(e, e->Z32, (size_t)e->n * e->ld));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld));
+  e->blockpiv = blockpiv;
+  e->stats.pivoting = blockpiv ? 1 : 0;
+  if (blockpiv) {
+    const int rc = run_lu_blockpiv(e, e->Z32);
+    if (rc != NECGPU_ERR_SINGULAR && rc != NECGPU_ERR_NONFINITE) return rc;
+    // a diagonal block without a usable pivot: full partial pivoting
+    CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+    return factor_mixed(e, false);
+  }
+  return run_lu<float>(e, e->Z32);
+}
+
+// Iterative refinement with the complex64 factors against the FP64 matrix:
+// x = 0, r = b; repeat d = LU^-1 r, x += d, r = b - Z x (FP64) until the
+// relative residual reaches the tolerance or stops decreasing.
+int refine(necgpu_engine* e, int* iters, double* rel_out) {
+  const int64_t n = e->n;
+  const unsigned g1 = (unsigned)((n + 255) / 256);
+  float2* w1 = reinterpret_cast<float2*>(e->d_w1);
+  float2* w2 = reinterpret_cast<float2*>(e->d_w2);
+  CUDA_TRY(cudaMemsetAsync(e->d_x, 0, n * sizeof(double2), e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_r, e->d_b, n * sizeof(double2), cudaMemcpyDeviceToDevice, e->stream));
+  const unsigned gr = (unsigned)std::min<int64_t>((n + 7) / 8, 8 * e->nsm);
+  CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, 2 * sizeof(double), e->stream));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, norm2_kernel<<<g1, 256, 0, e->stream>>>(e->d_b, n, e->d_rn2 + 1));
+  double prev = 1e300, rel = 1.0;
+  int it = 0;
+  for (; it <= e->refine_max; it++) {
+    KLAUNCH(NECGPU_K_OTHER, 0.0, permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(e->d_r, e->d_perm, w1, n));
+    TRY(run_trsv<float>(e, e->Z32, w1, w2));
+    KLAUNCH(NECGPU_K_OTHER, 0.0, axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(e->d_x, w2, n));
+    CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
+    // bytes of FP64 Z read by the residual
+    KLAUNCH(NECGPU_K_RESID, (double)n * n * sizeof(double2),
+            residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, e->d_x, e->d_b, e->d_r, e->d_rn2));
+    double rn2[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(rn2, e->d_rn2, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    e->stats.d2h_bytes += 2 * sizeof(double);
+    kflush(e);
+    const double bn = std::sqrt(rn2[1]);
+    rel = bn > 0 ? std::sqrt(rn2[0]) / bn : 0.0;
+    if (!std::isfinite(rel)) {
+      *iters = it + 1;
+      *rel_out = rel;
+      return fail(e, NECGPU_ERR_NONFINITE, "refinement: non-finite residual");
+    }
+    if (rel <= e->refine_tol || rel > 0.5 * prev) {  // converged, or at the FP64 floor
+      it++;
+      break;
+    }
+    prev = rel;
+  }
+  *iters = it;
+  *rel_out = rel;
+  return 0;
+}
+
 // Solve Z x = b (d_b) into d_x (FP64) with the held factors; then the
 // current coefficients into d_abc / d_cur.
 int run_solve(necgpu_engine* e, bool sync_checks) {
@@ -452,43 +729,18 @@ int run_solve(necgpu_engine* e, bool sync_checks) {
             permute_kernel<double2, double2><<<g1, 256, 0, e->stream>>>(e->d_b, e->d_perm, e->d_w1, n));
     TRY(run_trsv<double>(e, e->Z64, e->d_w1, e->d_x));
   } else if (e->factored == NECGPU_MIXED) {
-    // x = 0, r = b; repeat: d = LU32^-1 r, x += d, r = b - Z64 x
-    float2* w1 = reinterpret_cast<float2*>(e->d_w1);
-    float2* w2 = reinterpret_cast<float2*>(e->d_w2);
-    CUDA_TRY(cudaMemsetAsync(e->d_x, 0, n * sizeof(double2), e->stream));
-    CUDA_TRY(cudaMemcpyAsync(e->d_r, e->d_b, n * sizeof(double2), cudaMemcpyDeviceToDevice, e->stream));
-    // ||b||^2 on the device (d_rn2[1])
-    const unsigned gr = (unsigned)std::min<int64_t>((n + 7) / 8, 8 * e->nsm);
-    CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, 2 * sizeof(double), e->stream));
-    KLAUNCH(NECGPU_K_OTHER, 0.0, norm2_kernel<<<g1, 256, 0, e->stream>>>(e->d_b, n, e->d_rn2 + 1));
-    double prev = 1e300, rel = 1.0, bn = 0.0;
     int it = 0;
-    for (; it <= e->refine_max; it++) {
-      KLAUNCH(NECGPU_K_OTHER, 0.0, permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(e->d_r, e->d_perm, w1, n));
-      TRY(run_trsv<float>(e, e->Z32, w1, w2));
-      KLAUNCH(NECGPU_K_OTHER, 0.0, axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(e->d_x, w2, n));
-      CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
-      // bytes of FP64 Z read by the residual
-      KLAUNCH(NECGPU_K_RESID, (double)n * n * sizeof(double2),
-              residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, e->d_x, e->d_b, e->d_r, e->d_rn2));
-      double rn2[2] = {0, 0};
-      CUDA_TRY(cudaMemcpyAsync(rn2, e->d_rn2, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
-      CUDA_TRY(cudaStreamSynchronize(e->stream));
-      e->stats.d2h_bytes += 2 * sizeof(double);
-      kflush(e);
-      bn = std::sqrt(rn2[1]);
-      rel = bn > 0 ? std::sqrt(rn2[0]) / bn : 0.0;
-      if (!std::isfinite(rel)) return fail(e, NECGPU_ERR_NONFINITE, "refinement: non-finite residual");
-      if (rel <= e->refine_tol) {
-        it++;
-        break;
-      }
-      if (rel > 0.5 * prev) {  // stagnated at the FP64 floor (or diverging)
-        it++;
-        break;
-      }
-      prev = rel;
+    double rel = 1.0;
+    int rc = refine(e, &it, &rel);
+    if ((rc == NECGPU_ERR_NONFINITE || rel > kRefineFallback) && e->blockpiv) {
+      // block-local pivoting was not good enough for this matrix: refactor
+      // the FP32 copy with full partial pivoting and refine again
+      TRY(factor_mixed(e, false));
+      int it2 = 0;
+      rc = refine(e, &it2, &rel);
+      it += it2;
     }
+    if (rc) return rc;
     e->stats.refine_iters = it;
     e->stats.refine_residual = rel;
     if (rel > 1e-6) return fail(e, NECGPU_ERR_REFINE, "refinement did not converge");
@@ -546,9 +798,7 @@ int run_factor(necgpu_engine* e, int precision) {
     TRY(run_lu<double>(e, e->Z64));
     e->filled = false;  // Z64 now holds the factors
   } else if (precision == NECGPU_MIXED) {
-    if (!e->Z32) TRY(dalloc(e, e->Z32, (size_t)e->n * e->ld));
-    KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld));
-    TRY(run_lu<float>(e, e->Z32));
+    TRY(factor_mixed(e, e->prefer_blockpiv));
   } else {
     return fail(e, NECGPU_ERR_ARG, "factor: unknown precision");
   }
@@ -586,6 +836,9 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (prop.major < 10) return fail(e, NECGPU_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
   if (!prop.cooperativeLaunch) return fail(e, NECGPU_ERR_NO_DEVICE, "device lacks cooperative launch");
   e->nsm = prop.multiProcessorCount;
+  if (const char* s = std::getenv("NECPP_B200_NO_TC")) e->use_tc = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_BLOCKED_TRSV")) e->sweep_trsv = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   e->own_stream = true;
   CUDA_TRY(cudaEventCreate(&e->ev0));
@@ -658,6 +911,12 @@ int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter) {
   if (!e || !(tol > 0) || max_iter < 0) return NECGPU_ERR_ARG;
   e->refine_tol = tol;
   e->refine_max = max_iter;
+  return NECGPU_OK;
+}
+
+int necgpu_set_pivoting(necgpu_engine* e, int mode) {
+  if (!e || (mode != 0 && mode != 1)) return NECGPU_ERR_ARG;
+  e->prefer_blockpiv = (mode == 1);
   return NECGPU_OK;
 }
 
@@ -927,6 +1186,48 @@ int necgpu_step_resident(necgpu_engine* e, int precision) {
   TRY(sync_status(e, &st));
   if (st & (kStatSommerfeldTab | kStatIterCap)) return fail(e, NECGPU_ERR_UNSUPPORTED, "step: fill status");
   return NECGPU_OK;
+}
+
+int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, double* max_abs_diff,
+                         double* max_abs_ref) {
+  if (!e || m < 1 || n < 1 || kb < 1 || kb > 1024 || !max_abs_diff || !max_abs_ref) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int64_t rows = (int64_t)kb + m, cols = (int64_t)kb + n, ld = cols;
+  float2 *X = nullptr, *Y = nullptr;
+  float* d = nullptr;
+  TRY(dalloc(e, X, (size_t)rows * ld));
+  int rc = dalloc(e, Y, (size_t)rows * ld);
+  if (!rc) rc = dalloc(e, d, 2);
+  if (!rc) {
+    const int64_t cnt = rows * ld;
+    fill_random_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(X, cnt, seed);
+    cudaMemcpyAsync(Y, X, cnt * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream);
+    cudaMemsetAsync(d, 0, 2 * sizeof(float), e->stream);
+    cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream);
+    // X: tensor cores; Y: CUDA-core FP32 reference of the same update
+    rc = tc_gemm_sub(e, X + (int64_t)kb * ld, X + kb, X + (int64_t)kb * ld + kb, ld, m, n, kb);
+    if (!rc) {
+      dim3 g((unsigned)((n + 63) / 64), (unsigned)((m + 63) / 64));
+      gemm_sub_kernel<float><<<g, 256, 0, e->stream>>>(Y + (int64_t)kb * ld, ld, Y + kb, ld, Y + (int64_t)kb * ld + kb,
+                                                       ld, m, n, kb);
+      max_diff_kernel<<<256, 256, 0, e->stream>>>(X + (int64_t)kb * ld + kb, Y + (int64_t)kb * ld + kb, ld, m, n, d);
+      float h[2] = {0, 0};
+      int st = 0;
+      cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, e->stream);
+      rc = sync_status(e, &st);
+      if (!rc && (st & tc::kStatTimeout)) rc = fail(e, NECGPU_ERR_CUDA, "tensor-core GEMM pipeline timed out");
+      if (!rc) {
+        cudaError_t ce = cudaGetLastError();
+        if (ce != cudaSuccess) rc = fail(e, NECGPU_ERR_CUDA, cudaGetErrorString(ce));
+      }
+      *max_abs_diff = h[0];
+      *max_abs_ref = h[1];
+    }
+  }
+  dfree(X);
+  dfree(Y);
+  dfree(d);
+  return rc;
 }
 
 int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph) {

@@ -1,0 +1,345 @@
+// Trailing update of the mixed-precision LU on the 5th-generation tensor
+// cores: C -= A * B for complex64 A (m x kb), B (kb x n), C (m x n), all
+// row-major, as ONE real BF16 GEMM with FP32 accumulation in TMEM.
+//
+// Real formulation.  Each complex FP32 operand is split into BF16 hi/lo parts
+// (x = hi + lo + O(2^-16 x)); with K' = 6 * kbp (kbp = kb rounded up to 64):
+//   A'[i]    = [ Ar_hi | Ai_hi | Ar_hi | Ai_hi | Ar_lo | Ai_lo ]          (m rows)
+//   B'[2j]   = [ Br_hi |-Bi_hi | Br_lo |-Bi_lo | Br_hi |-Bi_hi ]  -> Re(AB)_j
+//   B'[2j+1] = [ Bi_hi | Br_hi | Bi_lo | Br_lo | Bi_hi | Br_hi ]  -> Im(AB)_j
+// so D = A' B'^T (m x 2n) holds (Re, Im) of A*B interleaved per column: the
+// accumulator row of output row i is a contiguous run of complex values of
+// C's row i.  Products kept: hi*hi + hi*lo + lo*hi (the lo*lo term, ~2^-16
+// relative, is dropped); the FP64 refinement of the solve removes the rest.
+//
+// Kernel: persistent, one CTA per SM, 6 warps:
+//   warp 0  TMA producer: A' (128 x 64) and B' (256 x 64) tiles, 128B swizzle,
+//           into a 4-stage shared-memory ring (48 KB per stage);
+//   warp 1  MMA issuer: tcgen05.mma.cta_group::1.kind::f16, M=128 N=256 K=16,
+//           accumulating in one of two 128 x 256 FP32 TMEM buffers;
+//   warps 2-5 epilogue: tcgen05.ld of the finished buffer, C -= D in place,
+//           while the MMA warp fills the other buffer.
+// Every wait on an mbarrier is bounded; on timeout the kernel records an
+// error bit and winds down (outstanding TMA copies are waited for, TMEM is
+// freed).  TMA loads never use cluster multicast.
+#pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace necb {
+namespace tc {
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
+constexpr int A_BYTES = BM * BK * 2;            // 16 KB
+constexpr int B_BYTES = BN * BK * 2;            // 32 KB
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 48 KB
+constexpr int THREADS = 192;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr uint32_t TMEM_COLS = 512;  // two 256-column FP32 accumulators
+constexpr long long kWaitLimit = 1LL << 20;
+
+enum : int { kStatTimeout = 1 << 12 };
+
+// ---- PTX helpers --------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (long long i = 0; i < kWaitLimit; i++)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int c0, int c1, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(map), "r"(c0), "r"(c1), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// K-major, 128B-swizzled operand tile: rows of 128 B, 8-row atoms of 1 KB
+// (leading offset 16 B, stride offset 1 KB, descriptor version 1).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = (uint64_t)((addr & 0x3FFFF) >> 4);
+  d |= (uint64_t)1 << 16;          // leading byte offset (16 B units)
+  d |= (uint64_t)(1024 >> 4) << 32; // stride byte offset
+  d |= (uint64_t)1 << 46;          // version
+  d |= (uint64_t)2 << 61;          // SWIZZLE_128B
+  return d;
+}
+// BF16 x BF16 -> FP32, both K-major, M = 128, N = 256
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---- operand packing ----------------------------------------------------
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+// A' from A (m x kb complex, row-major lda): one thread per (row, k)
+__global__ void pack_a_kernel(const float2* A, int64_t lda, int m, int kb, int kbp, __nv_bfloat16* Ap) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)m * kbp) return;
+  const int i = (int)(idx / kbp), k = (int)(idx - (int64_t)i * kbp);
+  float2 a = k < kb ? A[(int64_t)i * lda + k] : make_float2(0.f, 0.f);
+  __nv_bfloat16 rh, rl, ih, il;
+  split_bf16(a.x, rh, rl);
+  split_bf16(a.y, ih, il);
+  __nv_bfloat16* row = Ap + (int64_t)i * 6 * kbp;
+  row[0 * kbp + k] = rh;
+  row[1 * kbp + k] = ih;
+  row[2 * kbp + k] = rh;
+  row[3 * kbp + k] = ih;
+  row[4 * kbp + k] = rl;
+  row[5 * kbp + k] = il;
+}
+
+// B' from B (kb x n complex, row-major ldb): tile of 64 k x 32 columns
+// through shared memory so both the reads (along n) and the writes (along k)
+// are contiguous.
+__global__ void __launch_bounds__(256) pack_b_kernel(const float2* B, int64_t ldb, int kb, int kbp, int n,
+                                                     __nv_bfloat16* Bp) {
+  __shared__ float2 t[64][33];
+  const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int kk = ty; kk < 64; kk += 8) {
+    const int k = k0 + kk, j = j0 + tx;
+    t[kk][tx] = (k < kb && j < n) ? B[(int64_t)k * ldb + j] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int64_t K2 = 6 * (int64_t)kbp;
+  // each warp writes rows (2j, 2j+1) for 4 columns j; lane covers k pairs
+  for (int jj = ty; jj < 32; jj += 8) {
+    const int j = j0 + jj;
+    if (j >= n) continue;
+    __nv_bfloat16* re = Bp + (int64_t)(2 * j) * K2 + k0;
+    __nv_bfloat16* im = re + K2;
+    for (int kk = tx; kk < 64; kk += 32) {
+      float2 b = t[kk][jj];
+      __nv_bfloat16 rh, rl, ih, il;
+      split_bf16(b.x, rh, rl);
+      split_bf16(b.y, ih, il);
+      const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
+      re[0 * kbp + kk] = rh;
+      re[1 * kbp + kk] = nih;
+      re[2 * kbp + kk] = rl;
+      re[3 * kbp + kk] = nil;
+      re[4 * kbp + kk] = rh;
+      re[5 * kbp + kk] = nih;
+      im[0 * kbp + kk] = ih;
+      im[1 * kbp + kk] = rh;
+      im[2 * kbp + kk] = il;
+      im[3 * kbp + kk] = rl;
+      im[4 * kbp + kk] = ih;
+      im[5 * kbp + kk] = rh;
+    }
+  }
+}
+
+// ---- the GEMM -----------------------------------------------------------
+// C (m x n complex, row-major ldc) -= D, D = A' B'^T, K' = kdim (multiple of 64)
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float2* C,
+                   int64_t ldc, int m, int n, int kdim, int* status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  // bars: full[STAGES], empty[STAGES], tfull[2], tempty[2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m_tiles = (m + BM - 1) / BM;
+  const int n_tiles = (2 * n + BN - 1) / BN;
+  const int total = m_tiles * n_tiles;
+  const int kblocks = kdim / BK;
+
+  auto bar = [&](int i) { return smem_u32(bars + i); };
+  const int FULL = 0, EMPTY = STAGES, TFULL = 2 * STAGES, TEMPTY = 2 * STAGES + 2;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(bar(FULL + s), 1);
+      mbar_init(bar(EMPTY + s), 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      mbar_init(bar(TFULL + a), 1);
+      mbar_init(bar(TEMPTY + a), 128);
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      int it = 0;
+      for (int tile = blockIdx.x; tile < total && !*abort_flag; tile += gridDim.x) {
+        const int mt = tile / n_tiles, nt = tile - mt * n_tiles;
+        for (int kb = 0; kb < kblocks; kb++, it++) {
+          const int s = it % STAGES;
+          const uint32_t ph = (it / STAGES) & 1;
+          if (!mbar_wait(bar(EMPTY + s), ph ^ 1)) {
+            atomicOr(status, kStatTimeout);
+            *abort_flag = 1;
+            break;
+          }
+          uint8_t* a_dst = smem + s * STAGE_BYTES;
+          uint8_t* b_dst = a_dst + A_BYTES;
+          mbar_expect_tx(bar(FULL + s), STAGE_BYTES);
+          tma_load_2d(smem_u32(a_dst), &tmA, kb * BK, mt * BM, bar(FULL + s));
+          tma_load_2d(smem_u32(b_dst), &tmB, kb * BK, nt * BN, bar(FULL + s));
+        }
+      }
+      // drain: every issued stage must have landed before the CTA may exit
+      for (int k = 0; k < STAGES && it > 0; k++) {
+        const int j = it - 1 - k;
+        if (j < 0) break;
+        mbar_wait(bar(FULL + (j % STAGES)), (j / STAGES) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int it = 0, tc = 0;
+      for (int tile = blockIdx.x; tile < total && !*abort_flag; tile += gridDim.x, tc++) {
+        const int acc = tc & 1;
+        const uint32_t aph = (tc >> 1) & 1;
+        if (!mbar_wait(bar(TEMPTY + acc), aph ^ 1)) {
+          atomicOr(status, kStatTimeout);
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+        for (int kb = 0; kb < kblocks; kb++, it++) {
+          const int s = it % STAGES;
+          const uint32_t ph = (it / STAGES) & 1;
+          if (!mbar_wait(bar(FULL + s), ph)) {
+            atomicOr(status, kStatTimeout);
+            *abort_flag = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+          for (int k = 0; k < BK / 16; k++)
+            mma_bf16(d_tmem, smem_desc(a_addr + k * 32), smem_desc(b_addr + k * 32), (kb | k) != 0);
+          mma_commit(bar(EMPTY + s));  // frees the stage once these MMAs retire
+        }
+        if (*abort_flag) break;
+        mma_commit(bar(TFULL + acc));  // accumulator ready for the epilogue
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5) ----------------
+    const int q = warp & 3;  // TMEM lane quarter this warp may access
+    int tc = 0;
+    for (int tile = blockIdx.x; tile < total; tile += gridDim.x, tc++) {
+      const int acc = tc & 1;
+      const uint32_t aph = (tc >> 1) & 1;
+      bool ok = mbar_wait(bar(TFULL + acc), aph);
+      if (!ok || *abort_flag) {
+        if (!ok) {
+          atomicOr(status, kStatTimeout);
+          *abort_flag = 1;
+        }
+        break;
+      }
+      tc_fence_after();
+      const int mt = tile / n_tiles, nt = tile - mt * n_tiles;
+      const int64_t row = (int64_t)mt * BM + q * 32 + lane;
+      const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+      for (int c = 0; c < BN / 32; c++) {
+        uint32_t r[32];
+        tmem_ld32(taddr + c * 32, r);
+        const int64_t col = (int64_t)nt * (BN / 2) + c * 16;  // complex column
+        if (row < m) {
+          float2* dst = C + row * ldc + col;
+#pragma unroll
+          for (int j = 0; j < 16; j++) {
+            if (col + j < n) {
+              float2 v = dst[j];
+              v.x -= __uint_as_float(r[2 * j]);
+              v.y -= __uint_as_float(r[2 * j + 1]);
+              dst[j] = v;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(bar(TEMPTY + acc));
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS) : "memory");
+  }
+}
+
+}  // namespace tc
+}  // namespace necb

@@ -270,6 +270,129 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs<R> A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Block-local pivoting (mixed-precision path).  The pivot of column k is the
+// largest entry among the rows of k's own 64-row diagonal block instead of
+// the whole column, so a panel needs no grid-wide reduction: one CTA factors
+// the diagonal block, a row-parallel kernel forms L21 = A21 U11^-1.  The
+// mixed path refines every solution against the FP64 matrix and falls back
+// to full partial pivoting if the refinement does not converge.
+
+// LU with partial pivoting inside the kb x kb diagonal block at (k0, k0).
+// 64 threads; thread t owns row t.  piv[k0 + c] receives the global row.
+template <typename T, int NB>
+__global__ void __launch_bounds__(NB) diag_lu_kernel(T* M, int64_t ld, int64_t k0, int kb, int* piv, int* status) {
+  using R = decltype(T{}.x);
+  __shared__ T D[NB][NB + 1];
+  __shared__ R rv[NB / 32];
+  __shared__ int ri[NB / 32];
+  __shared__ int s_p;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int r = 0; r < kb; r++)
+    if (t < kb) D[r][t] = M[(k0 + r) * ld + k0 + t];
+  __syncthreads();
+  for (int c = 0; c < kb; c++) {
+    R best = (R)-1;
+    int brow = 0x7fffffff;
+    if (t >= c && t < kb) {
+      T v = D[t][c];
+      best = v.x * v.x + v.y * v.y;
+      brow = t;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      R ov = __shfl_down_sync(0xffffffffu, best, off);
+      int orow = __shfl_down_sync(0xffffffffu, brow, off);
+      if (ov > best || (ov == best && orow < brow)) {
+        best = ov;
+        brow = orow;
+      }
+    }
+    if (lane == 0) {
+      rv[warp] = best;
+      ri[warp] = brow;
+    }
+    __syncthreads();
+    if (t == 0) {
+      for (int w = 1; w < NB / 32; w++)
+        if (rv[w] > best || (rv[w] == best && ri[w] < brow)) {
+          best = rv[w];
+          brow = ri[w];
+        }
+      if (!(best > (R)0)) {
+        atomicOr(status, best == (R)0 ? kLuStatSingular : kLuStatNonFinite);
+        brow = c;
+      }
+      s_p = brow;
+      piv[k0 + c] = (int)(k0 + brow);
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p != c && t < kb) {
+      T a = D[c][t];
+      D[c][t] = D[p][t];
+      D[p][t] = a;
+    }
+    __syncthreads();
+    if (t > c && t < kb) {
+      T l = cdiv(D[t][c], D[c][c]);
+      D[t][c] = l;
+      for (int q = c + 1; q < kb; q++) {
+        T u = D[c][q];
+        T a = D[t][q];
+        a.x -= l.x * u.x - l.y * u.y;
+        a.y -= l.x * u.y + l.y * u.x;
+        D[t][q] = a;
+      }
+    }
+    __syncthreads();
+  }
+  for (int r = 0; r < kb; r++)
+    if (t < kb) M[(k0 + r) * ld + k0 + t] = D[r][t];
+}
+
+// L21 = A21 U11^-1 for rows [k0+kb, n) of the panel columns: one thread per
+// row, U11 in shared memory, the row staged through shared memory.
+template <typename T, int NB>
+__global__ void __launch_bounds__(128) trsm_right_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int kb) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* U = reinterpret_cast<T*>(smem_raw);  // [NB][NB+1]
+  T* X = U + NB * (NB + 1);                // [128][NB+1]
+  const int t = threadIdx.x;
+  const int64_t r0 = k0 + kb + (int64_t)blockIdx.x * 128;
+  for (int idx = t; idx < kb * kb; idx += 128) {
+    const int r = idx / kb, c = idx - r * kb;
+    U[r * (NB + 1) + c] = M[(k0 + r) * ld + k0 + c];
+  }
+  // coalesced staging of 128 rows x kb
+  for (int idx = t; idx < 128 * kb; idx += 128) {
+    const int r = idx / kb, c = idx - r * kb;
+    T v;
+    v.x = 0;
+    v.y = 0;
+    if (r0 + r < n) v = M[(r0 + r) * ld + k0 + c];
+    X[r * (NB + 1) + c] = v;
+  }
+  __syncthreads();
+  T* x = X + t * (NB + 1);
+  for (int q = 0; q < kb; q++) {
+    T v = cdiv(x[q], U[q * (NB + 1) + q]);
+    x[q] = v;
+    for (int p = q + 1; p < kb; p++) {
+      T u = U[q * (NB + 1) + p];
+      T a = x[p];
+      a.x -= v.x * u.x - v.y * u.y;
+      a.y -= v.x * u.y + v.y * u.x;
+      x[p] = a;
+    }
+  }
+  __syncthreads();
+  for (int idx = t; idx < 128 * kb; idx += 128) {
+    const int r = idx / kb, c = idx - r * kb;
+    if (r0 + r < n) M[(r0 + r) * ld + k0 + c] = X[r * (NB + 1) + c];
+  }
+}
+
 // Row interchanges of one panel on the columns outside it.
 template <typename T>
 __global__ void laswp_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int kb, const int* piv) {

@@ -97,6 +97,157 @@ __global__ void __launch_bounds__(256) trsv_update_kernel(const T* M, int64_t ld
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent triangular sweep: one cooperative launch per triangle.
+//
+// Row block v (64 rows) is owned by CTA v % grid (blocks visited in order, so
+// every wait is on a block owned by a CTA that is already running and never
+// waits on a later block: no deadlock with all CTAs co-resident).  For block
+// v the CTA accumulates -sum_j M[rows][cols_j] x_j over every earlier block j
+// as soon as block j's solution is published (flag == epoch), keeping per-lane
+// partial sums (one warp-reduction per row at the end), then one warp solves
+// the 64 x 64 diagonal block with register shuffles and publishes x_v.
+// LOWER: unit lower L, blocks in ascending order; else upper U (non-unit),
+// blocks in descending order.  Reads every element of the triangle once.
+constexpr int kSweepThreads = 256;
+constexpr long long kSweepSpinLimit = 1LL << 26;
+
+template <typename T, bool LOWER>
+__global__ void __launch_bounds__(kSweepThreads) trsv_sweep_kernel(const T* M, int64_t ld, int64_t n,
+                                                                   const T* b, T* x, int* flags, int epoch,
+                                                                   int* status) {
+  using R = decltype(T{}.x);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*D)[kTrsvB + 1] = reinterpret_cast<T(*)[kTrsvB + 1]>(smem_raw);  // dynamic: trsv_diag_smem<T>()
+  __shared__ T xs[kTrsvB];
+  __shared__ T acc[kTrsvB];
+  __shared__ int s_abort;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (int)((n + kTrsvB - 1) / kTrsvB);
+  if (tid == 0) s_abort = 0;
+  for (int v = blockIdx.x; v < nblk; v += gridDim.x) {
+    const int blk = LOWER ? v : nblk - 1 - v;
+    const int64_t r0 = (int64_t)blk * kTrsvB;
+    const int bs = (int)min((int64_t)kTrsvB, n - r0);
+    // each warp owns rows warp, warp+8, ... of the block (8 rows)
+    R pr[8], pi[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      pr[q] = 0;
+      pi[q] = 0;
+    }
+    // the diagonal block does not depend on earlier solutions: stage it first
+    for (int idx = tid; idx < bs * bs; idx += kSweepThreads) {
+      const int r = idx / bs, q = idx - r * bs;
+      D[r][q] = M[(r0 + r) * ld + r0 + q];
+    }
+    for (int u = 0; u < v; u++) {  // earlier blocks in solve order
+      const int jb = LOWER ? u : nblk - 1 - u;
+      if (tid == 0) {
+        long long spins = 0;
+        while (*((volatile int*)(flags + jb)) != epoch) {
+          if (++spins > kSweepSpinLimit) {
+            atomicOr(status, 1 << 9);
+            s_abort = 1;
+            break;
+          }
+          __nanosleep(20);
+        }
+        __threadfence();
+      }
+      __syncthreads();
+      if (s_abort) return;
+      const int64_t c0 = (int64_t)jb * kTrsvB;
+      const int cs = (int)min((int64_t)kTrsvB, n - c0);
+      if (tid < cs) xs[tid] = __ldcg(x + c0 + tid);
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const int rr = warp + 8 * q;
+        if (rr < bs) {
+          const T* row = M + (r0 + rr) * ld + c0;
+          for (int c = lane; c < cs; c += 32) {
+            T a = row[c];
+            T xv = xs[c];
+            pr[q] += a.x * xv.x - a.y * xv.y;
+            pi[q] += a.x * xv.y + a.y * xv.x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // reduce partial sums, acc = b - sum
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      R sr = pr[q], si = pi[q];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        sr += __shfl_down_sync(0xffffffffu, sr, off);
+        si += __shfl_down_sync(0xffffffffu, si, off);
+      }
+      const int rr = warp + 8 * q;
+      if (lane == 0 && rr < bs) {
+        T bb = b[r0 + rr];
+        T o;
+        o.x = bb.x - sr;
+        o.y = bb.y - si;
+        acc[rr] = o;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // lane owns rows lane and lane+32; column sweep with shuffles
+      T v0 = lane < bs ? acc[lane] : T{};
+      T v1 = lane + 32 < bs ? acc[lane + 32] : T{};
+      if (LOWER) {
+        for (int q = 0; q < bs - 1; q++) {
+          T xq;
+          xq.x = __shfl_sync(0xffffffffu, q < 32 ? v0.x : v1.x, q & 31);
+          xq.y = __shfl_sync(0xffffffffu, q < 32 ? v0.y : v1.y, q & 31);
+          if (lane > q && lane < bs) {
+            T l = D[lane][q];
+            v0.x -= l.x * xq.x - l.y * xq.y;
+            v0.y -= l.x * xq.y + l.y * xq.x;
+          }
+          if (lane + 32 > q && lane + 32 < bs) {
+            T l = D[lane + 32][q];
+            v1.x -= l.x * xq.x - l.y * xq.y;
+            v1.y -= l.x * xq.y + l.y * xq.x;
+          }
+        }
+      } else {
+        for (int q = bs - 1; q >= 0; q--) {
+          // finalise x_q = v_q / U_qq on its owner, then broadcast
+          if (q < 32) {
+            if (lane == q) v0 = cdiv(v0, D[q][q]);
+          } else {
+            if (lane == q - 32) v1 = cdiv(v1, D[q][q]);
+          }
+          T xq;
+          xq.x = __shfl_sync(0xffffffffu, q < 32 ? v0.x : v1.x, q & 31);
+          xq.y = __shfl_sync(0xffffffffu, q < 32 ? v0.y : v1.y, q & 31);
+          if (lane < q) {
+            T u = D[lane][q];
+            v0.x -= u.x * xq.x - u.y * xq.y;
+            v0.y -= u.x * xq.y + u.y * xq.x;
+          }
+          if (lane + 32 < q) {
+            T u = D[lane + 32][q];
+            v1.x -= u.x * xq.x - u.y * xq.y;
+            v1.y -= u.x * xq.y + u.y * xq.x;
+          }
+        }
+      }
+      if (lane < bs) x[r0 + lane] = v0;
+      if (lane + 32 < bs) x[r0 + lane + 32] = v1;
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) atomicExch(flags + blk, epoch);
+    }
+    __syncthreads();
+  }
+}
+
 // y[i] = src[perm[i]] converted to the factor precision.
 template <typename TO, typename TI>
 __global__ void permute_kernel(const TI* src, const int* perm, TO* dst, int64_t n) {

@@ -15,6 +15,14 @@ class NecgpuStructure(C.Structure):
         ("eta", C.c_double)]
 
 
+class NecgpuStats(C.Structure):
+    _fields_ = [("refine_iters", C.c_int), ("refine_residual", C.c_double),
+                ("ms_fill", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
+                ("ms_pattern", C.c_double), ("launches", C.c_int64), ("h2d_bytes", C.c_int64),
+                ("d2h_bytes", C.c_int64), ("k_ms", C.c_double * 9), ("k_launches", C.c_int64 * 9),
+                ("k_flops", C.c_double * 9), ("pivoting", C.c_int)]
+
+
 class Engine:
     def __init__(self, lib, device=0):
         self.lib = lib
@@ -30,6 +38,8 @@ class Engine:
         L.necgpu_pattern.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp]
         L.necgpu_copy_z.argtypes = [C.c_void_p, _dp]
         L.necgpu_set_refinement.argtypes = [C.c_void_p, C.c_double, C.c_int]
+        L.necgpu_set_pivoting.argtypes = [C.c_void_p, C.c_int]
+        L.necgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(NecgpuStats)]
         self.h = C.c_void_p()
         rc = L.necgpu_create(C.byref(self.h), device)
         if rc != 0:
@@ -93,6 +103,14 @@ class Engine:
         self.check(self.lib.necgpu_pattern(self.h, nd, th.ctypes.data_as(_dp), ph.ctypes.data_as(_dp),
                                            eth.ctypes.data_as(_dp), eph.ctypes.data_as(_dp)))
         return eth[0::2] + 1j * eth[1::2], eph[0::2] + 1j * eph[1::2]
+
+    def set_pivoting(self, mode):
+        self.check(self.lib.necgpu_set_pivoting(self.h, mode))
+
+    def stats(self):
+        st = NecgpuStats()
+        self.check(self.lib.necgpu_get_stats(self.h, C.byref(st)))
+        return st
 
     def close(self):
         if self.h:

@@ -151,6 +151,30 @@ def test_solve_and_pattern_match_oracle(nb, oracle, engine, name, precision):
     nb.nec_delete(ctx)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("name", ["yagi_ground", "mesh_small", "helix2"])
+def test_mixed_pivoting_modes(nb, oracle, engine, name, mode):
+    """Mixed precision with partial pivoting (0) and block-local pivoting (1):
+    both refine to the FP64 floor and match the oracle's currents."""
+    ctx, st, rhs, _ = host_case(nb, CASES[name][0])
+    Zo, _ = oracle.fill(st)
+    x, _ = oracle.solve(Zo, rhs)
+    _, cur_o = oracle.coefficients(st, x)
+    engine.set_pivoting(mode)
+    try:
+        engine.set_structure(st)
+        engine.fill()
+        engine.factor(1)
+        cur_g, _ = engine.solve(rhs)
+        s = engine.stats()
+    finally:
+        engine.set_pivoting(1)
+    assert s.pivoting == mode
+    assert s.refine_residual <= 1e-12
+    assert np.max(np.abs(cur_g - cur_o)) / np.max(np.abs(cur_o)) <= 1e-9
+    nb.nec_delete(ctx)
+
+
 def test_fill_is_deterministic(nb, engine):
     ctx, st, _, _ = host_case(nb, CASES["helix2"][0])
     engine.set_structure(st)
