@@ -27,7 +27,7 @@ _LIBPATH = _os.path.join(_HERE, "libnecpp_b200.so")
 
 if not _os.path.exists(_LIBPATH):
     raise ImportError(
-        "libnecpp_b200.so is not built (run python -m necpp_b200.build or "
+        "libnecpp_b200.so is not built (run python necpp_b200/build.py or "
         "__graft_entry__.build()); there is no CPU fallback")
 
 lib = _C.CDLL(_LIBPATH)

@@ -1,7 +1,7 @@
 """GPU parity (the tests proper): the CUDA path, called through the C-ABI,
 against the reference's golden fixtures and the oracle on the same inputs.
 
-Tolerances: currents and Zin within 1e-9 relative on the
+Tolerances (the headline metric's accuracy bar): currents and Zin within 1e-9 relative on the
 plain FP64 path and 1e-6 on the mixed path; gain within 0.01 dB.  The FP64
 fill is checked element-wise against the oracle's to 1e-12 of max|Z|.
 """
