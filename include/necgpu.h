@@ -177,6 +177,41 @@ int necgpu_step_resident(necgpu_engine* e, int precision);
 /* Copy results of the last resident step (cur: n complex, eth/eph: n_dir complex). */
 int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph);
 
+/* Allocation-free solve.  No counterpart in the reference (its solves runs on
+ * host arrays the caller already owns); this is an addition for callers that
+ * must not allocate.
+ *
+ * The same solution as necgpu_solve on the held factors (FP64, or mixed with
+ * its FP64 refinement), but rhs_dev (n complex), cur_dev (n complex) and
+ * abc_dev (6*n doubles, or NULL) are device memory of the engine's device,
+ * and every scratch vector lives in one static device array of 1,574,144
+ * bytes per device, sized for n <= 16384 unknowns; larger n is rejected with
+ * NECGPU_ERR_ARG.  No call after the first allocates host or device memory
+ * on success (a failure stores its message in the engine).  Who needs it: a
+ * caller that reserved the device's memory up front for its own pool (a
+ * frequency sweep or an optimiser holding thousands of matrices, a PyTorch
+ * process whose caching allocator owns the HBM) and calls the solver inside
+ * its inner loop, where a cudaMalloc can fail or fragment that pool and a
+ * cudaFree waits for the whole device, stalling the caller's other streams.
+ *
+ * The first call on a device does the set-up, with that device current:
+ * it looks up the static array, zeroes the sweep flag words (they must start
+ * at zero; nothing else in the array needs to), and sets the kernels'
+ * attributes.  Make that first call before any stream capture.  The work
+ * runs on the engine's stream; the call returns when it has finished
+ * (mixed refinement also waits once per refinement step).  The engine's own
+ * solution (for necgpu_pattern) is left as it was.
+ *
+ * All engines on one device share the one array: calls that overlap in time
+ * on the same device (from two threads, or two engines on different
+ * streams) race on it and give wrong results.  Serialise them.
+ *
+ * If the mixed refinement stalls on block-pivoted factors, the call fails
+ * with NECGPU_ERR_REFINE instead of refactoring (which would allocate);
+ * necgpu_solve refactors with partial pivoting, after which this call
+ * converges. */
+int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_dev, double* abc_dev);
+
 /* Diagnostic: apply one complex64 update C -= A B (m x n, inner kb) to a
  * seeded random matrix with the tensor-core kernel and with the CUDA-core
  * FP32 kernel; report max |difference| and max |reference| over C. */

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <type_traits>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1239,6 +1240,224 @@ int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph
   if (eph && e->res_ndir > 0)
     CUDA_TRY(cudaMemcpyAsync(eph, e->d_eph, e->res_ndir * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return NECGPU_OK;
+}
+
+}  // extern "C"
+
+// ---------------- allocation-free solve ----------------
+// necgpu_solve_noalloc: the solve of necgpu_solve on the held factors, with
+// the right-hand side and the results in caller-owned device memory and every
+// scratch vector in one static device array, so that no call after the first
+// allocates host or device memory.
+namespace {
+
+// Largest system the static scratch holds, and its layout (byte offsets):
+// x and r (complex128), two complex64 work vectors, the 6n coefficient
+// doubles used when the caller passes none, the residual norms and status
+// words, and one flag word per 64-row block of the triangular sweeps.
+constexpr int64_t kNoAllocMaxN = 16384;
+static_assert(kNoAllocMaxN % kTrsvB == 0, "flag words per sweep block");
+constexpr size_t kNoAllocOffX = 0;
+constexpr size_t kNoAllocOffR = kNoAllocOffX + 16 * kNoAllocMaxN;
+constexpr size_t kNoAllocOffW1 = kNoAllocOffR + 16 * kNoAllocMaxN;
+constexpr size_t kNoAllocOffW2 = kNoAllocOffW1 + 8 * kNoAllocMaxN;
+constexpr size_t kNoAllocOffAbc = kNoAllocOffW2 + 8 * kNoAllocMaxN;
+constexpr size_t kNoAllocOffMisc = kNoAllocOffAbc + 48 * kNoAllocMaxN;  // rn2: 2 doubles, status: 4 ints
+constexpr size_t kNoAllocOffFlags = kNoAllocOffMisc + 256;
+constexpr size_t kNoAllocFlagBytes = sizeof(int) * (kNoAllocMaxN / kTrsvB);
+constexpr size_t kNoAllocBytes = kNoAllocOffFlags + kNoAllocFlagBytes;  // 1,574,144 bytes
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+  unsigned char* base = nullptr;  // device address of g_noalloc_scratch on this device
+  int sweep_per_sm[2] = {0, 0};   // resident sweep CTAs per SM: [0] complex64, [1] complex128
+  int epoch = 0;                  // last flag epoch of the sweeps on this device
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+// Once per device, with that device current: look up the scratch array,
+// zero its flag words (a sweep waits for a flag equal to its epoch, and the
+// first epoch is 1), set the sweep kernels' shared-memory limits and size
+// their cooperative grids.
+int noalloc_setup(necgpu_engine* e, NoAllocDevice** out) {
+  if (e->device < 0 || e->device >= kNoAllocMaxDevices)
+    return fail(e, NECGPU_ERR_ARG, "solve_noalloc: device index beyond the per-device table");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoAllocDevice& d = g_noalloc_dev[e->device];
+  if (!d.base) {
+    void* p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    if (reinterpret_cast<uintptr_t>(p) & 255)
+      return fail(e, NECGPU_ERR_CUDA, "solve_noalloc: static scratch is not 256-byte aligned");
+    constexpr size_t dsm32 = trsv_diag_smem<float2>(), dsm64 = trsv_diag_smem<double2>();
+    CUDA_TRY(cudaFuncSetAttribute(trsv_sweep_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dsm32));
+    CUDA_TRY(cudaFuncSetAttribute(trsv_sweep_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dsm32));
+    CUDA_TRY(cudaFuncSetAttribute(trsv_sweep_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dsm64));
+    CUDA_TRY(cudaFuncSetAttribute(trsv_sweep_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)dsm64));
+    int per_sm[2] = {0, 0};
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], trsv_sweep_kernel<float2, true>,
+                                                           kSweepThreads, dsm32));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], trsv_sweep_kernel<double2, true>,
+                                                           kSweepThreads, dsm64));
+    if (per_sm[0] < 1 || per_sm[1] < 1) return fail(e, NECGPU_ERR_CUDA, "solve_noalloc: sweep kernel cannot be resident");
+    unsigned char* base = static_cast<unsigned char*>(p);
+    CUDA_TRY(cudaMemsetAsync(base + kNoAllocOffFlags, 0, kNoAllocFlagBytes, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    d.sweep_per_sm[0] = per_sm[0];
+    d.sweep_per_sm[1] = per_sm[1];
+    d.epoch = 0;
+    d.base = base;
+  }
+  *out = &d;
+  return 0;
+}
+
+// Forward and backward sweeps over the held factors M (the kernels of the
+// engine's own solves) with the flag words in the static scratch.  rhs is
+// consumed; the solution lands in sol.
+template <typename T>
+int noalloc_sweeps(necgpu_engine* e, NoAllocDevice& d, const T* M, T* rhs, T* sol, int* flags, int* status) {
+  const int64_t n = e->n, ld = e->ld;
+  const int nblk = (int)((n + kTrsvB - 1) / kTrsvB);
+  constexpr bool f64 = std::is_same<T, double2>::value;
+  constexpr size_t dsm = trsv_diag_smem<T>();
+  const int grid = std::max(1, std::min(nblk, d.sweep_per_sm[f64 ? 1 : 0] * e->nsm));
+  if (d.epoch > (1 << 30)) {  // restart the epochs long before the counter wraps
+    CUDA_TRY(cudaMemsetAsync(flags, 0, kNoAllocFlagBytes, e->stream));
+    d.epoch = 0;
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    int epoch = ++d.epoch;
+    const T* src = pass == 0 ? rhs : sol;
+    T* dst = pass == 0 ? sol : rhs;
+    void* args[] = {(void*)&M, (void*)&ld, (void*)&n, (void*)&src, (void*)&dst, (void*)&flags, (void*)&epoch,
+                    (void*)&status};
+    CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)trsv_sweep_kernel<T, true>
+                                                   : (const void*)trsv_sweep_kernel<T, false>,
+                                         dim3(grid), dim3(kSweepThreads), args, dsm, e->stream));
+    LAUNCHED();
+  }
+  CUDA_TRY(cudaMemcpyAsync(sol, rhs, n * sizeof(T), cudaMemcpyDeviceToDevice, e->stream));
+  return 0;
+}
+
+int noalloc_device_buffer(necgpu_engine* e, const void* p, size_t bytes, size_t align, const char* what) {
+  if (reinterpret_cast<uintptr_t>(p) % align)
+    return fail(e, NECGPU_ERR_ARG, std::string("solve_noalloc: ") + what + " is not aligned");
+  cudaPointerAttributes at;
+  CUDA_TRY(cudaPointerGetAttributes(&at, p));
+  if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != e->device)
+    return fail(e, NECGPU_ERR_ARG, std::string("solve_noalloc: ") + what + " is not device memory of the engine's device");
+  (void)bytes;
+  return 0;
+}
+
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(a), b0 = reinterpret_cast<uintptr_t>(b);
+  return a0 < b0 + nb && b0 < a0 + na;
+}
+
+}  // namespace
+
+extern "C" {
+
+int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_dev, double* abc_dev) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (!rhs_dev || !cur_dev) return fail(e, NECGPU_ERR_ARG, "solve_noalloc: null argument");
+  const int64_t n = e->n;
+  if (n > kNoAllocMaxN)
+    return fail(e, NECGPU_ERR_ARG,
+                "solve_noalloc: n = " + std::to_string(n) + " exceeds the static scratch limit of " +
+                    std::to_string(kNoAllocMaxN) + " unknowns; use necgpu_solve");
+  if (e->factored != NECGPU_FP64 && e->factored != NECGPU_MIXED)
+    return fail(e, NECGPU_ERR_ARG, "solve_noalloc: no factorisation held");
+  CUDA_TRY(cudaSetDevice(e->device));
+  const size_t vec = (size_t)n * sizeof(double2);
+  TRY(noalloc_device_buffer(e, rhs_dev, vec, 16, "rhs"));
+  TRY(noalloc_device_buffer(e, cur_dev, vec, 16, "cur"));
+  if (abc_dev) TRY(noalloc_device_buffer(e, abc_dev, 6 * (size_t)n * sizeof(double), 8, "abc"));
+  if (overlaps(rhs_dev, vec, cur_dev, vec) || (abc_dev && (overlaps(abc_dev, 48 * (size_t)n, rhs_dev, vec) ||
+                                                           overlaps(abc_dev, 48 * (size_t)n, cur_dev, vec))))
+    return fail(e, NECGPU_ERR_ARG, "solve_noalloc: rhs, cur and abc must not overlap");
+  NoAllocDevice* d = nullptr;
+  TRY(noalloc_setup(e, &d));
+  unsigned char* base = d->base;
+  double2* x = reinterpret_cast<double2*>(base + kNoAllocOffX);
+  double2* r = reinterpret_cast<double2*>(base + kNoAllocOffR);
+  float2* w1 = reinterpret_cast<float2*>(base + kNoAllocOffW1);
+  float2* w2 = reinterpret_cast<float2*>(base + kNoAllocOffW2);
+  double* abc = abc_dev ? abc_dev : reinterpret_cast<double*>(base + kNoAllocOffAbc);
+  double* rn2 = reinterpret_cast<double*>(base + kNoAllocOffMisc);
+  int* status = reinterpret_cast<int*>(base + kNoAllocOffMisc + 2 * sizeof(double));
+  int* flags = reinterpret_cast<int*>(base + kNoAllocOffFlags);
+  const double2* b = reinterpret_cast<const double2*>(rhs_dev);
+  const unsigned g1 = (unsigned)((n + 255) / 256);
+  CUDA_TRY(cudaMemsetAsync(status, 0, 4 * sizeof(int), e->stream));
+  int iters = 0;
+  double rel = 0.0;
+  if (e->factored == NECGPU_FP64) {
+    permute_kernel<double2, double2><<<g1, 256, 0, e->stream>>>(b, e->d_perm, r, n);
+    LAUNCHED();
+    TRY(noalloc_sweeps<double2>(e, *d, e->Z64, r, x, flags, status));
+  } else {
+    // the refinement of the engine's mixed solve, on the static vectors
+    CUDA_TRY(cudaMemsetAsync(x, 0, vec, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(r, b, vec, cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemsetAsync(rn2, 0, 2 * sizeof(double), e->stream));
+    norm2_kernel<<<g1, 256, 0, e->stream>>>(b, n, rn2 + 1);
+    LAUNCHED();
+    const unsigned gr = (unsigned)std::min<int64_t>((n + 7) / 8, 8 * e->nsm);
+    double prev = 1e300;
+    rel = 1.0;
+    for (; iters <= e->refine_max; iters++) {
+      permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(r, e->d_perm, w1, n);
+      LAUNCHED();
+      TRY(noalloc_sweeps<float2>(e, *d, e->Z32, w1, w2, flags, status));
+      axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(x, w2, n);
+      LAUNCHED();
+      CUDA_TRY(cudaMemsetAsync(rn2, 0, sizeof(double), e->stream));
+      residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, x, b, r, rn2);
+      LAUNCHED();
+      struct {
+        double rn2[2];
+        int status[4];
+      } h{};  // the norms and the status words are adjacent in the scratch
+      static_assert(sizeof(h) == 2 * sizeof(double) + 4 * sizeof(int), "misc block layout");
+      CUDA_TRY(cudaMemcpyAsync(&h, rn2, sizeof(h), cudaMemcpyDeviceToHost, e->stream));
+      CUDA_TRY(cudaStreamSynchronize(e->stream));
+      if (h.status[0]) return fail(e, NECGPU_ERR_CUDA, "solve_noalloc: triangular sweep gave up waiting on a block");
+      const double bn = std::sqrt(h.rn2[1]);
+      rel = bn > 0 ? std::sqrt(h.rn2[0]) / bn : 0.0;
+      if (!std::isfinite(rel)) return fail(e, NECGPU_ERR_NONFINITE, "solve_noalloc: non-finite residual");
+      if (rel <= e->refine_tol || rel > 0.5 * prev) {
+        iters++;
+        break;
+      }
+      prev = rel;
+    }
+    if (e->blockpiv && rel > kRefineFallback)
+      return fail(e, NECGPU_ERR_REFINE,
+                  "solve_noalloc: refinement stalled on the block-pivoted factors; necgpu_solve refactors "
+                  "with partial pivoting, after which this call converges");
+    if (rel > 1e-6) return fail(e, NECGPU_ERR_REFINE, "solve_noalloc: refinement did not converge");
+  }
+  coeff_kernel<<<g1, 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc,
+                                          e->d_ccoef + 2 * e->nc, x, abc, reinterpret_cast<double2*>(cur_dev));
+  LAUNCHED();
+  int st[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (st[0]) return fail(e, NECGPU_ERR_CUDA, "solve_noalloc: triangular sweep gave up waiting on a block");
+  e->stats.refine_iters = iters;
+  e->stats.refine_residual = rel;
   return NECGPU_OK;
 }
 
