@@ -379,11 +379,25 @@ int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, i
           tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, e->d_Ap));
   dim3 g((unsigned)((n + 31) / 32), (unsigned)(kbp / 64));
   KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, e->d_Bp));
+  // C as m rows x 2n FP32 (re, im interleaved), 32 x 32 boxes for the
+  // reduce-add epilogue; TMA clips the boxes at the edges of C
+  CUtensorMap tmC;
+  {
+    cuuint64_t dims[2] = {(cuuint64_t)(2 * n), (cuuint64_t)m};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float2)};
+    cuuint32_t box[2] = {32, 32};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_tiled()(&tmC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)C, dims, strides, box, estr,
+                                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled (C) failed: " + std::to_string((int)r));
+  }
   const int m_tiles = (int)((m + tc::BM - 1) / tc::BM);
   const int n_tiles = (int)((2 * n + tc::BN - 1) / tc::BN);
   const int grid = std::max(1, std::min(m_tiles * n_tiles, e->nsm));
   KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)m * n * kb,
-          tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, e->stream>>>(e->tmA, e->tmB, C, ld, (int)m, (int)n,
+          tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, e->stream>>>(e->tmA, e->tmB, tmC, (int)m, (int)n,
                                                                               kdim, e->d_status));
   return 0;
 }
@@ -938,7 +952,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   if (n != e->n) free_all(e);
   e->n = n;
-  e->ld = n;
+  e->ld = (n + 63) / 64 * 64;  // 512 B-aligned FP32 rows: TMA bases of every 64-block sub-matrix
   e->ground = s->ground;
   e->use_exk = s->use_exk;
   e->P.rkh = s->rkh;
@@ -1144,7 +1158,8 @@ int necgpu_copy_z(necgpu_engine* e, double* out) {
   if (!e || !out) return NECGPU_ERR_ARG;
   if (!e->filled || !e->Z64) return fail(e, NECGPU_ERR_ARG, "copy_z: no unfactored matrix held");
   CUDA_TRY(cudaSetDevice(e->device));
-  CUDA_TRY(cudaMemcpyAsync(out, e->Z64, (size_t)e->n * e->ld * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaMemcpy2DAsync(out, (size_t)e->n * sizeof(double2), e->Z64, (size_t)e->ld * sizeof(double2),
+                               (size_t)e->n * sizeof(double2), (size_t)e->n, cudaMemcpyDeviceToHost, e->stream));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   return NECGPU_OK;
 }
@@ -1193,7 +1208,10 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
                          double* max_abs_ref) {
   if (!e || m < 1 || n < 1 || kb < 1 || kb > 1024 || !max_abs_diff || !max_abs_ref) return NECGPU_ERR_ARG;
   CUDA_TRY(cudaSetDevice(e->device));
-  const int64_t rows = (int64_t)kb + m, cols = (int64_t)kb + n, ld = cols;
+  // operands at a 64-aligned offset o: A = X[o.., 0..kb), B = X[0..kb, o..),
+  // C = X[o.., o..); rows of ld (a multiple of 64) keep C 16-byte aligned
+  const int64_t o = ((int64_t)kb + 63) / 64 * 64;
+  const int64_t rows = o + m, ld = (o + n + 63) / 64 * 64;
   float2 *X = nullptr, *Y = nullptr;
   float* d = nullptr;
   TRY(dalloc(e, X, (size_t)rows * ld));
@@ -1206,12 +1224,11 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
     cudaMemsetAsync(d, 0, 2 * sizeof(float), e->stream);
     cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream);
     // X: tensor cores; Y: CUDA-core FP32 reference of the same update
-    rc = tc_gemm_sub(e, X + (int64_t)kb * ld, X + kb, X + (int64_t)kb * ld + kb, ld, m, n, kb);
+    rc = tc_gemm_sub(e, X + o * ld, X + o, X + o * ld + o, ld, m, n, kb);
     if (!rc) {
       dim3 g((unsigned)((n + 63) / 64), (unsigned)((m + 63) / 64));
-      gemm_sub_kernel<float><<<g, 256, 0, e->stream>>>(Y + (int64_t)kb * ld, ld, Y + kb, ld, Y + (int64_t)kb * ld + kb,
-                                                       ld, m, n, kb);
-      max_diff_kernel<<<256, 256, 0, e->stream>>>(X + (int64_t)kb * ld + kb, Y + (int64_t)kb * ld + kb, ld, m, n, d);
+      gemm_sub_kernel<float><<<g, 256, 0, e->stream>>>(Y + o * ld, ld, Y + o, ld, Y + o * ld + o, ld, m, n, kb);
+      max_diff_kernel<<<256, 256, 0, e->stream>>>(X + o * ld + o, Y + o * ld + o, ld, m, n, d);
       float h[2] = {0, 0};
       int st = 0;
       cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, e->stream);

@@ -17,8 +17,12 @@
 //           into a 4-stage shared-memory ring (48 KB per stage);
 //   warp 1  MMA issuer: tcgen05.mma.cta_group::1.kind::f16, M=128 N=256 K=16,
 //           accumulating in one of two 128 x 256 FP32 TMEM buffers;
-//   warps 2-5 epilogue: tcgen05.ld of the finished buffer, C -= D in place,
-//           while the MMA warp fills the other buffer.
+//   warps 2-5 epilogue: tcgen05.ld of the finished buffer (32 rows x 32
+//           columns per load), negated into a 128B-swizzled 4 KB staging
+//           tile in shared memory (two per warp), and added to C by a TMA
+//           bulk tensor reduction (cp.reduce.async.bulk.tensor .add.f32):
+//           the read-modify-write of C happens in L2, fully coalesced, while
+//           the MMA warp fills the other accumulator.
 // Every wait on an mbarrier is bounded; on timeout the kernel records an
 // error bit and winds down (outstanding TMA copies are waited for, TMEM is
 // freed).  TMA loads never use cluster multicast.
@@ -37,7 +41,11 @@ constexpr int A_BYTES = BM * BK * 2;            // 16 KB
 constexpr int B_BYTES = BN * BK * 2;            // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 48 KB
 constexpr int THREADS = 192;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+constexpr int EPI_WARPS = 4;
+constexpr int EPI_TILE_BYTES = 32 * 32 * 4;  // 32 rows x 128 B
+constexpr int EPI_BYTES = EPI_WARPS * 2 * EPI_TILE_BYTES;  // 32 KB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+static_assert(SMEM_BYTES <= 232448, "dynamic shared memory per CTA");
 constexpr uint32_t TMEM_COLS = 512;  // two 256-column FP32 accumulators
 constexpr long long kWaitLimit = 1LL << 20;
 
@@ -79,6 +87,18 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       "l"(map), "r"(c0), "r"(c1), "r"(bar)
       : "memory");
 }
+// C[box at (x, y)] += smem tile, reduced in L2 (no multicast; C is local)
+__device__ __forceinline__ void tma_reduce_add_2d(const CUtensorMap* map, int c0, int c1, uint32_t src) {
+  asm volatile("cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map),
+               "r"(c0), "r"(c1), "r"(src)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// at most one committed group still reading its shared-memory source
+__device__ __forceinline__ void bulk_wait_read1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -185,13 +205,15 @@ __global__ void __launch_bounds__(256) pack_b_kernel(const float2* B, int64_t ld
 }
 
 // ---- the GEMM -----------------------------------------------------------
-// C (m x n complex, row-major ldc) -= D, D = A' B'^T, K' = kdim (multiple of 64)
+// C (m x n complex, row-major; tmC views it as m rows x 2n FP32 with 32 x 32
+// boxes, 128B swizzle) -= D, D = A' B'^T, K' = kdim (multiple of 64)
 __global__ void __launch_bounds__(THREADS, 1)
-    gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, float2* C,
-                   int64_t ldc, int m, int n, int kdim, int* status) {
+    gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const __grid_constant__ CUtensorMap tmC, int m, int n, int kdim, int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint8_t* epi = smem + STAGES * STAGE_BYTES;  // 1 KB aligned (the swizzle atom)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(epi + EPI_BYTES);
   // bars: full[STAGES], empty[STAGES], tfull[2], tempty[2]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -218,6 +240,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmA) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(&tmB) : "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"(&tmC) : "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -295,7 +318,11 @@ __global__ void __launch_bounds__(THREADS, 1)
   } else {
     // ---------------- epilogue (warps 2..5) ----------------
     const int q = warp & 3;  // TMEM lane quarter this warp may access
-    int tc = 0;
+    uint8_t* stage0 = epi + (warp - 2) * 2 * EPI_TILE_BYTES;
+    // this lane's row in a staging tile; 16-byte chunk j sits at j ^ (row % 8)
+    const uint32_t row_off = (uint32_t)lane * 128;
+    const uint32_t swz = (uint32_t)(lane & 7);
+    int tc = 0, issued = 0;
     for (int tile = blockIdx.x; tile < total; tile += gridDim.x, tc++) {
       const int acc = tc & 1;
       const uint32_t aph = (tc >> 1) & 1;
@@ -309,29 +336,40 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       tc_fence_after();
       const int mt = tile / n_tiles, nt = tile - mt * n_tiles;
-      const int64_t row = (int64_t)mt * BM + q * 32 + lane;
+      const int y = mt * BM + q * 32;  // first C row of this warp's quarter
       const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1
       for (int c = 0; c < BN / 32; c++) {
         uint32_t r[32];
         tmem_ld32(taddr + c * 32, r);
-        const int64_t col = (int64_t)nt * (BN / 2) + c * 16;  // complex column
-        if (row < m) {
-          float2* dst = C + row * ldc + col;
-#pragma unroll
-          for (int j = 0; j < 16; j++) {
-            if (col + j < n) {
-              float2 v = dst[j];
-              v.x -= __uint_as_float(r[2 * j]);
-              v.y -= __uint_as_float(r[2 * j + 1]);
-              dst[j] = v;
-            }
-          }
+        if (c == BN / 32 - 1) {
+          // the accumulator is in registers: hand TMEM back to the MMA warp
+          tc_fence_before();
+          mbar_arrive(bar(TEMPTY + acc));
         }
+        const int x = nt * BN + c * 32;  // first FP32 column of the box
+        if (y >= m || x >= 2 * n) continue;  // box entirely outside C
+        uint8_t* st = stage0 + (issued & 1) * EPI_TILE_BYTES;
+        if (lane == 0) bulk_wait_read1();  // the reduction that used st two boxes ago has read it
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          float4 v = make_float4(-__uint_as_float(r[4 * j]), -__uint_as_float(r[4 * j + 1]),
+                                 -__uint_as_float(r[4 * j + 2]), -__uint_as_float(r[4 * j + 3]));
+          *reinterpret_cast<float4*>(st + row_off + (((uint32_t)j ^ swz) << 4)) = v;
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          tma_reduce_add_2d(&tmC, x, y, smem_u32(st));
+          bulk_commit();
+        }
+        issued++;
       }
-      tc_fence_before();
-      mbar_arrive(bar(TEMPTY + acc));
     }
+    // every reduction must be complete (not only read) before the CTA exits
+    if (lane == 0) bulk_wait_all();
+    __syncwarp();
   }
   tc_fence_before();
   __syncthreads();

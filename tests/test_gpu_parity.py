@@ -175,6 +175,24 @@ def test_mixed_pivoting_modes(nb, oracle, engine, name, mode):
     nb.nec_delete(ctx)
 
 
+@pytest.mark.parametrize("m,n,kb", [(300, 200, 64), (1000, 517, 64), (129, 1, 13), (2500, 2500, 64),
+                                    (777, 1500, 256), (64, 4000, 64)])
+def test_tensor_core_update_matches_fp32(nb, engine, m, n, kb):
+    """The tcgen05 split-BF16x3 trailing update C -= A B against the CUDA-core
+    FP32 update of the same seeded operands, including ragged edges (m, n
+    not multiples of the 128 x 128-complex tile)."""
+    import ctypes as C
+    L = nb.lib
+    L.necgpu_check_tc_gemm.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    diff, ref = C.c_double(), C.c_double()
+    rc = L.necgpu_check_tc_gemm(engine.h, m, n, kb, 1234, C.byref(diff), C.byref(ref))
+    assert rc == 0, engine.err()
+    assert ref.value > 0.1
+    # dropped lo*lo products and BF16 rounding: ~2^-16 |a||b| per product
+    assert diff.value <= 2e-4 * math.sqrt(kb), (diff.value, ref.value)
+
+
 def test_fill_is_deterministic(nb, engine):
     ctx, st, _, _ = host_case(nb, CASES["helix2"][0])
     engine.set_structure(st)
