@@ -101,6 +101,7 @@ struct necgpu_engine {
   int64_t tc_rows = 0;
   int tc_kdim = 0;
   CUtensorMap tmA{}, tmB{};
+  float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
   // mixed path: block-local pivoting first, full partial pivoting as fallback
   bool prefer_blockpiv = true;
   bool blockpiv = false;
@@ -236,6 +237,7 @@ void free_all(necgpu_engine* e) {
   dfree(e->d_cbasis);
   dfree(e->d_ccoef);
   dfree(e->Z64);
+  dfree(e->d_dinv);
   dfree(e->Z32);
   dfree(e->d_piv);
   dfree(e->d_perm);
@@ -534,38 +536,42 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
   return 0;
 }
 
-// FP32 LU with block-local pivoting (mixed path): no grid-wide reductions;
-// the panel is one CTA on the diagonal block plus row-parallel kernels.
+// FP32 LU with block-local pivoting (mixed path): per 64-column panel, one
+// CTA factors the diagonal block, the exchanges are a per-column gather
+// inside the block, L21 and U12 are row/column-parallel triangular solves,
+// and the trailing update runs on the tensor cores.
 int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   using T = float2;
   const int64_t n = e->n, ld = e->ld;
+  const int64_t nblk = (n + kBlk - 1) / kBlk;
   if (!e->d_piv) TRY(dalloc(e, e->d_piv, (size_t)n));
-  const size_t trsm_smem = (size_t)(kNB * kNB + kNB * 32) * sizeof(T);
-  CUDA_TRY(cudaFuncSetAttribute(trsm_kernel<T, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
-  const size_t right_smem = (size_t)(kNB + 128) * (kNB + 1) * sizeof(T);
-  CUDA_TRY(cudaFuncSetAttribute(trsm_right_kernel<T, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)right_smem));
-  for (int64_t k0 = 0; k0 < n; k0 += kNB) {
-    const int kb = (int)std::min<int64_t>(kNB, n - k0);
-    KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * kb / 3.0,
-            diag_lu_kernel<T, kNB><<<1, kNB, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_status));
+  if (!e->d_dinv) TRY(dalloc(e, e->d_dinv, (size_t)nblk * kBlk));
+  CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm_panel_smem<T>()));
+  CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm_panel_smem<T>()));
+  for (int64_t k0 = 0; k0 < n; k0 += kBlk) {
+    const int kb = (int)std::min<int64_t>(kBlk, n - k0);
+    T* dinv = e->d_dinv + k0;
+    KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
+            diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, dinv, e->d_status));
     if (n > kb)
       KLAUNCH(NECGPU_K_LASWP, 0.0,
-              laswp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
-    const int64_t rest = n - k0 - kb;
+              laswp_block_kernel<T><<<(unsigned)((n + 31) / 32), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
+    const int64_t r0 = k0 + kb, rest = n - r0;
     if (rest > 0) {
+      const unsigned g = (unsigned)((rest + kTrsmW - 1) / kTrsmW);
       KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * rest,
-              trsm_right_kernel<T, kNB><<<(unsigned)((rest + 127) / 128), 128, right_smem, e->stream>>>(M, ld, n, k0,
-                                                                                                         kb));
+              trsm_panel_kernel<T, false><<<g, kTrsmW, trsm_panel_smem<T>(), e->stream>>>(M, ld, n, k0, r0, dinv));
       KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * rest,
-              trsm_kernel<T, kNB><<<(unsigned)((rest + 31) / 32), 256, trsm_smem, e->stream>>>(M, ld, n, k0, kb));
+              trsm_panel_kernel<T, true><<<g, kTrsmW, trsm_panel_smem<T>(), e->stream>>>(M, ld, n, k0, r0, dinv));
       if (e->use_tc) {
         TRY(tc_update(e, M, k0, kb));
       } else {
-        dim3 g((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
+        dim3 gg((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
         KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
-                gemm_sub_kernel<float><<<g, 256, 0, e->stream>>>(M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb,
-                                                                 ld, M + (k0 + kb) * ld + k0 + kb, ld, rest, rest, kb));
+                gemm_sub_kernel<float><<<gg, 256, 0, e->stream>>>(M + r0 * ld + k0, ld, M + k0 * ld + r0, ld,
+                                                                  M + r0 * ld + r0, ld, rest, rest, kb));
       }
     }
   }

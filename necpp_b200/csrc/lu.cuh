@@ -274,122 +274,378 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs<R> A) {
 // Block-local pivoting (mixed-precision path).  The pivot of column k is the
 // largest entry among the rows of k's own 64-row diagonal block instead of
 // the whole column, so a panel needs no grid-wide reduction: one CTA factors
-// the diagonal block, a row-parallel kernel forms L21 = A21 U11^-1.  The
-// mixed path refines every solution against the FP64 matrix and falls back
-// to full partial pivoting if the refinement does not converge.
+// the diagonal block, then
+//   L21 = A21 U11^-1   trsm_panel_kernel<RIGHT>, one row of A21 per thread
+//   U12 = L11^-1 A12   trsm_panel_kernel<LEFT>,  one column of A12 per thread
+// The mixed path refines every solution against the FP64 matrix and falls
+// back to full partial pivoting if the refinement does not converge.
 
-// LU with partial pivoting inside the kb x kb diagonal block at (k0, k0).
-// 64 threads; thread t owns row t.  piv[k0 + c] receives the global row.
-template <typename T, int NB>
-__global__ void __launch_bounds__(NB) diag_lu_kernel(T* M, int64_t ld, int64_t k0, int kb, int* piv, int* status) {
-  using R = decltype(T{}.x);
-  __shared__ T D[NB][NB + 1];
-  __shared__ R rv[NB / 32];
-  __shared__ int ri[NB / 32];
-  __shared__ int s_p;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  for (int r = 0; r < kb; r++)
-    if (t < kb) D[r][t] = M[(k0 + r) * ld + k0 + t];
-  __syncthreads();
-  for (int c = 0; c < kb; c++) {
-    R best = (R)-1;
-    int brow = 0x7fffffff;
-    if (t >= c && t < kb) {
-      T v = D[t][c];
-      best = v.x * v.x + v.y * v.y;
-      brow = t;
-    }
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      R ov = __shfl_down_sync(0xffffffffu, best, off);
-      int orow = __shfl_down_sync(0xffffffffu, brow, off);
-      if (ov > best || (ov == best && orow < brow)) {
-        best = ov;
-        brow = orow;
-      }
-    }
-    if (lane == 0) {
-      rv[warp] = best;
-      ri[warp] = brow;
-    }
-    __syncthreads();
-    if (t == 0) {
-      for (int w = 1; w < NB / 32; w++)
-        if (rv[w] > best || (rv[w] == best && ri[w] < brow)) {
-          best = rv[w];
-          brow = ri[w];
-        }
-      if (!(best > (R)0)) {
-        atomicOr(status, best == (R)0 ? kLuStatSingular : kLuStatNonFinite);
-        brow = c;
-      }
-      s_p = brow;
-      piv[k0 + c] = (int)(k0 + brow);
-    }
-    __syncthreads();
-    const int p = s_p;
-    if (p != c && t < kb) {
-      T a = D[c][t];
-      D[c][t] = D[p][t];
-      D[p][t] = a;
-    }
-    __syncthreads();
-    if (t > c && t < kb) {
-      T l = cdiv(D[t][c], D[c][c]);
-      D[t][c] = l;
-      for (int q = c + 1; q < kb; q++) {
-        T u = D[c][q];
-        T a = D[t][q];
-        a.x -= l.x * u.x - l.y * u.y;
-        a.y -= l.x * u.y + l.y * u.x;
-        D[t][q] = a;
-      }
-    }
-    __syncthreads();
-  }
-  for (int r = 0; r < kb; r++)
-    if (t < kb) M[(k0 + r) * ld + k0 + t] = D[r][t];
+constexpr int kBlk = 64;  // diagonal block edge
+constexpr int kDiagThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ T czero() {
+  T z;
+  z.x = 0;
+  z.y = 0;
+  return z;
 }
 
-// L21 = A21 U11^-1 for rows [k0+kb, n) of the panel columns: one thread per
-// row, U11 in shared memory, the row staged through shared memory.
-template <typename T, int NB>
-__global__ void __launch_bounds__(128) trsm_right_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int kb) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* U = reinterpret_cast<T*>(smem_raw);  // [NB][NB+1]
-  T* X = U + NB * (NB + 1);                // [128][NB+1]
-  const int t = threadIdx.x;
-  const int64_t r0 = k0 + kb + (int64_t)blockIdx.x * 128;
-  for (int idx = t; idx < kb * kb; idx += 128) {
-    const int r = idx / kb, c = idx - r * kb;
-    U[r * (NB + 1) + c] = M[(k0 + r) * ld + k0 + c];
+template <typename T>
+__device__ __forceinline__ T crecip(T b) {  // 1 / b, Smith's algorithm
+  T r;
+  if (fabs(b.x) < fabs(b.y)) {
+    const auto ratio = b.x / b.y;
+    const auto den = (b.x * ratio) + b.y;
+    r.x = ratio / den;
+    r.y = -1 / den;
+  } else {
+    const auto ratio = b.y / b.x;
+    const auto den = (b.y * ratio) + b.x;
+    r.x = 1 / den;
+    r.y = -ratio / den;
   }
-  // coalesced staging of 128 rows x kb
-  for (int idx = t; idx < 128 * kb; idx += 128) {
-    const int r = idx / kb, c = idx - r * kb;
-    T v;
-    v.x = 0;
-    v.y = 0;
-    if (r0 + r < n) v = M[(r0 + r) * ld + k0 + c];
-    X[r * (NB + 1) + c] = v;
-  }
-  __syncthreads();
-  T* x = X + t * (NB + 1);
-  for (int q = 0; q < kb; q++) {
-    T v = cdiv(x[q], U[q * (NB + 1) + q]);
-    x[q] = v;
-    for (int p = q + 1; p < kb; p++) {
-      T u = U[q * (NB + 1) + p];
-      T a = x[p];
-      a.x -= v.x * u.x - v.y * u.y;
-      a.y -= v.x * u.y + v.y * u.x;
-      x[p] = a;
+  return r;
+}
+
+// LU with partial pivoting inside the kb x kb diagonal block at (k0, k0)
+// (kb <= 64), in place.  piv[k0 + c] receives the global row exchanged with
+// row k0 + c (exchanges applied in order, as LAPACK's ipiv); dinv[c]
+// receives 1 / U[c][c].
+//
+// Warp w owns columns w, w+8, ..., and its lanes are rows, so column access
+// is free of bank conflicts.  Step c, between two barriers: every warp
+// applies the exchange (c, p_c) to its columns and updates its columns q > c
+// with the published multipliers of column c; the owner of column c+1
+// updates that column first, then finds its pivot, exchanges and scales it,
+// and publishes p_{c+1} and the multipliers of column c+1 in the other half
+// of a double buffer.  One barrier per column.
+template <typename T>
+__global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(T* M, int64_t ld, int64_t k0, int kb, int* piv,
+                                                               T* dinv, int* status) {
+  using R = decltype(T{}.x);
+  constexpr int NB = kBlk, PER = NB * NB / kDiagThreads, NW = kDiagThreads / 32;
+  __shared__ T D[NB][NB + 1];
+  __shared__ T Lc[2][NB];  // multipliers of the current / next column
+  __shared__ int s_p[2];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  {
+    T v[PER];  // all loads in flight before the first shared-memory store
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+      const int e = t + i * kDiagThreads, r = e / NB, c = e % NB;
+      v[i] = (r < kb && c < kb) ? M[(k0 + r) * ld + k0 + c] : czero<T>();
+    }
+#pragma unroll
+    for (int i = 0; i < PER; i++) {
+      const int e = t + i * kDiagThreads;
+      D[e / NB][e % NB] = v[i];
     }
   }
   __syncthreads();
-  for (int idx = t; idx < 128 * kb; idx += 128) {
-    const int r = idx / kb, c = idx - r * kb;
-    if (r0 + r < n) M[(r0 + r) * ld + k0 + c] = X[r * (NB + 1) + c];
+
+  // pivot of column q over rows [q, kb), exchange within column q, scale:
+  // run by the warp that owns column q once the column is up to date
+  auto pivot_column = [&](int q) {
+    const int r0 = q + lane, r1 = q + 32 + lane;
+    R best = (R)-1;
+    int brow = q;
+    if (r0 < kb) {
+      const T v = D[r0][q];
+      const R a = v.x * v.x + v.y * v.y;
+      if (a > best) {
+        best = a;
+        brow = r0;
+      }
+    }
+    if (r1 < kb) {
+      const T v = D[r1][q];
+      const R a = v.x * v.x + v.y * v.y;
+      if (a > best) {  // NaN never wins
+        best = a;
+        brow = r1;
+      }
+    }
+    // warp argmax: |v|^2 >= 0 orders like its bit pattern (-1: no row);
+    // the lowest lane holding the maximum supplies the row
+    const unsigned key = best >= (R)0 ? __float_as_uint((float)best) : 0u;
+    const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+    const int src = __ffs(__ballot_sync(0xffffffffu, key == kmax && best >= (R)0)) - 1;
+    brow = src >= 0 ? __shfl_sync(0xffffffffu, brow, src) : q;
+    if (!(kmax > 0u)) {  // all zero, or no finite candidate
+      if (lane == 0) atomicOr(status, src >= 0 ? kLuStatSingular : kLuStatNonFinite);
+      brow = q;
+    }
+    const T pv = D[brow][q];  // every lane reads the pivot before the exchange
+    __syncwarp();
+    if (lane == 0 && brow != q) {
+      D[brow][q] = D[q][q];
+      D[q][q] = pv;
+    }
+    __syncwarp();
+    // 1/pv = conj(pv) / |pv|^2, with Smith's division outside the safe range
+    const R d2 = pv.x * pv.x + pv.y * pv.y;
+    T pinv;
+    if (d2 > (R)1e-30 && d2 < (R)1e30) {
+      const R rr = (R)1 / d2;
+      pinv.x = pv.x * rr;
+      pinv.y = -pv.y * rr;
+    } else {
+      pinv = crecip(pv);
+    }
+    T* L = Lc[q & 1];
+    if (r0 > q && r0 < kb) {
+      const T l = cmul(D[r0][q], pinv);
+      D[r0][q] = l;
+      L[r0] = l;
+    }
+    if (r1 < kb) {
+      const T l = cmul(D[r1][q], pinv);
+      D[r1][q] = l;
+      L[r1] = l;
+    }
+    if (lane == 0) {
+      s_p[q & 1] = brow;
+      dinv[q] = pinv;
+      piv[k0 + q] = (int)(k0 + brow);
+    }
+  };
+
+  if (warp == 0) pivot_column(0);
+  __syncthreads();
+  for (int c = 0; c < kb; c++) {
+    const int pc = s_p[c & 1];
+    const T* L = Lc[c & 1];
+    // 1. the exchange (c, pc) on this warp's columns (the owner of c did its own)
+    if (pc != c && lane < NB / NW) {
+      const int q = warp + NW * lane;
+      if (q < kb && q != c) {
+        const T a = D[c][q];
+        D[c][q] = D[pc][q];
+        D[pc][q] = a;
+      }
+    }
+    __syncwarp();
+    // 2. rank-1 update of this warp's columns q > c: the owner of c+1 does
+    //    that column first and pivots it, then all columns in one batch
+    const int r0 = c + 1 + lane, r1 = c + 33 + lane;
+    const T l0 = r0 < kb ? L[r0] : czero<T>();
+    const T l1 = r1 < kb ? L[r1] : czero<T>();
+    const int first = c + 1;
+    int q0 = warp;  // this warp's first column beyond c
+    if (q0 < first) q0 += (first - q0 + NW - 1) / NW * NW;
+    if (first < kb && q0 == first) {
+      const T u = D[c][first];
+      if (r0 < kb) {
+        T a = D[r0][first];
+        a.x -= l0.x * u.x - l0.y * u.y;
+        a.y -= l0.x * u.y + l0.y * u.x;
+        D[r0][first] = a;
+      }
+      if (r1 < kb) {
+        T a = D[r1][first];
+        a.x -= l1.x * u.x - l1.y * u.y;
+        a.y -= l1.x * u.y + l1.y * u.x;
+        D[r1][first] = a;
+      }
+      __syncwarp();
+      pivot_column(first);
+      q0 += NW;
+    }
+    {
+      constexpr int J = NB / NW;
+      T u[J], a0[J], a1[J];
+#pragma unroll
+      for (int j = 0; j < J; j++) {
+        const int q = q0 + NW * j;
+        if (q < kb) {
+          u[j] = D[c][q];
+          if (r0 < kb) a0[j] = D[r0][q];
+          if (r1 < kb) a1[j] = D[r1][q];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < J; j++) {
+        const int q = q0 + NW * j;
+        if (q < kb) {
+          if (r0 < kb) {
+            a0[j].x -= l0.x * u[j].x - l0.y * u[j].y;
+            a0[j].y -= l0.x * u[j].y + l0.y * u[j].x;
+            D[r0][q] = a0[j];
+          }
+          if (r1 < kb) {
+            a1[j].x -= l1.x * u[j].x - l1.y * u[j].y;
+            a1[j].y -= l1.x * u[j].y + l1.y * u[j].x;
+            D[r1][q] = a1[j];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int c = kb + t; c < NB; c += kDiagThreads) dinv[c] = czero<T>();
+#pragma unroll
+  for (int i = 0; i < PER; i++) {
+    const int e = t + i * kDiagThreads, r = e / NB, c = e % NB;
+    if (r < kb && c < kb) M[(k0 + r) * ld + k0 + c] = D[r][c];
+  }
+}
+
+// Panel triangular solves with one 64-vector per thread, staged through
+// shared memory with coalesced rows:
+//   RIGHT: rows [s0, n) of the panel columns at k0:  x <- x U11^-1 (L21)
+//   LEFT:  columns [s0, n) of the panel rows at k0:   x <- L11^-1 x (U12)
+// Both are the row-vector solve x <- x T^-1 with T upper triangular (U11,
+// or L11 transposed with a unit diagonal), done in 8 x 8 register blocks so
+// the loop body stays small (a fully unrolled 64 x 64 solve outgrows the
+// instruction cache).
+constexpr int kTrsmW = 128;  // vectors per CTA (= threads)
+template <typename T>
+constexpr size_t trsm_panel_smem() {
+  return (size_t)(kBlk * (kBlk + 1) + kTrsmW * (kBlk + 1) + kBlk) * sizeof(T);
+}
+
+template <typename T, bool LEFT>
+__global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
+                                                            const T* dinv) {
+  constexpr int NB = kBlk, W = kTrsmW, B = 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T(*Tri)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
+  T(*X)[NB + 1] = Tri + NB;
+  T* di = reinterpret_cast<T*>(X + W);
+  const int t = threadIdx.x;
+  const int64_t s0 = sbeg + (int64_t)blockIdx.x * W;
+  const int cnt = (int)min((int64_t)W, n - s0);
+  // triangle: 32 elements per thread, loads batched by 8
+  for (int b = 0; b < NB * NB / W; b += 8) {
+    T v[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int e = t + (b + i) * W;
+      v[i] = M[(k0 + e / NB) * ld + k0 + e % NB];
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int e = t + (b + i) * W, r = e / NB, c = e % NB;
+      if (LEFT)
+        Tri[c][r] = r > c ? v[i] : czero<T>();  // L11^T, strictly upper part
+      else
+        Tri[r][c] = v[i];
+    }
+  }
+  if (!LEFT && t < NB) di[t] = dinv[t];
+  // the vectors: 64 elements per thread, loads batched by 16
+  for (int b = 0; b < NB; b += 16) {
+    T v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const int e = t + (b + i) * W;
+      if (LEFT) {
+        const int r = e / W, cc = e % W;
+        v[i] = cc < cnt ? M[(k0 + r) * ld + s0 + cc] : czero<T>();
+      } else {
+        const int rr = e / NB, c = e % NB;
+        v[i] = rr < cnt ? M[(s0 + rr) * ld + k0 + c] : czero<T>();
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const int e = t + (b + i) * W;
+      if (LEFT)
+        X[e % W][e / W] = v[i];
+      else
+        X[e / NB][e % NB] = v[i];
+    }
+  }
+  __syncthreads();
+  T* x = X[t];
+#pragma unroll 1
+  for (int Q = 0; Q < NB; Q += B) {
+    T xq[B];
+#pragma unroll
+    for (int i = 0; i < B; i++) xq[i] = x[Q + i];
+#pragma unroll
+    for (int i = 0; i < B; i++) {
+      if (!LEFT) xq[i] = cmul(xq[i], di[Q + i]);
+#pragma unroll
+      for (int j = i + 1; j < B; j++) {
+        const T u = Tri[Q + i][Q + j];
+        xq[j].x -= xq[i].x * u.x - xq[i].y * u.y;
+        xq[j].y -= xq[i].x * u.y + xq[i].y * u.x;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < B; i++) x[Q + i] = xq[i];
+#pragma unroll 1
+    for (int P = Q + B; P < NB; P += B) {
+      T xp[B];
+#pragma unroll
+      for (int j = 0; j < B; j++) xp[j] = x[P + j];
+#pragma unroll
+      for (int i = 0; i < B; i++)
+#pragma unroll
+        for (int j = 0; j < B; j++) {
+          const T u = Tri[Q + i][P + j];
+          xp[j].x -= xq[i].x * u.x - xq[i].y * u.y;
+          xp[j].y -= xq[i].x * u.y + xq[i].y * u.x;
+        }
+#pragma unroll
+      for (int j = 0; j < B; j++) x[P + j] = xp[j];
+    }
+  }
+  __syncthreads();
+  for (int b = 0; b < NB; b += 16) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const int e = t + (b + i) * W;
+      if (LEFT) {
+        const int r = e / W, cc = e % W;
+        if (cc < cnt) M[(k0 + r) * ld + s0 + cc] = X[cc][r];
+      } else {
+        const int rr = e / NB, c = e % NB;
+        if (rr < cnt) M[(s0 + rr) * ld + k0 + c] = X[rr][c];
+      }
+    }
+  }
+}
+
+// Row interchanges of a block-pivoted panel: the kb <= 64 exchanges stay
+// inside rows [k0, k0+kb), so each column is one gather of those rows.  A
+// CTA covers 32 columns with 8 row groups; all reads finish (barrier) before
+// any write.  Columns [k0, k0+kb) (the diagonal block) are skipped.
+template <typename T>
+__global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int kb,
+                                                          const int* piv) {
+  constexpr int NB = kBlk, RG = 8, PER = NB / RG;
+  __shared__ int sp[NB];
+  __shared__ int src[NB];
+  const int t = threadIdx.x, tx = t & 31, g = t >> 5;
+  if (t < NB) sp[t] = t < kb ? piv[k0 + t] - (int)k0 : t;
+  __syncthreads();
+  if (t == 0) {
+    // src[r]: the original row that ends up in row r
+    for (int i = 0; i < NB; i++) src[i] = i;
+    for (int c = 0; c < kb; c++) {
+      const int p = min(max(sp[c], 0), NB - 1);
+      const int a = src[c];
+      src[c] = src[p];
+      src[p] = a;
+    }
+  }
+  __syncthreads();
+  const int64_t col = (int64_t)blockIdx.x * 32 + tx;
+  const bool act = col < n && !(col >= k0 && col < k0 + kb);
+  T v[PER];
+#pragma unroll
+  for (int i = 0; i < PER; i++) {
+    const int r = g + RG * i;
+    if (act && r < kb && src[r] != r) v[i] = M[(k0 + src[r]) * ld + col];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < PER; i++) {
+    const int r = g + RG * i;
+    if (act && r < kb && src[r] != r) M[(k0 + r) * ld + col] = v[i];
   }
 }
 
