@@ -102,6 +102,9 @@ struct necgpu_engine {
   int tc_kdim = 0;
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
+  float2* d_tinv = nullptr;  // inverted 64 x 64 diagonal blocks of the complex64 factors
+  unsigned* d_sweep_ctr = nullptr;  // progress of the refinement sweeps
+  bool inv_sweep = true;
   // mixed path: block-local pivoting first, full partial pivoting as fallback
   bool prefer_blockpiv = true;
   bool blockpiv = false;
@@ -238,6 +241,8 @@ void free_all(necgpu_engine* e) {
   dfree(e->d_ccoef);
   dfree(e->Z64);
   dfree(e->d_dinv);
+  dfree(e->d_tinv);
+  dfree(e->d_sweep_ctr);
   dfree(e->Z32);
   dfree(e->d_piv);
   dfree(e->d_perm);
@@ -675,6 +680,49 @@ int ensure_vectors(necgpu_engine* e) {
   return 0;
 }
 
+// Inverses of the 64 x 64 diagonal blocks of the complex64 factors, for the
+// refinement sweeps (one CTA per block, all blocks at once).
+int invert_diag_blocks(necgpu_engine* e) {
+  if (!e->inv_sweep) return 0;
+  const int64_t nblk = (e->n + kBlk - 1) / kBlk;
+  if (!e->d_tinv) TRY(dalloc(e, e->d_tinv, (size_t)nblk * 2 * kBlk * kBlk));
+  if (!e->d_sweep_ctr) TRY(dalloc(e, e->d_sweep_ctr, 4));
+  CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_inv_smem()));
+  KLAUNCH(NECGPU_K_OTHER, 0.0,
+          tri_inv_kernel<<<(unsigned)nblk, 128, tri_inv_smem(), e->stream>>>(e->Z32, e->ld, e->n, e->d_tinv));
+  return 0;
+}
+
+// sol = U^-1 L^-1 rhs on the complex64 factors with inverted diagonal
+// blocks (rhs is overwritten): two persistent sweeps
+int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
+  const int64_t n = e->n, ld = e->ld;
+  const int nblk = (int)((n + kBlk - 1) / kBlk);
+  int per_sm = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, inv_sweep_kernel<true>, kInvSweepThreads, 0));
+  if (per_sm < 1) return fail(e, NECGPU_ERR_CUDA, "sweep kernel cannot be resident");
+  const int grid = std::max(1, std::min(nblk, per_sm * e->nsm));
+  const double tri_bytes = 0.5 * (double)n * (double)n * sizeof(float2);
+  for (int pass = 0; pass < 2; pass++) {
+    const float2* src = pass == 0 ? rhs : sol;
+    float2* dst = pass == 0 ? sol : rhs;
+    const float2* tinv = e->d_tinv;
+    unsigned* counter = e->d_sweep_ctr;
+    CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), e->stream));
+    void* args[] = {(void*)&e->Z32, (void*)&ld, (void*)&n, (void*)&tinv, (void*)&src, (void*)&dst, (void*)&counter,
+                    (void*)&e->d_status};
+    const int kt = kbegin(e);
+    CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)inv_sweep_kernel<true>
+                                                   : (const void*)inv_sweep_kernel<false>,
+                                         dim3(grid), dim3(kInvSweepThreads), args, 0, e->stream));
+    kend(e, kt, NECGPU_K_TRSV, tri_bytes);
+    LAUNCHED();
+  }
+  // the backward pass wrote the solution into rhs
+  CUDA_TRY(cudaMemcpyAsync(sol, rhs, n * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
+  return 0;
+}
+
 // Mixed-precision factorisation of the FP64 matrix: demote to complex64, then
 // LU with block-local pivoting (blockpiv) or full partial pivoting.
 int factor_mixed(necgpu_engine* e, bool blockpiv) {
@@ -684,12 +732,13 @@ int factor_mixed(necgpu_engine* e, bool blockpiv) {
   e->stats.pivoting = blockpiv ? 1 : 0;
   if (blockpiv) {
     const int rc = run_lu_blockpiv(e, e->Z32);
-    if (rc != NECGPU_ERR_SINGULAR && rc != NECGPU_ERR_NONFINITE) return rc;
+    if (rc != NECGPU_ERR_SINGULAR && rc != NECGPU_ERR_NONFINITE) return rc ? rc : invert_diag_blocks(e);
     // a diagonal block without a usable pivot: full partial pivoting
     CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
     return factor_mixed(e, false);
   }
-  return run_lu<float>(e, e->Z32);
+  TRY(run_lu<float>(e, e->Z32));
+  return invert_diag_blocks(e);
 }
 
 // Iterative refinement with the complex64 factors against the FP64 matrix:
@@ -709,7 +758,10 @@ int refine(necgpu_engine* e, int* iters, double* rel_out) {
   int it = 0;
   for (; it <= e->refine_max; it++) {
     KLAUNCH(NECGPU_K_OTHER, 0.0, permute_kernel<float2, double2><<<g1, 256, 0, e->stream>>>(e->d_r, e->d_perm, w1, n));
-    TRY(run_trsv<float>(e, e->Z32, w1, w2));
+    if (e->inv_sweep && e->sweep_trsv)
+      TRY(run_trsv_inv(e, w1, w2));
+    else
+      TRY(run_trsv<float>(e, e->Z32, w1, w2));
     KLAUNCH(NECGPU_K_OTHER, 0.0, axpy_kernel<float2><<<g1, 256, 0, e->stream>>>(e->d_x, w2, n));
     CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
     // bytes of FP64 Z read by the residual
@@ -860,6 +912,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_NO_TC")) e->use_tc = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_BLOCKED_TRSV")) e->sweep_trsv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_FLAG_SWEEP")) e->inv_sweep = (s[0] == '0');
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   e->own_stream = true;
   CUDA_TRY(cudaEventCreate(&e->ev0));

@@ -346,4 +346,205 @@ __global__ void demote_kernel(const double2* src, float2* dst, int64_t count) {
   for (; i < count; i += stride) dst[i] = make_float2((float)src[i].x, (float)src[i].y);
 }
 
+// ---------------------------------------------------------------------------
+// Triangular sweeps of the mixed-precision refinement, on complex64 factors
+// whose 64 x 64 diagonal blocks have been inverted once per factorisation
+// (tri_inv_kernel).  Block v of the sweep computes
+//     x_v = inv(T_vv) (b_v - sum_{u before v} T_vu x_u)
+// One CTA per block (persistent, cooperative).  A single counter holds how
+// many blocks of the sweep are complete; blocks complete in sweep order, so
+// a CTA reads the counter once and folds in every finished block it has not
+// yet seen.  The off-diagonal tile row of each block is loaded before the
+// wait, and the diagonal solve is a parallel 64 x 64 product with the
+// inverse, so the chain between two blocks is one counter hand-off, one
+// read of x_u and two block reductions.
+
+// tinv[2*blk] = L_bb^-1 (unit lower), tinv[2*blk+1] = U_bb^-1, 64 x 64
+// row-major each, zero outside the kb x kb triangle.  128 threads: threads
+// 0..63 build the columns of L^-1, threads 64..127 those of U^-1.
+constexpr size_t tri_inv_smem() { return (size_t)3 * kBlk * (kBlk + 1) * sizeof(float2); }
+__global__ void __launch_bounds__(128) tri_inv_kernel(const float2* M, int64_t ld, int64_t n, float2* tinv) {
+  constexpr int NB = kBlk;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2(*D)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(smem_raw);
+  float2(*X)[NB + 1] = D + NB;
+  float2(*Y)[NB + 1] = D + 2 * NB;
+  const int t = threadIdx.x;
+  const int64_t b0 = (int64_t)blockIdx.x * NB;
+  const int kb = (int)min((int64_t)NB, n - b0);
+  for (int e = t; e < NB * NB; e += 128) {
+    const int r = e / NB, c = e % NB;
+    D[r][c] = (r < kb && c < kb) ? M[(b0 + r) * ld + b0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  if (t < NB) {
+    // column j of L^-1: X[j][j] = 1, X[i][j] = -sum_{k=j}^{i-1} L[i][k] X[k][j]
+    const int j = t;
+    for (int i = 0; i < NB; i++) {
+      float2 v = make_float2(0.f, 0.f);
+      if (j < kb && i < kb && i >= j) {
+        if (i == j) {
+          v.x = 1.f;
+        } else {
+          float sr = 0.f, si = 0.f;
+          for (int k = j; k < i; k++) {
+            const float2 a = D[i][k], b = X[k][j];
+            sr += a.x * b.x - a.y * b.y;
+            si += a.x * b.y + a.y * b.x;
+          }
+          v = make_float2(-sr, -si);
+        }
+      }
+      X[i][j] = v;
+    }
+  } else {
+    // column j of U^-1: Y[j][j] = 1/U[j][j],
+    // Y[i][j] = -(sum_{k=i+1}^{j} U[i][k] Y[k][j]) / U[i][i] for i < j
+    const int j = t - NB;
+    for (int i = NB - 1; i >= 0; i--) {
+      float2 v = make_float2(0.f, 0.f);
+      if (j < kb && i <= j) {
+        const float2 di = crecip(D[i][i]);
+        if (i == j) {
+          v = di;
+        } else {
+          float sr = 0.f, si = 0.f;
+          for (int k = i + 1; k <= j; k++) {
+            const float2 a = D[i][k], b = Y[k][j];
+            sr += a.x * b.x - a.y * b.y;
+            si += a.x * b.y + a.y * b.x;
+          }
+          v = cmul(make_float2(-sr, -si), di);
+        }
+      }
+      Y[i][j] = v;
+    }
+  }
+  __syncthreads();
+  float2* out = tinv + (int64_t)blockIdx.x * 2 * NB * NB;
+  for (int e = t; e < NB * NB; e += 128) {
+    out[e] = X[e / NB][e % NB];
+    out[NB * NB + e] = Y[e / NB][e % NB];
+  }
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+constexpr int kInvSweepThreads = 256;
+
+// LOWER: x = L^-1 b (unit lower); !LOWER: x = U^-1 b.  counter must be 0 at
+// launch.  On a wait that runs out the kernel sets bit 9 of *status and
+// every CTA returns.
+template <bool LOWER>
+__global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float2* M, int64_t ld, int64_t n,
+                                                                     const float2* tinv, const float2* b, float2* x,
+                                                                     unsigned* counter, int* status) {
+  constexpr int NB = kBlk, QW = NB / 4;  // four column quarters of 16
+  __shared__ float2 part[4][NB];
+  __shared__ float2 sv[NB];
+  __shared__ volatile int s_abort;
+  const int t = threadIdx.x, lane = t & 31;
+  const int r = t & (NB - 1), q = t >> 6;  // row in the block, column quarter
+  const int nblk = (int)((n + NB - 1) / NB);
+  if (t == 0) s_abort = 0;
+  __syncthreads();
+  for (int s = blockIdx.x; s < nblk; s += gridDim.x) {  // s: position in sweep order
+    const int v = LOWER ? s : nblk - 1 - s;
+    const int64_t r0 = (int64_t)v * NB;
+    const int bs = (int)min((int64_t)NB, n - r0);
+    const bool rowok = r < bs;
+    // this thread's 16 entries of row r of inv(T_vv)
+    float2 inv[QW];
+    {
+      const float4* ip =
+          reinterpret_cast<const float4*>(tinv + ((int64_t)v * 2 + (LOWER ? 0 : 1)) * NB * NB + r * NB + q * QW);
+#pragma unroll
+      for (int k = 0; k < QW / 2; k++) {
+        const float4 w = ip[k];
+        inv[2 * k] = make_float2(w.x, w.y);
+        inv[2 * k + 1] = make_float2(w.z, w.w);
+      }
+    }
+    float accr = 0.f, acci = 0.f;
+    int done = 0;  // sweep positions known to be complete
+    for (int i = 0; i < s; i++) {
+      const int u = LOWER ? i : nblk - 1 - i;
+      const int64_t c0 = (int64_t)u * NB + q * QW;
+      // the tile row is independent of x: in flight before the wait
+      float2 m[QW];
+      if (rowok && c0 + QW <= n) {
+        const float4* mp = reinterpret_cast<const float4*>(M + (r0 + r) * ld + c0);
+#pragma unroll
+        for (int k = 0; k < QW / 2; k++) {
+          const float4 w = mp[k];
+          m[2 * k] = make_float2(w.x, w.y);
+          m[2 * k + 1] = make_float2(w.z, w.w);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < QW; k++)
+          m[k] = (rowok && c0 + k < n) ? M[(r0 + r) * ld + c0 + k] : make_float2(0.f, 0.f);
+      }
+      if (i >= done) {
+        int seen = 0;
+        if (lane == 0) {
+          long long spins = 0;
+          unsigned c = ld_acquire_u32(counter);
+          while ((int)c <= i) {
+            if (s_abort || ++spins > kSweepSpinLimit) {
+              if (!s_abort) atomicOr(status, 1 << 9);
+              s_abort = 1;
+              break;
+            }
+            __nanosleep(32);
+            c = ld_acquire_u32(counter);
+          }
+          seen = (int)c > i ? (int)c : -1;
+        }
+        done = __shfl_sync(0xffffffffu, seen, 0);  // the same decision in every lane
+        __syncwarp();                               // x reads below are ordered after the acquire
+        if (done < 0) break;
+      }
+#pragma unroll
+      for (int k = 0; k < QW; k++) {
+        const float2 xv = c0 + k < n ? __ldcg(x + c0 + k) : make_float2(0.f, 0.f);
+        accr += m[k].x * xv.x - m[k].y * xv.y;
+        acci += m[k].x * xv.y + m[k].y * xv.x;
+      }
+    }
+    part[q][r] = make_float2(accr, acci);
+    __syncthreads();
+    if (t < NB) {
+      float2 a = make_float2(0.f, 0.f);
+      if (t < bs) {
+        const float2 bb = b[r0 + t];
+        a.x = bb.x - (part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x);
+        a.y = bb.y - (part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
+      }
+      sv[t] = a;
+    }
+    __syncthreads();
+    accr = 0.f;
+    acci = 0.f;
+#pragma unroll
+    for (int k = 0; k < QW; k++) {
+      const float2 a = sv[q * QW + k];
+      accr += inv[k].x * a.x - inv[k].y * a.y;
+      acci += inv[k].x * a.y + inv[k].y * a.x;
+    }
+    part[q][r] = make_float2(accr, acci);
+    __syncthreads();
+    if (t < bs && !s_abort) {
+      x[r0 + t] = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
+                              part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_abort) return;
+    if (t == 0) st_release_u32(counter, (unsigned)(s + 1));
+  }
+}
+
 }  // namespace necb
