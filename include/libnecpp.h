@@ -174,6 +174,17 @@ long nec_get_rhs(nec_context* in_context, double* out);
 /* The context's GPU engine (include/necgpu.h), created on first use; NULL
    with nec_error_message() set when no usable device exists. */
 void* nec_gpu_engine(nec_context* in_context);
+/* Adjoint gradients (no counterpart in the reference).  After an XQ or RP
+   card has solved `base` (one voltage source, mixed precision), returns
+   value[3] = {Re Zin, Im Zin, gain in dB at (theta, phi)} and
+   grad[3*k + i] = d value[i] / d p_k for nparam geometry parameters p_k.
+   plus[k] / minus[k] are contexts holding the same cards with parameter k
+   moved by +h[k] / -h[k] (geometry complete and excitation given, not
+   solved).  One transposed solve per output on the held factors; the
+   matrix derivative is recomputed tile by tile from the perturbed
+   structures and never stored. */
+long nec_gradient(nec_context* base, int nparam, nec_context** plus, nec_context** minus, const double* h,
+                  double theta_deg, double phi_deg, double* value, double* grad);
 /* Refinement diagnostics of the last solve (mixed precision). */
 long nec_last_refinement(nec_context* in_context, int* iters, double* residual);
 /* Complex far field E_theta / E_phi (V/m x wavelength, as stored by the

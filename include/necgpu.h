@@ -212,6 +212,32 @@ int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph
  * converges. */
 int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_dev, double* abc_dev);
 
+/* ---- adjoint gradients (no counterpart in the reference; they serve the
+ * gradient extension of the host library, nec_gradient) ---- */
+
+/* Copy the basis amplitudes x of the last necgpu_solve (n complex; Z x = e). */
+int necgpu_copy_solution(necgpu_engine* e, double* x);
+
+/* Solve Z^T w_k = phi_k for nrhs right-hand sides (n complex each, host
+ * arrays) on the held mixed-precision factors: the transposed factors and
+ * diagonal-block inverses drive the same triangular sweeps, refined in FP64
+ * against Z^T to the refinement tolerance.  NECGPU_ERR_UNSUPPORTED after an
+ * FP64 factorisation (it overwrites Z). */
+int necgpu_adjoint_solve(necgpu_engine* e, int nrhs, const double* phi, double* w);
+
+/* E_theta = phi_t^T x and E_phi = phi_p^T x: the far field of one direction
+ * (radians) as linear functionals of the basis amplitudes (n complex each). */
+int necgpu_pattern_weights(necgpu_engine* e, double theta, double phi, double* phi_t, double* phi_p);
+
+/* For each of nstruct perturbed copies of the held structure (same segment
+ * count, basis-table layout and medium; geometry and coefficients may
+ * differ): zx[s][k] = w_k^T Z_s x for the nw <= 4 vectors w (nw x n complex)
+ * and the held solution x, from a fill of Z_s contracted on the fly (Z_s is
+ * not stored); efar[s] = (E_theta, E_phi) of x on structure s at one
+ * direction.  zx: nstruct x nw complex; efar: nstruct x 2 complex. */
+int necgpu_perturbed_terms(necgpu_engine* e, int nstruct, const necgpu_structure* structs, int nw, const double* w,
+                           double theta, double phi, double* zx, double* efar);
+
 /* Diagnostic: apply one complex64 update C -= A B (m x n, inner kb) to a
  * seeded random matrix with the tensor-core kernel and with the CUDA-core
  * FP32 kernel; report max |difference| and max |reference| over C. */

@@ -319,6 +319,12 @@ void* nec_gpu_engine(nec_context* c) {
   }
 }
 
+long nec_gradient(nec_context* base, int nparam, nec_context** plus, nec_context** minus, const double* h,
+                  double theta_deg, double phi_deg, double* value, double* grad) {
+  if (!base) return 1;
+  NEC_TRY(base->gradient(nparam, plus, minus, h, theta_deg, phi_deg, value, grad));
+}
+
 long nec_last_refinement(nec_context* c, int* iters, double* residual) {
   if (!c) return 1;
   *iters = c->last_refine_iters;

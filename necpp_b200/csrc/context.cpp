@@ -480,8 +480,7 @@ void Context::build_tables() {
 
 // structure_segment_loading, src/nec_context.cpp:1523-1558: ground
 // environment and tables, then fill and factor on the GPU.
-void Context::structure_loading() {
-  build_tables();
+necgpu_structure Context::structure_view() const {
   const int64_t n = geo_.n;
   necgpu_structure s{};
   s.n = n;
@@ -508,7 +507,12 @@ void Context::structure_loading() {
   s.frati_re = tables.fr_re;
   s.frati_im = tables.fr_im;
   s.eta = tables.eta;
+  return s;
+}
 
+void Context::structure_loading() {
+  build_tables();
+  const necgpu_structure s = structure_view();
   necgpu_engine* e = engine();
   check(e, necgpu_set_structure(e, &s));
   check(e, necgpu_fill(e));
@@ -911,6 +915,94 @@ double RadiationPattern::stat_sd(const std::vector<double>& v) const {
     }
   int64_t len = (int64_t)nth * nph;
   return std::sqrt(sum / (double(len * 2) / kPi));
+}
+
+// Adjoint gradients.  Each output is built from three complex-linear
+// functionals of the basis amplitudes x (Z x = e):
+//   J = cur_f (feed current / wavelength), E_theta, E_phi = phi^T x,
+// whose total derivative is
+//   dPhi/dp = (d phi/dp)^T x + w^T (de/dp - (dZ/dp) x),   Z^T w = phi.
+// The adjoint vectors w come from one transposed solve each on the held
+// factors; w^T (dZ/dp) x from fills of the perturbed structures contracted
+// on the fly; the explicit terms from the perturbed tables, right-hand side
+// and far-field geometry.  Central differences of width 2 h_k resolve the
+// parameter dependence of those explicit and contracted terms.
+void Context::gradient(int nparam, Context* const* plus, Context* const* minus, const double* h,
+                       double theta_deg, double phi_deg, double* value, double* grad) {
+  if (nparam < 1 || !plus || !minus || !h || !value || !grad) fail("gradient: bad arguments");
+  if (!have_factor_ || !eng_ || inputs.empty()) fail("gradient: run the forward solve (an XQ or RP card) first");
+  if (src_seg.size() != 1) fail("gradient: exactly one voltage source is supported");
+  if (precision_ != 1) fail("gradient: needs the mixed-precision path (nec_set_precision(ctx, 1))");
+  necgpu_engine* e = eng_;
+  const int64_t n = geo_.n;
+  const int64_t f = src_seg[0] - 1;
+  const cd V = src_volt[0];
+  const double lam = wavelength_;
+  // forward quantities
+  std::vector<cd> x(n);
+  check(e, necgpu_copy_solution(e, reinterpret_cast<double*>(x.data())));
+  const double th = degrees_to_rad(theta_deg), ph = degrees_to_rad(phi_deg);
+  cd Et, Ep;
+  check(e, necgpu_pattern(e, 1, &th, &ph, reinterpret_cast<double*>(&Et), reinterpret_cast<double*>(&Ep)));
+  auto feed_current = [&](const Tables& t) {  // J = sum (a + c) x over the feed segment's bases
+    cd J(0, 0);
+    for (int32_t k = t.tptr[f]; k < t.tptr[f + 1]; k++) J += (t.ta[k] + t.tc[k]) * x[t.tbasis[k]];
+    return J;
+  };
+  const cd J = solution[f];
+  // adjoint right-hand sides: phi_J, phi_theta, phi_phi
+  std::vector<cd> phis(3 * n, cd(0, 0)), w(3 * n);
+  for (int32_t k = tables.tptr[f]; k < tables.tptr[f + 1]; k++) phis[tables.tbasis[k]] += tables.ta[k] + tables.tc[k];
+  check(e, necgpu_pattern_weights(e, th, ph, reinterpret_cast<double*>(phis.data() + n),
+                                  reinterpret_cast<double*>(phis.data() + 2 * n)));
+  check(e, necgpu_adjoint_solve(e, 3, reinterpret_cast<const double*>(phis.data()), reinterpret_cast<double*>(w.data())));
+  // perturbed structures at this frequency: tables, right-hand sides
+  std::vector<necgpu_structure> structs;
+  std::vector<std::vector<cd>> rhss;
+  std::vector<cd> Jp;
+  structs.reserve(2 * nparam);
+  for (int k = 0; k < nparam; k++)
+    for (int side = 0; side < 2; side++) {
+      Context* c = side == 0 ? plus[k] : minus[k];
+      if (!c) fail("gradient: missing perturbed context");
+      c->prepare_structure(freq_mhz);
+      if (c->geo_.n != n) fail("gradient: a perturbed structure has a different segment count");
+      if (c->src_seg.size() != 1 || c->src_seg[0] != src_seg[0] || c->src_volt[0] != V)
+        fail("gradient: a perturbed structure has a different excitation");
+      structs.push_back(c->structure_view());
+      rhss.emplace_back();
+      c->rhs(rhss.back());
+      Jp.push_back(feed_current(c->tables));
+    }
+  std::vector<cd> zx(2 * nparam * 3), efar(2 * nparam * 2);
+  check(e, necgpu_perturbed_terms(e, 2 * nparam, structs.data(), 3, reinterpret_cast<const double*>(w.data()), th, ph,
+                                  reinterpret_cast<double*>(zx.data()), reinterpret_cast<double*>(efar.data())));
+  // outputs and their derivatives
+  const cd zin = V / (J * lam);
+  const double e2 = std::norm(Et) + std::norm(Ep);
+  const double P = 0.5 * std::real(V * std::conj(J * lam));
+  const double gcop = lam * lam * 2.0 * kPi / (impedance() * P);
+  value[0] = zin.real();
+  value[1] = zin.imag();
+  value[2] = db10(gcop * e2);
+  for (int k = 0; k < nparam; k++) {
+    const int qp = 2 * k, qm = 2 * k + 1;
+    const double inv2h = 1.0 / (2.0 * h[k]);
+    cd wde[3] = {cd(0, 0), cd(0, 0), cd(0, 0)};
+    for (int64_t i = 0; i < n; i++) {
+      const cd de = rhss[qp][i] - rhss[qm][i];
+      for (int a = 0; a < 3; a++) wde[a] += w[a * n + i] * de;
+    }
+    const cd explicit_[3] = {Jp[qp] - Jp[qm], efar[2 * qp] - efar[2 * qm], efar[2 * qp + 1] - efar[2 * qm + 1]};
+    cd d[3];
+    for (int a = 0; a < 3; a++) d[a] = (explicit_[a] + wde[a] - (zx[3 * qp + a] - zx[3 * qm + a])) * inv2h;
+    const cd dzin = -zin * d[0] / J;
+    const double dP = 0.5 * std::real(V * std::conj(d[0] * lam));
+    const double dlng = 2.0 * std::real(std::conj(Et) * d[1] + std::conj(Ep) * d[2]) / e2 - dP / P;
+    grad[3 * k] = dzin.real();
+    grad[3 * k + 1] = dzin.imag();
+    grad[3 * k + 2] = 10.0 / std::log(10.0) * dlng;
+  }
 }
 
 }  // namespace necb

@@ -12,9 +12,9 @@
 #include <string>
 #include <vector>
 
+#include "../../include/necgpu.h"
 #include "geometry.h"
 
-struct necgpu_engine;
 
 namespace necb {
 
@@ -92,6 +92,16 @@ class Context {
   // Applied-field vector of the current excitation at the prepared
   // frequency (etmns), host only.
   void rhs(std::vector<cd>& e) { build_rhs(e); }
+  // Gradient of (Re Zin, Im Zin, gain in dB at (theta, phi)) of the last
+  // solve with respect to nparam geometry parameters, by the adjoint method
+  // on the held factors.  plus[k] / minus[k] hold the same cards with
+  // parameter k moved by +h[k] / -h[k] (geometry complete, excitation set,
+  // no solve).  One voltage source; mixed-precision factors.  value: 3,
+  // grad: 3 * nparam (row k: d/dp_k of the three outputs).
+  void gradient(int nparam, Context* const* plus, Context* const* minus, const double* h, double theta_deg,
+                double phi_deg, double* value, double* grad);
+  // the current structure as the GPU receives it (views of this context's arrays)
+  necgpu_structure structure_view() const;
   struct Tables {
     std::vector<int32_t> tptr, tbasis, ind1, ind2;
     std::vector<double> ta, tb, tc;

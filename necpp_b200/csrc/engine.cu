@@ -103,6 +103,22 @@ struct necgpu_engine {
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
   float2* d_tinv = nullptr;  // inverted 64 x 64 diagonal blocks of the complex64 factors
+  // adjoint solves: transposed factors, matrix and block inverses
+  float2* ZT32 = nullptr;
+  double2* ZT64 = nullptr;
+  float2* d_tinvT = nullptr;
+  bool adj_ready = false;
+  double2 *d_adj_phi = nullptr, *d_adj_w = nullptr, *d_adj_r = nullptr;
+  int adj_cap = 0;  // right-hand sides the adjoint buffers hold
+  // perturbed structures (adjoint gradients)
+  double *d_pseg = nullptr, *d_pecoef = nullptr, *d_pccoef = nullptr, *d_pout = nullptr;
+  double2 *d_pw = nullptr, *d_pfar = nullptr;
+  FillArgs* d_pargs = nullptr;
+  ContractArgs* d_pcargs = nullptr;
+  int p_cap = 0, pw_cap = 0;
+  double2* d_pwts = nullptr;  // far-field weights (2 n)
+  // host copies of the basis-table layout and end flags (adjoint gradients)
+  std::vector<int32_t> h_tptr, h_tbasis, h_ind;
   unsigned* d_sweep_ctr = nullptr;  // progress of the refinement sweeps
   bool inv_sweep = true;
   // mixed path: block-local pivoting first, full partial pivoting as fallback
@@ -243,6 +259,25 @@ void free_all(necgpu_engine* e) {
   dfree(e->d_dinv);
   dfree(e->d_tinv);
   dfree(e->d_sweep_ctr);
+  dfree(e->ZT32);
+  dfree(e->ZT64);
+  dfree(e->d_tinvT);
+  dfree(e->d_adj_phi);
+  dfree(e->d_adj_w);
+  dfree(e->d_adj_r);
+  e->adj_cap = 0;
+  e->adj_ready = false;
+  dfree(e->d_pseg);
+  dfree(e->d_pecoef);
+  dfree(e->d_pccoef);
+  dfree(e->d_pout);
+  dfree(e->d_pw);
+  dfree(e->d_pfar);
+  dfree(e->d_pargs);
+  dfree(e->d_pcargs);
+  dfree(e->d_pwts);
+  e->p_cap = 0;
+  e->pw_cap = 0;
   dfree(e->Z32);
   dfree(e->d_piv);
   dfree(e->d_perm);
@@ -682,8 +717,8 @@ int ensure_vectors(necgpu_engine* e) {
 
 // Inverses of the 64 x 64 diagonal blocks of the complex64 factors, for the
 // refinement sweeps (one CTA per block, all blocks at once).
-int invert_diag_blocks(necgpu_engine* e) {
-  if (!e->inv_sweep) return 0;
+int invert_diag_blocks(necgpu_engine* e, bool force = false) {
+  if (!e->inv_sweep && !force) return 0;
   const int64_t nblk = (e->n + kBlk - 1) / kBlk;
   if (!e->d_tinv) TRY(dalloc(e, e->d_tinv, (size_t)nblk * 2 * kBlk * kBlk));
   if (!e->d_sweep_ctr) TRY(dalloc(e, e->d_sweep_ctr, 4));
@@ -695,7 +730,7 @@ int invert_diag_blocks(necgpu_engine* e) {
 
 // sol = U^-1 L^-1 rhs on the complex64 factors with inverted diagonal
 // blocks (rhs is overwritten): two persistent sweeps
-int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
+int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_blocks, float2* rhs, float2* sol) {
   const int64_t n = e->n, ld = e->ld;
   const int nblk = (int)((n + kBlk - 1) / kBlk);
   int per_sm = 0;
@@ -706,10 +741,10 @@ int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
   for (int pass = 0; pass < 2; pass++) {
     const float2* src = pass == 0 ? rhs : sol;
     float2* dst = pass == 0 ? sol : rhs;
-    const float2* tinv = e->d_tinv;
+    const float2* tinv = tinv_blocks;
     unsigned* counter = e->d_sweep_ctr;
     CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), e->stream));
-    void* args[] = {(void*)&e->Z32, (void*)&ld, (void*)&n, (void*)&tinv, (void*)&src, (void*)&dst, (void*)&counter,
+    void* args[] = {(void*)&Mf, (void*)&ld, (void*)&n, (void*)&tinv, (void*)&src, (void*)&dst, (void*)&counter,
                     (void*)&e->d_status};
     const int kt = kbegin(e);
     CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)inv_sweep_kernel<true>
@@ -722,6 +757,7 @@ int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
   CUDA_TRY(cudaMemcpyAsync(sol, rhs, n * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
   return 0;
 }
+int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) { return run_trsv_inv_on(e, e->Z32, e->d_tinv, rhs, sol); }
 
 // Mixed-precision factorisation of the FP64 matrix: demote to complex64, then
 // LU with block-local pivoting (blockpiv) or full partial pivoting.
@@ -730,6 +766,7 @@ int factor_mixed(necgpu_engine* e, bool blockpiv) {
   KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld));
   e->blockpiv = blockpiv;
   e->stats.pivoting = blockpiv ? 1 : 0;
+  e->adj_ready = false;
   if (blockpiv) {
     const int rc = run_lu_blockpiv(e, e->Z32);
     if (rc != NECGPU_ERR_SINGULAR && rc != NECGPU_ERR_NONFINITE) return rc ? rc : invert_diag_blocks(e);
@@ -788,6 +825,77 @@ int refine(necgpu_engine* e, int* iters, double* rel_out) {
   *iters = it;
   *rel_out = rel;
   return 0;
+}
+
+// ---------------- adjoint solves ----------------
+// Transposed copies of the held mixed factors, of the FP64 matrix and of the
+// inverted diagonal blocks (once per factorisation).
+int ensure_adjoint(necgpu_engine* e) {
+  if (e->factored != NECGPU_MIXED)
+    return fail(e, NECGPU_ERR_UNSUPPORTED,
+                "adjoint: needs the mixed-precision factorisation (the FP64 path factors Z in place)");
+  if (e->adj_ready) return 0;
+  const int64_t n = e->n, ld = e->ld, nblk = (n + kBlk - 1) / kBlk;
+  if (!e->inv_sweep || !e->d_tinv) TRY(invert_diag_blocks(e, true));
+  if (!e->ZT32) TRY(dalloc(e, e->ZT32, (size_t)n * ld));
+  if (!e->ZT64) TRY(dalloc(e, e->ZT64, (size_t)n * ld));
+  if (!e->d_tinvT) TRY(dalloc(e, e->d_tinvT, (size_t)nblk * 2 * kBlk * kBlk));
+  const dim3 g((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, transpose_kernel<float2><<<g, 256, 0, e->stream>>>(e->Z32, ld, e->ZT32, ld, n));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, transpose_kernel<double2><<<g, 256, 0, e->stream>>>(e->Z64, ld, e->ZT64, ld, n));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, tinv_transpose_kernel<<<(unsigned)nblk, 256, 0, e->stream>>>(e->d_tinv, e->d_tinvT));
+  e->adj_ready = true;
+  return 0;
+}
+
+// Z^T w = phi (device vectors), refined in FP64 against Z^T like the forward
+// solve: w = 0, r = phi; repeat d = P^T L^-T U^-T r, w += d, r = phi - Z^T w.
+int refine_T(necgpu_engine* e, const double2* phi, double2* w, int* iters, double* rel_out) {
+  const int64_t n = e->n;
+  const unsigned g1 = (unsigned)((n + 255) / 256);
+  float2* w1 = reinterpret_cast<float2*>(e->d_w1);
+  float2* w2 = reinterpret_cast<float2*>(e->d_w2);
+  double2* r = e->d_adj_r;
+  CUDA_TRY(cudaMemsetAsync(w, 0, n * sizeof(double2), e->stream));
+  CUDA_TRY(cudaMemcpyAsync(r, phi, n * sizeof(double2), cudaMemcpyDeviceToDevice, e->stream));
+  const unsigned gr = (unsigned)std::min<int64_t>((n + 7) / 8, 8 * e->nsm);
+  CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, 2 * sizeof(double), e->stream));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, norm2_kernel<<<g1, 256, 0, e->stream>>>(phi, n, e->d_rn2 + 1));
+  double prev = 1e300, rel = 1.0;
+  int it = 0;
+  for (; it <= e->refine_max; it++) {
+    KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<g1, 256, 0, e->stream>>>(r, w1, n));
+    TRY(run_trsv_inv_on(e, e->ZT32, e->d_tinvT, w1, w2));
+    KLAUNCH(NECGPU_K_OTHER, 0.0, axpy_scatter_kernel<<<g1, 256, 0, e->stream>>>(w, w2, e->d_perm, n));
+    CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
+    KLAUNCH(NECGPU_K_RESID, (double)n * n * sizeof(double2),
+            residual_kernel<<<gr, 256, 0, e->stream>>>(e->ZT64, e->ld, n, w, phi, r, e->d_rn2));
+    double rn2[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(rn2, e->d_rn2, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    e->stats.d2h_bytes += 2 * sizeof(double);
+    kflush(e);
+    const double bn = std::sqrt(rn2[1]);
+    rel = bn > 0 ? std::sqrt(rn2[0]) / bn : 0.0;
+    if (!std::isfinite(rel)) {
+      *iters = it + 1;
+      *rel_out = rel;
+      return fail(e, NECGPU_ERR_NONFINITE, "adjoint: non-finite residual");
+    }
+    if (rel <= e->refine_tol || rel > 0.5 * prev) {
+      it++;
+      break;
+    }
+    prev = rel;
+  }
+  *iters = it;
+  *rel_out = rel;
+  return 0;
+}
+
+FarDir engine_far_dir(const necgpu_engine* e, double theta, double phi) {
+  return far_dir(theta, phi, e->ground == kGroundNone ? 1 : 2, e->ground == kGroundPerfect ? 1 : 0, e->P.zrati,
+                 e->P.eta);
 }
 
 // Solve Z x = b (d_b) into d_x (FP64) with the held factors; then the
@@ -876,6 +984,7 @@ int run_factor(necgpu_engine* e, int precision) {
     return fail(e, NECGPU_ERR_ARG, "factor: unknown precision");
   }
   e->factored = precision;
+  e->adj_ready = false;
   return 0;
 }
 
@@ -890,6 +999,93 @@ int fill_checked(necgpu_engine* e, bool want32) {
 }  // namespace
 
 // ======================= C-ABI =======================
+
+namespace {
+
+// Column-tile source lists of a structure's basis tables (fill.cuh): for
+// every tile of 32 basis columns, the distinct contributing source segments
+// (ascending) and their (column, a, b, c) entries.  ecoef = a | b | c.
+struct TileLists {
+  std::vector<int32_t> tile_ptr, tsrc, tsrc_eptr;
+  std::vector<uint8_t> ecol;
+  std::vector<double> ecoef;
+};
+void build_tile_lists(const necgpu_structure* s, int64_t n, int ntiles, TileLists& L) {
+  const int32_t* tp = s->trio_ptr;
+  struct Ent {
+    int32_t j;
+    uint8_t col;
+    double a, b, c;
+  };
+  std::vector<std::vector<Ent>> tiles(ntiles);
+  for (int64_t j = 0; j < n; j++)
+    for (int32_t k = tp[j]; k < tp[j + 1]; k++) {
+      int32_t bas = s->trio_basis[k];
+      tiles[bas / kFillTB].push_back(
+          Ent{(int32_t)j, (uint8_t)(bas % kFillTB), s->trio_a[k], s->trio_b[k], s->trio_c[k]});
+    }
+  L.tile_ptr.assign(ntiles + 1, 0);
+  L.tsrc.clear();
+  L.tsrc_eptr.clear();
+  L.ecol.clear();
+  std::vector<double> ea, eb, ec;
+  for (int t = 0; t < ntiles; t++) {
+    auto& v = tiles[t];  // pushed in ascending source order
+    L.tile_ptr[t] = (int32_t)L.tsrc.size();
+    size_t k = 0;
+    while (k < v.size()) {
+      const int32_t j = v[k].j;
+      L.tsrc.push_back(j);
+      L.tsrc_eptr.push_back((int32_t)L.ecol.size());
+      while (k < v.size() && v[k].j == j) {
+        L.ecol.push_back(v[k].col);
+        ea.push_back(v[k].a);
+        eb.push_back(v[k].b);
+        ec.push_back(v[k].c);
+        k++;
+      }
+    }
+  }
+  L.tile_ptr[ntiles] = (int32_t)L.tsrc.size();
+  L.tsrc_eptr.push_back((int32_t)L.ecol.size());
+  const size_t ne = L.ecol.size();
+  L.ecoef.assign(3 * std::max<size_t>(ne, 1), 0.0);
+  std::copy(ea.begin(), ea.end(), L.ecoef.begin());
+  std::copy(eb.begin(), eb.end(), L.ecoef.begin() + ne);
+  std::copy(ec.begin(), ec.end(), L.ecoef.begin() + 2 * ne);
+}
+
+// Per segment: the basis functions with support on it, ascending basis (the
+// accumulation order of get_current_coefficients).  ccoef = a | b | c.
+struct CoefLists {
+  std::vector<int32_t> cptr, cbasis;
+  std::vector<double> ccoef;
+};
+void build_coef_lists(const necgpu_structure* s, int64_t n, CoefLists& C) {
+  const int32_t* tp = s->trio_ptr;
+  const int64_t ntrio = tp[n];
+  C.cptr.assign(n + 1, 0);
+  C.cbasis.assign(std::max<int64_t>(ntrio, 1), 0);
+  C.ccoef.assign(3 * std::max<int64_t>(ntrio, 1), 0.0);
+  std::vector<int> order;
+  for (int64_t j = 0; j < n; j++) {
+    order.clear();
+    for (int32_t k = tp[j]; k < tp[j + 1]; k++) order.push_back(k);
+    std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return s->trio_basis[p] < s->trio_basis[q]; });
+    C.cptr[j] = tp[j];
+    for (size_t q = 0; q < order.size(); q++) {
+      const int k = order[q];
+      C.cbasis[tp[j] + q] = s->trio_basis[k];
+      C.ccoef[tp[j] + q] = s->trio_a[k];
+      C.ccoef[ntrio + tp[j] + q] = s->trio_b[k];
+      C.ccoef[2 * ntrio + tp[j] + q] = s->trio_c[k];
+    }
+  }
+  C.cptr[n] = tp[n];
+}
+
+}  // namespace
+
 extern "C" {
 
 int necgpu_create(necgpu_engine** out, int device) {
@@ -1023,6 +1219,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   e->factored = -1;
   e->filled = false;
   e->have_solution = false;
+  e->adj_ready = false;
   dfree(e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
 
   std::vector<double> seg(8 * n);
@@ -1052,72 +1249,26 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
     if (s->trio_basis[k] < 0 || s->trio_basis[k] >= n)
       return fail(e, NECGPU_ERR_ARG, "set_structure: basis index out of range");
 
-  // column tiles: for every tile, the distinct contributing sources
-  // (ascending) and their (column, a, b, c) entries
   const int ntiles = (int)((n + kFillTB - 1) / kFillTB);
   e->ntiles = ntiles;
-  struct Ent {
-    int32_t j;
-    uint8_t col;
-    double a, b, c;
-  };
-  std::vector<std::vector<Ent>> tiles(ntiles);
-  for (int64_t j = 0; j < n; j++)
-    for (int32_t k = tp[j]; k < tp[j + 1]; k++) {
-      int32_t bas = s->trio_basis[k];
-      tiles[bas / kFillTB].push_back(
-          Ent{(int32_t)j, (uint8_t)(bas % kFillTB), s->trio_a[k], s->trio_b[k], s->trio_c[k]});
-    }
-  std::vector<int32_t> tile_ptr(ntiles + 1), tsrc, tsrc_eptr;
-  std::vector<uint8_t> ecol;
-  std::vector<double> ea, eb, ec;
-  for (int t = 0; t < ntiles; t++) {
-    auto& v = tiles[t];  // pushed in ascending source order
-    tile_ptr[t] = (int32_t)tsrc.size();
-    size_t k = 0;
-    while (k < v.size()) {
-      const int32_t j = v[k].j;
-      tsrc.push_back(j);
-      tsrc_eptr.push_back((int32_t)ecol.size());
-      while (k < v.size() && v[k].j == j) {
-        ecol.push_back(v[k].col);
-        ea.push_back(v[k].a);
-        eb.push_back(v[k].b);
-        ec.push_back(v[k].c);
-        k++;
-      }
-    }
-  }
-  tile_ptr[ntiles] = (int32_t)tsrc.size();
-  tsrc_eptr.push_back((int32_t)ecol.size());
+  TileLists TL;
+  build_tile_lists(s, n, ntiles, TL);
+  const std::vector<int32_t>& tile_ptr = TL.tile_ptr;
+  const std::vector<int32_t>& tsrc = TL.tsrc;
+  const std::vector<int32_t>& tsrc_eptr = TL.tsrc_eptr;
+  const std::vector<uint8_t>& ecol = TL.ecol;
   e->ne = (int64_t)ecol.size();
-  std::vector<double> ecoef(3 * std::max<int64_t>(e->ne, 1));
-  std::copy(ea.begin(), ea.end(), ecoef.begin());
-  std::copy(eb.begin(), eb.end(), ecoef.begin() + e->ne);
-  std::copy(ec.begin(), ec.end(), ecoef.begin() + 2 * e->ne);
-
-  // per segment: basis functions with support on it, ascending basis
+  const std::vector<double>& ecoef = TL.ecoef;
+  CoefLists CL;
+  build_coef_lists(s, n, CL);
   e->nc = ntrio;
-  std::vector<int32_t> cptr(n + 1), cbasis(std::max<int64_t>(ntrio, 1));
-  std::vector<double> ccoef(3 * std::max<int64_t>(ntrio, 1));
-  {
-    std::vector<int> order;
-    for (int64_t j = 0; j < n; j++) {
-      order.clear();
-      for (int32_t k = tp[j]; k < tp[j + 1]; k++) order.push_back(k);
-      std::stable_sort(order.begin(), order.end(),
-                       [&](int p, int q) { return s->trio_basis[p] < s->trio_basis[q]; });
-      cptr[j] = tp[j];
-      for (size_t q = 0; q < order.size(); q++) {
-        const int k = order[q];
-        cbasis[tp[j] + q] = s->trio_basis[k];
-        ccoef[tp[j] + q] = s->trio_a[k];
-        ccoef[ntrio + tp[j] + q] = s->trio_b[k];
-        ccoef[2 * ntrio + tp[j] + q] = s->trio_c[k];
-      }
-    }
-    cptr[n] = tp[n];
-  }
+  const std::vector<int32_t>& cptr = CL.cptr;
+  const std::vector<int32_t>& cbasis = CL.cbasis;
+  const std::vector<double>& ccoef = CL.ccoef;
+  // kept to check perturbed structures (adjoint gradients) against this one
+  e->h_tptr.assign(tp, tp + n + 1);
+  e->h_tbasis.assign(s->trio_basis, s->trio_basis + ntrio);
+  e->h_ind = ind;
 
   TRY(upload(e, e->d_seg, seg.data(), seg.size()));
   TRY(upload(e, e->d_ind, ind.data(), ind.size()));
@@ -1305,6 +1456,210 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
   dfree(Y);
   dfree(d);
   return rc;
+}
+
+int necgpu_copy_solution(necgpu_engine* e, double* x) {
+  if (!e || !x) return NECGPU_ERR_ARG;
+  if (!e->have_solution) return fail(e, NECGPU_ERR_ARG, "copy_solution: no solution held");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaMemcpyAsync(x, e->d_x, e->n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->stats.d2h_bytes += e->n * sizeof(double2);
+  return NECGPU_OK;
+}
+
+int necgpu_adjoint_solve(necgpu_engine* e, int nrhs, const double* phi, double* w) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (nrhs < 1 || !phi || !w) return fail(e, NECGPU_ERR_ARG, "adjoint: bad arguments");
+  CUDA_TRY(cudaSetDevice(e->device));
+  TRY(ensure_adjoint(e));
+  const int64_t n = e->n;
+  if (nrhs > e->adj_cap || !e->d_adj_r) {
+    TRY(dalloc(e, e->d_adj_phi, (size_t)nrhs * n));
+    TRY(dalloc(e, e->d_adj_w, (size_t)nrhs * n));
+    TRY(dalloc(e, e->d_adj_r, (size_t)n));
+    e->adj_cap = nrhs;
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_adj_phi, phi, (size_t)nrhs * n * sizeof(double2), cudaMemcpyHostToDevice, e->stream));
+  e->stats.h2d_bytes += (int64_t)nrhs * n * sizeof(double2);
+  CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+  for (int k = 0; k < nrhs; k++) {
+    int it = 0;
+    double rel = 0.0;
+    TRY(refine_T(e, e->d_adj_phi + (int64_t)k * n, e->d_adj_w + (int64_t)k * n, &it, &rel));
+    e->stats.refine_iters = it;
+    e->stats.refine_residual = rel;
+    if (rel > 1e-6) return fail(e, NECGPU_ERR_REFINE, "adjoint: refinement did not converge");
+  }
+  CUDA_TRY(cudaMemcpyAsync(w, e->d_adj_w, (size_t)nrhs * n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  e->stats.d2h_bytes += (int64_t)nrhs * n * sizeof(double2);
+  int st = 0;
+  TRY(sync_status(e, &st));
+  if (st & (1 << 9)) return fail(e, NECGPU_ERR_CUDA, "adjoint: triangular sweep gave up waiting on a block");
+  return NECGPU_OK;
+}
+
+int necgpu_pattern_weights(necgpu_engine* e, double theta, double phi, double* phi_t, double* phi_p) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (!phi_t || !phi_p) return fail(e, NECGPU_ERR_ARG, "pattern_weights: null argument");
+  if (e->n <= 0) return fail(e, NECGPU_ERR_ARG, "pattern_weights: no structure set");
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int64_t n = e->n;
+  if (!e->d_pwts) TRY(dalloc(e, e->d_pwts, 2 * (size_t)n));
+  CUDA_TRY(cudaMemsetAsync(e->d_pwts, 0, 2 * n * sizeof(double2), e->stream));
+  const FarDir d = engine_far_dir(e, theta, phi);
+  double* pt = reinterpret_cast<double*>(e->d_pwts);
+  KLAUNCH(NECGPU_K_PATTERN, (double)n * d.ksymp,
+          pattern_weights_kernel<<<(unsigned)((n + 127) / 128), 128, 0, e->stream>>>(
+              n, d, e->d_seg, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc, e->d_ccoef + 2 * e->nc, pt,
+              pt + 2 * n));
+  CUDA_TRY(cudaMemcpyAsync(phi_t, e->d_pwts, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(phi_p, e->d_pwts + n, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+  e->stats.d2h_bytes += 2 * n * sizeof(double2);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  kflush(e);
+  return NECGPU_OK;
+}
+
+int necgpu_perturbed_terms(necgpu_engine* e, int nstruct, const necgpu_structure* structs, int nw, const double* w,
+                           double theta, double phi, double* zx, double* efar) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (nstruct < 1 || nstruct > 65535 || !structs || nw < 0 || nw > kMaxContract || (nw > 0 && (!w || !zx)) || !efar)
+    return fail(e, NECGPU_ERR_ARG, "perturbed_terms: bad arguments");
+  if (!e->have_solution) return fail(e, NECGPU_ERR_ARG, "perturbed_terms: no solution held");
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int64_t n = e->n, ne = e->ne, nc = e->nc;
+  // every perturbed structure must share the held one's table layout and medium
+  std::vector<double> seg((size_t)nstruct * 8 * n), pe((size_t)nstruct * 3 * std::max<int64_t>(ne, 1)),
+      pc((size_t)nstruct * 3 * std::max<int64_t>(nc, 1));
+  for (int q = 0; q < nstruct; q++) {
+    const necgpu_structure* s = structs + q;
+    if (s->n != n) return fail(e, NECGPU_ERR_ARG, "perturbed_terms: segment count differs from the held structure");
+    if (s->ground != e->ground || (s->use_exk != 0) != (e->use_exk != 0) || s->rkh != e->P.rkh ||
+        s->eta != e->P.eta || s->zrati_re != e->P.zrati.re || s->zrati_im != e->P.zrati.im ||
+        s->frati_re != e->P.frati.re || s->frati_im != e->P.frati.im)
+      return fail(e, NECGPU_ERR_ARG, "perturbed_terms: medium, ground or kernel settings differ from the held structure");
+    if (!std::equal(s->trio_ptr, s->trio_ptr + n + 1, e->h_tptr.begin()) ||
+        !std::equal(s->trio_basis, s->trio_basis + e->h_tptr[n], e->h_tbasis.begin()))
+      return fail(e, NECGPU_ERR_ARG, "perturbed_terms: basis-table layout differs from the held structure");
+    if (s->ek_ind1 && s->ek_ind2)
+      for (int64_t i = 0; i < n; i++)
+        if (s->ek_ind1[i] != e->h_ind[i] || s->ek_ind2[i] != e->h_ind[n + i])
+          return fail(e, NECGPU_ERR_ARG, "perturbed_terms: extended-kernel end flags differ from the held structure");
+    double* g = seg.data() + (size_t)q * 8 * n;
+    const double* src[8] = {s->x, s->y, s->z, s->length, s->radius, s->cab, s->sab, s->salp};
+    for (int a = 0; a < 8; a++) std::copy(src[a], src[a] + n, g + (size_t)a * n);
+    TileLists TL;
+    build_tile_lists(s, n, e->ntiles, TL);
+    if ((int64_t)TL.ecol.size() != ne) return fail(e, NECGPU_ERR_ARG, "perturbed_terms: tile layout differs");
+    std::copy(TL.ecoef.begin(), TL.ecoef.end(), pe.begin() + (size_t)q * 3 * std::max<int64_t>(ne, 1));
+    CoefLists CL;
+    build_coef_lists(s, n, CL);
+    std::copy(CL.ccoef.begin(), CL.ccoef.end(), pc.begin() + (size_t)q * 3 * std::max<int64_t>(nc, 1));
+  }
+  const size_t pes = 3 * std::max<int64_t>(ne, 1), pcs = 3 * std::max<int64_t>(nc, 1);
+  if (nstruct > e->p_cap) {
+    TRY(dalloc(e, e->d_pseg, (size_t)nstruct * 8 * n));
+    TRY(dalloc(e, e->d_pecoef, (size_t)nstruct * pes));
+    TRY(dalloc(e, e->d_pccoef, (size_t)nstruct * pcs));
+    TRY(dalloc(e, e->d_pout, (size_t)nstruct * 2 * kMaxContract));
+    TRY(dalloc(e, e->d_pfar, (size_t)nstruct * 2));
+    TRY(dalloc(e, e->d_pargs, (size_t)nstruct));
+    TRY(dalloc(e, e->d_pcargs, (size_t)nstruct));
+    e->p_cap = nstruct;
+  }
+  if (nw > e->pw_cap || !e->d_pw) {
+    TRY(dalloc(e, e->d_pw, (size_t)std::max(nw, 1) * n));
+    e->pw_cap = std::max(nw, 1);
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_pseg, seg.data(), seg.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_pecoef, pe.data(), pe.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_pccoef, pc.data(), pc.size() * sizeof(double), cudaMemcpyHostToDevice, e->stream));
+  if (nw > 0)
+    CUDA_TRY(cudaMemcpyAsync(e->d_pw, w, (size_t)nw * n * sizeof(double2), cudaMemcpyHostToDevice, e->stream));
+  e->stats.h2d_bytes += (int64_t)(seg.size() + pe.size() + pc.size()) * sizeof(double) + (int64_t)nw * n * 16;
+  std::vector<FillArgs> fa(nstruct);
+  std::vector<ContractArgs> ca(nstruct);
+  for (int q = 0; q < nstruct; q++) {
+    FillArgs& a = fa[q];
+    const double* g = e->d_pseg + (size_t)q * 8 * n;
+    a.n = n;
+    a.ld = e->ld;
+    a.x = g;
+    a.y = g + n;
+    a.z = g + 2 * n;
+    a.s = g + 3 * n;
+    a.b = g + 4 * n;
+    a.cab = g + 5 * n;
+    a.sab = g + 6 * n;
+    a.salp = g + 7 * n;
+    a.ind1 = e->d_ind;
+    a.ind2 = e->d_ind + n;
+    a.tile_src_ptr = e->d_tile_ptr;
+    a.tsrc = e->d_tsrc;
+    a.tsrc_eptr = e->d_tsrc_eptr;
+    a.ecol = e->d_ecol;
+    const double* c = e->d_pecoef + (size_t)q * pes;
+    a.ea = c;
+    a.eb = c + ne;
+    a.ec = c + 2 * ne;
+    a.P = e->P;
+    a.Z64 = nullptr;
+    a.Z32 = nullptr;
+    a.status = e->d_status;
+    ca[q].x = e->d_x;
+    ca[q].w = e->d_pw;
+    ca[q].nw = nw;
+    ca[q].out = e->d_pout + (size_t)q * 2 * kMaxContract;
+  }
+  CUDA_TRY(cudaMemcpyAsync(e->d_pargs, fa.data(), fa.size() * sizeof(FillArgs), cudaMemcpyHostToDevice, e->stream));
+  CUDA_TRY(cudaMemcpyAsync(e->d_pcargs, ca.data(), ca.size() * sizeof(ContractArgs), cudaMemcpyHostToDevice,
+                           e->stream));
+  CUDA_TRY(cudaMemsetAsync(e->d_pout, 0, (size_t)nstruct * 2 * kMaxContract * sizeof(double), e->stream));
+  CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+  if (nw > 0) {
+    const dim3 grid((unsigned)((n + kFillTI - 1) / kFillTI), (unsigned)e->ntiles, (unsigned)nstruct);
+    const bool xk = e->use_exk != 0;
+#define NECB_CONTRACT(G)                                                                                      \
+  (xk ? (fill_contract_kernel<G, true><<<grid, kFillTI, 0, e->stream>>>(e->d_pargs, e->d_pcargs), 0)           \
+      : (fill_contract_kernel<G, false><<<grid, kFillTI, 0, e->stream>>>(e->d_pargs, e->d_pcargs), 0))
+    switch (e->ground) {
+      case kGroundNone: KLAUNCH(NECGPU_K_FILL, (double)nstruct * n * n, NECB_CONTRACT(kGroundNone)); break;
+      case kGroundPerfect: KLAUNCH(NECGPU_K_FILL, (double)nstruct * n * n, NECB_CONTRACT(kGroundPerfect)); break;
+      case kGroundReflection:
+        KLAUNCH(NECGPU_K_FILL, (double)nstruct * n * n, NECB_CONTRACT(kGroundReflection));
+        break;
+      default: KLAUNCH(NECGPU_K_FILL, (double)nstruct * n * n, NECB_CONTRACT(kGroundSommerfeld)); break;
+    }
+#undef NECB_CONTRACT
+  }
+  const FarDir d = engine_far_dir(e, theta, phi);
+  KLAUNCH(NECGPU_K_PATTERN, (double)nstruct * n * d.ksymp,
+          far_batch_kernel<<<(unsigned)nstruct, kFarBatchThreads, 0, e->stream>>>(
+              n, nc, d, e->d_pseg, e->d_cptr, e->d_cbasis, e->d_pccoef, e->d_x, e->d_pfar));
+  if (nw > 0) {
+    std::vector<double> out((size_t)nstruct * 2 * kMaxContract);
+    CUDA_TRY(cudaMemcpyAsync(out.data(), e->d_pout, out.size() * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(efar, e->d_pfar, (size_t)nstruct * 2 * sizeof(double2), cudaMemcpyDeviceToHost,
+                             e->stream));
+    int st = 0;
+    TRY(sync_status(e, &st));
+    for (int q = 0; q < nstruct; q++)
+      for (int k = 0; k < nw; k++) {
+        zx[((size_t)q * nw + k) * 2] = out[(size_t)q * 2 * kMaxContract + 2 * k];
+        zx[((size_t)q * nw + k) * 2 + 1] = out[(size_t)q * 2 * kMaxContract + 2 * k + 1];
+      }
+    if (st & kStatSommerfeldTab)
+      return fail(e, NECGPU_ERR_UNSUPPORTED, "perturbed_terms: a segment pair needs the Sommerfeld table path");
+    if (st & kStatIterCap) return fail(e, NECGPU_ERR_NONFINITE, "perturbed_terms: quadrature did not terminate");
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(efar, e->d_pfar, (size_t)nstruct * 2 * sizeof(double2), cudaMemcpyDeviceToHost,
+                             e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+  }
+  e->stats.d2h_bytes += (int64_t)nstruct * (2 * kMaxContract * 8 + 32);
+  kflush(e);
+  return NECGPU_OK;
 }
 
 int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph) {

@@ -39,11 +39,21 @@ struct FillArgs {
   int* status;
 };
 
-template <int GROUND, bool EXK>
-__global__ void __launch_bounds__(kFillTI) fill_kernel(FillArgs A) {
+// Contraction instead of storage (adjoint gradients): out[k] +=
+// w_k^T Z x over this structure's Z, for nw vectors w_k (n complex each).
+struct ContractArgs {
+  const double2* x;  // n
+  const double2* w;  // nw x n
+  int nw;
+  double* out;       // nw complex
+};
+constexpr int kMaxContract = 4;
+
+// One tile of Z: rows [row0, row0+64) x basis columns of column tile `tile`.
+// CONTRACT = false stores the tile (Z64 / Z32); true folds it into C.out.
+template <int GROUND, bool EXK, bool CONTRACT>
+__device__ __forceinline__ void fill_tile(const FillArgs& A, const ContractArgs& C, int tile, int64_t row0) {
   __shared__ double2 acc[kFillTB][kFillTI + 1];
-  const int tile = blockIdx.y;
-  const int64_t row0 = (int64_t)blockIdx.x * kFillTI;
   const int tid = threadIdx.x;
   const int64_t i = row0 + tid;
   const bool active = i < A.n;
@@ -92,8 +102,38 @@ __global__ void __launch_bounds__(kFillTI) fill_kernel(FillArgs A) {
   }
   if (status) atomicOr(A.status, status);
   __syncthreads();
-  // write out: one warp per row, lanes along the (contiguous) columns
   const int lane = tid & 31, warp = tid >> 5;
+  if (CONTRACT) {
+    // row i: t = sum_c Z[i][col0+c] x[col0+c]; out[k] += w_k[i] t
+    double tr = 0, ti = 0;
+    if (active) {
+      const int64_t col0 = (int64_t)tile * kFillTB;
+      for (int c = 0; c < kFillTB && col0 + c < A.n; c++) {
+        const double2 z = acc[c][tid], xv = C.x[col0 + c];
+        tr += z.x * xv.x - z.y * xv.y;
+        ti += z.x * xv.y + z.y * xv.x;
+      }
+    }
+    for (int k = 0; k < C.nw; k++) {
+      double pr = 0, pi = 0;
+      if (active) {
+        const double2 wv = C.w[(int64_t)k * A.n + i];
+        pr = wv.x * tr - wv.y * ti;
+        pi = wv.x * ti + wv.y * tr;
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        pr += __shfl_down_sync(0xffffffffu, pr, off);
+        pi += __shfl_down_sync(0xffffffffu, pi, off);
+      }
+      if (lane == 0) {
+        atomicAdd(C.out + 2 * k, pr);
+        atomicAdd(C.out + 2 * k + 1, pi);
+      }
+    }
+    return;
+  }
+  // write out: one warp per row, lanes along the (contiguous) columns
   const int64_t col = (int64_t)tile * kFillTB + lane;
   for (int r = warp; r < kFillTI; r += kFillTI / 32) {
     const int64_t row = row0 + r;
@@ -103,6 +143,19 @@ __global__ void __launch_bounds__(kFillTI) fill_kernel(FillArgs A) {
       if (A.Z32) A.Z32[row * A.ld + col] = make_float2((float)v.x, (float)v.y);
     }
   }
+}
+
+template <int GROUND, bool EXK>
+__global__ void __launch_bounds__(kFillTI) fill_kernel(FillArgs A) {
+  fill_tile<GROUND, EXK, false>(A, ContractArgs{}, blockIdx.y, (int64_t)blockIdx.x * kFillTI);
+}
+
+// Batched fill of perturbed structures (blockIdx.z), each contracted with
+// its own output slot: out_s[k] = w_k^T Z_s x.
+template <int GROUND, bool EXK>
+__global__ void __launch_bounds__(kFillTI) fill_contract_kernel(const FillArgs* __restrict__ As,
+                                                                const ContractArgs* __restrict__ Cs) {
+  fill_tile<GROUND, EXK, true>(As[blockIdx.z], Cs[blockIdx.z], blockIdx.y, (int64_t)blockIdx.x * kFillTI);
 }
 
 }  // namespace necb

@@ -547,4 +547,47 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
   }
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint (transposed) solves on the same factors.  With P A = L U,
+//   A^T w = phi  <=>  U^T L^T (P w) = phi,
+// so the transposed factors M^T (lower part U^T, upper part L^T) and the
+// transposed inverted diagonal blocks drive the same sweeps, and the result
+// is scattered back through the permutation.
+
+// B = A^T for the n x n leading block (row-major, leading dims lda, ldb)
+template <typename T>
+__global__ void __launch_bounds__(256) transpose_kernel(const T* A, int64_t lda, T* B, int64_t ldb, int64_t n) {
+  __shared__ T tile[32][33];
+  const int64_t r0 = (int64_t)blockIdx.y * 32, c0 = (int64_t)blockIdx.x * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  for (int r = ty; r < 32; r += 8)
+    if (r0 + r < n && c0 + tx < n) tile[r][tx] = A[(r0 + r) * lda + c0 + tx];
+  __syncthreads();
+  for (int c = ty; c < 32; c += 8)
+    if (c0 + c < n && r0 + tx < n) B[(c0 + c) * ldb + r0 + tx] = tile[tx][c];
+}
+
+// tinvT[2b] = (U_bb^-1)^T, tinvT[2b+1] = (L_bb^-1)^T: the lower- and
+// upper-triangle inverses of the transposed factors
+__global__ void __launch_bounds__(256) tinv_transpose_kernel(const float2* tinv, float2* tinvT) {
+  constexpr int NB = kBlk;
+  const float2* in = tinv + (int64_t)blockIdx.x * 2 * NB * NB;
+  float2* out = tinvT + (int64_t)blockIdx.x * 2 * NB * NB;
+  for (int e = threadIdx.x; e < NB * NB; e += 256) {
+    const int r = e / NB, c = e % NB;
+    out[e] = in[NB * NB + c * NB + r];
+    out[NB * NB + e] = in[c * NB + r];
+  }
+}
+
+// x[perm[i]] += d[i]   (x += P^T d)
+__global__ void axpy_scatter_kernel(double2* x, const float2* d, const int* perm, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double2 v = x[perm[i]];
+  v.x += (double)d[i].x;
+  v.y += (double)d[i].y;
+  x[perm[i]] = v;
+}
+
 }  // namespace necb

@@ -139,3 +139,27 @@ def yagi_ground(api, ctx, seed=0):
     return yagi(api, ctx, params, height=10.0, nfreq=1, f0=145.0, df=0.0,
                 ground=(2, 0, 13.0, 0.005, 0.0, 0.0, 0.0, 0.0),
                 pattern=(0, 1, 1, 1, 0, 0, 0, 80.0, 0.0, 0.0, 0.0, 0.0, 0.0))
+
+
+def yagi_ground_cards(api, ctx, p, nseg=21, height=10.0, ground=(2, 0, 13.0, 0.005, 0.0, 0.0, 0.0, 0.0)):
+    """Cards of the 9-element Yagi over Sommerfeld ground without frequency
+    or solve: p = (half lengths [m], x positions [m], radii [m]), element 2
+    centre-fed with 1 V.  For adjoint gradients (necpp_b200.adjoint)."""
+    c = lambda r, w: _check(api, ctx, r, w)
+    p = np.asarray(p, dtype=float)
+    ne = len(p) // 3
+    half, xs, rad = p[:ne], p[ne:2 * ne], p[2 * ne:]
+    for e in range(ne):
+        c(api.nec_wire(ctx, e + 1, nseg, float(xs[e]), 0.0, height - float(half[e]), float(xs[e]), 0.0,
+                       height + float(half[e]), float(rad[e]), 1.0, 1.0), "wire")
+    c(api.nec_geometry_complete(ctx, 0), "geometry_complete")
+    if ground is not None:
+        c(api.nec_gn_card(ctx, *ground), "gn")
+    c(api.nec_ex_card(ctx, 0, 2, (nseg + 1) // 2, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0), "ex")
+    return ne * nseg
+
+
+def yagi_ground_params(seed=0):
+    """The 27 parameters of the seeded 9-element Yagi (config of yagi_ground)."""
+    half, xs, rad, _ = yagi_params(np.random.default_rng(seed), n_elements=9, nseg=21)
+    return np.concatenate([half, xs, rad])
