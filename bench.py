@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-gradient", action="store_true")
     return p.parse_args()
 
 
@@ -198,6 +199,46 @@ K_BOUND = {"fill": ("compute", "pair evaluations"), "lu_gemm": ("tensor", "flops
            "lu_panel": ("latency", "flops"), "lu_trsm": ("compute", "flops"),
            "trsv": ("hbm", "bytes"), "refine_residual": ("hbm", "bytes"),
            "pattern": ("compute", "terms"), "lu_laswp": ("hbm", "bytes"), "other": ("hbm", "bytes")}
+
+
+def gradient_cost(nb, W, reps=5):
+    """grad/fwd cost on the adjoint workload: the seeded 9-element Yagi, 21
+    segments per element, 10 m over Sommerfeld ground, 145 MHz; outputs Re Zin,
+    Im Zin and gain at theta 80, phi 0; 27 parameters.  forward = one solve
+    through the C API with the gain direction (cards, fill, factorisation,
+    solve, far field); gradient = all 27 x 3 derivatives after it (perturbed
+    structures, 3 transposed solves, contracted perturbed fills, assembly).
+    Wall clock of the synchronous API calls, median of `reps`."""
+    from necpp_b200 import adjoint
+    p = W.yagi_ground_params(0)
+    build = lambda ctx, q: W.yagi_ground_cards(nb, ctx, q)
+
+    def forward():
+        t0 = time.perf_counter()
+        ctx = nb.nec_create()
+        nb.nec_set_precision(ctx, 1)
+        build(ctx, p)
+        nb.nec_fr_card(ctx, 0, 1, 145.0, 0.0)
+        if nb.nec_rp_card(ctx, 0, 1, 1, 1, 0, 0, 0, 80.0, 0.0, 0.0, 0.0, 0.0, 0.0) != 0:
+            raise RuntimeError(nb.nec_error_message())
+        g = nb.nec_gain(ctx, 0, 0, 0)
+        dt = time.perf_counter() - t0
+        nb.nec_delete(ctx)
+        return dt, g
+
+    forward()
+    adjoint.gradient(build, p, 145.0, 80.0, 0.0)  # warm-up
+    fw, gr = [], []
+    for _ in range(reps):
+        fw.append(forward()[0])
+        tm = {}
+        value, jac = adjoint.gradient(build, p, 145.0, 80.0, 0.0, timings=tm)
+        gr.append(tm["gradient_s"])
+    f, g = statistics.median(fw), statistics.median(gr)
+    return {"workload": "yagi9 over Sommerfeld ground, N=189, 145 MHz, 27 params x (Re Zin, Im Zin, gain)",
+            "forward_ms": f * 1e3, "gradient_ms": g * 1e3, "grad_fwd_cost": g / f,
+            "value": [float(v) for v in value], "timing": "wall clock of the synchronous C-API calls, median of %d"
+            % reps}
 
 
 def run_b200(args):
@@ -396,6 +437,9 @@ def run_b200(args):
         rel = np.abs(z_mixed - z_fp64) / np.abs(z_fp64)
         line["zin_rel_err_mixed_vs_fp64"] = float(np.max(rel))
     line.update(out)
+
+    if rank == 0 and not args.no_gradient:
+        line["gradient"] = gradient_cost(nb, W)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refwrap

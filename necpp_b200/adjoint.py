@@ -26,18 +26,25 @@ def _check(rc, what):
         raise RuntimeError("%s: %s" % (what, nec_error_message()))
 
 
-def gradient(build, params, freq_mhz, theta_deg, phi_deg, h=1e-6):
+def gradient(build, params, freq_mhz, theta_deg, phi_deg, h=1e-6, timings=None):
+    """See the module docstring.  If `timings` is a dict it receives the
+    wall-clock seconds of the forward solve ('forward_s': cards, fill,
+    factorisation, solve) and of everything after it ('gradient_s':
+    perturbed structures, adjoint solves, contractions, assembly)."""
+    import time
     p = _np.asarray(params, dtype=_np.float64)
     npar = len(p)
     hs = _np.broadcast_to(_np.asarray(h, dtype=_np.float64), (npar,)).copy()
     ctxs = []
     try:
+        t0 = time.perf_counter()
         base = nec_create()
         ctxs.append(base)
         _check(nec_set_precision(base, 1), "set_precision")
         build(base, p)
         _check(nec_fr_card(base, 0, 1, float(freq_mhz), 0.0), "fr card")
         _check(nec_xq_card(base, 0), "forward solve")
+        t1 = time.perf_counter()
         plus, minus = [], []
         for k in range(npar):
             for sign, lst in ((1.0, plus), (-1.0, minus)):
@@ -54,6 +61,9 @@ def gradient(build, params, freq_mhz, theta_deg, phi_deg, h=1e-6):
         _check(lib.nec_gradient(base, npar, parr, marr, hs.ctypes.data_as(_C.POINTER(_C.c_double)),
                                 float(theta_deg), float(phi_deg), value.ctypes.data_as(_C.POINTER(_C.c_double)),
                                 grad.ctypes.data_as(_C.POINTER(_C.c_double))), "gradient")
+        if timings is not None:
+            timings["forward_s"] = t1 - t0
+            timings["gradient_s"] = time.perf_counter() - t1
         return value, grad.reshape(npar, 3).T.copy()
     finally:
         for c in ctxs:

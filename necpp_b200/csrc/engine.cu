@@ -217,21 +217,25 @@ void kflush(necgpu_engine* e) {  // call after the stream has synchronised
     LAUNCHED();                         \
   } while (0)
 
+// Device buffers are stream-ordered allocations from the device's default
+// memory pool, whose release threshold necgpu_create raises: memory freed by
+// one engine (or one structure size) stays in the pool and serves the next
+// allocation instead of being handed back to the driver and mapped again.
 template <typename T>
-void dfree(T*& p) {
-  if (p) cudaFree((void*)p);
+void dfree(necgpu_engine* e, T*& p) {
+  if (p) cudaFreeAsync((void*)p, e->stream);
   p = nullptr;
 }
 
 template <typename T>
 int dalloc(necgpu_engine* e, T*& p, size_t count) {
-  dfree(p);
+  dfree(e, p);
   if (count == 0) count = 1;
-  cudaError_t st = cudaMalloc((void**)&p, count * sizeof(T));
+  cudaError_t st = cudaMallocAsync((void**)&p, count * sizeof(T), e->stream);
   if (st != cudaSuccess) {
     p = nullptr;
     return fail(e, NECGPU_ERR_CUDA,
-                std::string("cudaMalloc(") + std::to_string(count * sizeof(T)) + "): " + cudaGetErrorString(st));
+                std::string("cudaMallocAsync(") + std::to_string(count * sizeof(T)) + "): " + cudaGetErrorString(st));
   }
   return 0;
 }
@@ -245,63 +249,63 @@ int upload(necgpu_engine* e, T*& p, const T* h, size_t count) {
 }
 
 void free_all(necgpu_engine* e) {
-  dfree(e->d_seg);
-  dfree(e->d_ind);
-  dfree(e->d_tile_ptr);
-  dfree(e->d_tsrc);
-  dfree(e->d_tsrc_eptr);
-  dfree(e->d_ecol);
-  dfree(e->d_ecoef);
-  dfree(e->d_cptr);
-  dfree(e->d_cbasis);
-  dfree(e->d_ccoef);
-  dfree(e->Z64);
-  dfree(e->d_dinv);
-  dfree(e->d_tinv);
-  dfree(e->d_sweep_ctr);
-  dfree(e->ZT32);
-  dfree(e->ZT64);
-  dfree(e->d_tinvT);
-  dfree(e->d_adj_phi);
-  dfree(e->d_adj_w);
-  dfree(e->d_adj_r);
+  dfree(e, e->d_seg);
+  dfree(e, e->d_ind);
+  dfree(e, e->d_tile_ptr);
+  dfree(e, e->d_tsrc);
+  dfree(e, e->d_tsrc_eptr);
+  dfree(e, e->d_ecol);
+  dfree(e, e->d_ecoef);
+  dfree(e, e->d_cptr);
+  dfree(e, e->d_cbasis);
+  dfree(e, e->d_ccoef);
+  dfree(e, e->Z64);
+  dfree(e, e->d_dinv);
+  dfree(e, e->d_tinv);
+  dfree(e, e->d_sweep_ctr);
+  dfree(e, e->ZT32);
+  dfree(e, e->ZT64);
+  dfree(e, e->d_tinvT);
+  dfree(e, e->d_adj_phi);
+  dfree(e, e->d_adj_w);
+  dfree(e, e->d_adj_r);
   e->adj_cap = 0;
   e->adj_ready = false;
-  dfree(e->d_pseg);
-  dfree(e->d_pecoef);
-  dfree(e->d_pccoef);
-  dfree(e->d_pout);
-  dfree(e->d_pw);
-  dfree(e->d_pfar);
-  dfree(e->d_pargs);
-  dfree(e->d_pcargs);
-  dfree(e->d_pwts);
+  dfree(e, e->d_pseg);
+  dfree(e, e->d_pecoef);
+  dfree(e, e->d_pccoef);
+  dfree(e, e->d_pout);
+  dfree(e, e->d_pw);
+  dfree(e, e->d_pfar);
+  dfree(e, e->d_pargs);
+  dfree(e, e->d_pcargs);
+  dfree(e, e->d_pwts);
   e->p_cap = 0;
   e->pw_cap = 0;
-  dfree(e->Z32);
-  dfree(e->d_piv);
-  dfree(e->d_perm);
-  dfree(e->d_cand_val);
-  dfree(e->d_cand_valf);
-  dfree(e->d_cand_row);
-  dfree(e->d_cand_rows);
-  dfree(e->d_rowc);
-  dfree(e->d_counter);
-  dfree(e->d_b);
-  dfree(e->d_x);
-  dfree(e->d_r);
-  dfree(e->d_cur);
-  dfree(e->d_w1);
-  dfree(e->d_w2);
-  dfree(e->d_abc);
-  dfree(e->d_rn2);
-  dfree(e->d_theta);
-  dfree(e->d_phi);
-  dfree(e->d_eth);
-  dfree(e->d_eph);
-  dfree(e->d_flags);
-  dfree(e->d_Ap);
-  dfree(e->d_Bp);
+  dfree(e, e->Z32);
+  dfree(e, e->d_piv);
+  dfree(e, e->d_perm);
+  dfree(e, e->d_cand_val);
+  dfree(e, e->d_cand_valf);
+  dfree(e, e->d_cand_row);
+  dfree(e, e->d_cand_rows);
+  dfree(e, e->d_rowc);
+  dfree(e, e->d_counter);
+  dfree(e, e->d_b);
+  dfree(e, e->d_x);
+  dfree(e, e->d_r);
+  dfree(e, e->d_cur);
+  dfree(e, e->d_w1);
+  dfree(e, e->d_w2);
+  dfree(e, e->d_abc);
+  dfree(e, e->d_rn2);
+  dfree(e, e->d_theta);
+  dfree(e, e->d_phi);
+  dfree(e, e->d_eth);
+  dfree(e, e->d_eph);
+  dfree(e, e->d_flags);
+  dfree(e, e->d_Ap);
+  dfree(e, e->d_Bp);
   e->tc_rows = 0;
   e->pat_cap = 0;
   e->res_ndir = 0;
@@ -1113,7 +1117,18 @@ int necgpu_create(necgpu_engine** out, int device) {
   e->own_stream = true;
   CUDA_TRY(cudaEventCreate(&e->ev0));
   CUDA_TRY(cudaEventCreate(&e->ev1));
-  CUDA_TRY(cudaMalloc((void**)&e->d_status, 4 * sizeof(int)));
+  {
+    // keep freed device memory in the default pool for reuse (process-local;
+    // NECPP_B200_POOL_RELEASE=1 keeps the driver's default of releasing it)
+    const char* rel = std::getenv("NECPP_B200_POOL_RELEASE");
+    if (!(rel && rel[0] == '1')) {
+      cudaMemPool_t pool;
+      CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
+      uint64_t thr = UINT64_MAX;
+      CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    }
+  }
+  TRY(dalloc(e, e->d_status, 4));
   CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
   return NECGPU_OK;
 }
@@ -1125,7 +1140,7 @@ int necgpu_destroy(necgpu_engine* e) {
     cudaStreamSynchronize(e->stream);
   }
   free_all(e);
-  dfree(e->d_status);
+  dfree(e, e->d_status);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
@@ -1220,7 +1235,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   e->filled = false;
   e->have_solution = false;
   e->adj_ready = false;
-  dfree(e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
+  dfree(e, e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
 
   std::vector<double> seg(8 * n);
   for (int64_t i = 0; i < n; i++) {
@@ -1452,9 +1467,9 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
       *max_abs_ref = h[1];
     }
   }
-  dfree(X);
-  dfree(Y);
-  dfree(d);
+  dfree(e, X);
+  dfree(e, Y);
+  dfree(e, d);
   return rc;
 }
 

@@ -8,6 +8,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
+#include <unordered_map>
+#include <cstdint>
+#include <climits>
 
 #include "nec_constants.h"
 #include "nec_error.h"
@@ -236,6 +239,22 @@ void Geometry::scale(double f) {
 // itself, wrapping round; the first end within SMIN * length (L1 distance)
 // wins.  The sign of the stored index says whether the touching end is of
 // the same kind (negative) or the opposite kind (positive).
+namespace {
+// Endpoints of all segments bucketed on a cubic grid of edge 2 * max(slen):
+// every end within L1 distance slen of a point lies in the 27 cells around
+// the point's cell.  The search below returns what the reference's cyclic
+// scan returns (the first segment after i, wrapping, whose start and then
+// end satisfies the same test), looking only at those cells.
+struct EndGrid {
+  double cell = 0;
+  std::unordered_map<uint64_t, std::vector<int64_t>> cells;  // value: 2 * segment + (0 start, 1 end)
+  static int64_t idx(double v, double cell) { return (int64_t)std::floor(v / cell); }
+  static uint64_t key(int64_t a, int64_t b, int64_t c) {
+    return ((uint64_t)(a & 0x1FFFFF) << 42) | ((uint64_t)(b & 0x1FFFFF) << 21) | (uint64_t)(c & 0x1FFFFF);
+  }
+};
+}  // namespace
+
 void Geometry::build_connections(int ignd) {
   if (ignd != 0) {
     if (ipsym == 2) np = 2 * np;
@@ -245,6 +264,51 @@ void Geometry::build_connections(int ignd) {
   }
   icon1.assign(n, 0);
   icon2.assign(n, 0);
+  // Without a ground plane the coordinates do not change during the search,
+  // so it can use the endpoint grid (the O(N^2) scan dominates card
+  // processing of large structures otherwise).
+  double max_slen = 0.0;
+  for (int64_t i = 0; i < n; i++)
+    max_slen = std::max(max_slen, norm3(sub(V3{x2[i], y2[i], z2[i]}, V3{x[i], y[i], z[i]})) * kSmin);
+  const bool use_grid = ignd == 0 && n > 256 && std::isfinite(max_slen) && max_slen > 0.0;
+  EndGrid grid;
+  if (use_grid) {
+    grid.cell = 2.0 * max_slen;
+    for (int64_t i = 0; i < n; i++) {
+      grid.cells[EndGrid::key(EndGrid::idx(x[i], grid.cell), EndGrid::idx(y[i], grid.cell),
+                              EndGrid::idx(z[i], grid.cell))]
+          .push_back(2 * i);
+      grid.cells[EndGrid::key(EndGrid::idx(x2[i], grid.cell), EndGrid::idx(y2[i], grid.cell),
+                              EndGrid::idx(z2[i], grid.cell))]
+          .push_back(2 * i + 1);
+    }
+  }
+  // first match in the cyclic order i+1, i+2, ..., i-1 (start before end of
+  // the same segment): returns 2 * segment + end, or -1
+  auto grid_first = [&](int64_t i, const V3& v, double slen) -> int64_t {
+    const int64_t cx = EndGrid::idx(v.x, grid.cell), cy = EndGrid::idx(v.y, grid.cell),
+                  cz = EndGrid::idx(v.z, grid.cell);
+    int64_t best = -1, best_rank = INT64_MAX;
+    for (int64_t a = cx - 1; a <= cx + 1; a++)
+      for (int64_t b = cy - 1; b <= cy + 1; b++)
+        for (int64_t c = cz - 1; c <= cz + 1; c++) {
+          auto it = grid.cells.find(EndGrid::key(a, b, c));
+          if (it == grid.cells.end()) continue;
+          for (int64_t code : it->second) {
+            const int64_t ic = code >> 1;
+            if (ic == i) continue;
+            const int end = (int)(code & 1);
+            const V3 p = end == 0 ? V3{x[ic], y[ic], z[ic]} : V3{x2[ic], y2[ic], z2[ic]};
+            if (!(norm_l1(sub(v, p)) <= slen)) continue;
+            const int64_t rank = ((ic - i - 1 + n) % n) * 2 + end;
+            if (rank < best_rank) {
+              best_rank = rank;
+              best = code;
+            }
+          }
+        }
+    return best;
+  };
   for (int64_t i = 0; i < n; i++) {
     int64_t iz = i + 1;
     double zi1 = z[i], zi2 = z2[i];
@@ -260,7 +324,10 @@ void Geometry::build_connections(int ignd) {
         on_ground = true;
       }
     }
-    if (!on_ground) {
+    if (!on_ground && use_grid) {
+      const int64_t m = grid_first(i, v1, slen);
+      icon1[i] = m < 0 ? 0 : ((m & 1) == 0 ? -(int)((m >> 1) + 1) : (int)((m >> 1) + 1));
+    } else if (!on_ground) {
       int64_t ic = i;
       bool found = false;
       for (int64_t j = 1; j < n; j++) {
@@ -290,6 +357,11 @@ void Geometry::build_connections(int ignd) {
     }
     v1 = V3{x[i], y[i], z[i]};
     v2 = V3{x2[i], y2[i], z2[i]};
+    if (use_grid) {
+      const int64_t m = grid_first(i, v2, slen);
+      icon2[i] = m < 0 ? 0 : ((m & 1) == 0 ? (int)((m >> 1) + 1) : -(int)((m >> 1) + 1));
+      continue;
+    }
     int64_t ic = i;
     bool found = false;
     for (int64_t j = 1; j < n; j++) {

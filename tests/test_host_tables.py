@@ -24,6 +24,32 @@ def test_connection_tables_bit_exact(nb, name):
     nb.nec_delete(ctx)
 
 
+@pytest.mark.parametrize("nw,nseg,offset", [(11, 12, 0.0), (9, 16, 0.37)])
+def test_connection_grid_search_matches_reference(nb, ref, nw, nseg, offset):
+    """Structures above 256 segments use the bucketed endpoint search: a
+    wire mesh (4-way junctions, several candidate ends per end) and its
+    connection tables against the reference's cyclic scan, run here."""
+    from necpp_b200 import workloads as W
+    ctxs = []
+    for api in (nb, ref):
+        ctx = api.nec_create()
+        for k in range(nw):
+            y = -1.0 + 2.0 * k / (nw - 1) + offset
+            assert api.nec_wire(ctx, k + 1, nseg, -1.0 + offset, y, 0.2, 1.0 + offset, y, 0.2, 1e-3, 1.0, 1.0) == 0
+            x = -1.0 + 2.0 * k / (nw - 1) + offset
+            assert api.nec_wire(ctx, nw + k + 1, nseg, x, -1.0 + offset, 0.2, x, 1.0 + offset, 0.2, 1e-3, 1.0,
+                                1.0) == 0
+        assert api.nec_geometry_complete(ctx, 0) == 0
+        ctxs.append((api, ctx))
+    ours = nb.segments(ctxs[0][1])
+    theirs = ref.segments(ctxs[1][1])
+    assert len(ours["icon1"]) == 2 * nw * nseg > 256
+    for k in ("icon1", "icon2"):
+        assert np.array_equal(ours[k], theirs[k]), k
+    nb.nec_delete(ctxs[0][1])
+    ref.nec_delete(ctxs[1][1])
+
+
 @pytest.mark.parametrize("name", NAMES)
 def test_scaled_segments_bit_exact(nb, name):
     ctx, st, _, _ = host_case(nb, CASES[name][0])
