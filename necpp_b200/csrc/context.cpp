@@ -663,8 +663,16 @@ void Context::network_solve() {
   solution.assign(n, cd(0, 0));
   abc.assign(6 * n, 0.0);
   necgpu_engine* e = engine();
-  check(e, necgpu_solve(e, reinterpret_cast<const double*>(rhs.data()),
-                        reinterpret_cast<double*>(solution.data()), abc.data()));
+  int rc = necgpu_solve(e, reinterpret_cast<const double*>(rhs.data()), reinterpret_cast<double*>(solution.data()),
+                        abc.data());
+  if (rc == NECGPU_ERR_REFINE && precision_ == NECGPU_MIXED) {
+    // the complex64 factors could not be refined to the FP64 solution:
+    // factor the (intact) FP64 matrix instead and solve again
+    check(e, necgpu_factor(e, NECGPU_FP64));
+    rc = necgpu_solve(e, reinterpret_cast<const double*>(rhs.data()), reinterpret_cast<double*>(solution.data()),
+                      abc.data());
+  }
+  check(e, rc);
   necgpu_stats st{};
   necgpu_get_stats(e, &st);
   last_refine_residual = st.refine_residual;

@@ -129,7 +129,7 @@ class Context {
 
   Geometry geo_;
   necgpu_engine* eng_ = nullptr;
-  int precision_ = 0;
+  int precision_ = 1;  // NECGPU_MIXED; NECGPU_FP64 if its refinement fails
 
   // card state (names follow the reference's members)
   int iflow = 1, state_ = MEM;
