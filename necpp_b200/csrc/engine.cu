@@ -121,6 +121,7 @@ struct necgpu_engine {
   std::vector<int32_t> h_tptr, h_tbasis, h_ind;
   unsigned* d_sweep_ctr = nullptr;  // progress of the refinement sweeps
   bool inv_sweep = true;
+  int64_t outer = 256;  // outer block of the block-pivoted mixed LU (multiple of 64)
   // mixed path: block-local pivoting first, full partial pivoting as fallback
   bool prefer_blockpiv = true;
   bool blockpiv = false;
@@ -389,37 +390,43 @@ int run_fill(necgpu_engine* e, bool want64, bool want32) {
 }
 
 // ---------------- tensor-core trailing update ----------------
+// Packed-operand buffers sized for `rows` rows of up to `kdim` BF16 columns
+// (grown, never shrunk); the tensor maps are encoded per update for the
+// update's own K'.
 int ensure_tc(necgpu_engine* e, int kdim, int64_t rows) {
-  if (e->d_Ap && e->tc_rows >= rows && e->tc_kdim == kdim) return 0;
-  EncodeTiledFn enc = encode_tiled();
-  if (!enc) return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-  TRY(dalloc(e, e->d_Ap, (size_t)rows * kdim));
-  TRY(dalloc(e, e->d_Bp, (size_t)2 * rows * kdim));
-  auto make = [&](CUtensorMap* map, void* base, int64_t nrows, uint32_t box_rows) -> int {
-    cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)nrows};
-    cuuint64_t strides[1] = {(cuuint64_t)kdim * 2};
-    cuuint32_t box[2] = {(cuuint32_t)tc::BK, box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? 0 : fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
-  };
-  TRY(make(&e->tmA, e->d_Ap, rows, tc::BM));
-  TRY(make(&e->tmB, e->d_Bp, 2 * rows, tc::BN));
+  if (e->d_Ap && e->tc_rows >= rows && e->tc_kdim >= kdim) return 0;
+  if (!encode_tiled()) return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const int64_t r = std::max(rows, e->tc_rows);
+  const int k = std::max(kdim, e->tc_kdim);
+  TRY(dalloc(e, e->d_Ap, (size_t)r * k));
+  TRY(dalloc(e, e->d_Bp, (size_t)2 * r * k));
   CUDA_TRY(cudaFuncSetAttribute(tc::gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-  e->tc_rows = rows;
-  e->tc_kdim = kdim;
+  e->tc_rows = r;
+  e->tc_kdim = k;
   return 0;
 }
 
+// K-major BF16 operand map: nrows rows of kdim elements, 64 x box_rows boxes
+int encode_operand(necgpu_engine* e, CUtensorMap* map, void* base, int kdim, int64_t nrows, uint32_t box_rows) {
+  cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)nrows};
+  cuuint64_t strides[1] = {(cuuint64_t)kdim * 2};
+  cuuint32_t box[2] = {(cuuint32_t)tc::BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 0 : fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+}
+
 // C (m x n) -= A (m x kb) B (kb x n), complex64 row-major with leading
-// dimension ld, on the tensor cores.  m, n <= e->n (packed-buffer size).
+// dimension ld, on the tensor cores.
 int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, int64_t ld, int64_t m, int64_t n,
                 int kb) {
   const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
   const int kdim = 6 * kbp;
-  TRY(ensure_tc(e, kdim, std::max(e->n, std::max(m, n))));
+  TRY(ensure_tc(e, kdim, std::max(m, n)));
+  TRY(encode_operand(e, &e->tmA, e->d_Ap, kdim, m, tc::BM));
+  TRY(encode_operand(e, &e->tmB, e->d_Bp, kdim, 2 * n, tc::BN));
   const int64_t cnt = m * kbp;
   KLAUNCH(NECGPU_K_OTHER, 0.0,
           tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, e->d_Ap));
@@ -594,30 +601,56 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm_panel_smem<T>()));
-  for (int64_t k0 = 0; k0 < n; k0 += kBlk) {
-    const int kb = (int)std::min<int64_t>(kBlk, n - k0);
-    T* dinv = e->d_dinv + k0;
-    KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
-            diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, dinv, e->d_status));
-    if (n > kb)
-      KLAUNCH(NECGPU_K_LASWP, 0.0,
-              laswp_block_kernel<T><<<(unsigned)((n + 31) / 32), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
-    const int64_t r0 = k0 + kb, rest = n - r0;
-    if (rest > 0) {
-      const unsigned g = (unsigned)((rest + kTrsmW - 1) / kTrsmW);
+  auto gemm = [&](int64_t r0, int64_t c0, int64_t kc, int64_t m, int64_t nc, int kk) -> int {
+    // M[r0.., c0..] (m x nc) -= M[r0.., kc..kc+kk) M[kc..kc+kk, c0..)
+    if (m <= 0 || nc <= 0 || kk <= 0) return 0;
+    if (e->use_tc) return tc_gemm_sub(e, M + r0 * ld + kc, M + kc * ld + c0, M + r0 * ld + c0, ld, m, nc, kk);
+    dim3 gg((unsigned)((nc + 63) / 64), (unsigned)((m + 63) / 64));
+    KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)m * nc * kk,
+            gemm_sub_kernel<float><<<gg, 256, 0, e->stream>>>(M + r0 * ld + kc, ld, M + kc * ld + c0, ld,
+                                                              M + r0 * ld + c0, ld, m, nc, kk));
+    return 0;
+  };
+  const unsigned smem = (unsigned)trsm_panel_smem<T>();
+  // Outer blocks of e->outer columns (a multiple of 64) factored with 64-wide
+  // inner panels whose updates stay inside the outer block's columns; the
+  // outer block's U12 rows are brought up to date left-looking, and one
+  // tensor-core update with K = outer covers the trailing matrix.
+  const int64_t outer = e->outer;
+  for (int64_t K0 = 0; K0 < n; K0 += outer) {
+    const int64_t KE = std::min<int64_t>(n, K0 + outer);  // end of the outer block
+    for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
+      const int kb = (int)std::min<int64_t>(kBlk, n - k0);
+      T* dinv = e->d_dinv + k0;
+      KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
+              diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, dinv, e->d_status));
+      if (n > kb)
+        KLAUNCH(NECGPU_K_LASWP, 0.0,
+                laswp_block_kernel<T><<<(unsigned)((n + 31) / 32), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
+      const int64_t r0 = k0 + kb, rest = n - r0;
+      if (rest <= 0) continue;
       KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * rest,
-              trsm_panel_kernel<T, false><<<g, kTrsmW, trsm_panel_smem<T>(), e->stream>>>(M, ld, n, k0, r0, dinv));
-      KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * rest,
-              trsm_panel_kernel<T, true><<<g, kTrsmW, trsm_panel_smem<T>(), e->stream>>>(M, ld, n, k0, r0, dinv));
-      if (e->use_tc) {
-        TRY(tc_update(e, M, k0, kb));
-      } else {
-        dim3 gg((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64));
-        KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
-                gemm_sub_kernel<float><<<gg, 256, 0, e->stream>>>(M + r0 * ld + k0, ld, M + k0 * ld + r0, ld,
-                                                                  M + r0 * ld + r0, ld, rest, rest, kb));
+              trsm_panel_kernel<T, false><<<(unsigned)((rest + kTrsmW - 1) / kTrsmW), kTrsmW, smem, e->stream>>>(
+                  M, ld, n, k0, r0, dinv));
+      const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
+      if (pc > 0) {
+        KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * pc,
+                trsm_panel_kernel<T, true><<<(unsigned)((pc + kTrsmW - 1) / kTrsmW), kTrsmW, smem, e->stream>>>(
+                    M, ld, KE, k0, r0, dinv));
+        TRY(gemm(r0, r0, k0, rest, pc, kb));
       }
     }
+    const int64_t rest = n - KE;
+    if (rest <= 0) continue;
+    // U12 of the outer row block: rows [K0, KE), columns [KE, n)
+    for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
+      TRY(gemm(k0, KE, K0, kBlk, rest, (int)(k0 - K0)));
+      KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kBlk * kBlk * rest,
+              trsm_panel_kernel<T, true><<<(unsigned)((rest + kTrsmW - 1) / kTrsmW), kTrsmW, smem, e->stream>>>(
+                  M, ld, n, k0, KE, e->d_dinv + k0));
+    }
+    // trailing update with K = outer
+    TRY(gemm(KE, KE, K0, rest, rest, (int)(KE - K0)));
   }
   std::vector<int> piv(n), perm(n);
   CUDA_TRY(cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
@@ -1113,6 +1146,10 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_BLOCKED_TRSV")) e->sweep_trsv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_FLAG_SWEEP")) e->inv_sweep = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_OUTER")) {
+    const int64_t v = std::atoll(s);
+    if (v >= 64 && v % 64 == 0 && v <= 1024) e->outer = v;
+  }
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   e->own_stream = true;
   CUDA_TRY(cudaEventCreate(&e->ev0));
