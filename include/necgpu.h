@@ -238,6 +238,26 @@ int necgpu_pattern_weights(necgpu_engine* e, double theta, double phi, double* p
 int necgpu_perturbed_terms(necgpu_engine* e, int nstruct, const necgpu_structure* structs, int nw, const double* w,
                            double theta, double phi, double* zx, double* efar);
 
+/* ---- batched sweeps (no counterpart in the reference, which solves one
+ * structure per context; this serves frequency sweeps and optimiser
+ * populations of small structures) ---- */
+
+/* Solve nprob independent structures (2..640 segments each; one medium,
+ * ground and kernel setting for all) in one pass: fill, complex64 LU with
+ * partial pivoting, solve refined in FP64 against the FP64 matrix,
+ * segment-centre currents, far field at ndir directions (radians; 0 for
+ * none).  rhs / cur: the problems' vectors concatenated (sum n complex).
+ * gain (or NULL): nprob x ndir power gain in dB, normalised by the input
+ * power of the one voltage source of each problem (feed: 0-based segment,
+ * volt: complex source voltage, wavelength in metres, per problem).
+ * eth / eph (both or neither): nprob x ndir complex fields.  status[p]:
+ * 0 ok, 1 singular, 2 non-finite, 3 refinement above 1e-6; residual[p]
+ * (or NULL): final relative FP64 residual. */
+int necgpu_batch_solve(necgpu_engine* e, int nprob, const necgpu_structure* structs, const double* rhs,
+                       const int* feed, const double* volt, const double* wavelength, int ndir, const double* theta,
+                       const double* phi, double* cur, float* gain, double* eth, double* eph, int* status,
+                       double* residual);
+
 /* Diagnostic: apply one complex64 update C -= A B (m x n, inner kb) to a
  * seeded random matrix with the tensor-core kernel and with the CUDA-core
  * FP32 kernel; report max |difference| and max |reference| over C. */

@@ -10,6 +10,9 @@
 #include <type_traits>
 #include <cstring>
 #include <mutex>
+#include <atomic>
+#include <thread>
+#include <numeric>
 #include <string>
 #include <vector>
 
@@ -19,6 +22,7 @@
 #include "lu.cuh"
 #include "pattern.cuh"
 #include "solve.cuh"
+#include "batch.cuh"
 
 using namespace necb;
 
@@ -1712,6 +1716,317 @@ int necgpu_perturbed_terms(necgpu_engine* e, int nstruct, const necgpu_structure
   e->stats.d2h_bytes += (int64_t)nstruct * (2 * kMaxContract * 8 + 32);
   kflush(e);
   return NECGPU_OK;
+}
+
+int necgpu_batch_solve(necgpu_engine* e, int nprob, const necgpu_structure* structs, const double* rhs,
+                       const int* feed, const double* volt, const double* wavelength, int ndir, const double* theta,
+                       const double* phi, double* cur, float* gain, double* eth, double* eph, int* status,
+                       double* residual) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (nprob < 1 || nprob > 65535 || !structs || !rhs || !cur || !status || ndir < 0 ||
+      (ndir > 0 && (!theta || !phi || (!eth) != (!eph))) || (gain && (!feed || !volt || !wavelength)))
+    return fail(e, NECGPU_ERR_ARG, "batch_solve: bad arguments");
+  CUDA_TRY(cudaSetDevice(e->device));
+  const necgpu_structure& s0 = structs[0];
+  // host tables of every problem, concatenated
+  std::vector<int64_t> seg_off(nprob + 1, 0), z_off(nprob + 1, 0);
+  for (int p = 0; p < nprob; p++) {
+    const necgpu_structure& s = structs[p];
+    if (s.n < 2 || s.n > kBatchMaxN)
+      return fail(e, NECGPU_ERR_ARG, "batch_solve: problem " + std::to_string(p) + " has " + std::to_string(s.n) +
+                                         " segments; the batched path takes 2.." + std::to_string(kBatchMaxN));
+    if (s.ground != s0.ground || (s.use_exk != 0) != (s0.use_exk != 0) || s.eta != s0.eta ||
+        s.zrati_re != s0.zrati_re || s.zrati_im != s0.zrati_im)
+      return fail(e, NECGPU_ERR_ARG, "batch_solve: all problems must share the medium, ground and kernel settings");
+    seg_off[p + 1] = seg_off[p] + s.n;
+    z_off[p + 1] = z_off[p] + s.n * s.n;
+  }
+  const int64_t T = seg_off[nprob], Zt = z_off[nprob];
+  std::vector<double> seg(8 * T);
+  std::vector<int32_t> ind(2 * T, 0);
+  std::vector<int32_t> tp_pool, ts_pool, te_pool, cptr_g(T + 1, 0), cbasis_pool;
+  std::vector<uint8_t> ecol_pool;
+  std::vector<double> ecoef_pool, ca_pool, cb_pool, cc_pool;
+  std::vector<int64_t> tp_off(nprob), ts_off(nprob), te_off(nprob), ec_off(nprob), ecf_off(nprob), ne_p(nprob);
+  std::vector<int> ntiles_p(nprob), seg_prob(T);
+  // per-problem tile and coefficient lists on all host cores, then concatenated
+  std::vector<TileLists> TLs(nprob);
+  std::vector<CoefLists> CLs(nprob);
+  std::vector<int> bad(nprob, 0);
+  {
+    const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 64));
+    std::atomic<int> nextp(0);
+    auto work = [&]() {
+      for (int p = nextp++; p < nprob; p = nextp++) {
+        const necgpu_structure& s = structs[p];
+        const int64_t n = s.n;
+        const int32_t* tp = s.trio_ptr;
+        bool ok = tp[0] == 0;
+        for (int64_t j = 0; ok && j < n; j++) ok = tp[j + 1] >= tp[j];
+        for (int64_t k = 0; ok && k < tp[n]; k++) ok = s.trio_basis[k] >= 0 && s.trio_basis[k] < n;
+        if (!ok) {
+          bad[p] = 1;
+          continue;
+        }
+        build_tile_lists(&s, n, (int)((n + kFillTB - 1) / kFillTB), TLs[p]);
+        build_coef_lists(&s, n, CLs[p]);
+      }
+    };
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nth; i++) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+  }
+  for (int p = 0; p < nprob; p++)
+    if (bad[p]) return fail(e, NECGPU_ERR_ARG, "batch_solve: basis tables of problem " + std::to_string(p) + " are malformed");
+  for (int p = 0; p < nprob; p++) {
+    const necgpu_structure& s = structs[p];
+    const int64_t n = s.n, o = seg_off[p];
+    const double* src[8] = {s.x, s.y, s.z, s.length, s.radius, s.cab, s.sab, s.salp};
+    for (int a = 0; a < 8; a++) std::copy(src[a], src[a] + n, seg.begin() + a * T + o);
+    if (s.ek_ind1 && s.ek_ind2) {
+      std::copy(s.ek_ind1, s.ek_ind1 + n, ind.begin() + o);
+      std::copy(s.ek_ind2, s.ek_ind2 + n, ind.begin() + T + o);
+    }
+    for (int64_t j = 0; j < n; j++) seg_prob[o + j] = p;
+    const int32_t* tp = s.trio_ptr;
+    ntiles_p[p] = (int)((n + kFillTB - 1) / kFillTB);
+    const TileLists& TL = TLs[p];
+    tp_off[p] = (int64_t)tp_pool.size();
+    ts_off[p] = (int64_t)ts_pool.size();
+    te_off[p] = (int64_t)te_pool.size();
+    ec_off[p] = (int64_t)ecol_pool.size();
+    ecf_off[p] = (int64_t)ecoef_pool.size();
+    ne_p[p] = (int64_t)TL.ecol.size();
+    tp_pool.insert(tp_pool.end(), TL.tile_ptr.begin(), TL.tile_ptr.end());
+    ts_pool.insert(ts_pool.end(), TL.tsrc.begin(), TL.tsrc.end());
+    te_pool.insert(te_pool.end(), TL.tsrc_eptr.begin(), TL.tsrc_eptr.end());
+    ecol_pool.insert(ecol_pool.end(), TL.ecol.begin(), TL.ecol.end());
+    ecoef_pool.insert(ecoef_pool.end(), TL.ecoef.begin(), TL.ecoef.end());
+    const CoefLists& CL = CLs[p];
+    const int64_t nt = tp[n], cbase = (int64_t)cbasis_pool.size();
+    for (int64_t j = 0; j < n; j++) cptr_g[o + j] = (int32_t)(cbase + CL.cptr[j]);
+    cbasis_pool.insert(cbasis_pool.end(), CL.cbasis.begin(), CL.cbasis.begin() + nt);
+    ca_pool.insert(ca_pool.end(), CL.ccoef.begin(), CL.ccoef.begin() + nt);
+    cb_pool.insert(cb_pool.end(), CL.ccoef.begin() + nt, CL.ccoef.begin() + 2 * nt);
+    cc_pool.insert(cc_pool.end(), CL.ccoef.begin() + 2 * nt, CL.ccoef.begin() + 3 * nt);
+  }
+  cptr_g[T] = (int32_t)cbasis_pool.size();
+  for (auto* v : {&ts_pool, &te_pool, &cbasis_pool})
+    if (v->empty()) v->push_back(0);
+  if (ecol_pool.empty()) ecol_pool.push_back(0);
+  for (auto* v : {&ca_pool, &cb_pool, &cc_pool, &ecoef_pool})
+    if (v->empty()) v->push_back(0.0);
+  // device pools (stream-ordered; freed at the end of the call)
+  double *d_seg = nullptr, *d_ecoef = nullptr, *d_ca = nullptr, *d_cb = nullptr, *d_cc = nullptr, *d_abc = nullptr,
+         *d_res = nullptr;
+  int32_t *d_ind = nullptr, *d_tp = nullptr, *d_ts = nullptr, *d_te = nullptr, *d_cptr = nullptr, *d_cbasis = nullptr;
+  uint8_t* d_ecol = nullptr;
+  double2 *d_Z64 = nullptr, *d_b = nullptr, *d_x = nullptr, *d_cur = nullptr, *d_eth = nullptr, *d_eph = nullptr,
+          *d_dirs = nullptr;
+  float2* d_Z32 = nullptr;
+  int *d_perm = nullptr, *d_segp = nullptr, *d_order = nullptr, *d_next = nullptr, *d_st = nullptr;
+  BatchProblem* d_probs = nullptr;
+  FillArgs* d_args = nullptr;
+  int4* d_items = nullptr;
+  auto release = [&]() {
+    dfree(e, d_seg), dfree(e, d_ecoef), dfree(e, d_ca), dfree(e, d_cb), dfree(e, d_cc), dfree(e, d_abc);
+    dfree(e, d_res), dfree(e, d_ind), dfree(e, d_tp), dfree(e, d_ts), dfree(e, d_te), dfree(e, d_cptr);
+    dfree(e, d_cbasis), dfree(e, d_ecol), dfree(e, d_Z64), dfree(e, d_b), dfree(e, d_x), dfree(e, d_cur);
+    dfree(e, d_eth), dfree(e, d_eph), dfree(e, d_dirs), dfree(e, d_Z32), dfree(e, d_perm), dfree(e, d_segp);
+    dfree(e, d_order), dfree(e, d_next), dfree(e, d_st), dfree(e, d_probs), dfree(e, d_args), dfree(e, d_items);
+  };
+  int rc = 0;
+  do {
+    if ((rc = upload(e, d_seg, seg.data(), seg.size()))) break;
+    if ((rc = upload(e, d_ind, ind.data(), ind.size()))) break;
+    if ((rc = upload(e, d_tp, tp_pool.data(), tp_pool.size()))) break;
+    if ((rc = upload(e, d_ts, ts_pool.data(), ts_pool.size()))) break;
+    if ((rc = upload(e, d_te, te_pool.data(), te_pool.size()))) break;
+    if ((rc = upload(e, d_ecol, ecol_pool.data(), ecol_pool.size()))) break;
+    if ((rc = upload(e, d_ecoef, ecoef_pool.data(), ecoef_pool.size()))) break;
+    if ((rc = upload(e, d_cptr, cptr_g.data(), cptr_g.size()))) break;
+    if ((rc = upload(e, d_cbasis, cbasis_pool.data(), cbasis_pool.size()))) break;
+    if ((rc = upload(e, d_ca, ca_pool.data(), ca_pool.size()))) break;
+    if ((rc = upload(e, d_cb, cb_pool.data(), cb_pool.size()))) break;
+    if ((rc = upload(e, d_cc, cc_pool.data(), cc_pool.size()))) break;
+    if ((rc = upload(e, d_segp, seg_prob.data(), seg_prob.size()))) break;
+    if ((rc = upload(e, d_b, reinterpret_cast<const double2*>(rhs), (size_t)T))) break;
+    if ((rc = dalloc(e, d_Z64, (size_t)Zt))) break;
+    if ((rc = dalloc(e, d_Z32, (size_t)Zt))) break;
+    if ((rc = dalloc(e, d_x, (size_t)T))) break;
+    if ((rc = dalloc(e, d_perm, (size_t)T))) break;
+    if ((rc = dalloc(e, d_cur, (size_t)T))) break;
+    if ((rc = dalloc(e, d_abc, 6 * (size_t)T))) break;
+    if ((rc = dalloc(e, d_st, (size_t)nprob))) break;
+    if ((rc = dalloc(e, d_res, (size_t)nprob))) break;
+    if ((rc = dalloc(e, d_next, 1))) break;
+    // per-problem fill arguments and the fill work list
+    std::vector<FillArgs> fa(nprob);
+    std::vector<BatchProblem> bp(nprob);
+    std::vector<int4> items;
+    for (int p = 0; p < nprob; p++) {
+      const necgpu_structure& s = structs[p];
+      const int64_t n = s.n, o = seg_off[p];
+      FillArgs& a = fa[p];
+      a.n = n;
+      a.ld = n;
+      a.x = d_seg + o;
+      a.y = d_seg + T + o;
+      a.z = d_seg + 2 * T + o;
+      a.s = d_seg + 3 * T + o;
+      a.b = d_seg + 4 * T + o;
+      a.cab = d_seg + 5 * T + o;
+      a.sab = d_seg + 6 * T + o;
+      a.salp = d_seg + 7 * T + o;
+      a.ind1 = d_ind + o;
+      a.ind2 = d_ind + T + o;
+      a.tile_src_ptr = d_tp + tp_off[p];
+      a.tsrc = d_ts + ts_off[p];
+      a.tsrc_eptr = d_te + te_off[p];
+      a.ecol = d_ecol + ec_off[p];
+      a.ea = d_ecoef + ecf_off[p];
+      a.eb = a.ea + ne_p[p];
+      a.ec = a.ea + 2 * ne_p[p];
+      a.P.rkh = s.rkh;
+      a.P.eta = s.eta;
+      a.P.zrati = mk(s.zrati_re, s.zrati_im);
+      a.P.frati = mk(s.frati_re, s.frati_im);
+      a.P.u = a.P.zrati;
+      a.P.u2 = a.P.zrati * a.P.zrati;
+      a.Z64 = d_Z64 + z_off[p];
+      a.Z32 = d_Z32 + z_off[p];
+      a.status = e->d_status;
+      bp[p] = BatchProblem{(int)n, z_off[p], o};
+      const int rt = (int)((n + kFillTI - 1) / kFillTI);
+      for (int r = 0; r < rt; r++)
+        for (int c = 0; c < ntiles_p[p]; c++) items.push_back(make_int4(p, r, c, 0));
+    }
+    std::vector<int> order(nprob);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return structs[a].n > structs[b].n; });
+    if ((rc = upload(e, d_args, fa.data(), fa.size()))) break;
+    if ((rc = upload(e, d_probs, bp.data(), bp.size()))) break;
+    if ((rc = upload(e, d_items, items.data(), items.size()))) break;
+    if ((rc = upload(e, d_order, order.data(), order.size()))) break;
+    CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+    CUDA_TRY(cudaMemsetAsync(d_next, 0, sizeof(int), e->stream));
+    // fill
+    const bool xk = s0.use_exk != 0;
+    const double pairs = (double)0 + [&] {
+      double q = 0;
+      for (int p = 0; p < nprob; p++) q += (double)structs[p].n * structs[p].n;
+      return q;
+    }();
+#define NECB_BFILL(G)                                                                                         \
+  (xk ? (batch_fill_kernel<G, true><<<(unsigned)items.size(), kFillTI, 0, e->stream>>>(d_args, d_items), 0)    \
+      : (batch_fill_kernel<G, false><<<(unsigned)items.size(), kFillTI, 0, e->stream>>>(d_args, d_items), 0))
+    switch (s0.ground) {
+      case kGroundNone: KLAUNCH(NECGPU_K_FILL, pairs, NECB_BFILL(kGroundNone)); break;
+      case kGroundPerfect: KLAUNCH(NECGPU_K_FILL, pairs, NECB_BFILL(kGroundPerfect)); break;
+      case kGroundReflection: KLAUNCH(NECGPU_K_FILL, pairs, NECB_BFILL(kGroundReflection)); break;
+      default: KLAUNCH(NECGPU_K_FILL, pairs, NECB_BFILL(kGroundSommerfeld)); break;
+    }
+#undef NECB_BFILL
+    // LU and refined solve, one problem per CTA at a time
+    CUDA_TRY(cudaFuncSetAttribute(batch_lu_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kBatchSmem));
+    double lu_flops = 0;
+    for (int p = 0; p < nprob; p++) lu_flops += 8.0 * std::pow((double)structs[p].n, 3) / 3.0;
+    KLAUNCH(NECGPU_K_PANEL, lu_flops,
+            batch_lu_solve_kernel<<<(unsigned)std::min(nprob, e->nsm), kBatchThreads, kBatchSmem, e->stream>>>(
+                nprob, d_order, d_probs, d_Z32, d_Z64, d_perm, d_b, d_x, e->refine_tol, d_next, d_st, d_res));
+    KLAUNCH(NECGPU_K_OTHER, 0.0,
+            batch_coeff_kernel<<<(unsigned)((T + 255) / 256), 256, 0, e->stream>>>(
+                T, d_segp, d_probs, d_cptr, d_cbasis, d_ca, d_cb, d_cc, d_x, d_abc, d_cur));
+    double* d_gcop = nullptr;
+    float* d_gain = nullptr;
+    int64_t* d_so = nullptr;
+    if (ndir > 0 && gain) {
+      std::vector<int> fd(feed, feed + nprob);
+      for (int p = 0; p < nprob; p++)
+        if (fd[p] < 0 || fd[p] >= structs[p].n) {
+          rc = fail(e, NECGPU_ERR_ARG, "batch_solve: feed segment out of range");
+          break;
+        }
+      if (rc) break;
+      int* d_feed = nullptr;
+      double2* d_volt = nullptr;
+      double* d_lam = nullptr;
+      if ((rc = upload(e, d_feed, fd.data(), fd.size()))) break;
+      if ((rc = upload(e, d_volt, reinterpret_cast<const double2*>(volt), (size_t)nprob))) break;
+      if ((rc = upload(e, d_lam, wavelength, (size_t)nprob))) break;
+      if ((rc = upload(e, d_so, seg_off.data(), seg_off.size()))) break;
+      if ((rc = dalloc(e, d_gcop, (size_t)nprob))) break;
+      KLAUNCH(NECGPU_K_OTHER, 0.0,
+              batch_gain_norm_kernel<<<(unsigned)((nprob + 127) / 128), 128, 0, e->stream>>>(
+                  nprob, d_so, d_feed, d_volt, d_lam, s0.eta, d_cur, d_gcop));
+      dfree(e, d_feed);
+      dfree(e, d_volt);
+      dfree(e, d_lam);
+      if ((rc = dalloc(e, d_gain, (size_t)nprob * ndir))) break;
+    }
+    if (ndir > 0) {
+      std::vector<double> dirs(2 * (size_t)ndir);
+      std::copy(theta, theta + ndir, dirs.begin());
+      std::copy(phi, phi + ndir, dirs.begin() + ndir);
+      double* dd = nullptr;
+      if ((rc = upload(e, dd, dirs.data(), dirs.size()))) break;
+      d_dirs = reinterpret_cast<double2*>(dd);
+      if (eth) {
+        if ((rc = dalloc(e, d_eth, (size_t)nprob * ndir))) break;
+        if ((rc = dalloc(e, d_eph, (size_t)nprob * ndir))) break;
+      }
+      BatchPatternArgs pa{};
+      pa.nprob = nprob;
+      pa.ndir = ndir;
+      pa.theta = dd;
+      pa.phi = dd + ndir;
+      if (!d_so && (rc = upload(e, d_so, seg_off.data(), seg_off.size()))) break;
+      pa.seg_off = d_so;
+      pa.seg = d_seg;
+      pa.abc = d_abc;
+      pa.nseg_total = T;
+      pa.ksymp = s0.ground == kGroundNone ? 1 : 2;
+      pa.perfect = s0.ground == kGroundPerfect ? 1 : 0;
+      pa.zrati = mk(s0.zrati_re, s0.zrati_im);
+      pa.eta = s0.eta;
+      pa.eth = d_eth;
+      pa.eph = d_eph;
+      pa.gcop = d_gcop;
+      pa.gain = d_gain;
+      const dim3 g((unsigned)((ndir + kPatDirs - 1) / kPatDirs), (unsigned)nprob);
+      KLAUNCH(NECGPU_K_PATTERN, (double)ndir * T * pa.ksymp,
+              batch_pattern_kernel<<<g, kPatDirs * 32, 0, e->stream>>>(pa));
+      if (eth) {
+        CUDA_TRY(cudaMemcpyAsync(eth, d_eth, (size_t)nprob * ndir * sizeof(double2), cudaMemcpyDeviceToHost,
+                                 e->stream));
+        CUDA_TRY(cudaMemcpyAsync(eph, d_eph, (size_t)nprob * ndir * sizeof(double2), cudaMemcpyDeviceToHost,
+                                 e->stream));
+      }
+      if (gain)
+        CUDA_TRY(cudaMemcpyAsync(gain, d_gain, (size_t)nprob * ndir * sizeof(float), cudaMemcpyDeviceToHost,
+                                 e->stream));
+    }
+    CUDA_TRY(cudaMemcpyAsync(cur, d_cur, (size_t)T * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(status, d_st, (size_t)nprob * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+    if (residual)
+      CUDA_TRY(cudaMemcpyAsync(residual, d_res, (size_t)nprob * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    int st = 0;
+    rc = sync_status(e, &st);
+    dfree(e, d_gcop);
+    dfree(e, d_gain);
+    dfree(e, d_so);
+    if (rc) break;
+    kflush(e);
+    if (st & kStatSommerfeldTab)
+      rc = fail(e, NECGPU_ERR_UNSUPPORTED, "batch_solve: a segment pair needs the Sommerfeld table path");
+    else if (st & kStatIterCap)
+      rc = fail(e, NECGPU_ERR_NONFINITE, "batch_solve: quadrature did not terminate");
+  } while (false);
+  release();
+  if (rc == 0) CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return rc;
 }
 
 int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph) {
