@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-gradient", action="store_true")
+    p.add_argument("--no-sweep", action="store_true")
     return p.parse_args()
 
 
@@ -239,6 +240,90 @@ def gradient_cost(nb, W, reps=5):
             "forward_ms": f * 1e3, "gradient_ms": g * 1e3, "grad_fwd_cost": g / f,
             "value": [float(v) for v in value], "timing": "wall clock of the synchronous C-API calls, median of %d"
             % reps}
+
+
+def batched_sweep(nb, rank, world, replicas, reps=3, ref_sample=16):
+    """The batched sweep: 256 seeded Yagi-Uda variants x 32 frequencies
+    (140-160 MHz) = 8192 solves of fill, LU, FP64-refined solve, currents
+    and a 91x72 gain pattern.  Problems are dealt to ranks by N^3
+    (round-robin in decreasing cost); the job rate is all solves over the
+    slowest rank's time.  `value` times the batched call from host
+    structures to host results (copies included); host_prep_s is building
+    the 8192 structures from cards; device_ms the kernels' CUDA-event time."""
+    import ctypes as _C
+    from necpp_b200 import batch as B
+    t0 = time.perf_counter()
+    problems, labels = B.yagi_problems(256, 32, seed=0)
+    prep = time.perf_counter() - t0
+    mine = replicas.partition_by_cost([float(p[0]["n"]) ** 3 for p in problems], world, rank)
+    sub = [problems[i] for i in mine]
+    th, ph = B.pattern_grid()
+    B.sweep(sub[:64], th, ph)  # warm-up (pool, module)
+    B.sweep(sub, th, ph)
+    ts = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        res = B.sweep(sub, th, ph)
+        ts.append(time.perf_counter() - t)
+    # kernel time of one more pass with per-launch events
+    eng = B._get_engine()
+    L = nb.lib
+    L.necgpu_enable_timing.argtypes = [_C.c_void_p, _C.c_int]
+    L.necgpu_reset_kernel_stats.argtypes = [_C.c_void_p]
+    L.necgpu_get_stats.argtypes = [_C.c_void_p, _C.POINTER(Stats)]
+    L.necgpu_enable_timing(eng, 2)
+    L.necgpu_reset_kernel_stats(eng)
+    B.sweep(sub, th, ph)
+    st = Stats()
+    L.necgpu_get_stats(eng, _C.byref(st))
+    L.necgpu_enable_timing(eng, 0)
+    dev = {K_NAMES[i]: st.k_ms[i] for i in range(9) if st.k_launches[i]}
+    t = statistics.median(ts)
+    rate, total, slowest = replicas.whole_job_rate(len(sub), t, device="cuda")
+    out = {"workload": "256 Yagi-Uda variants (3-15 elements, 11-41 segments each, N 33-615) x 32 "
+                       "frequencies 140-160 MHz, 91x72 gain pattern each",
+           "solves": int(total), "value": rate, "unit": "solves/s", "seconds": slowest,
+           "host_prep_s": prep, "device_ms": {"fill": dev.get("fill"), "lu_and_refined_solve": dev.get("lu_panel"),
+                                               "pattern": dev.get("pattern"), "other": dev.get("other")},
+           "status_ok": int(np.sum(res["status"] == 0)), "max_residual": float(np.max(res["residual"])),
+           "n_range": [int(min(p[0]["n"] for p in problems)), int(max(p[0]["n"] for p in problems))],
+           "partition": "N^3 round-robin over %d rank(s)" % world}
+    if rank == 0 and ref_sample:
+        from oracle import refwrap
+        if refwrap.available():
+            out["reference_cpu"] = reference_sweep_sample(problems, labels, ref_sample)
+    return out
+
+
+def reference_sweep_sample(problems, labels, k):
+    """The reference (oracle/_ref, one thread) on k of the sweep's problems
+    spread over its size range; solves/s = k / their total time."""
+    from oracle.refwrap import RefAPI
+    from necpp_b200 import workloads as W
+    ref = RefAPI()
+    order = sorted(range(len(problems)), key=lambda i: problems[i][0]["n"])
+    pick = [order[int(j * (len(order) - 1) / (k - 1))] for j in range(k)]
+    rng = np.random.default_rng(0)
+    params = [W.yagi_params(rng) for _ in range(256)]
+    t = 0.0
+    for i in pick:
+        v, f = labels[i]
+        half, xs, rad, segs = params[v]
+        ctx = ref.nec_create()
+        t0 = time.perf_counter()
+        for e in range(len(half)):
+            ref.nec_wire(ctx, e + 1, int(segs[e]), float(xs[e]), 0.0, -float(half[e]), float(xs[e]), 0.0,
+                         float(half[e]), float(rad[e]), 1.0, 1.0)
+        ref.nec_geometry_complete(ctx, 0)
+        ref.nec_fr_card(ctx, 0, 1, f, 0.0)
+        ref.nec_ex_card(ctx, 0, 2, (int(segs[1]) + 1) // 2, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+        ref.nec_rp_card(ctx, 0, 91, 72, 1, 0, 0, 0, 0.0, 0.0, 2.0, 5.0, 0.0, 0.0)
+        t += time.perf_counter() - t0
+        ref.nec_delete(ctx)
+    return {"value": k / t, "unit": "solves/s", "cores": 1, "kind": "reference",
+            "sample": "%d problems spread over the size range (N %d-%d), each cards + fill + LU + solve + "
+                      "91x72 pattern; the sweep's mix of sizes differs, so this is indicative"
+                      % (k, problems[pick[0]][0]["n"], problems[pick[-1]][0]["n"])}
 
 
 def run_b200(args):
@@ -440,6 +525,10 @@ def run_b200(args):
 
     if rank == 0 and not args.no_gradient:
         line["gradient"] = gradient_cost(nb, W)
+    if not args.no_sweep:
+        sw = batched_sweep(nb, rank, world, replicas, ref_sample=0 if args.no_cpu_baseline else 16)
+        if rank == 0:
+            line["batched_sweep"] = sw
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refwrap

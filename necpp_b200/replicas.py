@@ -42,3 +42,12 @@ def whole_job_rate(units, seconds, device="cpu"):
     if not slowest > 0:
         raise ValueError("whole_job_rate: non-positive time")
     return total / slowest, total, slowest
+
+
+def partition_by_cost(costs, world, rank):
+    """Indices of the units this rank solves when independent units of
+    uneven cost (e.g. N^3 of each problem of a batched sweep) are dealt
+    round-robin in order of decreasing cost; every rank gets a near-equal
+    share of the total cost."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    return [i for k, i in enumerate(order) if k % world == rank]

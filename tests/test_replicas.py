@@ -57,3 +57,16 @@ def test_single_process_needs_no_group():
     assert whole_job_rate(4, 2.0) == (2.0, 4.0, 2.0)
     with pytest.raises(ValueError):
         whole_job_rate(4, 0.0)
+
+
+def test_partition_by_cost_covers_all_units_evenly():
+    import numpy as np
+    from necpp_b200.replicas import partition_by_cost
+    rng = np.random.default_rng(0)
+    n = rng.integers(33, 616, size=1000)
+    cost = (n.astype(float)) ** 3
+    parts = [partition_by_cost(cost, 4, r) for r in range(4)]
+    allidx = sorted(i for p in parts for i in p)
+    assert allidx == list(range(1000))
+    shares = [cost[p].sum() / cost.sum() for p in parts]
+    assert max(shares) - min(shares) < 0.02
