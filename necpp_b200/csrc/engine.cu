@@ -19,6 +19,7 @@
 #include "../../include/necgpu.h"
 #include "fill.cuh"
 #include "gemm_tc.cuh"
+#include "gemm_dmma.cuh"
 #include "lu.cuh"
 #include "pattern.cuh"
 #include "solve.cuh"
@@ -125,6 +126,7 @@ struct necgpu_engine {
   std::vector<int32_t> h_tptr, h_tbasis, h_ind;
   unsigned* d_sweep_ctr = nullptr;  // progress of the refinement sweeps
   bool inv_sweep = true;
+  bool use_dmma = true;  // FP64 trailing update on the FP64 tensor cores
   int64_t outer = 256;  // outer block of the block-pivoted mixed LU (multiple of 64)
   // mixed path: block-local pivoting first, full partial pivoting as fallback
   bool prefer_blockpiv = true;
@@ -558,6 +560,17 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
       if constexpr (std::is_same<R, float>::value) {
         if (e->use_tc) {
           TRY(tc_update(e, M, k0, kb));
+          done = true;
+        }
+      }
+      if constexpr (std::is_same<R, double>::value) {
+        if (!done && e->use_dmma) {
+          // FP64 tensor cores (mma.sync m8n8k4 f64)
+          dim3 g((unsigned)((rest + kDmmaBN - 1) / kDmmaBN), (unsigned)((rest + kDmmaBM - 1) / kDmmaBM));
+          KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)rest * rest * kb,
+                  gemm_dmma_kernel<<<g, kDmmaThreads, sizeof(DmmaSmem), e->stream>>>(
+                      M + (k0 + kb) * ld + k0, ld, M + k0 * ld + k0 + kb, ld, M + (k0 + kb) * ld + k0 + kb, ld, rest,
+                      rest, kb));
           done = true;
         }
       }
@@ -1150,6 +1163,8 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_BLOCKED_TRSV")) e->sweep_trsv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_FLAG_SWEEP")) e->inv_sweep = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_NO_DMMA")) e->use_dmma = (s[0] == '0');
+  CUDA_TRY(cudaFuncSetAttribute(gemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DmmaSmem)));
   if (const char* s = std::getenv("NECPP_B200_OUTER")) {
     const int64_t v = std::atoll(s);
     if (v >= 64 && v % 64 == 0 && v <= 1024) e->outer = v;
