@@ -105,6 +105,16 @@ struct necgpu_engine {
   __nv_bfloat16 *d_Ap = nullptr, *d_Bp = nullptr;
   int64_t tc_rows = 0;
   int tc_kdim = 0;
+  // second packed-operand set (the lookahead's far update)
+  __nv_bfloat16 *d_Ap2 = nullptr, *d_Bp2 = nullptr;
+  int64_t tc_rows2 = 0;
+  int tc_kdim2 = 0;
+  // lookahead: the trailing update beyond the next outer block runs on
+  // stream2 with lookahead_sms SMs left free for the next panel
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
+  bool lookahead = true;
+  int lookahead_sms = 48;
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
   float2* d_tinv = nullptr;  // inverted 64 x 64 diagonal blocks of the complex64 factors
@@ -185,7 +195,7 @@ int fail(necgpu_engine* e, int code, const std::string& msg) {
 
 // Per-launch timing: an event pair on the launching stream around each
 // kernel of a class, resolved after the next stream synchronisation.
-int kbegin(necgpu_engine* e) {
+int kbegin(necgpu_engine* e, cudaStream_t st = nullptr) {
   if (e->timing_level < 2) return -1;
   while ((int)e->kev.size() < e->kev_used + 2) {
     cudaEvent_t ev;
@@ -194,12 +204,12 @@ int kbegin(necgpu_engine* e) {
   }
   const int i = e->kev_used;
   e->kev_used += 2;
-  cudaEventRecord(e->kev[i], e->stream);
+  cudaEventRecord(e->kev[i], st ? st : e->stream);
   return i;
 }
-void kend(necgpu_engine* e, int i, int cls, double flops) {
+void kend(necgpu_engine* e, int i, int cls, double flops, cudaStream_t st = nullptr) {
   if (i < 0) return;
-  cudaEventRecord(e->kev[i + 1], e->stream);
+  cudaEventRecord(e->kev[i + 1], st ? st : e->stream);
   e->kpend.push_back({cls, i, flops});
 }
 void kflush(necgpu_engine* e) {  // call after the stream has synchronised
@@ -268,6 +278,10 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->d_ccoef);
   dfree(e, e->Z64);
   dfree(e, e->d_dinv);
+  dfree(e, e->d_Ap2);
+  dfree(e, e->d_Bp2);
+  e->tc_rows2 = 0;
+  e->tc_kdim2 = 0;
   dfree(e, e->d_tinv);
   dfree(e, e->d_sweep_ctr);
   dfree(e, e->ZT32);
@@ -396,19 +410,23 @@ int run_fill(necgpu_engine* e, bool want64, bool want32) {
 }
 
 // ---------------- tensor-core trailing update ----------------
-// Packed-operand buffers sized for `rows` rows of up to `kdim` BF16 columns
-// (grown, never shrunk); the tensor maps are encoded per update for the
-// update's own K'.
-int ensure_tc(necgpu_engine* e, int kdim, int64_t rows) {
-  if (e->d_Ap && e->tc_rows >= rows && e->tc_kdim >= kdim) return 0;
+// Packed-operand buffers (set 0 or 1) sized for `rows` rows of up to `kdim`
+// BF16 columns (grown, never shrunk); the tensor maps are encoded per update
+// for the update's own K'.
+int ensure_tc(necgpu_engine* e, int kdim, int64_t rows, int set = 0) {
+  __nv_bfloat16*& Ap = set ? e->d_Ap2 : e->d_Ap;
+  __nv_bfloat16*& Bp = set ? e->d_Bp2 : e->d_Bp;
+  int64_t& trows = set ? e->tc_rows2 : e->tc_rows;
+  int& tkdim = set ? e->tc_kdim2 : e->tc_kdim;
+  if (Ap && trows >= rows && tkdim >= kdim) return 0;
   if (!encode_tiled()) return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-  const int64_t r = std::max(rows, e->tc_rows);
-  const int k = std::max(kdim, e->tc_kdim);
-  TRY(dalloc(e, e->d_Ap, (size_t)r * k));
-  TRY(dalloc(e, e->d_Bp, (size_t)2 * r * k));
+  const int64_t r = std::max(rows, trows);
+  const int k = std::max(kdim, tkdim);
+  TRY(dalloc(e, Ap, (size_t)r * k));
+  TRY(dalloc(e, Bp, (size_t)2 * r * k));
   CUDA_TRY(cudaFuncSetAttribute(tc::gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-  e->tc_rows = r;
-  e->tc_kdim = k;
+  trows = r;
+  tkdim = k;
   return 0;
 }
 
@@ -424,25 +442,36 @@ int encode_operand(necgpu_engine* e, CUtensorMap* map, void* base, int kdim, int
   return r == CUDA_SUCCESS ? 0 : fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
-// C (m x n) -= A (m x kb) B (kb x n), complex64 row-major with leading
-// dimension ld, on the tensor cores.
-int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, int64_t ld, int64_t m, int64_t n,
-                int kb) {
+// Pack A (m x kb) and B (kb x n), complex64 row-major with leading
+// dimension ld, into operand set `set` (on the engine's stream).
+int tc_pack(necgpu_engine* e, int set, const float2* A, const float2* B, int64_t ld, int64_t m, int64_t n, int kb) {
   const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
-  const int kdim = 6 * kbp;
-  TRY(ensure_tc(e, kdim, std::max(m, n)));
-  TRY(encode_operand(e, &e->tmA, e->d_Ap, kdim, m, tc::BM));
-  TRY(encode_operand(e, &e->tmB, e->d_Bp, kdim, 2 * n, tc::BN));
+  TRY(ensure_tc(e, 6 * kbp, std::max(m, n), set));
+  __nv_bfloat16* Ap = set ? e->d_Ap2 : e->d_Ap;
+  __nv_bfloat16* Bp = set ? e->d_Bp2 : e->d_Bp;
   const int64_t cnt = m * kbp;
   KLAUNCH(NECGPU_K_OTHER, 0.0,
-          tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, e->d_Ap));
+          tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, Ap));
   dim3 g((unsigned)((n + 31) / 32), (unsigned)(kbp / 64));
-  KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, e->d_Bp));
-  // C as m rows x 2n FP32 (re, im interleaved), 32 x 32 boxes for the
+  KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, Bp));
+  return 0;
+}
+
+// C (m x ncols) -= A' B'[columns j0, j0 + ncols) from operand set `set`, on
+// stream st with at most grid_max persistent CTAs.
+int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int kb, float2* C, int64_t ld,
+           cudaStream_t st, int grid_max) {
+  const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
+  const int kdim = 6 * kbp;
+  __nv_bfloat16* Ap = set ? e->d_Ap2 : e->d_Ap;
+  __nv_bfloat16* Bp = set ? e->d_Bp2 : e->d_Bp;
+  CUtensorMap tmA, tmB, tmC;
+  TRY(encode_operand(e, &tmA, Ap, kdim, m, tc::BM));
+  TRY(encode_operand(e, &tmB, Bp + 2 * j0 * kdim, kdim, 2 * ncols, tc::BN));
+  // C as m rows x 2 ncols FP32 (re, im interleaved), 32 x 32 boxes for the
   // reduce-add epilogue; TMA clips the boxes at the edges of C
-  CUtensorMap tmC;
   {
-    cuuint64_t dims[2] = {(cuuint64_t)(2 * n), (cuuint64_t)m};
+    cuuint64_t dims[2] = {(cuuint64_t)(2 * ncols), (cuuint64_t)m};
     cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float2)};
     cuuint32_t box[2] = {32, 32};
     cuuint32_t estr[2] = {1, 1};
@@ -453,12 +482,21 @@ int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, i
       return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled (C) failed: " + std::to_string((int)r));
   }
   const int m_tiles = (int)((m + tc::BM - 1) / tc::BM);
-  const int n_tiles = (int)((2 * n + tc::BN - 1) / tc::BN);
-  const int grid = std::max(1, std::min(m_tiles * n_tiles, e->nsm));
-  KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)m * n * kb,
-          tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, e->stream>>>(e->tmA, e->tmB, tmC, (int)m, (int)n,
-                                                                              kdim, e->d_status));
+  const int n_tiles = (int)((2 * ncols + tc::BN - 1) / tc::BN);
+  const int grid = std::max(1, std::min(m_tiles * n_tiles, grid_max));
+  const int kt = kbegin(e, st);
+  tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(tmA, tmB, tmC, (int)m, (int)ncols, kdim, e->d_status);
+  kend(e, kt, NECGPU_K_GEMM, 8.0 * (double)m * ncols * kb, st);
+  LAUNCHED();
   return 0;
+}
+
+// C (m x n) -= A (m x kb) B (kb x n), complex64 row-major with leading
+// dimension ld, on the tensor cores (operand set 0, whole device).
+int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, int64_t ld, int64_t m, int64_t n,
+                int kb, int grid_max = 0) {
+  TRY(tc_pack(e, 0, A, B, ld, m, n, kb));
+  return tc_run(e, 0, m, 0, n, kb, C, ld, e->stream, grid_max > 0 ? grid_max : e->nsm);
 }
 
 // trailing update of the FP32 LU for the panel at k0 of width kb
@@ -618,14 +656,25 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm_panel_smem<T>()));
+  // gemm_grid: CTAs the persistent tensor-core update may take (fewer while
+  // a far update runs beside the panel work)
+  int gemm_grid = e->nsm;
   auto gemm = [&](int64_t r0, int64_t c0, int64_t kc, int64_t m, int64_t nc, int kk) -> int {
     // M[r0.., c0..] (m x nc) -= M[r0.., kc..kc+kk) M[kc..kc+kk, c0..)
     if (m <= 0 || nc <= 0 || kk <= 0) return 0;
-    if (e->use_tc) return tc_gemm_sub(e, M + r0 * ld + kc, M + kc * ld + c0, M + r0 * ld + c0, ld, m, nc, kk);
+    if (e->use_tc)
+      return tc_gemm_sub(e, M + r0 * ld + kc, M + kc * ld + c0, M + r0 * ld + c0, ld, m, nc, kk, gemm_grid);
     dim3 gg((unsigned)((nc + 63) / 64), (unsigned)((m + 63) / 64));
     KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)m * nc * kk,
             gemm_sub_kernel<float><<<gg, 256, 0, e->stream>>>(M + r0 * ld + kc, ld, M + kc * ld + c0, ld,
                                                               M + r0 * ld + c0, ld, m, nc, kk));
+    return 0;
+  };
+  auto laswp = [&](int64_t k0, int kb, int64_t c_lo, int64_t c_hi) -> int {
+    if (c_hi <= c_lo) return 0;
+    KLAUNCH(NECGPU_K_LASWP, 0.0,
+            laswp_block_kernel<T><<<(unsigned)((c_hi - c_lo + 31) / 32), 256, 0, e->stream>>>(M, ld, c_lo, c_hi, k0,
+                                                                                               kb, e->d_piv));
     return 0;
   };
   const unsigned smem = (unsigned)trsm_panel_smem<T>();
@@ -633,17 +682,31 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // inner panels whose updates stay inside the outer block's columns; the
   // outer block's U12 rows are brought up to date left-looking, and one
   // tensor-core update with K = outer covers the trailing matrix.
+  //
+  // Lookahead: that trailing update is split.  Its first `outer` columns
+  // (the next outer block) are updated at once; the rest (the far update)
+  // runs on stream2 with lookahead_sms SMs left free, while the next outer
+  // block's panels are factored.  Those panels' row interchanges reach only
+  // columns left of the far update; the far columns get them after the far
+  // update has finished, before the next U12 rows are formed.
   const int64_t outer = e->outer;
+  const bool la = e->lookahead && e->use_tc && e->nsm > 2 * e->lookahead_sms;
+  if (la && !e->stream2) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_far, cudaEventDisableTiming));
+  }
+  bool far_pending = false;
   for (int64_t K0 = 0; K0 < n; K0 += outer) {
     const int64_t KE = std::min<int64_t>(n, K0 + outer);  // end of the outer block
+    const int64_t swap_hi = far_pending ? KE : n;          // columns the far update is not touching
+    gemm_grid = far_pending ? e->lookahead_sms : e->nsm;
     for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
       const int kb = (int)std::min<int64_t>(kBlk, n - k0);
       T* dinv = e->d_dinv + k0;
       KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
               diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, dinv, e->d_status));
-      if (n > kb)
-        KLAUNCH(NECGPU_K_LASWP, 0.0,
-                laswp_block_kernel<T><<<(unsigned)((n + 31) / 32), 256, 0, e->stream>>>(M, ld, n, k0, kb, e->d_piv));
+      if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
       const int64_t r0 = k0 + kb, rest = n - r0;
       if (rest <= 0) continue;
       KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * rest,
@@ -657,6 +720,14 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         TRY(gemm(r0, r0, k0, rest, pc, kb));
       }
     }
+    gemm_grid = e->nsm;
+    if (far_pending) {
+      // the far update of the previous block is complete: its columns get
+      // this block's interchanges
+      CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
+      far_pending = false;
+      for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
+    }
     const int64_t rest = n - KE;
     if (rest <= 0) continue;
     // U12 of the outer row block: rows [K0, KE), columns [KE, n)
@@ -667,8 +738,21 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                   M, ld, n, k0, KE, e->d_dinv + k0));
     }
     // trailing update with K = outer
-    TRY(gemm(KE, KE, K0, rest, rest, (int)(KE - K0)));
+    const int kk = (int)(KE - K0);
+    if (la && rest > outer) {
+      TRY(tc_pack(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk));
+      TRY(tc_run(e, 1, rest, 0, outer, kk, M + KE * ld + KE, ld, e->stream, e->nsm));  // next outer block
+      CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
+      CUDA_TRY(cudaStreamWaitEvent(e->stream2, e->ev_fork, 0));
+      TRY(tc_run(e, 1, rest, outer, rest - outer, kk, M + KE * ld + KE + outer, ld, e->stream2,
+                 e->nsm - e->lookahead_sms));
+      CUDA_TRY(cudaEventRecord(e->ev_far, e->stream2));
+      far_pending = true;
+    } else {
+      TRY(gemm(KE, KE, K0, rest, rest, kk));
+    }
   }
+  if (far_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
   std::vector<int> piv(n), perm(n);
   CUDA_TRY(cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
   e->stats.d2h_bytes += n * sizeof(int);
@@ -1164,6 +1248,11 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_FLAG_SWEEP")) e->inv_sweep = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_NO_DMMA")) e->use_dmma = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD")) e->lookahead = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD_SMS")) {
+    const int v = std::atoi(s);
+    if (v >= 1 && v < 128) e->lookahead_sms = v;
+  }
   CUDA_TRY(cudaFuncSetAttribute(gemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DmmaSmem)));
   if (const char* s = std::getenv("NECPP_B200_OUTER")) {
     const int64_t v = std::atoll(s);
@@ -1199,6 +1288,12 @@ int necgpu_destroy(necgpu_engine* e) {
   dfree(e, e->d_status);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->stream2) {
+    cudaStreamSynchronize(e->stream2);
+    cudaStreamDestroy(e->stream2);
+  }
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_far) cudaEventDestroy(e->ev_far);
   if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return NECGPU_OK;

@@ -611,11 +611,12 @@ __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, in
 
 // Row interchanges of a block-pivoted panel: the kb <= 64 exchanges stay
 // inside rows [k0, k0+kb), so each column is one gather of those rows.  A
-// CTA covers 32 columns with 8 row groups; all reads finish (barrier) before
-// any write.  Columns [k0, k0+kb) (the diagonal block) are skipped.
+// CTA covers 32 columns of [c_lo, c_hi) with 8 row groups; all reads finish
+// (barrier) before any write.  Columns [k0, k0+kb) (the diagonal block) are
+// skipped.
 template <typename T>
-__global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int kb,
-                                                          const int* piv) {
+__global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int64_t c_lo, int64_t c_hi, int64_t k0,
+                                                          int kb, const int* piv) {
   constexpr int NB = kBlk, RG = 8, PER = NB / RG;
   __shared__ int sp[NB];
   __shared__ int src[NB];
@@ -633,8 +634,8 @@ __global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int6
     }
   }
   __syncthreads();
-  const int64_t col = (int64_t)blockIdx.x * 32 + tx;
-  const bool act = col < n && !(col >= k0 && col < k0 + kb);
+  const int64_t col = c_lo + (int64_t)blockIdx.x * 32 + tx;
+  const bool act = col < c_hi && !(col >= k0 && col < k0 + kb);
   T v[PER];
 #pragma unroll
   for (int i = 0; i < PER; i++) {
