@@ -63,7 +63,8 @@ long nec_fr_card(nec_context* in_context, int in_ifrq, int in_nfrq, double in_fr
                  double in_del_freq);
 /* src/libnecpp.h:282 */
 long nec_ek_card(nec_context* in_context, int itmp1);
-/* src/libnecpp.h:303 (loads: returns 1) */
+/* src/libnecpp.h:303: impedance loading (types 0-5: series / parallel RLC,
+   per metre, fixed impedance, wire conductivity) */
 long nec_ld_card(nec_context* in_context, int ldtyp, int ldtag, int ldtagf, int ldtagt,
                  double tmp1, double tmp2, double tmp3);
 /* src/libnecpp.h:330 */
@@ -171,6 +172,9 @@ long nec_get_structure(nec_context* in_context, double* seg, int* tptr, int* tba
    frequency (nec_context::etmns, src/nec_context.cpp:3488-3550): n complex,
    interleaved; host only. */
 long nec_get_rhs(nec_context* in_context, double* out);
+/* Impedance loading (n complex: lambda x impedance per unit length, the
+   reference's zarray) of the structure prepared last; zeros if unloaded. */
+long nec_get_loads(nec_context* in_context, double* out);
 /* The context's GPU engine (include/necgpu.h), created on first use; NULL
    with nec_error_message() set when no usable device exists. */
 void* nec_gpu_engine(nec_context* in_context);

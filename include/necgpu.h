@@ -87,6 +87,12 @@ int necgpu_set_stream(necgpu_engine* e, void* stream);
 /* Upload one structure (host arrays, copied). */
 int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s);
 
+/* Impedance loading of the structure set last (n complex: the reference's
+ * zarray, lambda x impedance per unit length, from load(),
+ * src/nec_context.cpp:1861-2072), applied by every later necgpu_fill as
+ * cmset does (2127-2142); NULL removes it.  necgpu_set_structure clears it. */
+int necgpu_set_loads(necgpu_engine* e, const double* zload);
+
 /* Replaces cmset (src/nec_context.cpp:2077-2204) for wires: fills Z on the
  * device, row-major, Z[obs*n + basis] = field at obs due to basis (the
  * reference's cm layout). */

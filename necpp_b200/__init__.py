@@ -93,6 +93,7 @@ _sig("nec_get_currents", _l, [_p, _i, _dp, _l])
 _sig("nec_get_segments", _l, [_p] + [_dp] * 8 + [_ip] * 3)
 _sig("nec_get_trio", _l, [_p, _i, _ip, _dp, _dp, _dp, _l])
 _sig("nec_last_refinement", _l, [_p, _ip, _dp])
+_sig("nec_get_loads", _l, [_p, _dp])
 _sig("nec_gradient", _l, [_p, _i, _C.POINTER(_p), _C.POINTER(_p), _dp, _d, _d, _dp, _dp])
 _sig("nec_prepare_structure", _l, [_p, _d])
 _sig("nec_get_structure", _l, [_p, _dp, _ip, _ip, _dp, _ip, _dp])
@@ -199,6 +200,9 @@ def structure(nec, freq_mhz=None):
                           _iptr(st["ind"]), _dptr(st["params"]))
     st["tbasis"] = st["tbasis"][:nt]
     st["tabc"] = st["tabc"][:3 * nt].copy()
+    zl = _np.zeros(2 * n)
+    lib.nec_get_loads(nec, _dptr(zl))
+    st["zload"] = zl[0::2] + 1j * zl[1::2]
     return st
 
 

@@ -104,6 +104,8 @@ def host_problem(ctx, freq_mhz, feed_index, voltage=1.0 + 0j):
     """Tables and right-hand side of context ctx at freq_mhz (host only);
     feed_index: 0-based segment of the voltage source."""
     st = structure(ctx, freq_mhz)
+    if _np.any(st["zload"] != 0):
+        raise ValueError("batched sweeps do not carry impedance loading (LD cards)")
     b = _rhs(ctx)
     return st, b, int(feed_index), complex(voltage), _C0 / (freq_mhz * 1e6)
 

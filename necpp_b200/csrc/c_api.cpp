@@ -84,8 +84,20 @@ long nec_fr_card(nec_context* c, int ifrq, int nfrq, double f, double df) {
 
 long nec_ek_card(nec_context* c, int itmp1) { NEC_TRY(c->ek_card(itmp1)); }
 
-long nec_ld_card(nec_context*, int, int, int, int, double, double, double) {
-  NEC_UNSUPPORTED("LD (loading)");
+long nec_ld_card(nec_context* c, int ldtyp, int ldtag, int ldtagf, int ldtagt, double tmp1, double tmp2,
+                 double tmp3) {
+  NEC_TRY(c->ld_card(ldtyp, ldtag, ldtagf, ldtagt, tmp1, tmp2, tmp3));
+}
+
+long nec_get_loads(nec_context* c, double* out) {
+  if (!c || !out) return 1;
+  const auto& z = c->loads();
+  const int64_t n = c->geometry().n;
+  for (int64_t i = 0; i < n; i++) {
+    out[2 * i] = z.empty() ? 0.0 : z[i].real();
+    out[2 * i + 1] = z.empty() ? 0.0 : z[i].imag();
+  }
+  return 0;
 }
 
 long nec_ex_card(nec_context* c, int extype, int i2, int i3, int i4, double t1, double t2,

@@ -92,6 +92,163 @@ void Context::fr_card(int in_ifrq, int in_nfrq, double in_freq, double in_del) {
 
 // gn_card / nec_ground::parse_gn, src/nec_context.cpp:486-499,
 // src/nec_ground.cpp:75-120
+// ld_card, src/nec_context.cpp:424-473: consecutive LD cards accumulate;
+// the first after other cards (or type -1) clears the previous loads.
+void Context::ld_card(int type, int tag, int tag_from, int tag_to, double zr, double zi, double zc) {
+  if (iflow != 3) {
+    iflow = 3;
+    ldtyp.clear();
+    ldtag.clear();
+    ldtagf.clear();
+    ldtagt.clear();
+    zlr.clear();
+    zli.clear();
+    zlc.clear();
+    zarray.clear();
+    reset_to_structure_loading();
+    if (type == -1) return;
+  }
+  if (tag_to == 0) tag_to = tag_from;
+  ldtyp.push_back(type);
+  ldtag.push_back(tag);
+  ldtagf.push_back(tag_from);
+  ldtagt.push_back(tag_to);
+  // a faulty card stays in the list with zero impedance, as in the reference
+  zlr.push_back(0.0);
+  zli.push_back(0.0);
+  zlc.push_back(0.0);
+  if (tag_to < tag_from)
+    fail("DATA FAULT ON LOADING CARD No: ", (int)ldtyp.size(), ": ITAG STEP1: ", tag_from,
+         " IS GREATER THAN ITAG STEP2: ", tag_to);
+  zlr.back() = zr;
+  zli.back() = zi;
+  zlc.back() = zc;
+}
+
+namespace {
+// Internal impedance of a round wire of conductivity sigl (S/m, times the
+// wavelength) and radius rolam (wavelengths): the reference's zint
+// (src/nec_context.cpp:6321-6400), i.e. the NEC-2 ratio of Kelvin functions
+// from polynomial approximations for x <= 8, asymptotic series up to 110 and
+// the skin-effect limit beyond.
+cd wire_internal_impedance(double sigl, double rolam) {
+  const cd j1(0.0, 1.0);
+  const double tpcmu = 2.368705e+3, cmotp = 60.00;
+  const double x = std::sqrt(tpcmu * sigl) * rolam;
+  if (x > 110.0) {
+    const cd br1(0.70710678, -0.70710678);
+    return j1 * std::sqrt(cmotp / sigl) * br1 / rolam;
+  }
+  if (x > 8.0) {
+    const cd c1(6.0e-7, 1.9e-6), c2(-3.4e-6, 5.1e-6), c3(-2.52e-5, 0.0), c4(-9.06e-5, -9.01e-5),
+        c5(0., -9.765e-4), c6(.0110486, -.0110485), c7(0., -.3926991), c8(1.6e-6, -3.2e-6), c9(1.17e-5, -2.4e-6),
+        c10(3.46e-5, 3.38e-5), c11(5.0e-7, 2.452e-4), c12(-1.3813e-3, 1.3811e-3), c13(-6.25001e-2, -1.0e-7),
+        c14(.7071068, .7071068);
+    auto th = [&](double d) { return (((((c1 * d + c2) * d + c3) * d + c4) * d + c5) * d + c6) * d + c7; };
+    auto ph = [&](double d) { return (((((c8 * d + c9) * d + c10) * d + c11) * d + c12) * d + c13) * d + c14; };
+    const cd f = std::sqrt(kPi * 0.5 / x) * std::exp(-c14 * x + th(-8. / x));
+    const cd g = std::exp(c14 * x + th(8. / x)) / std::sqrt(kTwoPi * x);
+    cd br2 = j1 * f / kPi;
+    cd br1 = g + br2;
+    br2 = g * ph(8.0 / x) - br2 * ph(-8.0 / x);
+    br1 = br1 / br2;
+    return j1 * std::sqrt(cmotp / sigl) * br1 / rolam;
+  }
+  const double x8 = x / 8.0, y = x8 * x8, s = y * y;
+  double ber = ((((((-9.01e-6 * s + 1.22552e-3) * s - .08349609) * s + 2.6419140) * s - 32.363456) * s + 113.77778) * s -
+                64.) * s + 1.;
+  double bei = ((((((1.1346e-4 * s - .01103667) * s + .52185615) * s - 10.567658) * s + 72.817777) * s - 113.77778) * s +
+                16.) * y;
+  cd br1(ber, bei);
+  ber = (((((((-3.94e-6 * s + 4.5957e-4) * s - 0.02609253) * s + 0.66047849) * s - 6.0681481) * s + 14.222222) * s -
+          4.0) * y) * x;
+  bei = ((((((4.609e-5 * s - 3.79386e-3) * s + .14677204) * s - 2.3116751) * s + 11.377778) * s - 10.666667) * s + .5) *
+        x;
+  const cd br2(ber, bei);
+  br1 = br1 / br2;
+  return j1 * std::sqrt(cmotp / sigl) * br1 / rolam;
+}
+}  // namespace
+
+// load, src/nec_context.cpp:1861-2072: lambda x impedance per unit length of
+// every loaded segment at the current scaling (lengths in wavelengths).
+void Context::load() {
+  const int64_t n = geo_.n;
+  zarray.assign(n, cd(0, 0));
+  if (ldtyp.empty()) {
+    zarray.clear();
+    return;
+  }
+  const cd tpcj(0.0, 1.883698955e+9);
+  const double lam = wavelength_;
+  for (size_t k = 0; k < ldtyp.size(); k++) {
+    if (ldtyp[k] > 5 || ldtyp[k] < 0) fail("IMPROPER LOAD TYPE CHOSEN, REQUESTED TYPE IS ", ldtyp[k]);
+    const int tags = ldtag[k];
+    int64_t l1 = 1, l2 = n;
+    int ichk = 0;
+    if (tags == 0 && (ldtagf[k] != 0 || ldtagt[k] != 0)) {
+      l1 = ldtagf[k];
+      l2 = ldtagt[k];
+    }
+    for (int64_t i = l1 - 1; i < l2 && i < n; i++) {
+      if (i < 0) continue;
+      if (tags != 0) {
+        if (tags != geo_.tags[i]) continue;
+        if (ldtagf[k] != 0) {
+          ichk++;
+          if (ichk < ldtagf[k] || ichk > ldtagt[k]) continue;
+        } else {
+          ichk = 1;
+        }
+      } else {
+        ichk = 1;
+      }
+      const double sl = geo_.length[i];
+      cd zt;
+      switch (ldtyp[k]) {
+        case 0:  // series RLC
+          zt = zlr[k] / sl + tpcj * zli[k] / (sl * lam);
+          if (std::fabs(zlc[k]) > 1.0e-20) zt += lam / (tpcj * sl * zlc[k]);
+          break;
+        case 1:  // parallel RLC
+          zt = tpcj * sl * zlc[k] / lam;
+          if (std::fabs(zli[k]) > 1.0e-20) zt += sl * lam / (tpcj * zli[k]);
+          if (std::fabs(zlr[k]) > 1.0e-20) zt += sl / zlr[k];
+          zt = 1. / zt;
+          break;
+        case 2:  // series RLC per metre
+          zt = zlr[k] * lam + tpcj * zli[k];
+          if (std::fabs(zlc[k]) > 1.0e-20) zt += 1. / (tpcj * sl * sl * zlc[k]);
+          break;
+        case 3:  // parallel RLC per metre
+          zt = tpcj * sl * sl * zlc[k];
+          if (std::fabs(zli[k]) > 1.0e-20) zt += 1. / (tpcj * zli[k]);
+          if (std::fabs(zlr[k]) > 1.0e-20) zt += 1. / (zlr[k] * lam);
+          zt = 1. / zt;
+          break;
+        case 4:  // fixed impedance
+          zt = cd(zlr[k], zli[k]) / sl;
+          break;
+        default:  // wire conductivity
+          zt = wire_internal_impedance(zlr[k] * lam, geo_.radius[i]);
+      }
+      zarray[i] += zt;
+    }
+    if (ichk == 0) fail("LOADING DATA CARD ERROR, NO SEGMENT HAS AN ITAG = ", tags);
+  }
+}
+
+// compute_structure_power_loss, src/nec_context.cpp:1423-1441
+double Context::compute_structure_power_loss() const {
+  double loss = 0.0;
+  for (size_t i = 0; i < zarray.size(); i++)
+    if (std::fabs(zarray[i].real()) >= 1.e-20) {
+      const double cmag = std::abs(solution[i] * wavelength_);
+      loss += 0.5 * cmag * cmag * zarray[i].real() * geo_.length[i];
+    }
+  return loss;
+}
+
 void Context::gn_card(int itmp1, int itmp2, double t1, double t2, double t3,
                       double t4, double t5, double t6) {
   (void)t3;
@@ -326,15 +483,14 @@ int Context::excitation_loop(int state_in, int mhz) {
   }
 }
 
-// excitation_process_inner, src/nec_context.cpp:1622-1738 (no networks, no
-// loads, no coupling).
+// excitation_process_inner, src/nec_context.cpp:1622-1738 (no coupling).
 int Context::excitation_inner(int mhz) {
   (void)mhz;
   network_solve();
   if (iptflg < -2 || iptflg > 3) iptflg = -1;
   if (iptflq < -2 || iptflq > 0) iptflq = -1;
   if (ex_type != 1 && ex_type != 2 && ex_type != 3 && (iptflg == 2 || iptflg == 3)) iptflg = -1;
-  structure_power_loss = 0.0;
+  structure_power_loss = compute_structure_power_loss();
   if (iptflg != -1 || iptflq != -1) {
     if ((iptflg < 1 || iptflg == 3 || ((iptflg == 1 || iptflg == 2) && inc <= 1)) ||
         (iptflg == -1 && iptflq != -1)) {
@@ -385,6 +541,7 @@ void Context::prepare_structure(double freq) {
   wavelength_ = wavelength_of(1.0e6 * freq_mhz);
   geo_.frequency_scale(freq_mhz);
   build_tables();
+  load();
 }
 
 // Ground environment, basis tables (trio per source segment) and the
@@ -512,9 +669,11 @@ necgpu_structure Context::structure_view() const {
 
 void Context::structure_loading() {
   build_tables();
+  load();
   const necgpu_structure s = structure_view();
   necgpu_engine* e = engine();
   check(e, necgpu_set_structure(e, &s));
+  check(e, necgpu_set_loads(e, zarray.empty() ? nullptr : reinterpret_cast<const double*>(zarray.data())));
   check(e, necgpu_fill(e));
   check(e, necgpu_factor(e, precision_));
   have_factor_ = true;
@@ -673,6 +832,7 @@ void Context::network_solve() {
                       abc.data());
   }
   check(e, rc);
+  structure_power_loss = compute_structure_power_loss();
   necgpu_stats st{};
   necgpu_get_stats(e, &st);
   last_refine_residual = st.refine_residual;
@@ -941,6 +1101,7 @@ void Context::gradient(int nparam, Context* const* plus, Context* const* minus, 
   if (!have_factor_ || !eng_ || inputs.empty()) fail("gradient: run the forward solve (an XQ or RP card) first");
   if (src_seg.size() != 1) fail("gradient: exactly one voltage source is supported");
   if (precision_ != 1) fail("gradient: needs the mixed-precision path (nec_set_precision(ctx, 1))");
+  if (!zarray.empty()) fail("gradient: loaded structures (LD cards) are not supported");
   necgpu_engine* e = eng_;
   const int64_t n = geo_.n;
   const int64_t f = src_seg[0] - 1;

@@ -68,6 +68,7 @@ class Context {
                int xnda_a, double th0, double ph0, double dth, double dph,
                double rfld, double gnor);
   void kh_card(double rkh);
+  void ld_card(int type, int tag, int tag_from, int tag_to, double zr, double zi, double zc);
   void ek_card(int flag);
   void pt_card(int a, int b, int c, int d);
   void pq_card(int a, int b, int c, int d);
@@ -102,6 +103,9 @@ class Context {
                 double phi_deg, double* value, double* grad);
   // the current structure as the GPU receives it (views of this context's arrays)
   necgpu_structure structure_view() const;
+  // impedance loading of every segment at the prepared frequency (lambda x
+  // impedance per unit length, as the reference's zarray), empty if unloaded
+  const std::vector<cd>& loads() const { return zarray; }
   struct Tables {
     std::vector<int32_t> tptr, tbasis, ind1, ind2;
     std::vector<double> ta, tb, tc;
@@ -112,6 +116,12 @@ class Context {
 
  private:
   void build_tables();
+  void load();
+  double compute_structure_power_loss() const;
+  // LD cards (names follow the reference's members) and their zarray
+  std::vector<int> ldtyp, ldtag, ldtagf, ldtagt;
+  std::vector<double> zlr, zli, zlc;
+  std::vector<cd> zarray;
   enum State { MEM = 1, STRUCT = 2, EXSETUP = 3, EXLOOP = 4, NEAR = 5, FAR = 6 };
   enum Ret { PRINT_NORM = 0, FREQ_CONT = 1, CARD_CONT = 2, INNER_CONT = 3, PHASE_DONE = 4 };
 

@@ -117,6 +117,7 @@ struct necgpu_engine {
   int lookahead_sms = 48;
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
+  double2* d_zload = nullptr;  // impedance loading per segment (null: unloaded)
   float2* d_tinv = nullptr;  // inverted 64 x 64 diagonal blocks of the complex64 factors
   // adjoint solves: transposed factors, matrix and block inverses
   float2* ZT32 = nullptr;
@@ -278,6 +279,7 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->d_ccoef);
   dfree(e, e->Z64);
   dfree(e, e->d_dinv);
+  dfree(e, e->d_zload);
   dfree(e, e->d_Ap2);
   dfree(e, e->d_Bp2);
   e->tc_rows2 = 0;
@@ -400,13 +402,24 @@ int run_fill(necgpu_engine* e, bool want64, bool want32) {
   a.Z32 = want32 ? e->Z32 : nullptr;
   a.status = e->d_status;
   const bool x = e->use_exk != 0;
+  int rc;
   switch (e->ground) {
-    case kGroundNone: return x ? launch_fill_t<kGroundNone, true>(e, a) : launch_fill_t<kGroundNone, false>(e, a);
-    case kGroundPerfect: return x ? launch_fill_t<kGroundPerfect, true>(e, a) : launch_fill_t<kGroundPerfect, false>(e, a);
+    case kGroundNone: rc = x ? launch_fill_t<kGroundNone, true>(e, a) : launch_fill_t<kGroundNone, false>(e, a); break;
+    case kGroundPerfect:
+      rc = x ? launch_fill_t<kGroundPerfect, true>(e, a) : launch_fill_t<kGroundPerfect, false>(e, a);
+      break;
     case kGroundReflection:
-      return x ? launch_fill_t<kGroundReflection, true>(e, a) : launch_fill_t<kGroundReflection, false>(e, a);
-    default: return x ? launch_fill_t<kGroundSommerfeld, true>(e, a) : launch_fill_t<kGroundSommerfeld, false>(e, a);
+      rc = x ? launch_fill_t<kGroundReflection, true>(e, a) : launch_fill_t<kGroundReflection, false>(e, a);
+      break;
+    default: rc = x ? launch_fill_t<kGroundSommerfeld, true>(e, a) : launch_fill_t<kGroundSommerfeld, false>(e, a);
   }
+  if (rc) return rc;
+  if (e->d_zload && want64)
+    KLAUNCH(NECGPU_K_FILL, 0.0,
+            load_kernel<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef,
+                                                                            e->d_ccoef + 2 * e->nc, e->d_zload,
+                                                                            e->Z64, e->ld));
+  return 0;
 }
 
 // ---------------- tensor-core trailing update ----------------
@@ -1386,6 +1399,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   e->filled = false;
   e->have_solution = false;
   e->adj_ready = false;
+  dfree(e, e->d_zload);  // loads belong to one structure: set them after it
   dfree(e, e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
 
   std::vector<double> seg(8 * n);
@@ -1622,6 +1636,19 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
   dfree(e, Y);
   dfree(e, d);
   return rc;
+}
+
+int necgpu_set_loads(necgpu_engine* e, const double* zload) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (e->n <= 0) return fail(e, NECGPU_ERR_ARG, "set_loads: no structure set");
+  CUDA_TRY(cudaSetDevice(e->device));
+  if (!zload) {
+    dfree(e, e->d_zload);
+    return NECGPU_OK;
+  }
+  TRY(upload(e, e->d_zload, reinterpret_cast<const double2*>(zload), (size_t)e->n));
+  e->filled = false;
+  return NECGPU_OK;
 }
 
 int necgpu_copy_solution(necgpu_engine* e, double* x) {

@@ -590,4 +590,21 @@ __global__ void axpy_scatter_kernel(double2* x, const float2* d, const int* perm
   x[perm[i]] = v;
 }
 
+// Impedance loading (src/nec_context.cpp:2127-2142): row j of Z loses
+// (a + c) * zload[j] at every basis function with support on segment j.
+// One thread per segment; rows are distinct, so no two threads meet.
+__global__ void load_kernel(int64_t n, const int32_t* cptr, const int32_t* cbasis, const double* ca,
+                            const double* cc, const double2* zload, double2* Z, int64_t ld) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double2 zl = zload[j];
+  if (zl.x == 0.0 && zl.y == 0.0) return;
+  for (int e = cptr[j]; e < cptr[j + 1]; e++) {
+    const double w = ca[e] + cc[e];
+    double2* p = Z + j * ld + cbasis[e];
+    p->x -= w * zl.x;
+    p->y -= w * zl.y;
+  }
+}
+
 }  // namespace necb

@@ -609,6 +609,12 @@ int mo_fill(const mo_structure* S, double* zout) {
         z[i * n + b] += rmul(S->trio_a[k], etk) + rmul(S->trio_b[k], ets) + rmul(S->trio_c[k], etc);
       }
     }
+    /* loading of row j, after source j's contributions (2127-2142) */
+    if (S->zload) {
+      cx zaj = CMPLX(S->zload[2 * j], S->zload[2 * j + 1]);
+      for (int32_t k = S->trio_ptr[j]; k < S->trio_ptr[j + 1]; k++)
+        z[j * n + S->trio_basis[k]] -= rmul(S->trio_a[k] + S->trio_c[k], zaj);
+    }
   }
   return st;
 }

@@ -26,6 +26,9 @@ typedef struct mo_structure {
   int ground; /* 0 none, 1 perfect, 2 reflection coefficient, 3 Sommerfeld/Norton */
   double zrati_re, zrati_im, frati_re, frati_im;
   double eta;
+  /* impedance loading per segment (n complex, re/im interleaved; the
+     reference's zarray after load(), src/nec_context.cpp:1861-2072), or NULL */
+  const double* zload;
 } mo_structure;
 
 /* Fill: z[obs*n + basis] (interleaved re, im); returns status bits

@@ -21,7 +21,7 @@ class MoStructure(C.Structure):
         ("trio_ptr", _ip), ("trio_basis", _ip), ("trio_a", _dp), ("trio_b", _dp), ("trio_c", _dp),
         ("ind1", _ip), ("ind2", _ip), ("rkh", C.c_double), ("use_exk", C.c_int), ("ground", C.c_int),
         ("zrati_re", C.c_double), ("zrati_im", C.c_double), ("frati_re", C.c_double),
-        ("frati_im", C.c_double), ("eta", C.c_double)]
+        ("frati_im", C.c_double), ("eta", C.c_double), ("zload", _dp)]
 
 
 def build():
@@ -66,6 +66,10 @@ class Oracle:
         p = st["params"]
         s.rkh, s.use_exk, s.ground = p[0], int(p[1]), int(p[2])
         s.zrati_re, s.zrati_im, s.frati_re, s.frati_im, s.eta = p[3], p[4], p[5], p[6], p[7]
+        zl = st.get("zload")
+        if zl is not None and np.any(zl != 0):
+            st["_zload_ri"] = np.ascontiguousarray(np.asarray(zl, dtype=np.complex128)).view(np.float64)
+            s.zload = st["_zload_ri"].ctypes.data_as(_dp)
         return s
 
     def fill(self, st):

@@ -91,6 +91,43 @@ def _plane_wave_reflection(api, ctx):
     return 145.0
 
 
+def _yagi_loaded(api, ctx):
+    """Every load type: series / parallel RLC (lumped and per metre), fixed
+    impedance and wire conductivity, by tag, tag range and absolute segment
+    numbers; two frequencies (the loads are recomputed per frequency)."""
+    p = W.yagi_params(np.random.default_rng(3), n_elements=5, nseg=11)
+    half, xs, rad, segs = p
+    for e in range(len(half)):
+        api.nec_wire(ctx, e + 1, int(segs[e]), float(xs[e]), 0.0, -float(half[e]), float(xs[e]), 0.0,
+                     float(half[e]), float(rad[e]), 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 0)
+    api.nec_ld_card(ctx, 0, 2, 6, 6, 5.0, 2.0e-8, 3.0e-11)      # series RLC at the feed
+    api.nec_ld_card(ctx, 1, 3, 4, 8, 1.0e3, 4.0e-7, 2.0e-12)    # parallel RLC, segments 4-8 of tag 3
+    api.nec_ld_card(ctx, 2, 1, 0, 0, 0.5, 1.0e-7, 0.0)          # series per metre, all of tag 1
+    api.nec_ld_card(ctx, 3, 4, 2, 3, 2.0e4, 1.0e-6, 1.0e-12)    # parallel per metre
+    api.nec_ld_card(ctx, 4, 0, 50, 52, 3.0, -7.0, 0.0)          # fixed impedance, absolute segments 50-52
+    api.nec_ld_card(ctx, 5, 5, 0, 0, 3.7e7, 0.0, 0.0)           # aluminium wire, tag 5
+    api.nec_fr_card(ctx, 0, 2, 140.0, 10.0)
+    api.nec_ex_card(ctx, 0, 2, 6, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    # directive gain: normalised by the radiated power, input minus load loss
+    api.nec_rp_card(ctx, 0, 19, 8, 1, 0, 1, 0, 0.0, 0.0, 10.0, 45.0, 0.0, 0.0)
+    return 150.0
+
+
+def _dipoles_conductivity(api, ctx):
+    """Wire conductivity in the three ranges of the internal-impedance
+    approximation (x <= 8, 8 < x <= 110, x > 110) on three dipoles."""
+    for t, sig in enumerate((1.0e4, 5.0e5, 5.8e7)):
+        api.nec_wire(ctx, t + 1, 21, 0.8 * t, 0.0, -0.5, 0.8 * t, 0.0, 0.5, 1.0e-3, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 0)
+    for t, sig in enumerate((1.0e4, 5.0e5, 5.8e7)):
+        api.nec_ld_card(ctx, 5, t + 1, 0, 0, sig, 0.0, 0.0)
+    api.nec_fr_card(ctx, 0, 1, 150.0, 0.0)
+    api.nec_ex_card(ctx, 0, 2, 11, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_rp_card(ctx, 0, 19, 8, 1, 0, 0, 0, 0.0, 0.0, 10.0, 45.0, 0.0, 0.0)
+    return 150.0
+
+
 # name: (builder, pattern grid (n_theta, n_phi) or None)
 CASES = {
     "ex1": (_ex1, None),
@@ -105,4 +142,6 @@ CASES = {
     "yagi_ground": (_yagi_ground, (1, 1)),
     "yagi_ek_perfect": (_yagi_ek_perfect, (10, 4)),
     "plane_wave_reflection": (_plane_wave_reflection, (10, 4)),
+    "yagi_loaded": (_yagi_loaded, (19, 8)),
+    "dipoles_conductivity": (_dipoles_conductivity, (19, 8)),
 }

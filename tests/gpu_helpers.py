@@ -39,6 +39,7 @@ class Engine:
         L.necgpu_copy_z.argtypes = [C.c_void_p, _dp]
         L.necgpu_set_refinement.argtypes = [C.c_void_p, C.c_double, C.c_int]
         L.necgpu_set_pivoting.argtypes = [C.c_void_p, C.c_int]
+        L.necgpu_set_loads.argtypes = [C.c_void_p, _dp]
         L.necgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(NecgpuStats)]
         self.h = C.c_void_p()
         rc = L.necgpu_create(C.byref(self.h), device)
@@ -72,8 +73,11 @@ class Engine:
         p = st["params"]
         s.rkh, s.use_exk, s.ground = p[0], int(p[1]), int(p[2])
         s.zrati_re, s.zrati_im, s.frati_re, s.frati_im, s.eta = p[3], p[4], p[5], p[6], p[7]
-        self._keep = (st, s)
         self.check(self.lib.necgpu_set_structure(self.h, C.byref(s)))
+        zl = np.ascontiguousarray(st.get("zload", np.zeros(n, complex)), dtype=complex)
+        self._keep = (st, s, zl)
+        if np.any(zl != 0):
+            self.check(self.lib.necgpu_set_loads(self.h, zl.ctypes.data_as(_dp)))
         self.n = n
 
     def fill(self):
