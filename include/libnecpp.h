@@ -80,7 +80,9 @@ long nec_excitation_current(nec_context* in_context, double x, double y, double 
 long nec_excitation_planewave(nec_context* in_context, int n_theta, int n_phi, double theta,
                               double phi, double eta, double dtheta, double dphi,
                               double pol_ratio);
-/* src/libnecpp.h:387-388 (networks: return 1) */
+/* src/libnecpp.h:387-388: transmission lines (Z0 < 0 crosses the line;
+   length <= 0 takes the distance between the two port segments) and
+   two-port networks given by their short-circuit admittances */
 long nec_tl_card(nec_context* in_context, int itmp1, int itmp2, int itmp3, int itmp4,
                  double tmp1, double tmp2, double tmp3, double tmp4, double tmp5, double tmp6);
 long nec_nt_card(nec_context* in_context, int itmp1, int itmp2, int itmp3, int itmp4,
@@ -175,6 +177,8 @@ long nec_get_rhs(nec_context* in_context, double* out);
 /* Impedance loading (n complex: lambda x impedance per unit length, the
    reference's zarray) of the structure prepared last; zeros if unloaded. */
 long nec_get_loads(nec_context* in_context, double* out);
+/* Number of NT/TL networks on the context (0 if none). */
+long nec_network_count(nec_context* in_context);
 /* The context's GPU engine (include/necgpu.h), created on first use; NULL
    with nec_error_message() set when no usable device exists. */
 void* nec_gpu_engine(nec_context* in_context);

@@ -94,6 +94,7 @@ _sig("nec_get_segments", _l, [_p] + [_dp] * 8 + [_ip] * 3)
 _sig("nec_get_trio", _l, [_p, _i, _ip, _dp, _dp, _dp, _l])
 _sig("nec_last_refinement", _l, [_p, _ip, _dp])
 _sig("nec_get_loads", _l, [_p, _dp])
+_sig("nec_network_count", _l, [_p])
 _sig("nec_gradient", _l, [_p, _i, _C.POINTER(_p), _C.POINTER(_p), _dp, _d, _d, _dp, _dp])
 _sig("nec_prepare_structure", _l, [_p, _d])
 _sig("nec_get_structure", _l, [_p, _dp, _ip, _ip, _dp, _ip, _dp])
@@ -120,7 +121,7 @@ _PUBLIC = [
     "nec_sc_card", "nec_gx_card", "nec_tl_card", "nec_nt_card", "nec_ne_card", "nec_nh_card",
     "nec_gd_card", "nec_cp_card", "nec_gain", "nec_impedance_real", "nec_impedance_imag",
     "nec_impedance_real_indexed", "nec_impedance_imag_indexed", "nec_set_precision",
-    "nec_set_intersection_check", "nec_segment_count", "nec_frequency_scale",
+    "nec_set_intersection_check", "nec_segment_count", "nec_frequency_scale", "nec_network_count",
 ] + [p + s for s in ("max", "min", "mean", "sd")
      for p in ("nec_gain_", "nec_gain_rhcp_", "nec_gain_lhcp_")]
 
@@ -203,6 +204,7 @@ def structure(nec, freq_mhz=None):
     zl = _np.zeros(2 * n)
     lib.nec_get_loads(nec, _dptr(zl))
     st["zload"] = zl[0::2] + 1j * zl[1::2]
+    st["networks"] = int(lib.nec_network_count(nec))
     return st
 
 

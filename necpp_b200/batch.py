@@ -106,6 +106,8 @@ def host_problem(ctx, freq_mhz, feed_index, voltage=1.0 + 0j):
     st = structure(ctx, freq_mhz)
     if _np.any(st["zload"] != 0):
         raise ValueError("batched sweeps do not carry impedance loading (LD cards)")
+    if st["networks"]:
+        raise ValueError("batched sweeps do not carry networks or transmission lines (NT/TL cards)")
     b = _rhs(ctx)
     return st, b, int(feed_index), complex(voltage), _C0 / (freq_mhz * 1e6)
 

@@ -89,6 +89,8 @@ long nec_ld_card(nec_context* c, int ldtyp, int ldtag, int ldtagf, int ldtagt, d
   NEC_TRY(c->ld_card(ldtyp, ldtag, ldtagf, ldtagt, tmp1, tmp2, tmp3));
 }
 
+long nec_network_count(nec_context* c) { return c ? c->network_count() : -1; }
+
 long nec_get_loads(nec_context* c, double* out) {
   if (!c || !out) return 1;
   const auto& z = c->loads();
@@ -120,13 +122,13 @@ long nec_excitation_planewave(nec_context* c, int n_theta, int n_phi, double the
   NEC_TRY(c->ex_card(1, n_theta, n_phi, 0, theta, phi, eta, dtheta, dphi, pol_ratio));
 }
 
-long nec_tl_card(nec_context*, int, int, int, int, double, double, double, double, double,
-                 double) {
-  NEC_UNSUPPORTED("TL (transmission line)");
+long nec_tl_card(nec_context* c, int itmp1, int itmp2, int itmp3, int itmp4, double tmp1, double tmp2,
+                 double tmp3, double tmp4, double tmp5, double tmp6) {
+  NEC_TRY(c->tl_card(itmp1, itmp2, itmp3, itmp4, tmp1, tmp2, tmp3, tmp4, tmp5, tmp6));
 }
-long nec_nt_card(nec_context*, int, int, int, int, double, double, double, double, double,
-                 double) {
-  NEC_UNSUPPORTED("NT (network)");
+long nec_nt_card(nec_context* c, int itmp1, int itmp2, int itmp3, int itmp4, double tmp1, double tmp2,
+                 double tmp3, double tmp4, double tmp5, double tmp6) {
+  NEC_TRY(c->nt_card(itmp1, itmp2, itmp3, itmp4, tmp1, tmp2, tmp3, tmp4, tmp5, tmp6));
 }
 
 long nec_xq_card(nec_context* c, int itmp1) { NEC_TRY(c->xq_card(itmp1)); }

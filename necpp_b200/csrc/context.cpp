@@ -125,6 +125,70 @@ void Context::ld_card(int type, int tag, int tag_from, int tag_to, double zr, do
   zlc.back() = zc;
 }
 
+// nt_card / tl_card, src/nec_context.cpp:630-707: the first NT or TL card
+// after other cards clears the networks (seg1 == -1 cancels them all).
+void Context::network_card(int type, int tag1, int seg1, int tag2, int seg2, const double* x) {
+  if (iflow != 6) {
+    ntyp.clear();
+    iseg1.clear();
+    iseg2.clear();
+    x11r.clear();
+    x11i.clear();
+    x12r.clear();
+    x12i.clear();
+    x22r.clear();
+    x22i.clear();
+    ntsol = 0;
+    iflow = 6;
+    reset_to_excitation_setup();
+    if (seg1 == -1) return;
+  }
+  if (!geo_.completed) fail("NT/TL card before geometry_complete");
+  const int64_t s1 = geo_.segment_number(tag1, seg1);
+  const int64_t s2 = geo_.segment_number(tag2, seg2);
+  if (s1 < 1 || s1 > geo_.n || s2 < 1 || s2 > geo_.n)
+    fail("NETWORK DATA ERROR: SEGMENT NUMBER OUT OF RANGE (", s1, ", ", s2, ")");
+  ntyp.push_back(type);
+  iseg1.push_back(s1);
+  iseg2.push_back(s2);
+  x11r.push_back(x[0]);
+  x11i.push_back(x[1]);
+  x12r.push_back(x[2]);
+  x12i.push_back(x[3]);
+  x22r.push_back(x[4]);
+  x22i.push_back(x[5]);
+  if (type == 2 && x[0] <= 0.0) {  // a negative characteristic impedance is a crossed line
+    ntyp.back() = 3;
+    x11r.back() = -x[0];
+  }
+}
+
+void Context::nt_card(int tag1, int seg1, int tag2, int seg2, double y11r, double y11i, double y12r,
+                      double y12i, double y22r, double y22i) {
+  const double x[6] = {y11r, y11i, y12r, y12i, y22r, y22i};
+  network_card(1, tag1, seg1, tag2, seg2, x);
+}
+
+void Context::tl_card(int tag1, int seg1, int tag2, int seg2, double z0, double length, double y1r,
+                      double y1i, double y2r, double y2i) {
+  const double x[6] = {z0, length, y1r, y1i, y2r, y2i};
+  network_card(2, tag1, seg1, tag2, seg2, x);
+}
+
+// calculate_network_data, src/nec_context.cpp:1210-1243: a transmission line
+// given with length <= 0 takes the straight distance between its two port
+// segments (metres, kept for later frequencies).  Done once per excitation
+// sweep, before the first incidence angle.
+void Context::network_lengths() {
+  if (ntyp.empty() || inc > 1) return;
+  for (size_t j = 0; j < ntyp.size(); j++) {
+    if (ntyp[j] < 2 || x11i[j] > 0.0) continue;
+    const int64_t a = iseg1[j] - 1, b = iseg2[j] - 1;
+    const double dx = geo_.x[b] - geo_.x[a], dy = geo_.y[b] - geo_.y[a], dz = geo_.z[b] - geo_.z[a];
+    x11i[j] = wavelength_ * std::sqrt(dx * dx + dy * dy + dz * dz);
+  }
+}
+
 namespace {
 // Internal impedance of a round wire of conductivity sigl (S/m, times the
 // wavelength) and radius rolam (wavelengths): the reference's zint
@@ -296,6 +360,7 @@ void Context::ex_card(int type, int i2, int i3, int i4, double f1, double f2,
   masym = i4 / 10;
   ex_type = type;
   if (type == 0) {
+    ntsol = 0;
     int64_t seg = geo_.segment_number(i2, i3);
     if (seg > geo_.n)
       fail("CHECK DATA, PARAMETER SPECIFYING EXCITATION SOURCE SEGMENT [", seg, "] IS TOO LARGE");
@@ -486,7 +551,9 @@ int Context::excitation_loop(int state_in, int mhz) {
 // excitation_process_inner, src/nec_context.cpp:1622-1738 (no coupling).
 int Context::excitation_inner(int mhz) {
   (void)mhz;
+  network_lengths();
   network_solve();
+  ntsol = 1;
   if (iptflg < -2 || iptflg > 3) iptflg = -1;
   if (iptflq < -2 || iptflq > 0) iptflq = -1;
   if (ex_type != 1 && ex_type != 2 && ex_type != 3 && (iptflg == 2 || iptflg == 3)) iptflg = -1;
@@ -668,6 +735,7 @@ necgpu_structure Context::structure_view() const {
 }
 
 void Context::structure_loading() {
+  ntsol = 0;
   build_tables();
   load();
   const necgpu_structure s = structure_view();
@@ -813,41 +881,202 @@ void Context::build_rhs(std::vector<cd>& e) {
 
 // netwk without networks (src/nec_context.cpp:4494-5065): solve, currents,
 // antenna input parameters of the voltage sources.
-void Context::network_solve() {
-  input_power = 0.0;
-  network_power_loss = 0.0;
+// One structure solve on the held factors: segment-centre currents into
+// `solution`, current coefficients into `abc` (the reference's solves +
+// get_current_coefficients).  A mixed solve whose refinement fails
+// refactors the intact FP64 matrix and solves again.
+void Context::solve_structure(const std::vector<cd>& rhs) {
   const int64_t n = geo_.n;
-  std::vector<cd> rhs;
-  build_rhs(rhs);
   solution.assign(n, cd(0, 0));
   abc.assign(6 * n, 0.0);
   necgpu_engine* e = engine();
   int rc = necgpu_solve(e, reinterpret_cast<const double*>(rhs.data()), reinterpret_cast<double*>(solution.data()),
                         abc.data());
   if (rc == NECGPU_ERR_REFINE && precision_ == NECGPU_MIXED) {
-    // the complex64 factors could not be refined to the FP64 solution:
-    // factor the (intact) FP64 matrix instead and solve again
     check(e, necgpu_factor(e, NECGPU_FP64));
     rc = necgpu_solve(e, reinterpret_cast<const double*>(rhs.data()), reinterpret_cast<double*>(solution.data()),
                       abc.data());
   }
   check(e, rc);
-  structure_power_loss = compute_structure_power_loss();
   necgpu_stats st{};
   necgpu_get_stats(e, &st);
   last_refine_residual = st.refine_residual;
   last_refine_iters = st.refine_iters;
+}
+
+namespace {
+// Dense LU with partial pivoting of the small network matrix (row-major,
+// n x n) and the solve on it; stands in for lu_decompose / solve
+// (src/matrix_algebra.cpp:217-307) on the network equations.
+void small_lu(int n, std::vector<cd>& a, std::vector<int>& piv) {
+  piv.resize(n);
+  for (int k = 0; k < n; k++) {
+    int p = k;
+    for (int i = k + 1; i < n; i++)
+      if (std::abs(a[i * n + k]) > std::abs(a[p * n + k])) p = i;
+    piv[k] = p;
+    if (p != k)
+      for (int j = 0; j < n; j++) std::swap(a[k * n + j], a[p * n + j]);
+    const cd d = a[k * n + k];
+    if (d == cd(0, 0)) fail("NETWORK EQUATIONS ARE SINGULAR");
+    for (int i = k + 1; i < n; i++) {
+      const cd l = a[i * n + k] / d;
+      a[i * n + k] = l;
+      for (int j = k + 1; j < n; j++) a[i * n + j] -= l * a[k * n + j];
+    }
+  }
+}
+
+void small_solve(int n, const std::vector<cd>& a, const std::vector<int>& piv, cd* b) {
+  for (int k = 0; k < n; k++) std::swap(b[k], b[piv[k]]);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < i; j++) b[i] -= a[i * n + j] * b[j];
+  for (int i = n - 1; i >= 0; i--) {
+    for (int j = i + 1; j < n; j++) b[i] -= a[i * n + j] * b[j];
+    b[i] /= a[i * n + i];
+  }
+}
+
+double port_power(cd v, cd i) { return 0.5 * std::real(v * std::conj(i)); }
+}  // namespace
+
+// netwk, src/nec_context.cpp:4496-5066.  Without networks: one solve and
+// the inputs of the voltage sources.  With networks: every network port
+// that is not a source gets a unit-field solve on the held factors; its
+// port currents plus the networks' short-circuit admittances form the
+// network equations, which give the port voltages; those voltages are added
+// to the applied field and the structure is solved once more.  As in the
+// reference, the network equations exist only in the excitation pass that
+// builds them (ntsol == 0); later passes on the same factors see none.
+void Context::network_solve() {
+  input_power = 0.0;
+  network_power_loss = 0.0;
+  std::vector<cd> einc;
+  build_rhs(einc);
+  const int nsrc = (int)src_seg.size();
+  const int nnet = (ntsol == 0) ? (int)ntyp.size() : 0;
+  const int ndimn = 2 * (int)ntyp.size() + nsrc;
+  std::vector<cd> cmn, rhnx, rhnt, vsrc;
+  std::vector<int64_t> nteqa, ntsca;
+  int nteq = 0, ntsc = 0;
+  if (ntyp.empty()) {
+    solve_structure(einc);
+  } else {
+    cmn.assign((size_t)ndimn * ndimn, cd(0, 0));
+    rhnx.assign(ndimn, cd(0, 0));
+    rhnt.assign(ndimn, cd(0, 0));
+    vsrc.assign(ndimn, cd(0, 0));
+    nteqa.assign(ndimn, 0);
+    ntsca.assign(ndimn, 0);
+    // equation row of a port segment: sources count from the end
+    auto port_row = [&](int64_t seg, int& isc) {
+      isc = -1;
+      for (int i = 0; i < nsrc; i++)
+        if (src_seg[i] == seg) {
+          isc = i;
+          break;
+        }
+      if (isc < 0) {
+        for (int i = 0; i < nteq; i++)
+          if (nteqa[i] == seg) return i;
+        nteqa[nteq] = seg;
+        return nteq++;
+      }
+      for (int i = 0; i < ntsc; i++)
+        if (ntsca[i] == seg) return ndimn - (i + 1);
+      ntsca[ntsc] = seg;
+      vsrc[ntsc] = src_volt[isc];
+      ntsc++;
+      return ndimn - ntsc;
+    };
+    // cmn[c + r * ndimn] is row r, column c of the network matrix
+    for (int j = 0; j < nnet; j++) {
+      cd y11, y12, y22;
+      if (ntyp[j] <= 1) {
+        y11 = cd(x11r[j], x11i[j]);
+        y12 = cd(x12r[j], x12i[j]);
+        y22 = cd(x22r[j], x22i[j]);
+      } else {
+        // lossless line of impedance x11r and length x11i (m) plus the shunt
+        // admittances at its two ends; a crossed line flips y12
+        const double bl = kTwoPi * x11i[j] / wavelength_;
+        const double b12 = 1.0 / (x11r[j] * std::sin(bl));
+        const double b11 = -b12 * std::cos(bl);
+        y12 = cd(0.0, ntyp[j] == 2 ? b12 : -b12);
+        y11 = cd(x12r[j], b11 + x12i[j]);
+        y22 = cd(x22r[j], b11 + x22i[j]);
+      }
+      int isc1, isc2;
+      const int irow1 = port_row(iseg1[j], isc1);
+      const int irow2 = port_row(iseg2[j], isc2);
+      if (isc1 == -1) {
+        const double len = geo_.length[iseg1[j] - 1];
+        cmn[irow1 + (size_t)irow1 * ndimn] -= y11 * len;
+        cmn[irow1 + (size_t)irow2 * ndimn] -= y12 * len;
+      } else {
+        rhnx[irow1] += y11 * src_volt[isc1] / wavelength_;
+        rhnx[irow2] += y12 * src_volt[isc1] / wavelength_;
+      }
+      if (isc2 == -1) {
+        const double len = geo_.length[iseg2[j] - 1];
+        cmn[irow2 + (size_t)irow2 * ndimn] -= y22 * len;
+        cmn[irow2 + (size_t)irow1 * ndimn] -= y12 * len;
+      } else {
+        rhnx[irow1] += y12 * src_volt[isc2] / wavelength_;
+        rhnx[irow2] += y22 * src_volt[isc2] / wavelength_;
+      }
+    }
+    // structure admittance at the ports: one unit-field solve per port
+    std::vector<cd> unit(geo_.n, cd(0, 0));
+    for (int i = 0; i < nteq; i++) {
+      unit[nteqa[i] - 1] = cd(1, 0);
+      solve_structure(unit);
+      unit[nteqa[i] - 1] = cd(0, 0);
+      for (int j = 0; j < nteq; j++) cmn[i + (size_t)j * ndimn] += solution[nteqa[j] - 1];
+    }
+    std::vector<cd> a((size_t)nteq * nteq);
+    for (int r = 0; r < nteq; r++)
+      for (int c = 0; c < nteq; c++) a[(size_t)r * nteq + c] = cmn[c + (size_t)r * ndimn];
+    std::vector<int> piv;
+    small_lu(nteq, a, piv);
+    // port voltages from the currents the applied field drives
+    solve_structure(einc);
+    for (int i = 0; i < nteq; i++) rhnt[i] = rhnx[i] + solution[nteqa[i] - 1];
+    small_solve(nteq, a, piv, rhnt.data());
+    for (int i = 0; i < nteq; i++) einc[nteqa[i] - 1] -= rhnt[i];
+    if (nteq > 0) solve_structure(einc);
+    for (int i = 0; i < nteq; i++) {
+      const int64_t sidx = nteqa[i] - 1;
+      network_power_loss -= port_power(rhnt[i] * geo_.length[sidx] * wavelength_, solution[sidx] * wavelength_);
+    }
+    for (int i = 0; i < ntsc; i++)
+      network_power_loss -= port_power(vsrc[i], solution[ntsca[i] - 1] * wavelength_);
+  }
+  structure_power_loss = compute_structure_power_loss();
 
   if (src_seg.empty()) return;
   AntennaInput ai;
   ai.freq_hz = freq_mhz * 1.0e6;
-  for (size_t k = 0; k < src_seg.size(); k++) {
+  for (int k = 0; k < nsrc; k++) {
     int64_t s = src_seg[k] - 1;
     cd voltage = src_volt[k];
     cd current = solution[s] * wavelength_;
+    bool network_loss = false;
+    if (ntsc != 0) {
+      // a source that is also a network port: add the current its networks draw
+      int j = 0;
+      while (j < ntsc && ntsca[j] != s + 1) j++;
+      if (j == ntsc) fail("NETWORK DATA ERROR: SOURCE SEGMENT [", s + 1, "] NOT FOUND IN NETWORK TABLE");
+      const int row = ndimn - (j + 1);
+      cd temp = rhnx[row];
+      for (int m = 0; m < nteq; m++) temp -= cmn[m + (size_t)row * ndimn] * rhnt[m];
+      current = (solution[s] + temp) * wavelength_;
+      network_loss = true;
+    }
     cd admittance = current / voltage;
     cd imp = voltage / current;
-    double power = 0.5 * std::real(voltage * std::conj(current));
+    double power = port_power(voltage, current);
+    if (network_loss) network_power_loss += power;
     input_power += power;
     ai.tag.push_back(geo_.tags[s]);
     ai.seg.push_back((int)(s + 1));
@@ -1102,6 +1331,7 @@ void Context::gradient(int nparam, Context* const* plus, Context* const* minus, 
   if (src_seg.size() != 1) fail("gradient: exactly one voltage source is supported");
   if (precision_ != 1) fail("gradient: needs the mixed-precision path (nec_set_precision(ctx, 1))");
   if (!zarray.empty()) fail("gradient: loaded structures (LD cards) are not supported");
+  if (!ntyp.empty()) fail("gradient: networks and transmission lines (NT/TL cards) are not supported");
   necgpu_engine* e = eng_;
   const int64_t n = geo_.n;
   const int64_t f = src_seg[0] - 1;

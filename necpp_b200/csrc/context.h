@@ -69,6 +69,11 @@ class Context {
                double rfld, double gnor);
   void kh_card(double rkh);
   void ld_card(int type, int tag, int tag_from, int tag_to, double zr, double zi, double zc);
+  void nt_card(int tag1, int seg1, int tag2, int seg2, double y11r, double y11i, double y12r, double y12i,
+               double y22r, double y22i);
+  void tl_card(int tag1, int seg1, int tag2, int seg2, double z0, double length, double y1r, double y1i,
+               double y2r, double y2i);
+  int network_count() const { return (int)ntyp.size(); }
   void ek_card(int flag);
   void pt_card(int a, int b, int c, int d);
   void pq_card(int a, int b, int c, int d);
@@ -122,6 +127,15 @@ class Context {
   std::vector<int> ldtyp, ldtag, ldtagf, ldtagt;
   std::vector<double> zlr, zli, zlc;
   std::vector<cd> zarray;
+  // NT/TL cards (names follow the reference's members): type 1 network,
+  // 2 transmission line, 3 crossed line; ports as 1-based segment numbers
+  std::vector<int> ntyp;
+  std::vector<int64_t> iseg1, iseg2;
+  std::vector<double> x11r, x11i, x12r, x12i, x22r, x22i;
+  int ntsol = 0;  // network equations solved for the current structure
+  void network_card(int type, int tag1, int seg1, int tag2, int seg2, const double* x);
+  void network_lengths();
+  void solve_structure(const std::vector<cd>& rhs);
   enum State { MEM = 1, STRUCT = 2, EXSETUP = 3, EXLOOP = 4, NEAR = 5, FAR = 6 };
   enum Ret { PRINT_NORM = 0, FREQ_CONT = 1, CARD_CONT = 2, INNER_CONT = 3, PHASE_DONE = 4 };
 

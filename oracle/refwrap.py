@@ -44,6 +44,8 @@ class RefAPI:
         sig("nec_geometry_complete", _l, [_p, _i])
         sig("nec_gn_card", _l, [_p, _i, _i] + [_d] * 6)
         sig("nec_ld_card", _l, [_p, _i, _i, _i, _i] + [_d] * 3)
+        sig("nec_nt_card", _l, [_p, _i, _i, _i, _i] + [_d] * 6)
+        sig("nec_tl_card", _l, [_p, _i, _i, _i, _i] + [_d] * 6)
         sig("nec_fr_card", _l, [_p, _i, _i, _d, _d])
         sig("nec_ek_card", _l, [_p, _i])
         sig("nec_ex_card", _l, [_p, _i, _i, _i, _i] + [_d] * 6)

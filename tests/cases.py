@@ -128,6 +128,35 @@ def _dipoles_conductivity(api, ctx):
     return 150.0
 
 
+def _array_tl(api, ctx):
+    """Three dipoles fed through transmission lines from a source on the
+    first: a straight line of given length from the source, a crossed line
+    of computed length (0) with shunt admittances, and an NT two-port
+    between two non-source ports; two frequencies."""
+    for t in range(3):
+        api.nec_wire(ctx, t + 1, 21, 0.5 * t, 0.0, -0.48, 0.5 * t, 0.0, 0.48, 1.0e-3, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 0)
+    api.nec_tl_card(ctx, 1, 11, 2, 11, 50.0, 0.6, 0.0, 0.0, 0.0, 0.0)
+    api.nec_tl_card(ctx, 2, 11, 3, 11, -75.0, 0.0, 1.0e-3, 2.0e-3, 0.0, -1.0e-3)
+    api.nec_nt_card(ctx, 2, 4, 3, 18, 2.0e-3, -1.0e-3, -5.0e-4, 2.0e-4, 1.0e-3, 3.0e-3)
+    api.nec_fr_card(ctx, 0, 2, 145.0, 10.0)
+    api.nec_ex_card(ctx, 0, 1, 11, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_rp_card(ctx, 0, 19, 8, 1, 0, 1, 0, 0.0, 0.0, 10.0, 45.0, 0.0, 0.0)
+    return 150.0
+
+
+def _dipole_nt(api, ctx):
+    """A two-port network between two segments of a driven dipole, the
+    source off the network (the plain input path with network loss)."""
+    api.nec_wire(ctx, 1, 31, 0.0, 0.0, -0.5, 0.0, 0.0, 0.5, 1.0e-3, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 0)
+    api.nec_nt_card(ctx, 1, 6, 1, 26, 1.0e-2, 5.0e-3, -2.0e-3, 1.0e-3, 4.0e-3, -6.0e-3)
+    api.nec_fr_card(ctx, 0, 1, 150.0, 0.0)
+    api.nec_ex_card(ctx, 0, 1, 16, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_rp_card(ctx, 0, 19, 8, 1, 0, 1, 0, 0.0, 0.0, 10.0, 45.0, 0.0, 0.0)
+    return 150.0
+
+
 # name: (builder, pattern grid (n_theta, n_phi) or None)
 CASES = {
     "ex1": (_ex1, None),
@@ -144,4 +173,6 @@ CASES = {
     "plane_wave_reflection": (_plane_wave_reflection, (10, 4)),
     "yagi_loaded": (_yagi_loaded, (19, 8)),
     "dipoles_conductivity": (_dipoles_conductivity, (19, 8)),
+    "array_tl": (_array_tl, (19, 8)),
+    "dipole_nt": (_dipole_nt, (19, 8)),
 }

@@ -20,6 +20,15 @@ class HostOnly:
     def __init__(self, nb):
         self.nb = nb
         self.fr = None
+        self.networks = []   # (card, tag1, seg1, tag2, seg2, six reals)
+
+    def nec_nt_card(self, ctx, t1, s1, t2, s2, *x):
+        self.networks.append(("NT", t1, s1, t2, s2, x))
+        return self.nb.nec_nt_card(ctx, t1, s1, t2, s2, *x)
+
+    def nec_tl_card(self, ctx, t1, s1, t2, s2, *x):
+        self.networks.append(("TL", t1, s1, t2, s2, x))
+        return self.nb.nec_tl_card(ctx, t1, s1, t2, s2, *x)
 
     def __getattr__(self, k):
         return getattr(self.nb, k)

@@ -122,11 +122,16 @@ def test_errors_and_sentinels(nb):
     assert "NO SEGMENT HAS AN ITAG" in nb.nec_error_message()
     assert nb.nec_ex_card(ctx, 0, 7, 1, 0, 1.0, 0, 0, 0, 0, 0) == 1
     # cards outside the hot path exist and refuse
-    for call in (lambda: nb.nec_nt_card(ctx, 1, 1, 1, 2, 0, 0, 0, 0, 0, 0),
-                 lambda: nb.nec_ne_card(ctx, 0, 1, 1, 1, 0, 0, 0, 0, 0, 0),
+    for call in (lambda: nb.nec_ne_card(ctx, 0, 1, 1, 1, 0, 0, 0, 0, 0, 0),
                  lambda: nb.nec_sp_card(ctx, 0, 0, 0, 0, 0, 0, 0)):
         assert call() == 1
         assert "not part of the B200" in nb.nec_error_message()
+    # NT port on a tag that does not exist (c_geometry.cpp:76-99)
+    assert nb.nec_nt_card(ctx, 1, 1, 4, 2, 0, 0, 0, 0, 0, 0) == 1
+    assert "NO SEGMENT HAS AN ITAG OF 4" in nb.nec_error_message()
+    assert nb.nec_network_count(ctx) == 0
+    assert nb.nec_tl_card(ctx, 1, 2, 1, 8, 50.0, 0, 0, 0, 0, 0) == 0
+    assert nb.nec_network_count(ctx) == 1
     # LD range reversed (nec_context.cpp:465-470)
     assert nb.nec_ld_card(ctx, 0, 1, 5, 3, 10.0, 0, 0) == 1
     assert "ITAG STEP1: 5 IS GREATER THAN ITAG STEP2: 3" in nb.nec_error_message()

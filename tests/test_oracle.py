@@ -13,6 +13,8 @@ from conftest import golden
 from helpers import host_case
 
 NAMES = list(CASES)
+NETWORK_CASES = ("array_tl", "dipole_nt")
+PLAIN = [n for n in NAMES if n not in NETWORK_CASES]
 ETA = math.sqrt((4.0 * 3.1415926536 * 1.0e-7) / 8.854e-12)
 
 
@@ -47,7 +49,7 @@ def _solve_case(nb, oracle, name):
     return ctx, st, rhs, abc, cur
 
 
-@pytest.mark.parametrize("name", [n for n in NAMES if n != "plane_wave_reflection"])
+@pytest.mark.parametrize("name", [n for n in PLAIN if n != "plane_wave_reflection"])
 def test_oracle_solution_matches_reference(nb, oracle, name):
     """LU + solve + current coefficients of the oracle against the
     reference's current_vector and coefficients of its last solve."""
@@ -69,7 +71,7 @@ def _zin(g, nb, st, rhs, cur):
     return v / (cur[feeds] * lam), v, feeds
 
 
-@pytest.mark.parametrize("name", [n for n in NAMES if n not in ("mesh_small", "plane_wave_reflection")])
+@pytest.mark.parametrize("name", [n for n in PLAIN if n not in ("mesh_small", "plane_wave_reflection")])
 def test_oracle_zin_matches_reference(nb, oracle, name):
     ctx, st, rhs, abc, cur = _solve_case(nb, oracle, name)
     g = golden(name)
@@ -77,6 +79,49 @@ def test_oracle_zin_matches_reference(nb, oracle, name):
     ref = g["zin"][-1]
     ref = ref[~np.isnan(ref)]
     assert np.max(np.abs(zin - ref) / np.abs(ref)) <= 1e-10
+    nb.nec_delete(ctx)
+
+
+def _oracle_network(nb, oracle, name):
+    from oracle import network as NW
+    ctx, st, rhs, api = host_case(nb, CASES[name][0])
+    g = golden(name)
+    tags = g["seg_tags"]
+
+    def absolute(tag, m):
+        return m if tag == 0 else int(np.nonzero(tags == tag)[0][m - 1]) + 1
+
+    nets = []
+    for card, t1, s1, t2, s2, x in api.networks:
+        x = list(x)
+        typ = 1 if card == "NT" else 2
+        if typ == 2 and x[0] <= 0.0:
+            typ, x[0] = 3, -x[0]
+        nets.append((typ, absolute(t1, s1), absolute(t2, s2), x))
+    lam = float(g["wavelength"])
+    nets = NW.tl_lengths(st, lam, nets)
+    n = st["n"]
+    s = st["seg"][3 * n:4 * n]
+    feeds = np.nonzero(rhs)[0]
+    sources = [(int(f) + 1, -rhs[f] * s[f] * lam) for f in feeds]
+    Z, _ = oracle.fill(st)
+    return ctx, g, NW.netwk(oracle, st, Z, rhs, lam, nets, sources)
+
+
+@pytest.mark.parametrize("name", NETWORK_CASES)
+def test_oracle_network_matches_reference(nb, oracle, name):
+    """Network equations (NT two-ports, straight and crossed transmission
+    lines, computed line length) restated in numpy over the C oracle's
+    solves, against the reference's input impedances and last currents."""
+    ctx, g, (cur, abc, zin, pin, loss) = _oracle_network(nb, oracle, name)
+    ref = g["zin"][-1]
+    ref = ref[~np.isnan(ref)]
+    assert np.max(np.abs(zin - ref) / np.abs(ref)) <= 1e-10
+    scale = np.max(np.abs(g["current_vector"]))
+    assert np.max(np.abs(cur - g["current_vector"])) / scale <= 1e-10
+    assert np.max(np.abs(abc.reshape(6, -1) - g["abc"])) / np.max(np.abs(g["abc"])) <= 1e-10
+    # the ports really carry network current
+    assert abs(loss) > 1e-6 * pin
     nb.nec_delete(ctx)
 
 
