@@ -449,6 +449,148 @@ static void gwave(double r2, double zph, cx xx2, cx u, cx u2, double eta, cx* er
   *eph = -(x1 - x2 + x3 - x4 + x5 + x6) * (-C4);
 }
 
+/* Geometry of one near-ground pair as sflds sees it (nec_context.cpp:6024-6060). */
+typedef struct {
+  double xj, yj, zj, cabj, sabj, salpj, xo, yo, zo, xsn, ysn, sn;
+} sgeom_t;
+
+/* sflds with isnor = 1, nec_context.cpp:6024-6066, 6108-6137: field due to
+   ground of a current element at t from the source centre, read from the
+   interpolated Sommerfeld tables. */
+static void sflds_table(const mo_structure* S, const sgeom_t* G, double t, cx e[9]) {
+  double xt = G->xj + t * G->cabj, yt = G->yj + t * G->sabj, zt = G->zj + t * G->salpj;
+  double rhx = G->xo - xt, rhy = G->yo - yt, rhs = rhx * rhx + rhy * rhy, rho = sqrt(rhs), phx, phy;
+  if (rho <= 0.0) {
+    rhx = 1.0;
+    rhy = 0.0;
+    phx = 0.0;
+    phy = 1.0;
+  } else {
+    rhx = rhx / rho;
+    rhy = rhy / rho;
+    phx = -rhy;
+    phy = rhx;
+  }
+  double cph = rhx * G->xsn + rhy * G->ysn, sph = rhy * G->xsn - rhx * G->ysn;
+  if (fabs(cph) < 1.0e-10) cph = 0.0;
+  if (fabs(sph) < 1.0e-10) sph = 0.0;
+  double zph = G->zo + zt, zphs = zph * zph, r2s = rhs + zphs, r2 = sqrt(r2s), rk = r2 * TWO_PI;
+  cx xx2 = CMPLX(cos(rk), -sin(rk));
+  double thet = (rho >= 1.0e-12) ? atan(zph / rho) : PI / 2.0;
+  cx f[4];
+  mo_interpolate(S->interp, S->somm, r2, thet, S->interp_stateful, (double*)f);
+  cx erv = f[0], ezv = f[1], erh = f[2], eph = f[3];
+  xx2 = xx2 / r2;
+  double sfac = G->sn * cph;
+  erh = xx2 * (G->salpj * erv + sfac * erh);
+  cx ezh = xx2 * (G->salpj * ezv - sfac * erv);
+  eph = G->sn * sph * xx2 * eph;
+  e[0] = erh * rhx + eph * phx;
+  e[1] = erh * rhy + eph * phy;
+  e[2] = ezh;
+  rk = TWO_PI * t;
+  sfac = sin(rk);
+  e[3] = e[0] * sfac;
+  e[4] = e[1] * sfac;
+  e[5] = e[2] * sfac;
+  sfac = cos(rk);
+  e[6] = e[0] * sfac;
+  e[7] = e[1] * sfac;
+  e[8] = e[2] * sfac;
+}
+
+/* test_simple, c_evlcom.cpp:870-883 */
+static double test1(double f1r, double f2r, double dmin) {
+  double den = fabs(f2r);
+  if (den < dmin) den = dmin;
+  if (den < 1.0e-37) return 0.0;
+  return fabs((f1r - f2r) / den);
+}
+
+/* rom2, nec_context.cpp:5589-5834: Romberg integration of the table field
+   over the source segment; the finest step is s / n (n segments). */
+static void rom2(const mo_structure* S, const sgeom_t* G, double a, double b, cx sum[9], double dmin,
+                 int* st) {
+  const int n = 9, nts = 4, nx = 1;
+  const double rx = 1e-4;
+  double dz = 0.0, dzot = 0.0, z = a, ze = b, s = b - a;
+  cx g1[9], g2[9], g3[9], g4[9], g5[9], t01[9], t10[9], t20[9], t11[9];
+  const double ep = s / (1.0e4 * (double)S->n);
+  const double zend = ze - ep;
+  for (int i = 0; i < n; i++) sum[i] = 0;
+  int ns = nx, nt = 0;
+  sflds_table(S, G, z, g1);
+  for (;;) {
+    /* 3: next interval */
+    dz = s / ns;
+    if (z + dz >= ze) {
+      dz = ze - z;
+      if (dz <= ep) return;
+    }
+    dzot = dz * .5;
+    sflds_table(S, G, z + dzot, g3);
+    sflds_table(S, G, z + dz, g5);
+    for (;;) {
+      /* 5: three-point result */
+      for (int i = 0; i < n; i++) {
+        cx t00 = (g1[i] + g5[i]) * dzot;
+        t01[i] = (t00 + dz * g3[i]) * 0.5;
+        t10[i] = (4.0 * t01[i] - t00) / 3.;
+      }
+      double tmag1 = sqrt(creal(t01[0]) * creal(t01[0]) + cimag(t01[0]) * cimag(t01[0]) +
+                          (creal(t01[1]) * creal(t01[1]) + cimag(t01[1]) * cimag(t01[1])) +
+                          (creal(t01[2]) * creal(t01[2]) + cimag(t01[2]) * cimag(t01[2])));
+      double tmag2 = sqrt(creal(t10[0]) * creal(t10[0]) + cimag(t10[0]) * cimag(t10[0]) +
+                          (creal(t10[1]) * creal(t10[1]) + cimag(t10[1]) * cimag(t10[1])) +
+                          (creal(t10[2]) * creal(t10[2]) + cimag(t10[2]) * cimag(t10[2])));
+      if (test1(tmag1, tmag2, dmin) <= rx) {
+        for (int i = 0; i < n; i++) sum[i] += t10[i];
+        nt += 2;
+        goto advance;
+      }
+      sflds_table(S, G, z + dz * .25, g2);
+      sflds_table(S, G, z + dz * .75, g4);
+      for (int i = 0; i < n; i++) {
+        cx t02 = (t01[i] + dzot * (g2[i] + g4[i])) * 0.5;
+        t11[i] = (4.0 * t02 - t01[i]) / 3.0;
+        t20[i] = (16. * t11[i] - t10[i]) / 15.0;
+      }
+      tmag1 = sqrt(creal(t11[0]) * creal(t11[0]) + cimag(t11[0]) * cimag(t11[0]) +
+                   (creal(t11[1]) * creal(t11[1]) + cimag(t11[1]) * cimag(t11[1])) +
+                   (creal(t11[2]) * creal(t11[2]) + cimag(t11[2]) * cimag(t11[2])));
+      tmag2 = sqrt(creal(t20[0]) * creal(t20[0]) + cimag(t20[0]) * cimag(t20[0]) +
+                   (creal(t20[1]) * creal(t20[1]) + cimag(t20[1]) * cimag(t20[1])) +
+                   (creal(t20[2]) * creal(t20[2]) + cimag(t20[2]) * cimag(t20[2])));
+      if (test1(tmag1, tmag2, dmin) <= rx) break;
+      /* 14: halve the step, or accept at the limit */
+      nt = 0;
+      if (ns >= S->n) {
+        *st |= ST_STEP;
+        break;
+      }
+      ns = ns * 2;
+      dz = s / ns;
+      dzot = dz * .5;
+      for (int i = 0; i < n; i++) {
+        g5[i] = g3[i];
+        g3[i] = g2[i];
+      }
+    }
+    /* 10 */
+    for (int i = 0; i < n; i++) sum[i] += t20[i];
+    nt = nt + 1;
+  advance:
+    /* 12 */
+    z = z + dz;
+    if (z > zend) return;
+    for (int i = 0; i < n; i++) g1[i] = g5[i];
+    if ((nt >= nts) && (ns > nx)) {
+      ns = ns / 2;
+      nt = 1;
+    }
+  }
+}
+
 /* efld, 2845-3045 + projection of cmww, 2617-2619 */
 static void pair(const mo_structure* S, const src_t* J, int64_t i, int ij, cx* etk, cx* ets, cx* etc,
                  int* st) {
@@ -519,8 +661,19 @@ static void pair(const mo_structure* S, const src_t* J, int64_t i, int ij, cx* e
     }
     double r = xij * xij + yij * yij + zij * zij;
     if (r <= .95) {
-      *st |= ST_TABLE;
-      for (int k = 0; k < 9; k++) e[k] = 0.;
+      if (!S->somm) {
+        *st |= ST_TABLE;
+        for (int k = 0; k < 9; k++) e[k] = 0.;
+      } else {
+        /* isnor = 1: the table field integrated over the source segment */
+        double dmin = creal(ex[0]) * creal(ex[0]) + cimag(ex[0]) * cimag(ex[0]) +
+                      (creal(ex[1]) * creal(ex[1]) + cimag(ex[1]) * cimag(ex[1])) +
+                      (creal(ex[2]) * creal(ex[2]) + cimag(ex[2]) * cimag(ex[2]));
+        dmin = 0.01 * sqrt(dmin);
+        double shaf = 0.5 * J->s;
+        sgeom_t G = {J->x, J->y, J->z, cabj, sabj, salpj, xo, yo, zo, xsn, ysn, sn};
+        rom2(S, &G, -shaf, shaf, e, dmin, st);
+      }
     } else {
       /* sflds(0), isnor = 2: 6024-6098 */
       double xt = J->x + 0. * cabj, yt = J->y + 0. * sabj, zt = J->z + 0. * salpj;

@@ -21,16 +21,18 @@ class MoStructure(C.Structure):
         ("trio_ptr", _ip), ("trio_basis", _ip), ("trio_a", _dp), ("trio_b", _dp), ("trio_c", _dp),
         ("ind1", _ip), ("ind2", _ip), ("rkh", C.c_double), ("use_exk", C.c_int), ("ground", C.c_int),
         ("zrati_re", C.c_double), ("zrati_im", C.c_double), ("frati_re", C.c_double),
-        ("frati_im", C.c_double), ("eta", C.c_double), ("zload", _dp)]
+        ("frati_im", C.c_double), ("eta", C.c_double), ("zload", _dp), ("somm", _dp),
+        ("interp", C.c_void_p), ("interp_stateful", C.c_int)]
 
 
 def build():
     """Compile liboracle.so (gcc, no contraction) if missing or stale."""
-    src = [os.path.join(HERE, f) for f in ("mom_oracle.c", "mom_oracle.h")]
+    src = [os.path.join(HERE, f) for f in ("mom_oracle.c", "somm_oracle.c", "mom_oracle.h")]
     if not os.path.exists(SO) or any(os.path.getmtime(s) > os.path.getmtime(SO) for s in src):
         cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
         subprocess.run([cc, "-std=c11", "-O2", "-fPIC", "-shared", "-fno-fast-math", "-ffp-contract=off",
-                        "-o", SO, os.path.join(HERE, "mom_oracle.c"), "-lm"], check=True)
+                        "-o", SO, os.path.join(HERE, "mom_oracle.c"), os.path.join(HERE, "somm_oracle.c"),
+                        "-lm"], check=True)
     return SO
 
 
@@ -45,7 +47,33 @@ class Oracle:
         L.mo_solve.argtypes = [C.c_int64, _dp, _ip, _dp]
         L.mo_coefficients.argtypes = [C.POINTER(MoStructure), _dp, _dp, _dp]
         L.mo_ffld.argtypes = [C.POINTER(MoStructure), _dp, C.c_double, C.c_double, _dp, _dp]
+        L.mo_sommerfeld.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
+        L.mo_sommerfeld.restype = C.c_int
+        L.mo_interp_size.restype = C.c_int64
+        L.mo_interp_init.argtypes = [C.c_void_p]
+        L.mo_interpolate.argtypes = [C.c_void_p, _dp, C.c_double, C.c_double, C.c_int, _dp]
         self.L = L
+
+    def sommerfeld(self, epr, sig, wavelength, eta):
+        """Sommerfeld tables (1068 complex) and the complex permittivity used."""
+        t = np.zeros(2 * 1068)
+        eps = np.zeros(2)
+        bad = self.L.mo_sommerfeld(epr, sig, wavelength, eta, t.ctypes.data_as(_dp), eps.ctypes.data_as(_dp))
+        assert bad == 0, "Sommerfeld integral did not converge"
+        return t[0::2] + 1j * t[1::2], complex(eps[0], eps[1])
+
+    def new_interp(self):
+        """A fresh interpolation cache (the state a new context starts with)."""
+        buf = np.zeros(self.L.mo_interp_size(), dtype=np.uint8)
+        self.L.mo_interp_init(buf.ctypes.data_as(C.c_void_p))
+        return buf
+
+    def interpolate(self, interp, tables, x, y, stateful=True):
+        t = np.ascontiguousarray(tables, dtype=np.complex128).view(np.float64)
+        f = np.zeros(8)
+        self.L.mo_interpolate(interp.ctypes.data_as(C.c_void_p), t.ctypes.data_as(_dp), x, y, int(stateful),
+                              f.ctypes.data_as(_dp))
+        return f[0::2] + 1j * f[1::2]
 
     def structure(self, st):
         """st: dict from tests.helpers.export_structure (kept alive by the caller)."""
@@ -70,6 +98,14 @@ class Oracle:
         if zl is not None and np.any(zl != 0):
             st["_zload_ri"] = np.ascontiguousarray(np.asarray(zl, dtype=np.complex128)).view(np.float64)
             s.zload = st["_zload_ri"].ctypes.data_as(_dp)
+        somm = st.get("somm")
+        if somm is not None:
+            st["_somm_ri"] = np.ascontiguousarray(np.asarray(somm, dtype=np.complex128)).view(np.float64)
+            s.somm = st["_somm_ri"].ctypes.data_as(_dp)
+            if st.get("interp") is None:
+                st["interp"] = self.new_interp()
+            s.interp = st["interp"].ctypes.data_as(C.c_void_p)
+            s.interp_stateful = int(st.get("interp_stateful", True))
         return s
 
     def fill(self, st):

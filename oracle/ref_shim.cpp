@@ -16,7 +16,9 @@
  *     (src/nec_context.cpp:2077-2204), the LU factors and pivots left in the
  *     public members cm / ip (src/nec_context.h:834-842),
  *   - the currents and current coefficients (src/nec_context.h:846-849),
- *   - the far-field sum ffld (src/nec_context.cpp:6639-6888).
+ *   - the far-field sum ffld (src/nec_context.cpp:6639-6888),
+ *   - the Sommerfeld ground tables and their interpolation cache
+ *     (src/c_ggrid.h:36-76).
  *
  * cmset is a private member; it is reached through the standard
  * explicit-instantiation access idiom (a member pointer named in an explicit
@@ -43,6 +45,14 @@ struct cmset_tag {
   friend type access_member(cmset_tag);
 };
 template struct member_access<cmset_tag, &nec_context::cmset>;
+
+struct ggrid_tag {
+  typedef c_ggrid nec_ground::*type;
+  friend type access_member(ggrid_tag);
+};
+template struct member_access<ggrid_tag, &nec_ground::_ggrid>;
+
+c_ggrid& ggrid_of(nec_context* ctx) { return ctx->ground.*access_member(ggrid_tag()); }
 
 }  // namespace
 
@@ -153,6 +163,37 @@ long ref_fill(nec_context* ctx, double* out) {
     return 1;
   }
   return 0;
+}
+
+/* The Sommerfeld ground tables of the last frequency (c_ggrid::sommerfeld,
+   src/c_ggrid.cpp:164-288): ar1 (440), ar2 (340), ar3 (288) complex values,
+   interleaved re/im, and the complex permittivity they were made for. */
+void ref_somm_tables(nec_context* ctx, double* out, double* epscf) {
+  c_ggrid& g = ggrid_of(ctx);
+  int64_t k = 0;
+  for (const complex_array* a : {&g.m_ar1, &g.m_ar2, &g.m_ar3})
+    for (int64_t i = 0; i < a->size(); i++, k++) {
+      out[2 * k] = (*a)[i].real();
+      out[2 * k + 1] = (*a)[i].imag();
+    }
+  epscf[0] = g.m_epscf.real();
+  epscf[1] = g.m_epscf.imag();
+}
+
+/* Reset the interpolation cache to the state a new context starts with
+   (c_ggrid::initialize, src/c_ggrid.h:45-61; the tables are kept). */
+void ref_somm_interp_reset(nec_context* ctx) { ggrid_of(ctx).initialize(); }
+
+/* One call of c_ggrid::interpolate (src/c_ggrid.cpp:38-162) through the
+   context's cache: f = erv, ezv, erh, eph interleaved. */
+void ref_somm_interpolate(nec_context* ctx, double x, double y, double* f) {
+  nec_complex a, b, c, d;
+  ggrid_of(ctx).interpolate(x, y, &a, &b, &c, &d);
+  const nec_complex v[4] = {a, b, c, d};
+  for (int k = 0; k < 4; k++) {
+    f[2 * k] = v[k].real();
+    f[2 * k + 1] = v[k].imag();
+  }
 }
 
 /* LU factors (column-major, in place) and the 1-based permutation left by the

@@ -71,6 +71,9 @@ class RefAPI:
         sig("ref_wavelength", _d, [_p])
         sig("ref_fill", _l, [_p, _dp])
         sig("ref_lu", None, [_p, _dp, _ip])
+        sig("ref_somm_tables", None, [_p, _dp, _dp])
+        sig("ref_somm_interp_reset", None, [_p])
+        sig("ref_somm_interpolate", None, [_p, _d, _d, _dp])
         sig("ref_currents", None, [_p] + [_dp] * 7)
         sig("ref_ffld", None, [_p, _d, _d, _dp, _dp])
 
@@ -106,6 +109,18 @@ class RefAPI:
             raise RuntimeError(self.error())
         z = out[0::2] + 1j * out[1::2]
         return z.reshape(n, n)  # row = obs, column = basis (cm[basis + obs*n])
+
+    def somm_tables(self, ctx):
+        """Sommerfeld tables (1068 complex) of the last frequency and their
+        complex permittivity."""
+        out, eps = np.zeros(2 * 1068), np.zeros(2)
+        self.ref_somm_tables(ctx, out.ctypes.data_as(_dp), eps.ctypes.data_as(_dp))
+        return out[0::2] + 1j * out[1::2], complex(eps[0], eps[1])
+
+    def somm_interpolate(self, ctx, x, y):
+        f = np.zeros(8)
+        self.ref_somm_interpolate(ctx, x, y, f.ctypes.data_as(_dp))
+        return f[0::2] + 1j * f[1::2]
 
     def currents(self, ctx):
         n = self.ref_n_segments(ctx)

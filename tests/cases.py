@@ -157,6 +157,21 @@ def _dipole_nt(api, ctx):
     return 150.0
 
 
+def _near_ground(api, ctx):
+    """A dipole 0.05 wavelength above Sommerfeld ground and a tilted wire
+    touching down near it: most pairs are within a wavelength of their
+    image, so the fill integrates the interpolated Sommerfeld tables; two
+    frequencies (new tables, the interpolation cache carried over)."""
+    api.nec_wire(ctx, 1, 21, -0.5, 0.0, 0.1, 0.5, 0.0, 0.1, 1.0e-3, 1.0, 1.0)
+    api.nec_wire(ctx, 2, 9, 0.6, 0.0, 0.05, 0.6, 0.3, 0.4, 1.0e-3, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 1)
+    api.nec_gn_card(ctx, 2, 0, 10.0, 0.01, 0, 0, 0, 0)
+    api.nec_fr_card(ctx, 0, 2, 150.0, 12.0)
+    api.nec_ex_card(ctx, 0, 1, 11, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_rp_card(ctx, 0, 10, 4, 1, 0, 0, 0, 0.0, 0.0, 10.0, 90.0, 0.0, 0.0)
+    return 150.0
+
+
 # name: (builder, pattern grid (n_theta, n_phi) or None)
 CASES = {
     "ex1": (_ex1, None),
@@ -175,4 +190,5 @@ CASES = {
     "dipoles_conductivity": (_dipoles_conductivity, (19, 8)),
     "array_tl": (_array_tl, (19, 8)),
     "dipole_nt": (_dipole_nt, (19, 8)),
+    "near_ground": (_near_ground, (10, 4)),
 }

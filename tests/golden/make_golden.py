@@ -78,7 +78,14 @@ def collect(ref, name, builder, grid):
     out["trio_ptr"] = np.array(ptr, dtype=np.int32)
     out["trio_basis"] = np.array(basis, dtype=np.int32)
     out["trio_abc"] = np.array(coef, dtype=np.float64).reshape(-1, 3)
-    # interaction matrix (refilled by the reference's cmset)
+    # Sommerfeld tables of the last frequency (zero when the case has none)
+    tab, eps = ref.somm_tables(ctx)
+    if np.any(tab != 0):
+        out["somm_tables"] = tab
+        out["somm_epscf"] = np.array(eps)
+    # interaction matrix (refilled by the reference's cmset, its table
+    # interpolation cache reset to the state of a new context)
+    ref.ref_somm_interp_reset(ctx)
     z = ref.fill(ctx)
     if n <= 200:
         out["Z"] = z

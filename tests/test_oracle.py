@@ -29,20 +29,81 @@ def _zcheck(g, Z):
     return max(d.max(), dd.max()), np.mean(vals == g["Z_val"])
 
 
+# Sommerfeld-ground cases with pairs near their image: ground constants
+# (relative permittivity, conductivity S/m) of their GN card
+SOMM_GROUND = {"near_ground": (10.0, 0.01)}
+
+
+def _sweep(api):
+    from helpers import default_freq_mhz
+    if api.fr is None:
+        return [default_freq_mhz()]
+    ifrq, nfrq, f, df = api.fr
+    out = [f]
+    for _ in range(max(nfrq, 1) - 1):
+        f = f * df if ifrq == 1 else f + df
+        out.append(f)
+    return out
+
+
+def _oracle_fill(nb, oracle, name, ctx, st, api, fresh=False):
+    """The oracle's fill of the case's last frequency.  For near-ground
+    cases the tables come from the oracle and the interpolation cache
+    carries over from the earlier frequencies of the sweep, as in the
+    reference; fresh=True starts the last fill from a new cache instead."""
+    if name not in SOMM_GROUND:
+        return oracle.fill(st)
+    epr, sig = SOMM_GROUND[name]
+    interp = oracle.new_interp()
+    freqs = _sweep(api)[-1:] if fresh else _sweep(api)
+    for f in freqs:
+        sf = nb.structure(ctx, f)
+        lam = (1.0 / math.sqrt(((4.0 * 3.1415926536) * 1.0e-7) * 8.854e-12)) / (1.0e6 * f)
+        sf["somm"], _ = oracle.sommerfeld(epr, sig, lam, ETA)
+        sf["interp"] = interp
+        Z, status = oracle.fill(sf)
+    return Z, status
+
+
 @pytest.mark.parametrize("name", NAMES)
 def test_oracle_fill_matches_reference(nb, oracle, name):
-    ctx, st, _, _ = host_case(nb, CASES[name][0])
-    Z, status = oracle.fill(st)
-    assert status == 0
+    ctx, st, _, api = host_case(nb, CASES[name][0])
+    Z, status = _oracle_fill(nb, oracle, name, ctx, st, api, fresh=True)
+    # 1: rom2 reached its finest step (the reference prints a warning)
+    assert status & ~1 == 0 and (status == 0 or name in SOMM_GROUND)
     err, exact = _zcheck(golden(name), Z)
     assert err <= 1e-14, err
     assert exact >= 0.999, exact  # the restatement rounds as the reference does
     nb.nec_delete(ctx)
 
 
+@pytest.mark.parametrize("name", list(SOMM_GROUND))
+def test_oracle_sommerfeld_tables_and_cache(nb, oracle, ref, name):
+    """Sommerfeld tables (c_ggrid::sommerfeld) bit for bit, and the
+    interpolation cache through a long random sequence of points, against
+    the reference's own."""
+    g = golden(name)
+    ctx, st, _, api = host_case(nb, CASES[name][0])
+    epr, sig = SOMM_GROUND[name]
+    lam = float(g["wavelength"])
+    tab, eps = oracle.sommerfeld(epr, sig, lam, ETA)
+    assert eps == complex(g["somm_epscf"])
+    assert np.array_equal(tab, g["somm_tables"])
+    rc = ref.nec_create()
+    CASES[name][0](ref, rc)
+    ref.ref_somm_interp_reset(rc)
+    interp = oracle.new_interp()
+    rng = np.random.default_rng(3)
+    # points wander between the three grids, below their starts included
+    for x, y in zip(rng.uniform(0.0005, 0.99, 4000), rng.uniform(0.0, 1.5707963, 4000)):
+        assert np.array_equal(oracle.interpolate(interp, tab, x, y), ref.somm_interpolate(rc, x, y))
+    ref.nec_delete(rc)
+    nb.nec_delete(ctx)
+
+
 def _solve_case(nb, oracle, name):
     ctx, st, rhs, api = host_case(nb, CASES[name][0])
-    Z, _ = oracle.fill(st)
+    Z, _ = _oracle_fill(nb, oracle, name, ctx, st, api)
     x, bad = oracle.solve(Z, rhs)
     assert bad == 0
     abc, cur = oracle.coefficients(st, x)
