@@ -190,7 +190,7 @@ class Stats(C.Structure):
                 ("ms_fill", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
                 ("ms_pattern", C.c_double), ("launches", C.c_int64), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64), ("k_ms", C.c_double * 9), ("k_launches", C.c_int64 * 9),
-                ("k_flops", C.c_double * 9), ("pivoting", C.c_int)]
+                ("k_flops", C.c_double * 9), ("pivoting", C.c_int), ("near_passes", C.c_int)]
 
 
 K_NAMES = ["fill", "lu_panel", "lu_laswp", "lu_trsm", "lu_gemm", "trsv", "refine_residual",

@@ -166,8 +166,8 @@ long nec_get_trio(nec_context* in_context, int j, int* jco, double* ax, double* 
 long nec_prepare_structure(nec_context* in_context, double freq_mhz);
 /* Copy those tables out: seg (8n: x y z length radius cab sab salp, in
    wavelengths), tptr (n+1), tbasis (nt, 0-based), tabc (3nt: a b c),
-   ind (2n: EK end flags), params (8: rkh, use_exk, ground, zrati re/im,
-   frati re/im, eta).  Any pointer may be NULL; returns nt or -1. */
+   ind (2n: EK end flags), params (10: rkh, use_exk, ground, zrati re/im,
+   frati re/im, eta, complex permittivity re/im of a finite ground).  Any pointer may be NULL; returns nt or -1. */
 long nec_get_structure(nec_context* in_context, double* seg, int* tptr, int* tbasis, double* tabc,
                        int* ind, double* params);
 /* Applied-field right-hand side of the current excitation at the prepared

@@ -93,6 +93,24 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s);
  * cmset does (2127-2142); NULL removes it.  necgpu_set_structure clears it. */
 int necgpu_set_loads(necgpu_engine* e, const double* zload);
 
+/* Sommerfeld ground (structure ground type 3): computes on the device the
+   tables of the ground's reflected field for complex relative permittivity
+   eps_re + j eps_im (the reference's epscf) at the structure's medium
+   impedance; the next fills integrate them for segment pairs within
+   0.95 wavelength^2 (squared distance) of their image.  Replaces
+   c_ggrid::sommerfeld (src/c_ggrid.cpp:164-288) as called from
+   nec_ground::calculate_antenna_environment (src/nec_ground.cpp:204-209).
+   The tables belong to one structure and frequency: call after every
+   necgpu_set_structure.  The interpolation cache that the fill reads them
+   through persists across fills, as the reference's does
+   (src/c_ggrid.cpp:38-162). */
+int necgpu_set_sommerfeld(necgpu_engine* e, double eps_re, double eps_im);
+/* The tables (1068 complex, interleaved re/im: grids of 11x10, 17x5 and
+   9x8 points, 4 functions each, in the reference's m_ar1..m_ar3 layout). */
+int necgpu_copy_sommerfeld(necgpu_engine* e, double* tables);
+/* Returns the interpolation cache to the state of a new context. */
+int necgpu_reset_interpolation(necgpu_engine* e);
+
 /* Replaces cmset (src/nec_context.cpp:2077-2204) for wires: fills Z on the
  * device, row-major, Z[obs*n + basis] = field at obs due to basis (the
  * reference's cm layout). */
@@ -155,6 +173,9 @@ typedef struct necgpu_stats {
   /* pivoting of the last mixed factorisation: 0 partial (whole column),
      1 block-local (64-row diagonal block; refined in FP64, falls back to 0) */
   int pivoting;
+  /* near-ground fills (Sommerfeld tables): rounds of the last fill's column
+     scan (1: every column was right from a fresh interpolation cache) */
+  int near_passes;
 } necgpu_stats;
 int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out);
 /* 1: time each stage (fill / factor / solve / pattern) with CUDA events.

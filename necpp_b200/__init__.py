@@ -186,7 +186,7 @@ def pattern_fields(nec, index, n_cells):
 
 def structure(nec, freq_mhz=None):
     """The structure tables the GPU receives (wavelengths): dict with n, seg
-    (8n), tptr, tbasis, tabc (3nt), ind (2n), params (8).  With freq_mhz the
+    (8n), tptr, tbasis, tabc (3nt), ind (2n), params (10).  With freq_mhz the
     tables are (re)built on the host at that frequency first."""
     if freq_mhz is not None and lib.nec_prepare_structure(nec, freq_mhz) != 0:
         raise RuntimeError(nec_error_message())
@@ -196,7 +196,7 @@ def structure(nec, freq_mhz=None):
         raise RuntimeError("no structure tables built")
     st = {"n": n, "seg": _np.zeros(8 * n), "tptr": _np.zeros(n + 1, dtype=_np.int32),
           "tbasis": _np.zeros(max(nt, 1), dtype=_np.int32), "tabc": _np.zeros(3 * max(nt, 1)),
-          "ind": _np.zeros(2 * n, dtype=_np.int32), "params": _np.zeros(8)}
+          "ind": _np.zeros(2 * n, dtype=_np.int32), "params": _np.zeros(10)}
     lib.nec_get_structure(nec, _dptr(st["seg"]), _iptr(st["tptr"]), _iptr(st["tbasis"]), _dptr(st["tabc"]),
                           _iptr(st["ind"]), _dptr(st["params"]))
     st["tbasis"] = st["tbasis"][:nt]

@@ -313,6 +313,8 @@ long nec_get_structure(nec_context* c, double* seg, int* tptr, int* tbasis, doub
     params[5] = t.fr_re;
     params[6] = t.fr_im;
     params[7] = t.eta;
+    params[8] = t.eps_re;
+    params[9] = t.eps_im;
   }
   return (long)nt;
 }

@@ -698,6 +698,9 @@ void Context::build_tables() {
   tables.fr_re = frati.real();
   tables.fr_im = frati.imag();
   tables.eta = impedance();
+  const bool finite = ksymp == 2 && iperf != 1;
+  tables.eps_re = finite ? epsc.real() : 0.0;
+  tables.eps_im = finite ? epsc.imag() : 0.0;
   tables.rkh = rkh;
   tables.use_exk = use_exk ? 1 : 0;
 }
@@ -742,6 +745,9 @@ void Context::structure_loading() {
   necgpu_engine* e = engine();
   check(e, necgpu_set_structure(e, &s));
   check(e, necgpu_set_loads(e, zarray.empty() ? nullptr : reinterpret_cast<const double*>(zarray.data())));
+  // Sommerfeld tables of this frequency (calculate_antenna_environment,
+  // src/nec_ground.cpp:204-209)
+  if (tables.ground == NECGPU_GROUND_SOMMERFELD) check(e, necgpu_set_sommerfeld(e, tables.eps_re, tables.eps_im));
   check(e, necgpu_fill(e));
   check(e, necgpu_factor(e, precision_));
   have_factor_ = true;

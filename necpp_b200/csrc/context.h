@@ -116,6 +116,7 @@ class Context {
     std::vector<double> ta, tb, tc;
     int ground = 0;
     double zr_re = 1, zr_im = 0, fr_re = 1, fr_im = 0, eta = 0, rkh = 1;
+    double eps_re = 0, eps_im = 0;  // complex permittivity of a finite ground
     int use_exk = 0;
   } tables;
 

@@ -24,6 +24,7 @@
 #include "pattern.cuh"
 #include "solve.cuh"
 #include "batch.cuh"
+#include "somm.cuh"
 
 using namespace necb;
 
@@ -118,6 +119,19 @@ struct necgpu_engine {
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
   double2* d_zload = nullptr;  // impedance loading per segment (null: unloaded)
+  // Sommerfeld ground: tables of the current frequency, the interpolation
+  // cache the next fill starts from (kept across fills, as the reference's
+  // ground object keeps it), and the near-pair fields of the last fill
+  cplx* d_somm = nullptr;
+  bool somm_ready = false;
+  InterpKey interp_key{kInterpFresh, 0, 0, 0};
+  InterpCache* d_interp_carry = nullptr;  // the cache interp_key (carry = 1) stands for
+  cplx* d_near_g = nullptr;
+  int64_t near_g_cap = 0;
+  InterpKey* d_near_entry = nullptr;
+  NearRecord* d_near_rec = nullptr;
+  int* d_near_cols = nullptr;
+  int64_t near_cap = 0;
   float2* d_tinv = nullptr;  // inverted 64 x 64 diagonal blocks of the complex64 factors
   // adjoint solves: transposed factors, matrix and block inverses
   float2* ZT32 = nullptr;
@@ -280,6 +294,14 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->Z64);
   dfree(e, e->d_dinv);
   dfree(e, e->d_zload);
+  dfree(e, e->d_somm);
+  dfree(e, e->d_near_g);
+  dfree(e, e->d_near_entry);
+  dfree(e, e->d_near_rec);
+  dfree(e, e->d_near_cols);
+  e->somm_ready = false;
+  e->near_g_cap = 0;
+  e->near_cap = 0;
   dfree(e, e->d_Ap2);
   dfree(e, e->d_Bp2);
   e->tc_rows2 = 0;
@@ -372,6 +394,89 @@ int launch_fill_t(necgpu_engine* e, const FillArgs& a) {
   return 0;
 }
 
+// Near-ground pairs (Sommerfeld ground, within the table limit of their
+// image) in the reference's order.  Every source column is first integrated
+// from a fresh interpolation cache, one thread per column.  A column's
+// result depends on the cache it starts from only when its first table
+// point falls below the cached patch's grid and the cached cell passes the
+// reuse test; a host scan over the columns in order finds those whose true
+// starting cache (the one the previous column leaves) differs from the one
+// used, and only they are integrated again from it.  The scan repeats until
+// every column is consistent; after a bounded number of rounds the rest is
+// walked by one thread in order.
+template <bool X>
+int run_near_ground(necgpu_engine* e, const FillArgs& a) {
+  const int64_t n = e->n;
+  if ((size_t)n * n * 3 > ((size_t)1 << 31))
+    return fail(e, NECGPU_ERR_UNSUPPORTED, "fill: near-ground structures are limited to 26,000 segments");
+  if (e->near_g_cap < n * n * 3) {
+    dfree(e, e->d_near_g);
+    TRY(dalloc(e, e->d_near_g, (size_t)n * n * 3));
+    e->near_g_cap = n * n * 3;
+  }
+  if (e->near_cap < n) {
+    TRY(dalloc(e, e->d_near_rec, (size_t)n));
+    e->near_cap = n;
+  }
+  std::vector<InterpKey> entry((size_t)n, InterpKey{kInterpFresh, 0, 0, 0});
+  std::vector<int> cols((size_t)n);
+  std::iota(cols.begin(), cols.end(), 0);
+  std::vector<NearRecord> rec((size_t)n);
+  auto launch = [&](int ncols, int chain) -> int {
+    TRY(upload(e, e->d_near_entry, entry.data(), (size_t)n));
+    TRY(upload(e, e->d_near_cols, cols.data(), (size_t)ncols));
+    const unsigned blocks = chain ? 1u : (unsigned)((ncols + 63) / 64);
+    KLAUNCH(NECGPU_K_FILL, 0.0,
+            near_ground_kernel<X><<<blocks, chain ? 1 : 64, 0, e->stream>>>(
+                a, e->d_somm, e->d_near_cols, ncols, e->d_near_entry, e->d_interp_carry, e->d_near_rec,
+                e->d_near_g, chain));
+    return 0;
+  };
+  TRY(launch((int)n, 0));
+  auto equal = [](InterpKey p, InterpKey q) {
+    if (p.igrs == kInterpFresh || q.igrs == kInterpFresh) return p.igrs == q.igrs;
+    return p.igrs == q.igrs && p.ix == q.ix && p.iy == q.iy && p.carry == q.carry;
+  };
+  if (!e->d_interp_carry) TRY(dalloc(e, e->d_interp_carry, 1));
+  const int kMaxRounds = 8;
+  for (int round = 0;; round++) {
+    CUDA_TRY(cudaMemcpyAsync(rec.data(), e->d_near_rec, (size_t)n * sizeof(NearRecord), cudaMemcpyDeviceToHost,
+                             e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    InterpKey t = e->interp_key;
+    int ndirty = 0, first_dirty = -1;
+    for (int64_t j = 0; j < n; j++) {
+      const NearRecord& r = rec[j];
+      if (!r.has_near) continue;
+      const InterpKey need = interp_reuses(t, r.x1, r.y1) ? t : InterpKey{kInterpFresh, 0, 0, 0};
+      if (!equal(need, r.used)) {
+        if (first_dirty < 0) first_dirty = (int)j;
+        entry[j] = need;
+        cols[ndirty++] = (int)j;
+      }
+      t = r.exit;
+    }
+    e->stats.near_passes = round + 1;
+    if (ndirty == 0) {
+      // keep the cache this fill leaves, with this fill's coefficients
+      if (t.igrs != kInterpFresh && !t.carry)
+        KLAUNCH(NECGPU_K_FILL, 0.0, interp_store_kernel<<<1, 1, 0, e->stream>>>(t, e->d_somm, e->d_interp_carry));
+      if (t.igrs != kInterpFresh) t.carry = 1;
+      e->interp_key = t;
+      return 0;
+    }
+    if (round > kMaxRounds) return fail(e, NECGPU_ERR_CUDA, "fill: near-ground column order did not settle");
+    if (round + 1 < kMaxRounds) {
+      TRY(launch(ndirty, 0));
+      continue;
+    }
+    // walk every column from the first inconsistent one in order
+    int m = 0;
+    for (int64_t j = first_dirty; j < n; j++) cols[m++] = (int)j;
+    TRY(launch(m, 1));
+  }
+}
+
 int run_fill(necgpu_engine* e, bool want64, bool want32) {
   if (e->n <= 0) return fail(e, NECGPU_ERR_ARG, "fill: no structure set");
   const int64_t n = e->n;
@@ -398,10 +503,16 @@ int run_fill(necgpu_engine* e, bool want64, bool want32) {
   a.eb = e->d_ecoef + e->ne;
   a.ec = e->d_ecoef + 2 * e->ne;
   a.P = e->P;
+  a.P.near_g = nullptr;
   a.Z64 = want64 ? e->Z64 : nullptr;
   a.Z32 = want32 ? e->Z32 : nullptr;
   a.status = e->d_status;
   const bool x = e->use_exk != 0;
+  if (e->ground == kGroundSommerfeld && e->somm_ready) {
+    TRY(x ? run_near_ground<true>(e, a) : run_near_ground<false>(e, a));
+    a.P.near_g = e->d_near_g;
+    a.P.near_n = n;
+  }
   int rc;
   switch (e->ground) {
     case kGroundNone: rc = x ? launch_fill_t<kGroundNone, true>(e, a) : launch_fill_t<kGroundNone, false>(e, a); break;
@@ -1298,6 +1409,7 @@ int necgpu_destroy(necgpu_engine* e) {
     cudaStreamSynchronize(e->stream);
   }
   free_all(e);
+  dfree(e, e->d_interp_carry);  // the interpolation cache lives as long as the engine
   dfree(e, e->d_status);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
@@ -1400,6 +1512,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   e->have_solution = false;
   e->adj_ready = false;
   dfree(e, e->d_zload);  // loads belong to one structure: set them after it
+  e->somm_ready = false;   // so do the Sommerfeld tables (they follow the frequency)
   dfree(e, e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
 
   std::vector<double> seg(8 * n);
@@ -1475,8 +1588,8 @@ int necgpu_fill(necgpu_engine* e) {
   TRY(sync_status(e, &st));
   if (st & kStatSommerfeldTab)
     return fail(e, NECGPU_ERR_UNSUPPORTED,
-                "fill: a segment pair lies within 0.95 wavelength of its ground image; the "
-                "Sommerfeld table-interpolation path is not part of this build");
+                "fill: a segment pair lies within 0.95 wavelength of its ground image and no "
+                "Sommerfeld tables are set (necgpu_set_sommerfeld)");
   if (st & kStatIterCap) return fail(e, NECGPU_ERR_NONFINITE, "fill: quadrature did not terminate (non-finite geometry?)");
   return NECGPU_OK;
 }
@@ -1651,6 +1764,39 @@ int necgpu_set_loads(necgpu_engine* e, const double* zload) {
   return NECGPU_OK;
 }
 
+int necgpu_set_sommerfeld(necgpu_engine* e, double eps_re, double eps_im) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (e->n <= 0) return fail(e, NECGPU_ERR_ARG, "set_sommerfeld: no structure set");
+  if (e->ground != kGroundSommerfeld) return fail(e, NECGPU_ERR_ARG, "set_sommerfeld: the structure has no Sommerfeld ground");
+  CUDA_TRY(cudaSetDevice(e->device));
+  if (!e->d_somm) TRY(dalloc(e, e->d_somm, (size_t)kSommPoints));
+  CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+  const unsigned blocks = (unsigned)((kSommEvalPoints + 31) / 32);
+  KLAUNCH(NECGPU_K_FILL, 0.0,
+          somm_table_kernel<<<blocks, 32, 0, e->stream>>>(mk(eps_re, eps_im), e->P.eta, e->d_somm, e->d_status));
+  int st = 0;
+  TRY(sync_status(e, &st));
+  if (st & kStatIterCap) return fail(e, NECGPU_ERR_NONFINITE, "set_sommerfeld: a Sommerfeld integral did not converge");
+  e->somm_ready = true;
+  e->filled = false;
+  return NECGPU_OK;
+}
+
+int necgpu_copy_sommerfeld(necgpu_engine* e, double* tables) {
+  if (!e || !tables) return NECGPU_ERR_ARG;
+  if (!e->somm_ready) return fail(e, NECGPU_ERR_ARG, "copy_sommerfeld: no tables");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaMemcpyAsync(tables, e->d_somm, kSommPoints * sizeof(cplx), cudaMemcpyDeviceToHost, e->stream));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return NECGPU_OK;
+}
+
+int necgpu_reset_interpolation(necgpu_engine* e) {
+  if (!e) return NECGPU_ERR_ARG;
+  e->interp_key = InterpKey{kInterpFresh, 0, 0, 0};
+  return NECGPU_OK;
+}
+
 int necgpu_copy_solution(necgpu_engine* e, double* x) {
   if (!e || !x) return NECGPU_ERR_ARG;
   if (!e->have_solution) return fail(e, NECGPU_ERR_ARG, "copy_solution: no solution held");
@@ -1797,6 +1943,7 @@ int necgpu_perturbed_terms(necgpu_engine* e, int nstruct, const necgpu_structure
     a.eb = c + ne;
     a.ec = c + 2 * ne;
     a.P = e->P;
+    a.P.near_g = nullptr;
     a.Z64 = nullptr;
     a.Z32 = nullptr;
     a.status = e->d_status;

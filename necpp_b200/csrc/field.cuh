@@ -36,7 +36,19 @@ struct FieldParams {
   cplx zrati;       // 1/sqrt(eps_c)
   cplx frati;       // image scale factor
   cplx u, u2;       // ground-wave constants (u = zrati)
+  // Sommerfeld ground: projected fields (etk, ets, etc) of the pairs closer
+  // than the table limit to their image, precomputed in the reference's
+  // order by near_ground_kernel; [(obs * near_n + src) * 3 + k], or null
+  const cplx* near_g;
+  int64_t near_n;
 };
+
+// Squared distance from an observation point to a source's image (the
+// table / Norton switch of efld, 2993-2995), rounded as the reference rounds
+// it (no fused multiply-add) so every kernel takes the same branch.
+__device__ __forceinline__ double image_r2(double xij, double yij, double zij) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(xij, xij), __dmul_rn(yij, yij)), __dmul_rn(zij, zij));
+}
 
 // c_evlcom.cpp:845-868
 __device__ __forceinline__ void conv_test(double f1r, double f2r, double* tr, double f1i,
@@ -501,19 +513,15 @@ __device__ void gwave(double r2, double zph, cplx xx2, cplx u, cplx u2, double e
 
 enum { kGroundNone = 0, kGroundPerfect = 1, kGroundReflection = 2, kGroundSommerfeld = 3 };
 
-// Projected fields (etk, ets, etc) of source J on observation segment i:
-// efld (2845-3045) followed by the tangential projection of cmww (2617-2619).
+// Fields of source J at observation point i, direct plus (for a ground)
+// image: efld (2845-2956) up to the Sommerfeld/Norton part.
 template <int GROUND, bool EXK>
-__device__ void pair_field(const SrcSeg& J, double xi, double yi, double zi, double ai,
-                           double cabi, double sabi, double salpi, bool ij,
-                           const FieldParams& P, cplx* etk, cplx* ets, cplx* etc,
-                           int* status) {
+__device__ __forceinline__ void pair_fields9(const SrcSeg& J, double xi, double yi, double zi, double ai,
+                                             bool ij, const FieldParams& P, cplx ex[9], int* status) {
   cplx e[9];
   const double xij = xi - J.x;
   const double yij = yi - J.y;
-  efld_compute<EXK>(J, xij, yij, ai, J.salp, zi - J.z, ij, P, e, status);
-  cplx exk = e[0], eyk = e[1], ezk = e[2], exs = e[3], eys = e[4], ezs = e[5], exc = e[6],
-       eyc = e[7], ezc = e[8];
+  efld_compute<EXK>(J, xij, yij, ai, J.salp, zi - J.z, ij, P, ex, status);
   if (GROUND != kGroundNone) {
     const double zij = zi + J.z;
     double r = efld_compute<EXK>(J, xij, yij, ai, -J.salp, zij, true, P, e, status);
@@ -547,141 +555,176 @@ __device__ void pair_field(const SrcSeg& J, double xi, double yi, double zi, dou
         e[k + 2] = refs * e[k + 2];
       }
     }
-    exk -= e[0] * P.frati;
-    eyk -= e[1] * P.frati;
-    ezk -= e[2] * P.frati;
-    exs -= e[3] * P.frati;
-    eys -= e[4] * P.frati;
-    ezs -= e[5] * P.frati;
-    exc -= e[6] * P.frati;
-    eyc -= e[7] * P.frati;
-    ezc -= e[8] * P.frati;
+#pragma unroll
+    for (int k = 0; k < 9; k++) ex[k] -= e[k] * P.frati;
   }
+}
+
+// Horizontal direction of the source and the observation point displaced
+// by the observer's radius for the thin-wire approximation (2958-3000).
+struct SommGeom {
+  double xsn, ysn, sn, xo, yo, zo, rhox, rhoy, rhoz, rh;
+};
+
+__device__ __forceinline__ SommGeom somm_geometry(const SrcSeg& J, double xi, double yi, double zi, double ai) {
+  SommGeom g;
+  const double cabj = J.cab, sabj = J.sab, salpj = J.salp;
+  g.sn = sqrt(cabj * cabj + sabj * sabj);
+  if (g.sn >= 1.0e-5) {
+    g.xsn = cabj / g.sn;
+    g.ysn = sabj / g.sn;
+  } else {
+    g.sn = 0.0;
+    g.xsn = 1.0;
+    g.ysn = 0.0;
+  }
+  const double xij = xi - J.x, yij = yi - J.y, zij = zi + J.z;
+  const double salpr = -salpj;
+  g.rhox = sabj * zij - salpr * yij;
+  g.rhoy = salpr * xij - cabj * zij;
+  g.rhoz = cabj * yij - sabj * xij;
+  g.rh = sqrt(g.rhox * g.rhox + g.rhoy * g.rhoy + g.rhoz * g.rhoz);
+  if (g.rh <= 1.e-10) {
+    g.xo = xi - ai * g.ysn;
+    g.yo = yi + ai * g.xsn;
+    g.zo = zi;
+  } else {
+    // the reference takes sqrt of the already-rooted norm here
+    double rr = ai / sqrt(g.rh);
+    if (g.rhoz < 0.0) rr = -rr;
+    g.xo = xi + rr * g.rhox;
+    g.yo = yi + rr * g.rhoy;
+    g.zo = zi + rr * g.rhoz;
+  }
+  return g;
+}
+
+// Norton ground field of a source lumped at its centre (sflds, isnor = 2,
+// 6024-6098) with the thin-wire correction of efld (3009-3032).
+__device__ void norton_field(const SrcSeg& J, const SommGeom& g, double xij, double yij, double zij, double r,
+                             double ai, const FieldParams& P, cplx e[9]) {
+  const double cabj = J.cab, sabj = J.sab, salpj = J.salp, salpr = -salpj;
+  const double xsn = g.xsn, ysn = g.ysn, sn = g.sn;
+  double xt = J.x + 0. * cabj, yt = J.y + 0. * sabj, zt = J.z + 0. * salpj;
+  double rhx = g.xo - xt, rhy = g.yo - yt;
+  double rhs = rhx * rhx + rhy * rhy;
+  double rho = sqrt(rhs);
+  double phx, phy;
+  if (rho <= 0.0) {
+    rhx = 1.0;
+    rhy = 0.0;
+    phx = 0.0;
+    phy = 1.0;
+  } else {
+    rhx = rhx / rho;
+    rhy = rhy / rho;
+    phx = -rhy;
+    phy = rhx;
+  }
+  double cph = rhx * xsn + rhy * ysn;
+  double sph = rhy * xsn - rhx * ysn;
+  if (fabs(cph) < 1.0e-10) cph = 0.0;
+  if (fabs(sph) < 1.0e-10) sph = 0.0;
+  double zph = g.zo + zt;
+  double zphs = zph * zph;
+  double r2s = rhs + zphs;
+  double r2 = sqrt(r2s);
+  double rk = r2 * kTwoPiD;
+  double s_, c_;
+  sincos(rk, &s_, &c_);
+  cplx xx2 = mk(c_, -s_);
+  cplx erv, ezv, erh, ezh, eph;
+  gwave(r2, zph, xx2, P.u, P.u2, P.eta, &erv, &ezv, &erh, &ezh, &eph);
+  const cplx C1 = mk(0.0, kC1);
+  cplx et = -C1 * P.frati * xx2 / (r2s * r2);
+  cplx er = 2. * et * mk(1.0, rk);
+  et = et * mk(1.0 - rk * rk, rk);
+  cplx hrv = (er + et) * rho * zph / r2s;
+  cplx hzv = (zphs * er - rhs * et) / r2s;
+  cplx hrh = (rhs * er - zphs * et) / r2s;
+  erv = erv - hrv;
+  ezv = ezv - hzv;
+  erh = erh + hrh;
+  ezh = ezh + hrv;
+  eph = eph + et;
+  erv = erv * salpj;
+  ezv = ezv * salpj;
+  erh = erh * sn * cph;
+  ezh = ezh * sn * cph;
+  eph = eph * sn * sph;
+  erh = erv + erh;
+  e[0] = (erh * rhx + eph * phx) * J.s;
+  e[1] = (erh * rhy + eph * phy) * J.s;
+  e[2] = (ezv + ezh) * J.s;
+  e[3] = mk(0., 0.);
+  e[4] = mk(0., 0.);
+  e[5] = mk(0., 0.);
+  double sfac = kPiD * J.s;
+  sfac = sin(sfac) / sfac;
+  e[6] = e[0] * sfac;
+  e[7] = e[1] * sfac;
+  e[8] = e[2] * sfac;
+  // thin-wire correction, 3009-3032
+  double zp = xij * cabj + yij * sabj + zij * salpr;
+  double rh = r - zp * zp;
+  double dmin = (rh <= 1.e-10) ? 0.0 : sqrt(rh / (rh + ai * ai));
+  if (dmin <= .95) {
+    double pxx = 1. - dmin;
+#pragma unroll
+    for (int k = 0; k < 9; k += 3) {
+      cplx t = (e[k] * cabj + e[k + 1] * sabj + e[k + 2] * salpr) * pxx;
+      e[k] = dmin * e[k] + t * cabj;
+      e[k + 1] = dmin * e[k + 1] + t * sabj;
+      e[k + 2] = dmin * e[k + 2] + t * salpr;
+    }
+  }
+}
+
+// Tangential projection of cmww, 2617-2619
+__device__ __forceinline__ void project_fields(const cplx ex[9], double cabi, double sabi, double salpi, cplx* etk,
+                                               cplx* ets, cplx* etc) {
+  *etk = ex[0] * cabi + ex[1] * sabi + ex[2] * salpi;
+  *ets = ex[3] * cabi + ex[4] * sabi + ex[5] * salpi;
+  *etc = ex[6] * cabi + ex[7] * sabi + ex[8] * salpi;
+}
+
+// Projected fields (etk, ets, etc) of source J on observation segment i:
+// efld (2845-3045) followed by the tangential projection of cmww (2617-2619).
+// For Sommerfeld ground, a pair within the table limit of its image is read
+// from P.near_g at pair_index (obs * n + src) when those fields exist, and
+// is reported (kStatSommerfeldTab) otherwise.
+template <int GROUND, bool EXK>
+__device__ void pair_field(const SrcSeg& J, double xi, double yi, double zi, double ai,
+                           double cabi, double sabi, double salpi, bool ij,
+                           const FieldParams& P, cplx* etk, cplx* ets, cplx* etc,
+                           int* status, int64_t pair_index = -1) {
+  const double xij = xi - J.x, yij = yi - J.y;
+  double r_img = 0.0;
   if (GROUND == kGroundSommerfeld) {
-    // Sommerfeld/Norton, 2958-3042 (Norton branch)
-    const double cabj = J.cab, sabj = J.sab, salpj = J.salp;
-    double sn = sqrt(cabj * cabj + sabj * sabj);
-    double xsn, ysn;
-    if (sn >= 1.0e-5) {
-      xsn = cabj / sn;
-      ysn = sabj / sn;
-    } else {
-      sn = 0.0;
-      xsn = 1.0;
-      ysn = 0.0;
+    r_img = image_r2(xij, yij, zi + J.z);
+    if (r_img <= .95 && P.near_g != nullptr && pair_index >= 0) {
+      const cplx* g = P.near_g + pair_index * 3;
+      *etk = g[0];
+      *ets = g[1];
+      *etc = g[2];
+      return;
     }
-    const double zij = zi + J.z;
-    const double salpr = -salpj;
-    double rhox = sabj * zij - salpr * yij;
-    double rhoy = salpr * xij - cabj * zij;
-    double rhoz = cabj * yij - sabj * xij;
-    double rh = sqrt(rhox * rhox + rhoy * rhoy + rhoz * rhoz);
-    double xo, yo, zo;
-    if (rh <= 1.e-10) {
-      xo = xi - ai * ysn;
-      yo = yi + ai * xsn;
-      zo = zi;
-    } else {
-      // the reference takes sqrt of the already-rooted norm here
-      rh = ai / sqrt(rh);
-      if (rhoz < 0.0) rh = -rh;
-      xo = xi + rh * rhox;
-      yo = yi + rh * rhoy;
-      zo = zi + rh * rhoz;
-    }
-    double r = xij * xij + yij * yij + zij * zij;
-    if (r <= .95) {
+  }
+  cplx ex[9];
+  pair_fields9<GROUND, EXK>(J, xi, yi, zi, ai, ij, P, ex, status);
+  if (GROUND == kGroundSommerfeld) {
+    cplx e[9];
+    if (r_img <= .95) {
       *status |= kStatSommerfeldTab;
       for (int k = 0; k < 9; k++) e[k] = mk(0., 0.);
     } else {
-      // sflds(t=0), isnor=2: 6024-6098
-      double xt = J.x + 0. * cabj, yt = J.y + 0. * sabj, zt = J.z + 0. * salpj;
-      double rhx = xo - xt, rhy = yo - yt;
-      double rhs = rhx * rhx + rhy * rhy;
-      double rho = sqrt(rhs);
-      double phx, phy;
-      if (rho <= 0.0) {
-        rhx = 1.0;
-        rhy = 0.0;
-        phx = 0.0;
-        phy = 1.0;
-      } else {
-        rhx = rhx / rho;
-        rhy = rhy / rho;
-        phx = -rhy;
-        phy = rhx;
-      }
-      double cph = rhx * xsn + rhy * ysn;
-      double sph = rhy * xsn - rhx * ysn;
-      if (fabs(cph) < 1.0e-10) cph = 0.0;
-      if (fabs(sph) < 1.0e-10) sph = 0.0;
-      double zph = zo + zt;
-      double zphs = zph * zph;
-      double r2s = rhs + zphs;
-      double r2 = sqrt(r2s);
-      double rk = r2 * kTwoPiD;
-      double s_, c_;
-      sincos(rk, &s_, &c_);
-      cplx xx2 = mk(c_, -s_);
-      cplx erv, ezv, erh, ezh, eph;
-      gwave(r2, zph, xx2, P.u, P.u2, P.eta, &erv, &ezv, &erh, &ezh, &eph);
-      const cplx C1 = mk(0.0, kC1);
-      cplx et = -C1 * P.frati * xx2 / (r2s * r2);
-      cplx er = 2. * et * mk(1.0, rk);
-      et = et * mk(1.0 - rk * rk, rk);
-      cplx hrv = (er + et) * rho * zph / r2s;
-      cplx hzv = (zphs * er - rhs * et) / r2s;
-      cplx hrh = (rhs * er - zphs * et) / r2s;
-      erv = erv - hrv;
-      ezv = ezv - hzv;
-      erh = erh + hrh;
-      ezh = ezh + hrv;
-      eph = eph + et;
-      erv = erv * salpj;
-      ezv = ezv * salpj;
-      erh = erh * sn * cph;
-      ezh = ezh * sn * cph;
-      eph = eph * sn * sph;
-      erh = erv + erh;
-      e[0] = (erh * rhx + eph * phx) * J.s;
-      e[1] = (erh * rhy + eph * phy) * J.s;
-      e[2] = (ezv + ezh) * J.s;
-      e[3] = mk(0., 0.);
-      e[4] = mk(0., 0.);
-      e[5] = mk(0., 0.);
-      double sfac = kPiD * J.s;
-      sfac = sin(sfac) / sfac;
-      e[6] = e[0] * sfac;
-      e[7] = e[1] * sfac;
-      e[8] = e[2] * sfac;
-      // thin-wire correction, 3009-3032
-      double zp = xij * cabj + yij * sabj + zij * salpr;
-      rh = r - zp * zp;
-      double dmin = (rh <= 1.e-10) ? 0.0 : sqrt(rh / (rh + ai * ai));
-      if (dmin <= .95) {
-        double pxx = 1. - dmin;
-#pragma unroll
-        for (int k = 0; k < 9; k += 3) {
-          cplx t = (e[k] * cabj + e[k + 1] * sabj + e[k + 2] * salpr) * pxx;
-          e[k] = dmin * e[k] + t * cabj;
-          e[k + 1] = dmin * e[k + 1] + t * sabj;
-          e[k + 2] = dmin * e[k + 2] + t * salpr;
-        }
-      }
+      const SommGeom g = somm_geometry(J, xi, yi, zi, ai);
+      norton_field(J, g, xij, yij, zi + J.z, r_img, ai, P, e);
     }
-    exk = exk + e[0];
-    eyk = eyk + e[1];
-    ezk = ezk + e[2];
-    exs = exs + e[3];
-    eys = eys + e[4];
-    ezs = ezs + e[5];
-    exc = exc + e[6];
-    eyc = eyc + e[7];
-    ezc = ezc + e[8];
+#pragma unroll
+    for (int k = 0; k < 9; k++) ex[k] = ex[k] + e[k];
   }
-  *etk = exk * cabi + eyk * sabi + ezk * salpi;
-  *ets = exs * cabi + eys * sabi + ezs * salpi;
-  *etc = exc * cabi + eyc * sabi + ezc * salpi;
+  project_fields(ex, cabi, sabi, salpi, etk, ets, etc);
 }
 
 }  // namespace necb

@@ -88,7 +88,7 @@ __device__ __forceinline__ void fill_tile(const FillArgs& A, const ContractArgs&
     if (!active) continue;
     cplx etk, ets, etc;
     pair_field<GROUND, EXK>(J, xi, yi, zi, ai, cabi, sabi, salpi, i != j, A.P, &etk, &ets, &etc,
-                            &status);
+                            &status, i * A.n + j);
     const int e0 = __ldg(A.tsrc_eptr + sidx), e1 = __ldg(A.tsrc_eptr + sidx + 1);
     for (int e = e0; e < e1; e++) {
       const int c = A.ecol[e];

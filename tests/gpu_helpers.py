@@ -20,7 +20,7 @@ class NecgpuStats(C.Structure):
                 ("ms_fill", C.c_double), ("ms_factor", C.c_double), ("ms_solve", C.c_double),
                 ("ms_pattern", C.c_double), ("launches", C.c_int64), ("h2d_bytes", C.c_int64),
                 ("d2h_bytes", C.c_int64), ("k_ms", C.c_double * 9), ("k_launches", C.c_int64 * 9),
-                ("k_flops", C.c_double * 9), ("pivoting", C.c_int)]
+                ("k_flops", C.c_double * 9), ("pivoting", C.c_int), ("near_passes", C.c_int)]
 
 
 class Engine:
@@ -40,6 +40,9 @@ class Engine:
         L.necgpu_set_refinement.argtypes = [C.c_void_p, C.c_double, C.c_int]
         L.necgpu_set_pivoting.argtypes = [C.c_void_p, C.c_int]
         L.necgpu_set_loads.argtypes = [C.c_void_p, _dp]
+        L.necgpu_set_sommerfeld.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.necgpu_copy_sommerfeld.argtypes = [C.c_void_p, _dp]
+        L.necgpu_reset_interpolation.argtypes = [C.c_void_p]
         L.necgpu_get_stats.argtypes = [C.c_void_p, C.POINTER(NecgpuStats)]
         self.h = C.c_void_p()
         rc = L.necgpu_create(C.byref(self.h), device)
@@ -54,7 +57,9 @@ class Engine:
         if rc != 0:
             raise RuntimeError("necgpu rc=%d: %s" % (rc, self.err()))
 
-    def set_structure(self, st):
+    def set_structure(self, st, tables=True):
+        """Structure tables of st; for Sommerfeld ground also its tables
+        (unless tables=False)."""
         n = st["n"]
         s = NecgpuStructure()
         s.n = n
@@ -78,7 +83,17 @@ class Engine:
         self._keep = (st, s, zl)
         if np.any(zl != 0):
             self.check(self.lib.necgpu_set_loads(self.h, zl.ctypes.data_as(_dp)))
+        if tables and int(p[2]) == 3:
+            self.check(self.lib.necgpu_set_sommerfeld(self.h, p[8], p[9]))
         self.n = n
+
+    def sommerfeld_tables(self):
+        t = np.zeros(2 * 1068)
+        self.check(self.lib.necgpu_copy_sommerfeld(self.h, t.ctypes.data_as(_dp)))
+        return t[0::2] + 1j * t[1::2]
+
+    def reset_interpolation(self):
+        self.check(self.lib.necgpu_reset_interpolation(self.h))
 
     def fill(self):
         self.check(self.lib.necgpu_fill(self.h))

@@ -116,9 +116,13 @@ def test_case_matches_reference(nb, api, name, precision):
 def test_fill_matches_oracle(nb, oracle, engine, name):
     """Element-wise: the sm_100a fill against the oracle on identical tables."""
     ctx, st, _, _ = host_case(nb, CASES[name][0])
+    engine.reset_interpolation()
     engine.set_structure(st)
     engine.fill()
     Zg = engine.copy_z()
+    if int(st["params"][2]) == 3:
+        # the oracle integrates the device's own tables, from a new cache
+        st["somm"] = engine.sommerfeld_tables()
     Zo, _ = oracle.fill(st)
     scale = np.max(np.abs(Zo))
     assert np.max(np.abs(Zg - Zo)) <= 1e-12 * scale
@@ -282,16 +286,53 @@ def test_engine_rejects_bad_calls(nb):
     e.close()
 
 
-def test_sommerfeld_near_ground_is_reported(nb, api):
-    """A wire within 0.95 wavelength of its Sommerfeld-ground image needs the
-    table-interpolation path, which this build does not provide: the call
-    fails with a message rather than returning a wrong answer."""
-    ctx = nb.nec_create()
-    nb.nec_wire(ctx, 1, 11, 0, 0, 0.5, 0, 0, 1.5, 1e-3, 1, 1)
-    nb.nec_geometry_complete(ctx, 0)
-    nb.nec_gn_card(ctx, 2, 0, 13.0, 0.005, 0, 0, 0, 0)
-    nb.nec_fr_card(ctx, 0, 1, 145.0, 0)
-    nb.nec_ex_card(ctx, 0, 1, 6, 0, 1.0, 0, 0, 0, 0, 0)
-    assert nb.nec_xq_card(ctx, 0) == 1
-    assert "Sommerfeld" in nb.nec_error_message()
+def test_sommerfeld_tables_match_reference(nb, engine):
+    """The device's Sommerfeld tables (one thread per grid point) against
+    the reference's c_ggrid::sommerfeld for the near-ground case."""
+    g = golden("near_ground")
+    ctx, st, _, _ = host_case(nb, CASES["near_ground"][0])
+    assert complex(st["params"][8], st["params"][9]) == complex(g["somm_epscf"])
+    engine.set_structure(st)
+    t = engine.sommerfeld_tables()
+    ref = g["somm_tables"]
+    assert np.max(np.abs(t - ref)) <= 1e-12 * np.max(np.abs(ref))
+    big = np.abs(ref) > 1e-6 * np.max(np.abs(ref))
+    assert np.max(np.abs(t[big] - ref[big]) / np.abs(ref[big])) <= 1e-10
+    nb.nec_delete(ctx)
+
+
+def test_near_ground_without_tables_is_reported(nb, engine):
+    """A pair within 0.95 wavelength of its Sommerfeld-ground image needs the
+    tables: without them the fill fails with a message rather than
+    returning a wrong answer."""
+    ctx, st, _, _ = host_case(nb, CASES["near_ground"][0])
+    engine.set_structure(st, tables=False)
+    with pytest.raises(RuntimeError, match="Sommerfeld"):
+        engine.fill()
+    nb.nec_delete(ctx)
+
+
+def test_near_ground_cache_carries_over(nb, oracle, engine):
+    """The interpolation cache persists across fills as the reference's does:
+    a second fill of the same structure starts from the cache the first
+    left, and matches the oracle filling twice in a row."""
+    ctx, st, _, _ = host_case(nb, CASES["near_ground"][0])
+    engine.reset_interpolation()
+    engine.set_structure(st)
+    engine.fill()
+    engine.set_structure(st)
+    engine.fill()
+    Zg = engine.copy_z()
+    st["somm"] = engine.sommerfeld_tables()
+    oracle.fill(st)            # first fill: leaves the cache in st["interp"]
+    Zo, _ = oracle.fill(st)    # second fill from that cache
+    scale = np.max(np.abs(Zo))
+    assert np.max(np.abs(Zg - Zo)) <= 1e-12 * scale
+    assert engine.stats().near_passes >= 1
+    engine.reset_interpolation()
+    engine.set_structure(st)
+    engine.fill()
+    st["interp"] = None
+    Zf, _ = oracle.fill(st)
+    assert np.max(np.abs(engine.copy_z() - Zf)) <= 1e-12 * scale
     nb.nec_delete(ctx)
