@@ -101,7 +101,9 @@ long nec_pt_card(nec_context* in_context, int itmp1, int itmp2, int itmp3, int i
 long nec_pq_card(nec_context* in_context, int itmp1, int itmp2, int itmp3, int itmp4);
 /* src/libnecpp.h:509 */
 long nec_kh_card(nec_context* in_context, double tmp1);
-/* src/libnecpp.h:510-511 (near fields: return 1) */
+/* src/libnecpp.h:510-511: near electric / magnetic field over a grid of
+   points (near = 0 rectangular in metres, 1 spherical in degrees); results
+   through nec_near_field */
 long nec_ne_card(nec_context* in_context, int itmp1, int itmp2, int itmp3, int itmp4,
                  double tmp1, double tmp2, double tmp3, double tmp4, double tmp5, double tmp6);
 long nec_nh_card(nec_context* in_context, int itmp1, int itmp2, int itmp3, int itmp4,
@@ -177,6 +179,12 @@ long nec_get_rhs(nec_context* in_context, double* out);
 /* Impedance loading (n complex: lambda x impedance per unit length, the
    reference's zarray) of the structure prepared last; zeros if unloaded. */
 long nec_get_loads(nec_context* in_context, double* out);
+/* Near-field pattern `index` (0-based, in the order NE/NH requests ran;
+   the reference's nec_context::get_near_field_pattern): returns its point
+   count, or -1 if it does not exist.  nfeh receives 0 (electric) or 1
+   (magnetic); with non-null buffers, xyz the points (metres, 3 per point)
+   and fields 3 complex per point (x, y, z; re/im interleaved; V/m or A/m). */
+long nec_near_field(nec_context* in_context, int index, int* nfeh, double* xyz, double* fields);
 /* Number of NT/TL networks on the context (0 if none). */
 long nec_network_count(nec_context* in_context);
 /* The context's GPU engine (include/necgpu.h), created on first use; NULL

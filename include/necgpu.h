@@ -111,6 +111,15 @@ int necgpu_copy_sommerfeld(necgpu_engine* e, double* tables);
 /* Returns the interpolation cache to the state of a new context. */
 int necgpu_reset_interpolation(necgpu_engine* e);
 
+/* Near field of the last solution at npts points (pts: x, y, z per point in
+   wavelengths): magnetic = 0 the electric field (nefld,
+   src/nec_context.cpp:4304-4490), 1 the magnetic field (nhfld, 5189-5265).
+   fields: 3 complex per point (x, y, z; interleaved re/im), in the units of
+   the reference's nec_near_field_pattern.  With Sommerfeld ground the points
+   are taken in the given order through the tables' interpolation cache, as
+   nfpat takes them. */
+int necgpu_near_field(necgpu_engine* e, int magnetic, int npts, const double* pts, double* fields);
+
 /* Replaces cmset (src/nec_context.cpp:2077-2204) for wires: fills Z on the
  * device, row-major, Z[obs*n + basis] = field at obs due to basis (the
  * reference's cm layout). */

@@ -95,6 +95,7 @@ _sig("nec_get_trio", _l, [_p, _i, _ip, _dp, _dp, _dp, _l])
 _sig("nec_last_refinement", _l, [_p, _ip, _dp])
 _sig("nec_get_loads", _l, [_p, _dp])
 _sig("nec_network_count", _l, [_p])
+_sig("nec_near_field", _l, [_p, _i, _C.POINTER(_i), _dp, _dp])
 _sig("nec_gradient", _l, [_p, _i, _C.POINTER(_p), _C.POINTER(_p), _dp, _d, _d, _dp, _dp])
 _sig("nec_prepare_structure", _l, [_p, _d])
 _sig("nec_get_structure", _l, [_p, _dp, _ip, _ip, _dp, _ip, _dp])
@@ -182,6 +183,22 @@ def pattern_fields(nec, index, n_cells):
     if k < 0:
         raise IndexError("no pattern for index %d" % index)
     return eth[0::2] + 1j * eth[1::2], eph[0::2] + 1j * eph[1::2]
+
+
+def near_fields(nec):
+    """Every near-field pattern of the context: list of (nfeh, points (m,
+    np x 3), fields (np x 3 complex))."""
+    out = []
+    k = 0
+    while True:
+        nfeh = _i(0)
+        np_ = lib.nec_near_field(nec, k, _C.byref(nfeh), None, None)
+        if np_ < 0:
+            return out
+        xyz, f = _np.zeros(3 * np_), _np.zeros(6 * np_)
+        lib.nec_near_field(nec, k, _C.byref(nfeh), _dptr(xyz), _dptr(f))
+        out.append((nfeh.value, xyz.reshape(-1, 3), (f[0::2] + 1j * f[1::2]).reshape(-1, 3)))
+        k += 1
 
 
 def structure(nec, freq_mhz=None):

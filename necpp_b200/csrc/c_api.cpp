@@ -147,13 +147,33 @@ long nec_pq_card(nec_context* c, int a, int b, int cc, int d) { NEC_TRY(c->pq_ca
 
 long nec_kh_card(nec_context* c, double r) { NEC_TRY(c->kh_card(r)); }
 
-long nec_ne_card(nec_context*, int, int, int, int, double, double, double, double, double,
-                 double) {
-  NEC_UNSUPPORTED("NE (near electric field)");
+long nec_ne_card(nec_context* c, int itmp1, int itmp2, int itmp3, int itmp4, double tmp1, double tmp2,
+                 double tmp3, double tmp4, double tmp5, double tmp6) {
+  NEC_TRY(c->ne_nh_card(0, itmp1, itmp2, itmp3, itmp4, tmp1, tmp2, tmp3, tmp4, tmp5, tmp6));
 }
-long nec_nh_card(nec_context*, int, int, int, int, double, double, double, double, double,
-                 double) {
-  NEC_UNSUPPORTED("NH (near magnetic field)");
+long nec_nh_card(nec_context* c, int itmp1, int itmp2, int itmp3, int itmp4, double tmp1, double tmp2,
+                 double tmp3, double tmp4, double tmp5, double tmp6) {
+  NEC_TRY(c->ne_nh_card(1, itmp1, itmp2, itmp3, itmp4, tmp1, tmp2, tmp3, tmp4, tmp5, tmp6));
+}
+
+long nec_near_field(nec_context* c, int index, int* nfeh, double* xyz, double* fields) {
+  if (!c || index < 0 || index >= (int)c->near_fields.size()) return -1;
+  const necb::NearFieldPattern& p = c->near_fields[index];
+  if (nfeh) *nfeh = p.nfeh;
+  const size_t np = p.x.size();
+  for (size_t i = 0; xyz && i < np; i++) {
+    xyz[3 * i] = p.x[i];
+    xyz[3 * i + 1] = p.y[i];
+    xyz[3 * i + 2] = p.z[i];
+  }
+  for (size_t i = 0; fields && i < np; i++) {
+    const necb::cd v[3] = {p.fx[i], p.fy[i], p.fz[i]};
+    for (int k = 0; k < 3; k++) {
+      fields[6 * i + 2 * k] = v[k].real();
+      fields[6 * i + 2 * k + 1] = v[k].imag();
+    }
+  }
+  return (long)np;
 }
 long nec_cp_card(nec_context*, int, int, int, int) { NEC_UNSUPPORTED("CP (coupling)"); }
 long nec_pl_card(nec_context*, char*, int, int, int, int) { NEC_UNSUPPORTED("PL (plot file)"); }

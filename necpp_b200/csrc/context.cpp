@@ -175,6 +175,83 @@ void Context::tl_card(int tag1, int seg1, int tag2, int seg2, double z0, double 
   network_card(2, tag1, seg1, tag2, seg2, x);
 }
 
+// ne_nh_card, src/nec_context.cpp:928-961: a near-field request (electric
+// for nfeh 0, magnetic for 1) over nx x ny x nz points, rectangular
+// (near = 0: x, y, z from (x0, y0, z0) in steps (dx, dy, dz), metres) or
+// spherical (near = 1: r, phi, theta, degrees); blank counts mean 1.  With
+// one frequency the request runs at once.
+void Context::ne_nh_card(int in_nfeh, int near, int nx, int ny, int nz, double x0, double y0, double z0,
+                         double dx, double dy, double dz) {
+  nfeh = in_nfeh;
+  m_near = near;
+  nrx = nx == 0 ? 1 : nx;
+  nry = ny == 0 ? 1 : ny;
+  nrz = nz == 0 ? 1 : nz;
+  xnr = x0;
+  ynr = y0;
+  znr = z0;
+  dxnr = dx;
+  dynr = dy;
+  dznr = dz;
+  iflow = 8;
+  if (nfrq == 1) simulate(false);
+}
+
+// nfpat, src/nec_context.cpp:5068-5186: the points in the reference's order
+// (z outer, then y, then x), their fields from one device call.
+void Context::nfpat() {
+  NearFieldPattern p;
+  p.freq_hz = freq_mhz * 1.0e6;
+  p.nfeh = nfeh;
+  std::vector<double> pts;
+  double znrt = znr - dznr, cth = 0., sth = 0., cph = 0., sph = 0.;
+  for (int i = 0; i < nrz; i++) {
+    znrt += dznr;
+    if (m_near != 0) {
+      cth = std::cos(degrees_to_rad(znrt));
+      sth = std::sin(degrees_to_rad(znrt));
+    }
+    double ynrt = ynr - dynr;
+    for (int j = 0; j < nry; j++) {
+      ynrt += dynr;
+      if (m_near != 0) {
+        cph = std::cos(degrees_to_rad(ynrt));
+        sph = std::sin(degrees_to_rad(ynrt));
+      }
+      double xnrt = xnr - dxnr;
+      for (int k = 0; k < nrx; k++) {
+        xnrt += dxnr;
+        double xob, yob, zob;
+        if (m_near != 0) {
+          xob = xnrt * sth * cph;
+          yob = xnrt * sth * sph;
+          zob = xnrt * cth;
+        } else {
+          xob = xnrt;
+          yob = ynrt;
+          zob = znrt;
+        }
+        p.x.push_back(xob);
+        p.y.push_back(yob);
+        p.z.push_back(zob);
+        pts.push_back(xob / wavelength_);
+        pts.push_back(yob / wavelength_);
+        pts.push_back(zob / wavelength_);
+      }
+    }
+  }
+  const int np = (int)p.x.size();
+  std::vector<cd> f(3 * (size_t)np);
+  necgpu_engine* e = engine();
+  check(e, necgpu_near_field(e, nfeh == 1 ? 1 : 0, np, pts.data(), reinterpret_cast<double*>(f.data())));
+  for (int i = 0; i < np; i++) {
+    p.fx.push_back(f[3 * i]);
+    p.fy.push_back(f[3 * i + 1]);
+    p.fz.push_back(f[3 * i + 2]);
+  }
+  near_fields.push_back(std::move(p));
+}
+
 // calculate_network_data, src/nec_context.cpp:1210-1243: a transmission line
 // given with length <= 0 takes the straight distance between its two port
 // segments (metres, kept for later frequencies).  Done once per excitation
@@ -526,7 +603,12 @@ int Context::excitation_loop(int state_in, int mhz) {
       if (ret != PHASE_DONE) return ret;
     }
     if (state_in < NEAR) state_ = NEAR;
-    // near fields (NE/NH) are not part of the hot path: m_near stays -1
+    // near fields, excitation_compute_near_field (1741-1758)
+    if (state_in != FAR && m_near != -1) {
+      if (nrx * nry * nrz != 0) nfpat();
+      if (mhz == nfrq) m_near = -1;
+      if (nfrq == 1) return CARD_CONT;
+    }
     far_field();
     if (ex_type == 0 || ex_type == 4 || ex_type == 5) {
       if (mhz == nfrq) ifar = -1;

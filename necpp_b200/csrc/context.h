@@ -32,6 +32,15 @@ struct StructureCurrents {
   std::vector<cd> current;  // amperes (current_vector * wavelength)
 };
 
+// nec_near_field_pattern (src/nec_results.h:564-655): points in metres,
+// fields in V/m (electric) or A/m (magnetic)
+struct NearFieldPattern {
+  double freq_hz = 0;
+  int nfeh = 0;  // 0 electric, 1 magnetic
+  std::vector<double> x, y, z;
+  std::vector<cd> fx, fy, fz;
+};
+
 struct RadiationPattern {
   double freq_hz = 0;
   int nth = 0, nph = 0;
@@ -71,6 +80,8 @@ class Context {
   void ld_card(int type, int tag, int tag_from, int tag_to, double zr, double zi, double zc);
   void nt_card(int tag1, int seg1, int tag2, int seg2, double y11r, double y11i, double y12r, double y12i,
                double y22r, double y22i);
+  void ne_nh_card(int nfeh, int near, int nx, int ny, int nz, double x0, double y0, double z0, double dx,
+                  double dy, double dz);
   void tl_card(int tag1, int seg1, int tag2, int seg2, double z0, double length, double y1r, double y1i,
                double y2r, double y2i);
   int network_count() const { return (int)ntyp.size(); }
@@ -86,6 +97,7 @@ class Context {
   // results
   std::vector<AntennaInput> inputs;
   std::vector<RadiationPattern> patterns;
+  std::vector<NearFieldPattern> near_fields;
   std::vector<StructureCurrents> currents;
   double last_refine_residual = 0;
   int last_refine_iters = 0;
@@ -175,6 +187,9 @@ class Context {
   int iptflg = -2, iptag = 0, iptagf = 0, iptagt = 0;
   int iptflq = -1, iptaq = 0, iptaqf = 0, iptaqt = 0;
   int m_near = -1;
+  int nfeh = 0, nrx = 0, nry = 0, nrz = 0;
+  double xnr = 0, ynr = 0, znr = 0, dxnr = 0, dynr = 0, dznr = 0;
+  void nfpat();
   double input_power = 0, network_power_loss = 0, structure_power_loss = 0;
 
   // ground

@@ -25,6 +25,7 @@
 #include "solve.cuh"
 #include "batch.cuh"
 #include "somm.cuh"
+#include "nearfield.cuh"
 
 using namespace necb;
 
@@ -394,16 +395,72 @@ int launch_fill_t(necgpu_engine* e, const FillArgs& a) {
   return 0;
 }
 
-// Near-ground pairs (Sommerfeld ground, within the table limit of their
-// image) in the reference's order.  Every source column is first integrated
-// from a fresh interpolation cache, one thread per column.  A column's
-// result depends on the cache it starts from only when its first table
-// point falls below the cached patch's grid and the cached cell passes the
-// reuse test; a host scan over the columns in order finds those whose true
-// starting cache (the one the previous column leaves) differs from the one
-// used, and only they are integrated again from it.  The scan repeats until
-// every column is consistent; after a bounded number of rounds the rest is
-// walked by one thread in order.
+// Sommerfeld ground: evaluations that read the tables through the
+// interpolation cache, in the reference's order over `nunits` units (source
+// columns of the fill, or field points).  Every unit is first evaluated from
+// a fresh cache, one thread per unit.  A unit's result depends on the cache
+// it starts from only when its first table point falls below the cached
+// patch's grid and the cached cell passes the reuse test; a host scan over
+// the units in order finds those whose true starting cache (the one the
+// previous unit leaves, the first unit starting from the cache the engine
+// holds) differs from the one used, and only they are evaluated again from
+// it.  The scan repeats until every unit is consistent; after a bounded
+// number of rounds the rest is walked by one thread in order.  The cache
+// left at the end is kept, with its coefficients, for the next evaluation.
+// launch(entry, units, count, chain) runs the kernel; d_rec holds one
+// NearRecord per unit.
+template <typename Launch>
+int resolve_cache_order(necgpu_engine* e, int64_t nunits, NearRecord* d_rec, Launch launch) {
+  std::vector<InterpKey> entry((size_t)nunits, InterpKey{kInterpFresh, 0, 0, 0});
+  std::vector<int> units((size_t)nunits);
+  std::iota(units.begin(), units.end(), 0);
+  std::vector<NearRecord> rec((size_t)nunits);
+  if (!e->d_interp_carry) TRY(dalloc(e, e->d_interp_carry, 1));
+  TRY(launch(entry, units, (int)nunits, 0));
+  auto equal = [](InterpKey p, InterpKey q) {
+    if (p.igrs == kInterpFresh || q.igrs == kInterpFresh) return p.igrs == q.igrs;
+    return p.igrs == q.igrs && p.ix == q.ix && p.iy == q.iy && p.carry == q.carry;
+  };
+  const int kMaxRounds = 8;
+  for (int round = 0;; round++) {
+    CUDA_TRY(cudaMemcpyAsync(rec.data(), d_rec, (size_t)nunits * sizeof(NearRecord), cudaMemcpyDeviceToHost,
+                             e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    InterpKey t = e->interp_key;
+    int ndirty = 0, first_dirty = -1;
+    for (int64_t j = 0; j < nunits; j++) {
+      const NearRecord& r = rec[j];
+      if (!r.has_near) continue;
+      const InterpKey need = interp_reuses(t, r.x1, r.y1) ? t : InterpKey{kInterpFresh, 0, 0, 0};
+      if (!equal(need, r.used)) {
+        if (first_dirty < 0) first_dirty = (int)j;
+        entry[j] = need;
+        units[ndirty++] = (int)j;
+      }
+      t = r.exit;
+    }
+    e->stats.near_passes = round + 1;
+    if (ndirty == 0) {
+      if (t.igrs != kInterpFresh && !t.carry)
+        KLAUNCH(NECGPU_K_FILL, 0.0, interp_store_kernel<<<1, 1, 0, e->stream>>>(t, e->d_somm, e->d_interp_carry));
+      if (t.igrs != kInterpFresh) t.carry = 1;
+      e->interp_key = t;
+      return 0;
+    }
+    if (round > kMaxRounds) return fail(e, NECGPU_ERR_CUDA, "near-ground evaluation order did not settle");
+    if (round + 1 < kMaxRounds) {
+      TRY(launch(entry, units, ndirty, 0));
+      continue;
+    }
+    // walk every unit from the first inconsistent one in order
+    int m = 0;
+    for (int64_t j = first_dirty; j < nunits; j++) units[m++] = (int)j;
+    TRY(launch(entry, units, m, 1));
+  }
+}
+
+// Near-ground pairs of the fill (pairs within the table limit of their
+// image), one unit per source column in the reference's order (cmset).
 template <bool X>
 int run_near_ground(necgpu_engine* e, const FillArgs& a) {
   const int64_t n = e->n;
@@ -418,11 +475,8 @@ int run_near_ground(necgpu_engine* e, const FillArgs& a) {
     TRY(dalloc(e, e->d_near_rec, (size_t)n));
     e->near_cap = n;
   }
-  std::vector<InterpKey> entry((size_t)n, InterpKey{kInterpFresh, 0, 0, 0});
-  std::vector<int> cols((size_t)n);
-  std::iota(cols.begin(), cols.end(), 0);
-  std::vector<NearRecord> rec((size_t)n);
-  auto launch = [&](int ncols, int chain) -> int {
+  auto launch = [&](const std::vector<InterpKey>& entry, const std::vector<int>& cols, int ncols,
+                    int chain) -> int {
     TRY(upload(e, e->d_near_entry, entry.data(), (size_t)n));
     TRY(upload(e, e->d_near_cols, cols.data(), (size_t)ncols));
     const unsigned blocks = chain ? 1u : (unsigned)((ncols + 63) / 64);
@@ -432,49 +486,7 @@ int run_near_ground(necgpu_engine* e, const FillArgs& a) {
                 e->d_near_g, chain));
     return 0;
   };
-  TRY(launch((int)n, 0));
-  auto equal = [](InterpKey p, InterpKey q) {
-    if (p.igrs == kInterpFresh || q.igrs == kInterpFresh) return p.igrs == q.igrs;
-    return p.igrs == q.igrs && p.ix == q.ix && p.iy == q.iy && p.carry == q.carry;
-  };
-  if (!e->d_interp_carry) TRY(dalloc(e, e->d_interp_carry, 1));
-  const int kMaxRounds = 8;
-  for (int round = 0;; round++) {
-    CUDA_TRY(cudaMemcpyAsync(rec.data(), e->d_near_rec, (size_t)n * sizeof(NearRecord), cudaMemcpyDeviceToHost,
-                             e->stream));
-    CUDA_TRY(cudaStreamSynchronize(e->stream));
-    InterpKey t = e->interp_key;
-    int ndirty = 0, first_dirty = -1;
-    for (int64_t j = 0; j < n; j++) {
-      const NearRecord& r = rec[j];
-      if (!r.has_near) continue;
-      const InterpKey need = interp_reuses(t, r.x1, r.y1) ? t : InterpKey{kInterpFresh, 0, 0, 0};
-      if (!equal(need, r.used)) {
-        if (first_dirty < 0) first_dirty = (int)j;
-        entry[j] = need;
-        cols[ndirty++] = (int)j;
-      }
-      t = r.exit;
-    }
-    e->stats.near_passes = round + 1;
-    if (ndirty == 0) {
-      // keep the cache this fill leaves, with this fill's coefficients
-      if (t.igrs != kInterpFresh && !t.carry)
-        KLAUNCH(NECGPU_K_FILL, 0.0, interp_store_kernel<<<1, 1, 0, e->stream>>>(t, e->d_somm, e->d_interp_carry));
-      if (t.igrs != kInterpFresh) t.carry = 1;
-      e->interp_key = t;
-      return 0;
-    }
-    if (round > kMaxRounds) return fail(e, NECGPU_ERR_CUDA, "fill: near-ground column order did not settle");
-    if (round + 1 < kMaxRounds) {
-      TRY(launch(ndirty, 0));
-      continue;
-    }
-    // walk every column from the first inconsistent one in order
-    int m = 0;
-    for (int64_t j = first_dirty; j < n; j++) cols[m++] = (int)j;
-    TRY(launch(m, 1));
-  }
+  return resolve_cache_order(e, n, e->d_near_rec, launch);
 }
 
 int run_fill(necgpu_engine* e, bool want64, bool want32) {
@@ -530,6 +542,13 @@ int run_fill(necgpu_engine* e, bool want64, bool want32) {
             load_kernel<<<(unsigned)((n + 255) / 256), 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef,
                                                                             e->d_ccoef + 2 * e->nc, e->d_zload,
                                                                             e->Z64, e->ld));
+  return 0;
+}
+
+template <int G, bool X>
+int launch_near_e(necgpu_engine* e, const NearFieldArgs& a) {
+  KLAUNCH(NECGPU_K_PATTERN, (double)a.npts * (double)e->n,
+          near_e_kernel<G, X><<<(unsigned)((a.npts + kNearWarps - 1) / kNearWarps), 32 * kNearWarps, 0, e->stream>>>(a));
   return 0;
 }
 
@@ -1780,6 +1799,111 @@ int necgpu_set_sommerfeld(necgpu_engine* e, double eps_re, double eps_im) {
   e->somm_ready = true;
   e->filled = false;
   return NECGPU_OK;
+}
+
+// nefld / nhfld over a list of points (nfpat, src/nec_context.cpp:5068-5186).
+int necgpu_near_field(necgpu_engine* e, int magnetic, int npts, const double* pts, double* fields) {
+  if (!e || npts < 0 || (npts > 0 && (!pts || !fields))) return e ? fail(e, NECGPU_ERR_ARG, "near_field: bad argument") : NECGPU_ERR_ARG;
+  if (!e->have_solution) return fail(e, NECGPU_ERR_ARG, "near_field: no solution held (solve first)");
+  if (npts == 0) return NECGPU_OK;
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int64_t n = e->n;
+  double* d_pts = nullptr;
+  double2* d_out = nullptr;
+  double2* d_near = nullptr;
+  double* d_ax = nullptr;
+  NearRecord* d_rec = nullptr;
+  InterpKey* d_entry = nullptr;
+  int* d_units = nullptr;
+  auto cleanup = [&]() {
+    dfree(e, d_pts);
+    dfree(e, d_out);
+    dfree(e, d_near);
+    dfree(e, d_ax);
+    dfree(e, d_rec);
+    dfree(e, d_entry);
+    dfree(e, d_units);
+  };
+  int rc = 0;
+  do {
+    if ((rc = upload(e, d_pts, pts, 3 * (size_t)npts))) break;
+    if ((rc = dalloc(e, d_out, 3 * (size_t)npts))) break;
+    CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
+    NearFieldArgs a{};
+    a.n = n;
+    a.x = e->d_seg;
+    a.y = e->d_seg + n;
+    a.z = e->d_seg + 2 * n;
+    a.s = e->d_seg + 3 * n;
+    a.b = e->d_seg + 4 * n;
+    a.cab = e->d_seg + 5 * n;
+    a.sab = e->d_seg + 6 * n;
+    a.salp = e->d_seg + 7 * n;
+    a.ind1 = e->d_ind;
+    a.ind2 = e->d_ind + n;
+    a.P = e->P;
+    a.P.near_g = nullptr;
+    a.ground = e->ground;
+    a.abc = e->d_abc;
+    a.npts = npts;
+    a.pts = d_pts;
+    a.out = d_out;
+    a.near = nullptr;
+    a.status = e->d_status;
+    const unsigned blocks = (unsigned)((npts + kNearWarps - 1) / kNearWarps);
+    const bool x = e->use_exk != 0;
+    if (magnetic) {
+      KLAUNCH(NECGPU_K_PATTERN, (double)npts * (double)n,
+              near_h_kernel<<<blocks, 32 * kNearWarps, 0, e->stream>>>(a));
+    } else {
+      if (e->ground == kGroundSommerfeld && e->somm_ready) {
+        if ((rc = dalloc(e, d_near, 3 * (size_t)npts))) break;
+        if ((rc = dalloc(e, d_ax, (size_t)npts))) break;
+        if ((rc = dalloc(e, d_rec, (size_t)npts))) break;
+        KLAUNCH(NECGPU_K_PATTERN, 0.0, near_radius_kernel<<<blocks, 32 * kNearWarps, 0, e->stream>>>(a, d_ax));
+        auto launch = [&](const std::vector<InterpKey>& entry, const std::vector<int>& units, int count,
+                          int chain) -> int {
+          TRY(upload(e, d_entry, entry.data(), (size_t)npts));
+          TRY(upload(e, d_units, units.data(), (size_t)count));
+          const unsigned nb = chain ? 1u : (unsigned)((count + 63) / 64);
+          if (x)
+            KLAUNCH(NECGPU_K_PATTERN, 0.0,
+                    near_field_chain_kernel<true><<<nb, chain ? 1 : 64, 0, e->stream>>>(
+                        a, d_ax, e->d_somm, d_units, count, d_entry, e->d_interp_carry, d_rec, d_near, chain));
+          else
+            KLAUNCH(NECGPU_K_PATTERN, 0.0,
+                    near_field_chain_kernel<false><<<nb, chain ? 1 : 64, 0, e->stream>>>(
+                        a, d_ax, e->d_somm, d_units, count, d_entry, e->d_interp_carry, d_rec, d_near, chain));
+          return 0;
+        };
+        if ((rc = resolve_cache_order(e, npts, d_rec, launch))) break;
+        a.near = d_near;
+      }
+      switch (e->ground) {
+        case kGroundNone: rc = x ? launch_near_e<kGroundNone, true>(e, a) : launch_near_e<kGroundNone, false>(e, a); break;
+        case kGroundPerfect:
+          rc = x ? launch_near_e<kGroundPerfect, true>(e, a) : launch_near_e<kGroundPerfect, false>(e, a);
+          break;
+        case kGroundReflection:
+          rc = x ? launch_near_e<kGroundReflection, true>(e, a) : launch_near_e<kGroundReflection, false>(e, a);
+          break;
+        default:
+          rc = x ? launch_near_e<kGroundSommerfeld, true>(e, a) : launch_near_e<kGroundSommerfeld, false>(e, a);
+      }
+      if (rc) break;
+    }
+    CUDA_TRY(cudaMemcpyAsync(fields, d_out, 3 * (size_t)npts * sizeof(double2), cudaMemcpyDeviceToHost, e->stream));
+    int st = 0;
+    if ((rc = sync_status(e, &st))) break;
+    e->stats.d2h_bytes += 3 * (size_t)npts * sizeof(double2);
+    if (st & kStatSommerfeldTab)
+      rc = fail(e, NECGPU_ERR_UNSUPPORTED, "near_field: a point lies within 0.95 wavelength of a segment's ground "
+                                           "image and no Sommerfeld tables are set");
+    else if (st & kStatIterCap)
+      rc = fail(e, NECGPU_ERR_NONFINITE, "near_field: quadrature did not terminate (non-finite point?)");
+  } while (false);
+  cleanup();
+  return rc;
 }
 
 int necgpu_copy_sommerfeld(necgpu_engine* e, double* tables) {

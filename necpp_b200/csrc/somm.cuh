@@ -909,13 +909,13 @@ __device__ void rom2_table(const NearSrc& N, double a, double b, cplx sum[9], do
   *status |= kStatIterCap;
 }
 
-// One near-ground pair: direct and image fields plus the table field
-// integrated over the source (efld, 2993-3001), projected (cmww).
+// Fields of source J at a point within the table limit of J's image:
+// direct and image fields plus the table field integrated over the source
+// (efld, 2993-3001).
 template <bool EXK>
-__device__ void near_pair(const SrcSeg& J, double xi, double yi, double zi, double ai, double cabi, double sabi,
-                          double salpi, bool ij, const FieldParams& P, int64_t nseg, InterpCache& S,
-                          const cplx* tab, double2* first, cplx out[3], int* status) {
-  cplx ex[9];
+__device__ void near_efld9(const SrcSeg& J, double xi, double yi, double zi, double ai, bool ij,
+                           const FieldParams& P, int64_t nseg, InterpCache& S, const cplx* tab, double2* first,
+                           cplx ex[9], int* status) {
   pair_fields9<kGroundSommerfeld, EXK>(J, xi, yi, zi, ai, ij, P, ex, status);
   double dmin = cnorm(ex[0]) + cnorm(ex[1]) + cnorm(ex[2]);
   dmin = 0.01 * sqrt(dmin);
@@ -932,6 +932,15 @@ __device__ void near_pair(const SrcSeg& J, double xi, double yi, double zi, doub
   rom2_table(N, -shaf, shaf, e, dmin, nseg, S, tab, first, status);
 #pragma unroll
   for (int k = 0; k < 9; k++) ex[k] = ex[k] + e[k];
+}
+
+// One near-ground pair of the fill, projected (cmww 2617-2619).
+template <bool EXK>
+__device__ void near_pair(const SrcSeg& J, double xi, double yi, double zi, double ai, double cabi, double sabi,
+                          double salpi, bool ij, const FieldParams& P, int64_t nseg, InterpCache& S,
+                          const cplx* tab, double2* first, cplx out[3], int* status) {
+  cplx ex[9];
+  near_efld9<EXK>(J, xi, yi, zi, ai, ij, P, nseg, S, tab, first, ex, status);
   project_fields(ex, cabi, sabi, salpi, &out[0], &out[1], &out[2]);
 }
 

@@ -592,14 +592,14 @@ static void rom2(const mo_structure* S, const sgeom_t* G, double a, double b, cx
 }
 
 /* efld, 2845-3045 + projection of cmww, 2617-2619 */
-static void pair(const mo_structure* S, const src_t* J, int64_t i, int ij, cx* etk, cx* ets, cx* etc,
-                 int* st) {
-  double xi = S->x[i], yi = S->y[i], zi = S->z[i], ai = S->b[i];
+/* efld, 2845-3045: the nine field components of source J at (xi, yi, zi)
+   with observer radius ai. */
+static void efld_point(const mo_structure* S, const src_t* J, double xi, double yi, double zi, double ai, int ij,
+                       cx ex[9], int* st) {
   cx e[9];
   double xij = xi - J->x, yij = yi - J->y;
   efld_compute(S, J, xij, yij, ai, J->salp, zi - J->z, ij, e, st);
-  cx ex[9];
-  memcpy(ex, e, sizeof(ex));
+  memcpy(ex, e, sizeof(e));
   const cx zrati = CMPLX(S->zrati_re, S->zrati_im), frati = CMPLX(S->frati_re, S->frati_im);
   if (S->ground != 0) {
     double zij = zi + J->z;
@@ -738,6 +738,12 @@ static void pair(const mo_structure* S, const src_t* J, int64_t i, int ij, cx* e
     }
     for (int k = 0; k < 9; k++) ex[k] = ex[k] + e[k];
   }
+}
+
+static void pair(const mo_structure* S, const src_t* J, int64_t i, int ij, cx* etk, cx* ets, cx* etc,
+                 int* st) {
+  cx ex[9];
+  efld_point(S, J, S->x[i], S->y[i], S->z[i], S->b[i], ij, ex, st);
   double cabi = S->cab[i], sabi = S->sab[i], salpi = S->salp[i];
   *etk = rmul(cabi, ex[0]) + rmul(sabi, ex[1]) + rmul(salpi, ex[2]);
   *ets = rmul(cabi, ex[3]) + rmul(sabi, ex[4]) + rmul(salpi, ex[5]);
@@ -935,4 +941,286 @@ void mo_ffld(const mo_structure* S, const double* abc, double thet, double phi, 
   eth_[1] = cimag(eth);
   eph_[0] = creal(eph);
   eph_[1] = cimag(eph);
+}
+
+/* ---- near fields (nefld 4304-4490, nhfld 5189-5265) ---- */
+
+static src_t source_of(const mo_structure* S, int64_t i) {
+  src_t J = {S->x[i], S->y[i], S->z[i], S->s[i], S->b[i], S->cab[i], S->sab[i], S->salp[i],
+             S->ind1 ? S->ind1[i] : 0, S->ind2 ? S->ind2[i] : 0};
+  return J;
+}
+
+/* radius of the segment whose volume holds the point, else 0 (4316-4334) */
+static double point_radius(const mo_structure* S, double xob, double yob, double zob) {
+  for (int64_t i = 0; i < S->n; i++) {
+    double xj = xob - S->x[i], yj = yob - S->y[i], zj = zob - S->z[i];
+    double zp = S->cab[i] * xj + S->sab[i] * yj + S->salp[i] * zj;
+    if (fabs(zp) > 0.5001 * S->s[i]) continue;
+    zp = xj * xj + yj * yj + zj * zj - zp * zp;
+    xj = S->b[i];
+    if (zp > 0.9 * xj * xj) continue;
+    return xj;
+  }
+  return 0.0;
+}
+
+static cx seg_coef(const double* abc, int64_t n, int64_t i, int k) {
+  return CMPLX(abc[2 * k * n + i], abc[(2 * k + 1) * n + i]);
+}
+
+void mo_nefld(const mo_structure* S, const double* abc, double xob, double yob, double zob, double* out) {
+  const int64_t n = S->n;
+  cx f[3] = {0, 0, 0};
+  const double ax = point_radius(S, xob, yob, zob);
+  int st = 0;
+  for (int64_t i = 0; i < n; i++) {
+    src_t J = source_of(S, i);
+    cx e[9];
+    efld_point(S, &J, xob, yob, zob, ax, 1, e, &st);
+    cx acx = seg_coef(abc, n, i, 0), bcx = seg_coef(abc, n, i, 1), ccx = seg_coef(abc, n, i, 2);
+    f[0] += e[0] * acx + e[3] * bcx + e[6] * ccx;
+    f[1] += e[1] * acx + e[4] * bcx + e[7] * ccx;
+    f[2] += e[2] * acx + e[5] * bcx + e[8] * ccx;
+  }
+  for (int k = 0; k < 3; k++) {
+    out[2 * k] = creal(f[k]);
+    out[2 * k + 1] = cimag(f[k]);
+  }
+}
+
+typedef struct {
+  double zpka, rhks;
+} ghstate;
+
+/* gh, 3582-3600 */
+static void gh(const ghstate* g, double zk, double* hr, double* hi) {
+  double rs = zk - g->zpka;
+  rs = g->rhks + rs * rs;
+  double r = sqrt(rs), ckr = cos(r), skr = sin(r), rr2 = 1. / rs, rr3 = rr2 / r;
+  *hr = skr * rr2 + ckr * rr3;
+  *hi = ckr * rr2 - skr * rr3;
+}
+
+/* hfk, 3681-3822: H field of a uniform filament by Romberg integration */
+static void hfk(double el1, double el2, double rhk, double zpkx, double* sgr, double* sgi) {
+  const int nx = 1, nma = 65536, nts = 4;
+  const double rx = 1.0e-4;
+  ghstate G = {zpkx, rhk * rhk};
+  double z = el1, ze = el2, s = ze - z, ep = s / (10. * nma), zend = ze - ep, dz = 0., dzot = 0., zp;
+  double g1r, g1i, g2r, g2i, g3r, g3i, g4r, g4i, g5r, g5i, te1r, te1i, te2r, te2i;
+  *sgr = 0.0;
+  *sgi = 0.0;
+  int ns = nx, nt = 0, flag = 1;
+  gh(&G, z, &g1r, &g1i);
+  for (;;) {
+    if (flag) {
+      dz = s / ns;
+      zp = z + dz;
+      if (zp > ze) {
+        dz = ze - z;
+        if (fabs(dz) <= ep) {
+          *sgr = *sgr * rhk * .5;
+          *sgi = *sgi * rhk * .5;
+          return;
+        }
+      }
+      dzot = dz * .5;
+      zp = z + dzot;
+      gh(&G, zp, &g3r, &g3i);
+      zp = z + dz;
+      gh(&G, zp, &g5r, &g5i);
+    }
+    double t00r = (g1r + g5r) * dzot, t00i = (g1i + g5i) * dzot;
+    double t01r = (t00r + dz * g3r) * 0.5, t01i = (t00i + dz * g3i) * 0.5;
+    double t10r = (4.0 * t01r - t00r) / 3.0, t10i = (4.0 * t01i - t00i) / 3.0;
+    test2(t01r, t10r, &te1r, t01i, t10i, &te1i);
+    if ((te1i <= rx) && (te1r <= rx)) {
+      *sgr = *sgr + t10r;
+      *sgi = *sgi + t10i;
+      nt += 2;
+      z += dz;
+      if (z >= zend) {
+        *sgr = *sgr * rhk * .5;
+        *sgi = *sgi * rhk * .5;
+        return;
+      }
+      g1r = g5r;
+      g1i = g5i;
+      if (nt >= nts && ns > nx) {
+        ns = ns / 2;
+        nt = 1;
+      }
+      flag = 1;
+      continue;
+    }
+    zp = z + dz * 0.25;
+    gh(&G, zp, &g2r, &g2i);
+    zp = z + dz * 0.75;
+    gh(&G, zp, &g4r, &g4i);
+    double t02r = (t01r + dzot * (g2r + g4r)) * 0.5, t02i = (t01i + dzot * (g2i + g4i)) * 0.5;
+    double t11r = (4.0 * t02r - t01r) / 3.0, t11i = (4.0 * t02i - t01i) / 3.0;
+    double t20r = (16.0 * t11r - t10r) / 15.0, t20i = (16.0 * t11i - t10i) / 15.0;
+    test2(t11r, t20r, &te2r, t11i, t20i, &te2i);
+    if ((te2i > rx) || (te2r > rx)) {
+      nt = 0;
+      if (ns < nma) {
+        ns = ns * 2;
+        dz = s / ns;
+        dzot = dz * 0.5;
+        g5r = g3r;
+        g5i = g3i;
+        g3r = g2r;
+        g3i = g2i;
+        flag = 0;
+        continue;
+      }
+    }
+    *sgr = *sgr + t20r;
+    *sgi = *sgi + t20i;
+    nt++;
+    z += dz;
+    if (z >= zend) {
+      *sgr = *sgr * rhk * .5;
+      *sgi = *sgi * rhk * .5;
+      return;
+    }
+    g1r = g5r;
+    g1i = g5i;
+    if (nt >= nts && ns > nx) {
+      ns = ns / 2;
+      nt = 1;
+    }
+    flag = 1;
+  }
+}
+
+/* hsflx, 4059-4133: H of the constant, sine and cosine currents of a segment */
+static void hsflx(double s, double rh, double zpx, cx* hpk, cx* hps, cx* hpc) {
+  const double pi8 = PI * 8.0;
+  const cx fjk = -CMPLX(0.0, TWO_PI);
+  if (rh >= 1.0e-10) {
+    double zp, hss;
+    if (zpx >= 0.0) {
+      zp = zpx;
+      hss = 1.;
+    } else {
+      zp = -zpx;
+      hss = -1.;
+    }
+    double dh = 0.5 * s, z1 = zp + dh, z2a = zp - dh, rhz;
+    if (z2a >= 1.0e-7)
+      rhz = rh / z2a;
+    else
+      rhz = 1.;
+    double dk = TWO_PI * dh, cdk = cos(dk), sdk = sin(dk), hkr, hki;
+    hfk(-dk, dk, rh * TWO_PI, zp * TWO_PI, &hkr, &hki);
+    *hpk = CMPLX(hkr, hki);
+    if (rhz >= 1.0e-3) {
+      double rh2 = rh * rh, r1 = sqrt(rh2 + z1 * z1), r2 = sqrt(rh2 + z2a * z2a);
+      cx ekr1 = cexp(fjk * r1), ekr2 = cexp(fjk * r2);
+      cx t1 = z1 * ekr1 / r1, t2 = z2a * ekr2 / r2;
+      *hps = (cdk * (ekr2 - ekr1) - I * sdk * (t2 + t1)) * hss;
+      *hpc = -sdk * (ekr2 + ekr1) - I * cdk * (t2 - t1);
+      cx cons = -I / (2.0 * TWO_PI * rh);
+      *hps = cons * *hps;
+      *hpc = cons * *hpc;
+      return;
+    }
+    cx ekr1 = CMPLX(cdk, sdk) / (z2a * z2a), ekr2 = CMPLX(cdk, -sdk) / (z1 * z1);
+    double t1 = TWO_PI * (1.0 / z1 - 1.0 / z2a);
+    cx t2 = cexp(fjk * zp) * rh / pi8;
+    *hps = t2 * (t1 + (ekr1 + ekr2) * sdk) * hss;
+    *hpc = t2 * (-I * t1 + (ekr1 - ekr2) * cdk);
+    return;
+  }
+  *hps = 0;
+  *hpc = 0;
+  *hpk = 0;
+}
+
+/* hsfld, 3927-4056: H of segment J at (xi, yi, zi) with its image */
+static void hsfld(const mo_structure* S, const src_t* J, double xi, double yi, double zi, double ai, cx h[9]) {
+  const double xij = xi - J->x, yij = yi - J->y;
+  const int ksymp = (S->ground != 0) ? 2 : 1;
+  double rfl = -1.;
+  for (int k = 0; k < 9; k++) h[k] = 0;
+  for (int gl = 0; gl < ksymp; gl++) {
+    rfl = -rfl;
+    double salpr = J->salp * rfl, zij = zi - rfl * J->z;
+    double zp = xij * J->cab + yij * J->sab + zij * salpr;
+    double rhox = xij - J->cab * zp, rhoy = yij - J->sab * zp, rhoz = zij - salpr * zp;
+    double rh = sqrt(rhox * rhox + rhoy * rhoy + rhoz * rhoz + ai * ai);
+    if (rh <= 1.0e-10) {
+      for (int k = 0; k < 9; k++) h[k] = 0;
+      continue;
+    }
+    rhox = rhox / rh;
+    rhoy = rhoy / rh;
+    rhoz = rhoz / rh;
+    double phx = J->sab * rhoz - salpr * rhoy, phy = salpr * rhox - J->cab * rhoz, phz = J->cab * rhoy - J->sab * rhox;
+    cx hp[3];
+    hsflx(J->s, rh, zp, &hp[0], &hp[1], &hp[2]);
+    if (gl == 1) {
+      if (S->ground != 1) {
+        cx zratx = CMPLX(S->zrati_re, S->zrati_im), rrv, rrh;
+        double rmag = sqrt(zp * zp + rh * rh), xymag = sqrt(xij * xij + yij * yij), px, py, cth;
+        if (xymag <= 1.0e-6) {
+          px = 0.;
+          py = 0.;
+          cth = 1.;
+          rrv = 1.0;
+        } else {
+          px = -yij / xymag;
+          py = xij / xymag;
+          cth = zij / rmag;
+          rrv = csqrt(1. - zratx * zratx * (1. - cth * cth));
+        }
+        rrh = zratx * cth;
+        rrh = -(rrh - rrv) / (rrh + rrv);
+        rrv = zratx * rrv;
+        rrv = (cth - rrv) / (cth + rrv);
+        cx qy = (phx * px + phy * py) * (rrv - rrh);
+        cx qx = qy * px + phx * rrh;
+        qy = qy * py + phy * rrh;
+        cx qz = phz * rrh;
+        for (int k = 0; k < 3; k++) {
+          h[3 * k] = h[3 * k] - hp[k] * qx;
+          h[3 * k + 1] = h[3 * k + 1] - hp[k] * qy;
+          h[3 * k + 2] = h[3 * k + 2] - hp[k] * qz;
+        }
+        continue;
+      }
+      for (int k = 0; k < 3; k++) {
+        h[3 * k] = h[3 * k] - hp[k] * phx;
+        h[3 * k + 1] = h[3 * k + 1] - hp[k] * phy;
+        h[3 * k + 2] = h[3 * k + 2] - hp[k] * phz;
+      }
+      continue;
+    }
+    for (int k = 0; k < 3; k++) {
+      h[3 * k] = hp[k] * phx;
+      h[3 * k + 1] = hp[k] * phy;
+      h[3 * k + 2] = hp[k] * phz;
+    }
+  }
+}
+
+void mo_nhfld(const mo_structure* S, const double* abc, double xob, double yob, double zob, double* out) {
+  const int64_t n = S->n;
+  cx f[3] = {0, 0, 0};
+  const double ax = point_radius(S, xob, yob, zob);
+  for (int64_t i = 0; i < n; i++) {
+    src_t J = source_of(S, i);
+    cx h[9];
+    hsfld(S, &J, xob, yob, zob, ax, h);
+    cx acx = seg_coef(abc, n, i, 0), bcx = seg_coef(abc, n, i, 1), ccx = seg_coef(abc, n, i, 2);
+    f[0] += h[0] * acx + h[3] * bcx + h[6] * ccx;
+    f[1] += h[1] * acx + h[4] * bcx + h[7] * ccx;
+    f[2] += h[2] * acx + h[5] * bcx + h[8] * ccx;
+  }
+  for (int k = 0; k < 3; k++) {
+    out[2 * k] = creal(f[k]);
+    out[2 * k + 1] = cimag(f[k]);
+  }
 }

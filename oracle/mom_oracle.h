@@ -67,6 +67,10 @@ void mo_interp_init(mo_interp* s);
 /* The four interpolated functions (erv, ezv, erh, eph; complex) at
    R = x (wavelengths), theta = y (radians). */
 void mo_interpolate(mo_interp* s, const double* tables, double x, double y, int stateful, double* f);
+/* Near electric (nefld) and magnetic (nhfld) field at a point (wavelengths)
+   from current coefficients abc: out = 3 complex (x, y, z), interleaved. */
+void mo_nefld(const mo_structure* s, const double* abc, double x, double y, double z, double* out);
+void mo_nhfld(const mo_structure* s, const double* abc, double x, double y, double z, double* out);
 /* Far field at (thet, phi) radians: eth, eph (complex, interleaved). */
 void mo_ffld(const mo_structure* s, const double* abc, double thet, double phi, double* eth,
              double* eph);

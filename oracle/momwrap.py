@@ -47,6 +47,8 @@ class Oracle:
         L.mo_solve.argtypes = [C.c_int64, _dp, _ip, _dp]
         L.mo_coefficients.argtypes = [C.POINTER(MoStructure), _dp, _dp, _dp]
         L.mo_ffld.argtypes = [C.POINTER(MoStructure), _dp, C.c_double, C.c_double, _dp, _dp]
+        L.mo_nefld.argtypes = [C.POINTER(MoStructure), _dp, C.c_double, C.c_double, C.c_double, _dp]
+        L.mo_nhfld.argtypes = [C.POINTER(MoStructure), _dp, C.c_double, C.c_double, C.c_double, _dp]
         L.mo_sommerfeld.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp]
         L.mo_sommerfeld.restype = C.c_int
         L.mo_interp_size.restype = C.c_int64
@@ -134,6 +136,16 @@ class Oracle:
         self.L.mo_coefficients(C.byref(s), xx.view(np.float64).ctypes.data_as(_dp),
                                abc.ctypes.data_as(_dp), cur.ctypes.data_as(_dp))
         return abc, cur[0::2] + 1j * cur[1::2]
+
+    def near_field(self, st, abc, pts, magnetic=False):
+        """Near E (or H) at points (wavelengths, np x 3) in order: np x 3 complex."""
+        s = self.structure(st)
+        f = self.L.mo_nhfld if magnetic else self.L.mo_nefld
+        out = np.zeros((len(pts), 6))
+        a = np.ascontiguousarray(abc, dtype=np.float64)
+        for k, (x, y, z) in enumerate(pts):
+            f(C.byref(s), a.ctypes.data_as(_dp), float(x), float(y), float(z), out[k].ctypes.data_as(_dp))
+        return out[:, 0::2] + 1j * out[:, 1::2]
 
     def ffld(self, st, abc, thet, phi):
         s = self.structure(st)

@@ -32,6 +32,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 namespace {
 
@@ -194,6 +195,31 @@ void ref_somm_interpolate(nec_context* ctx, double x, double y, double* f) {
     f[2 * k] = v[k].real();
     f[2 * k + 1] = v[k].imag();
   }
+}
+
+/* Near-field pattern `index` (nfpat, src/nec_context.cpp:5068-5186): its
+   kind (0 electric, 1 magnetic) and point count; with non-null buffers the
+   points (metres, 3 per point) and fields (3 complex per point). */
+long ref_near_field(nec_context* ctx, long index, int* nfeh, double* xyz, double* f) {
+  nec_near_field_pattern* p = ctx->get_near_field_pattern(index);
+  if (!p) return -1;
+  std::vector<nec_float> x = p->get_x(), y = p->get_y(), z = p->get_z();
+  std::vector<nec_complex> fx = p->get_field_x(), fy = p->get_field_y(), fz = p->get_field_z();
+  if (nfeh) *nfeh = p->get_nfeh();
+  const long np = (long)x.size();
+  for (long i = 0; xyz && i < np; i++) {
+    xyz[3 * i] = x[i];
+    xyz[3 * i + 1] = y[i];
+    xyz[3 * i + 2] = z[i];
+  }
+  for (long i = 0; f && i < np; i++) {
+    const nec_complex v[3] = {fx[i], fy[i], fz[i]};
+    for (int k = 0; k < 3; k++) {
+      f[6 * i + 2 * k] = v[k].real();
+      f[6 * i + 2 * k + 1] = v[k].imag();
+    }
+  }
+  return np;
 }
 
 /* LU factors (column-major, in place) and the 1-based permutation left by the

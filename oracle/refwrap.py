@@ -72,6 +72,9 @@ class RefAPI:
         sig("ref_fill", _l, [_p, _dp])
         sig("ref_lu", None, [_p, _dp, _ip])
         sig("ref_somm_tables", None, [_p, _dp, _dp])
+        sig("ref_near_field", _l, [_p, _l, C.POINTER(C.c_int), _dp, _dp])
+        sig("nec_ne_card", _l, [_p, _i, _i, _i, _i] + [_d] * 6)
+        sig("nec_nh_card", _l, [_p, _i, _i, _i, _i] + [_d] * 6)
         sig("ref_somm_interp_reset", None, [_p])
         sig("ref_somm_interpolate", None, [_p, _d, _d, _dp])
         sig("ref_currents", None, [_p] + [_dp] * 7)
@@ -121,6 +124,21 @@ class RefAPI:
         f = np.zeros(8)
         self.ref_somm_interpolate(ctx, x, y, f.ctypes.data_as(_dp))
         return f[0::2] + 1j * f[1::2]
+
+    def near_fields(self, ctx):
+        """Every near-field pattern: list of (nfeh, points (m, np x 3),
+        fields (np x 3 complex))."""
+        out = []
+        k = 0
+        while True:
+            nfeh = C.c_int(0)
+            np_ = self.ref_near_field(ctx, k, C.byref(nfeh), None, None)
+            if np_ < 0:
+                return out
+            xyz, f = np.zeros(3 * np_), np.zeros(6 * np_)
+            self.ref_near_field(ctx, k, C.byref(nfeh), xyz.ctypes.data_as(_dp), f.ctypes.data_as(_dp))
+            out.append((nfeh.value, xyz.reshape(-1, 3), (f[0::2] + 1j * f[1::2]).reshape(-1, 3)))
+            k += 1
 
     def currents(self, ctx):
         n = self.ref_n_segments(ctx)

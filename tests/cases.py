@@ -168,8 +168,51 @@ def _near_ground(api, ctx):
     api.nec_gn_card(ctx, 2, 0, 10.0, 0.01, 0, 0, 0, 0)
     api.nec_fr_card(ctx, 0, 2, 150.0, 12.0)
     api.nec_ex_card(ctx, 0, 1, 11, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    # near field over the ground at both frequencies: its table reads move
+    # the interpolation cache the next fill starts from
+    api.nec_ne_card(ctx, 0, 3, 2, 2, -0.4, 0.1, 0.02, 0.4, 0.2, 0.15)
     api.nec_rp_card(ctx, 0, 10, 4, 1, 0, 0, 0, 0.0, 0.0, 10.0, 90.0, 0.0, 0.0)
     return 150.0
+
+
+def _dipole_fields(api, ctx):
+    """Near electric field on a rectangular grid through and around a
+    dipole (points inside a segment's volume included) and the magnetic
+    field on a spherical grid, free space."""
+    api.nec_wire(ctx, 1, 21, 0.0, 0.0, -0.5, 0.0, 0.0, 0.5, 1.0e-3, 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 0)
+    api.nec_fr_card(ctx, 0, 1, 150.0, 0.0)
+    api.nec_ex_card(ctx, 0, 1, 11, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_ne_card(ctx, 0, 4, 3, 5, 0.0, -0.0005, -0.6, 0.1, 0.0005, 0.3)
+    api.nec_nh_card(ctx, 1, 3, 4, 3, 0.8, 0.0, 10.0, 0.5, 30.0, 40.0)
+    api.nec_rp_card(ctx, 0, 10, 4, 1, 0, 0, 0, 0.0, 0.0, 20.0, 90.0, 0.0, 0.0)
+    return 150.0
+
+
+def _yagi_fields_ground(api, ctx, gn):
+    p = W.yagi_params(np.random.default_rng(17), n_elements=3, nseg=11)
+    half, xs, rad, segs = p
+    for e in range(len(half)):
+        api.nec_wire(ctx, e + 1, int(segs[e]), float(xs[e]), 0.0, 1.5 - float(half[e]), float(xs[e]), 0.0,
+                     1.5 + float(half[e]), float(rad[e]), 1.0, 1.0)
+    api.nec_geometry_complete(ctx, 1)
+    api.nec_gn_card(ctx, *gn)
+    api.nec_fr_card(ctx, 0, 1, 145.0, 0.0)
+    api.nec_ex_card(ctx, 0, 2, (int(segs[1]) + 1) // 2, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    api.nec_ne_card(ctx, 0, 3, 2, 4, -0.5, 0.3, 0.2, 0.6, 0.5, 0.7)
+    api.nec_nh_card(ctx, 0, 3, 2, 4, -0.5, 0.3, 0.2, 0.6, 0.5, 0.7)
+    api.nec_rp_card(ctx, 0, 10, 4, 1, 0, 0, 0, 0.0, 0.0, 10.0, 90.0, 0.0, 0.0)
+    return 145.0
+
+
+def _yagi_fields_reflection(api, ctx):
+    """Near E and H over a finite ground in the reflection-coefficient
+    approximation (the image terms of efld and hsfld)."""
+    return _yagi_fields_ground(api, ctx, (0, 0, 13.0, 0.005, 0, 0, 0, 0))
+
+
+def _yagi_fields_perfect(api, ctx):
+    return _yagi_fields_ground(api, ctx, (1, 0, 0, 0, 0, 0, 0, 0))
 
 
 # name: (builder, pattern grid (n_theta, n_phi) or None)
@@ -191,4 +234,7 @@ CASES = {
     "array_tl": (_array_tl, (19, 8)),
     "dipole_nt": (_dipole_nt, (19, 8)),
     "near_ground": (_near_ground, (10, 4)),
+    "dipole_fields": (_dipole_fields, (10, 4)),
+    "yagi_fields_reflection": (_yagi_fields_reflection, (10, 4)),
+    "yagi_fields_perfect": (_yagi_fields_perfect, (10, 4)),
 }

@@ -64,6 +64,13 @@ def collect(ref, name, builder, grid):
             i += 1
         out["gains"] = np.array(gains).reshape(len(gains), nth, nph)
         out["gain_stats"] = np.array(stats).reshape(len(stats), 12)
+    # near-field patterns
+    nf = ref.near_fields(ctx)
+    if nf:
+        out["near_nfeh"] = np.array([k for k, _, _ in nf], dtype=np.int32)
+        out["near_np"] = np.array([len(x) for _, x, _ in nf], dtype=np.int32)
+        out["near_xyz"] = np.concatenate([x for _, x, _ in nf])
+        out["near_f"] = np.concatenate([f for _, _, f in nf])
     # last solution
     cur, abc = ref.currents(ctx)
     out["current_vector"] = cur

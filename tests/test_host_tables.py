@@ -122,8 +122,8 @@ def test_errors_and_sentinels(nb):
     assert "NO SEGMENT HAS AN ITAG" in nb.nec_error_message()
     assert nb.nec_ex_card(ctx, 0, 7, 1, 0, 1.0, 0, 0, 0, 0, 0) == 1
     # cards outside the hot path exist and refuse
-    for call in (lambda: nb.nec_ne_card(ctx, 0, 1, 1, 1, 0, 0, 0, 0, 0, 0),
-                 lambda: nb.nec_sp_card(ctx, 0, 0, 0, 0, 0, 0, 0)):
+    for call in (lambda: nb.nec_sp_card(ctx, 0, 0, 0, 0, 0, 0, 0),
+                 lambda: nb.nec_cp_card(ctx, 1, 1, 1, 2)):
         assert call() == 1
         assert "not part of the B200" in nb.nec_error_message()
     # NT port on a tag that does not exist (c_geometry.cpp:76-99)

@@ -46,22 +46,52 @@ def _sweep(api):
     return out
 
 
+def _wavelength(f_mhz):
+    return (1.0 / math.sqrt(((4.0 * 3.1415926536) * 1.0e-7) * 8.854e-12)) / (1.0e6 * f_mhz)
+
+
+def _oracle_sweep(nb, oracle, name, ctx, api):
+    """The case's frequency sweep on the oracle, in the reference's order:
+    per frequency the fill, the solve and the near-field requests at the
+    golden points.  Near-ground cases integrate the oracle's tables through
+    one interpolation cache over the whole sweep.  Returns per frequency
+    (Z, status, structure, abc, currents, near fields)."""
+    g = golden(name)
+    interp = oracle.new_interp()
+    nearf = list(zip(g["near_nfeh"], np.split(g["near_xyz"], np.cumsum(g["near_np"])[:-1]))) \
+        if "near_nfeh" in g else []
+    freqs = _sweep(api)
+    per = len(nearf) // len(freqs) if nearf else 0
+    out = []
+    for k, f in enumerate(freqs):
+        sf = nb.structure(ctx, f)
+        if name in SOMM_GROUND:
+            epr, sig = SOMM_GROUND[name]
+            sf["somm"], _ = oracle.sommerfeld(epr, sig, _wavelength(f), ETA)
+            sf["interp"] = interp
+        Z, status = oracle.fill(sf)
+        rhs = nb.rhs(ctx)
+        x, bad = oracle.solve(Z, rhs)
+        assert bad == 0
+        abc, cur = oracle.coefficients(sf, x)
+        fields = [(nfeh, oracle.near_field(sf, abc, xyz / _wavelength(f), magnetic=nfeh == 1))
+                  for nfeh, xyz in nearf[k * per:(k + 1) * per]]
+        out.append((Z, status, sf, abc, cur, fields))
+    return out
+
+
 def _oracle_fill(nb, oracle, name, ctx, st, api, fresh=False):
     """The oracle's fill of the case's last frequency.  For near-ground
-    cases the tables come from the oracle and the interpolation cache
-    carries over from the earlier frequencies of the sweep, as in the
-    reference; fresh=True starts the last fill from a new cache instead."""
+    cases the interpolation cache carries over from the earlier work of the
+    sweep, as in the reference; fresh=True starts the last fill from a new
+    cache instead."""
     if name not in SOMM_GROUND:
         return oracle.fill(st)
-    epr, sig = SOMM_GROUND[name]
-    interp = oracle.new_interp()
-    freqs = _sweep(api)[-1:] if fresh else _sweep(api)
-    for f in freqs:
-        sf = nb.structure(ctx, f)
-        lam = (1.0 / math.sqrt(((4.0 * 3.1415926536) * 1.0e-7) * 8.854e-12)) / (1.0e6 * f)
-        sf["somm"], _ = oracle.sommerfeld(epr, sig, lam, ETA)
-        sf["interp"] = interp
-        Z, status = oracle.fill(sf)
+    if fresh:
+        epr, sig = SOMM_GROUND[name]
+        st["somm"], _ = oracle.sommerfeld(epr, sig, _wavelength(_sweep(api)[-1]), ETA)
+        return oracle.fill(st)
+    Z, status = _oracle_sweep(nb, oracle, name, ctx, api)[-1][:2]
     return Z, status
 
 
@@ -183,6 +213,26 @@ def test_oracle_network_matches_reference(nb, oracle, name):
     assert np.max(np.abs(abc.reshape(6, -1) - g["abc"])) / np.max(np.abs(g["abc"])) <= 1e-10
     # the ports really carry network current
     assert abs(loss) > 1e-6 * pin
+    nb.nec_delete(ctx)
+
+
+NEAR_CASES = [n for n in NAMES if "near_nfeh" in golden(n)]
+
+
+@pytest.mark.parametrize("name", NEAR_CASES)
+def test_oracle_near_fields_match_reference(nb, oracle, name):
+    """Near E and H fields (nefld / nhfld over the nfpat grid) of the oracle
+    against the reference's near-field patterns, every frequency."""
+    ctx, st, rhs, api = host_case(nb, CASES[name][0])
+    g = golden(name)
+    ours = [f for step in _oracle_sweep(nb, oracle, name, ctx, api) for f in step[5]]
+    offs = np.cumsum(np.concatenate([[0], g["near_np"]]))
+    assert len(ours) == len(g["near_nfeh"])
+    for k, (nfeh, f) in enumerate(ours):
+        ref = g["near_f"][offs[k]:offs[k + 1]]
+        assert nfeh == g["near_nfeh"][k]
+        scale = np.max(np.abs(ref))
+        assert np.max(np.abs(f - ref)) <= 1e-10 * scale, (k, np.max(np.abs(f - ref)) / scale)
     nb.nec_delete(ctx)
 
 
