@@ -185,6 +185,13 @@ long nec_get_loads(nec_context* in_context, double* out);
    (magnetic); with non-null buffers, xyz the points (metres, 3 per point)
    and fields 3 complex per point (x, y, z; re/im interleaved; V/m or A/m). */
 long nec_near_field(nec_context* in_context, int index, int* nfeh, double* xyz, double* fields);
+/* Runs a NEC input deck (nec2++'s card images: comments, geometry up to GE,
+   program-control cards to EN; several jobs separated by NX) and writes the
+   antenna input, power budget, radiation pattern and near-field sections of
+   nec2++'s text output to output_path (standard output if NULL or empty).
+   Returns 0, or 1 with the message in nec_deck_error(). */
+long nec_run_deck(const char* input_path, const char* output_path);
+const char* nec_deck_error(void);
 /* Number of NT/TL networks on the context (0 if none). */
 long nec_network_count(nec_context* in_context);
 /* The context's GPU engine (include/necgpu.h), created on first use; NULL

@@ -14,7 +14,9 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libnecpp_b200.so")
 
-HOST_SRCS = ["geometry.cpp", "context.cpp", "c_api.cpp"]
+HOST_SRCS = ["geometry.cpp", "context.cpp", "c_api.cpp", "deck.cpp"]
+CLI_SRC = "nec2b200_main.cpp"
+CLI = os.path.join(HERE, "nec2b200")
 CUDA_SRCS = ["engine.cu"]
 CUDA_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -78,6 +80,11 @@ def build(verbose=False, force=False):
         objs.append(o)
     if force or _newer(LIB, objs):
         _run([nvcc] + CUDA_ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs)
+    # the deck-file command line (nec2++'s -i / -o), linked to the library
+    cli_src = os.path.join(CSRC, CLI_SRC)
+    if force or _newer(CLI, [cli_src, LIB]):
+        _run([_cxx(), "-std=c++17", "-O2", "-I", os.path.join(HERE, ".."), cli_src, "-o", CLI,
+              "-L", HERE, "-lnecpp_b200", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

@@ -249,6 +249,7 @@ void Context::nfpat() {
     p.fy.push_back(f[3 * i + 1]);
     p.fz.push_back(f[3 * i + 2]);
   }
+  p.seq = next_seq();
   near_fields.push_back(std::move(p));
 }
 
@@ -640,6 +641,17 @@ int Context::excitation_inner(int mhz) {
   if (iptflq < -2 || iptflq > 0) iptflq = -1;
   if (ex_type != 1 && ex_type != 2 && ex_type != 3 && (iptflg == 2 || iptflg == 3)) iptflg = -1;
   structure_power_loss = compute_structure_power_loss();
+  if (ex_type == 0 || ex_type == 5) {
+    PowerBudget b;
+    b.seq = next_seq();
+    b.freq_hz = freq_mhz * 1.0e6;
+    b.input = input_power;
+    b.structure_loss = structure_power_loss;
+    b.network_loss = network_power_loss;
+    b.radiated = input_power - network_power_loss - structure_power_loss;
+    b.efficiency = 100.0 * b.radiated / input_power;
+    budgets.push_back(b);
+  }
   if (iptflg != -1 || iptflq != -1) {
     if ((iptflg < 1 || iptflg == 3 || ((iptflg == 1 || iptflg == 2) && inc <= 1)) ||
         (iptflg == -1 && iptflq != -1)) {
@@ -1174,6 +1186,7 @@ void Context::network_solve() {
     ai.admittance.push_back(admittance);
     ai.power.push_back(power);
   }
+  ai.seq = next_seq();
   inputs.push_back(std::move(ai));
 }
 
@@ -1192,6 +1205,11 @@ void Context::far_field() {
   rp.ph0 = phis;
   rp.dth = dth;
   rp.dph = dph;
+  rp.ground = ground;
+  rp.fmt = rp_fmt;
+  rp.ipd = ipd;
+  rp.range = rfld;
+  rp.wavelength = wavelength_;
   const size_t cells = (size_t)nth * nph;
   rp.gain.assign(cells, 0.0);
   rp.gain_vert.assign(cells, 0.0);
@@ -1372,6 +1390,7 @@ void Context::far_field() {
     rp.average_power_solid_angle = solid / kPi;
   }
   rp.max_gain = *std::max_element(rp.gain.begin(), rp.gain.end());
+  rp.seq = next_seq();
   patterns.push_back(std::move(rp));
 }
 

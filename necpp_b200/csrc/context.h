@@ -20,7 +20,10 @@ namespace necb {
 
 using cd = std::complex<double>;
 
+// Results carry `seq`, the order in which the context produced them (the
+// order of the reference's printed output).
 struct AntennaInput {
+  int seq = 0;
   double freq_hz = 0;
   std::vector<int> tag, seg;
   std::vector<cd> voltage, current, impedance, admittance;
@@ -35,16 +38,28 @@ struct StructureCurrents {
 // nec_near_field_pattern (src/nec_results.h:564-655): points in metres,
 // fields in V/m (electric) or A/m (magnetic)
 struct NearFieldPattern {
+  int seq = 0;
   double freq_hz = 0;
   int nfeh = 0;  // 0 electric, 1 magnetic
   std::vector<double> x, y, z;
   std::vector<cd> fx, fy, fz;
 };
 
+// print_power_budget, src/nec_context.cpp:1443-1466 (voltage excitation)
+struct PowerBudget {
+  int seq = 0;
+  double freq_hz = 0;
+  double input = 0, radiated = 0, structure_loss = 0, network_loss = 0, efficiency = 0;
+};
+
 struct RadiationPattern {
+  int seq = 0;
   double freq_hz = 0;
   int nth = 0, nph = 0;
   double th0 = 0, ph0 = 0, dth = 0, dph = 0;
+  bool ground = false;  // directions below the horizon are not evaluated
+  int fmt = 0, ipd = 0;  // RP card's X (axis labels) and D (directive gain)
+  double range = 0, wavelength = 0;
   // (kth, kph) stored at kth + kph * nth
   std::vector<double> gain, gain_vert, gain_horiz, gain_tot, gain_rhcp, gain_lhcp;
   std::vector<double> axial_ratio, tilt, avg_scale;
@@ -98,6 +113,8 @@ class Context {
   std::vector<AntennaInput> inputs;
   std::vector<RadiationPattern> patterns;
   std::vector<NearFieldPattern> near_fields;
+  std::vector<PowerBudget> budgets;
+  int next_seq() { return ++result_seq_; }
   std::vector<StructureCurrents> currents;
   double last_refine_residual = 0;
   int last_refine_iters = 0;
@@ -186,6 +203,7 @@ class Context {
   double thets = 0, phis = 0, dth = 0, dph = 0, rfld = 0, gnor = 0;
   int iptflg = -2, iptag = 0, iptagf = 0, iptagt = 0;
   int iptflq = -1, iptaq = 0, iptaqf = 0, iptaqt = 0;
+  int result_seq_ = 0;
   int m_near = -1;
   int nfeh = 0, nrx = 0, nry = 0, nrz = 0;
   double xnr = 0, ynr = 0, znr = 0, dxnr = 0, dynr = 0, dznr = 0;

@@ -93,6 +93,36 @@ void Geometry::wire(int tag, int nseg, double xw1, double yw1, double zw1,
   z2[n - 1] = zw2;
 }
 
+// Arc of radius rada in the x-z plane from ang1 to ang2 degrees (GA card),
+// c_geometry.cpp:2077-2127: nseg chords of equal angle.
+void Geometry::arc(int tag, int nseg, double rada, double ang1, double ang2, double rad) {
+  if (completed) fail("GEOMETRY ALREADY COMPLETE");
+  const int64_t istart = n;
+  n += nseg;
+  np = n;
+  ipsym = 0;
+  if (nseg < 1) return;
+  if (std::fabs(ang2 - ang1) > 360.0) fail("ERROR -- ARC ANGLE EXCEEDS 360 DEGREES");
+  grow(n);
+  double ang = degrees_to_rad(ang1);
+  const double dang = degrees_to_rad(ang2 - ang1) / nseg;
+  double xs1 = rada * std::cos(ang), zs1 = rada * std::sin(ang);
+  for (int64_t i = istart; i < n; i++) {
+    ang += dang;
+    const double xs2 = rada * std::cos(ang), zs2 = rada * std::sin(ang);
+    x[i] = xs1;
+    y[i] = 0.;
+    z[i] = zs1;
+    x2[i] = xs2;
+    y2[i] = 0.;
+    z2[i] = zs2;
+    xs1 = xs2;
+    zs1 = zs2;
+    radius[i] = rad;
+    tags[i] = tag;
+  }
+}
+
 // Helix / spiral: c_geometry.cpp:698-826 (the printout is not reproduced).
 void Geometry::helix(int tag, int nseg, double s, double hl, double a1,
                      double b1, double a2, double b2, double rad) {
@@ -253,6 +283,57 @@ struct EndGrid {
     return ((uint64_t)(a & 0x1FFFFF) << 42) | ((uint64_t)(b & 0x1FFFFF) << 21) | (uint64_t)(c & 0x1FFFFF);
   }
 };
+
+// Points bucketed on a cubic grid without per-cell allocations: the items
+// sorted by cell, and an open-addressing table from a cell's key to its
+// range in that order.
+struct FlatGrid {
+  double cell = 1;
+  std::vector<int64_t> order;                  // item ids sorted by cell key
+  std::vector<uint64_t> slot_key;              // table: key + 1 (0 = empty)
+  std::vector<std::pair<int64_t, int64_t>> slot_range;
+  uint64_t mask = 0;
+  static uint64_t hash(uint64_t k) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    return k;
+  }
+  template <typename Pos>
+  void build(size_t count, double c, Pos pos) {
+    cell = c;
+    std::vector<uint64_t> keys(count);
+    for (size_t i = 0; i < count; i++) {
+      const V3 v = pos(i);
+      keys[i] = EndGrid::key(EndGrid::idx(v.x, c), EndGrid::idx(v.y, c), EndGrid::idx(v.z, c));
+    }
+    order.resize(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int64_t l, int64_t r) { return keys[l] < keys[r]; });
+    size_t cap = 16;
+    while (cap < 2 * count) cap *= 2;
+    mask = cap - 1;
+    slot_key.assign(cap, 0);
+    slot_range.assign(cap, {0, 0});
+    for (size_t b = 0; b < count;) {
+      size_t e = b;
+      const uint64_t k = keys[order[b]];
+      while (e < count && keys[order[e]] == k) e++;
+      uint64_t h = hash(k) & mask;
+      while (slot_key[h]) h = (h + 1) & mask;
+      slot_key[h] = k + 1;
+      slot_range[h] = {(int64_t)b, (int64_t)e};
+      b = e;
+    }
+  }
+  // the range in `order` of the cell with key k (empty if none)
+  std::pair<int64_t, int64_t> find(uint64_t k) const {
+    for (uint64_t h = hash(k) & mask;; h = (h + 1) & mask) {
+      if (!slot_key[h]) return {0, 0};
+      if (slot_key[h] == k + 1) return slot_range[h];
+    }
+  }
+};
 }  // namespace
 
 void Geometry::build_connections(int ignd) {
@@ -271,18 +352,12 @@ void Geometry::build_connections(int ignd) {
   for (int64_t i = 0; i < n; i++)
     max_slen = std::max(max_slen, norm3(sub(V3{x2[i], y2[i], z2[i]}, V3{x[i], y[i], z[i]})) * kSmin);
   const bool use_grid = ignd == 0 && n > 256 && std::isfinite(max_slen) && max_slen > 0.0;
-  EndGrid grid;
-  if (use_grid) {
-    grid.cell = 2.0 * max_slen;
-    for (int64_t i = 0; i < n; i++) {
-      grid.cells[EndGrid::key(EndGrid::idx(x[i], grid.cell), EndGrid::idx(y[i], grid.cell),
-                              EndGrid::idx(z[i], grid.cell))]
-          .push_back(2 * i);
-      grid.cells[EndGrid::key(EndGrid::idx(x2[i], grid.cell), EndGrid::idx(y2[i], grid.cell),
-                              EndGrid::idx(z2[i], grid.cell))]
-          .push_back(2 * i + 1);
-    }
-  }
+  FlatGrid grid;
+  if (use_grid)
+    grid.build((size_t)(2 * n), 2.0 * max_slen, [&](size_t code) {
+      const int64_t i = (int64_t)(code >> 1);
+      return (code & 1) ? V3{x2[i], y2[i], z2[i]} : V3{x[i], y[i], z[i]};
+    });
   // first match in the cyclic order i+1, i+2, ..., i-1 (start before end of
   // the same segment): returns 2 * segment + end, or -1
   auto grid_first = [&](int64_t i, const V3& v, double slen) -> int64_t {
@@ -292,9 +367,9 @@ void Geometry::build_connections(int ignd) {
     for (int64_t a = cx - 1; a <= cx + 1; a++)
       for (int64_t b = cy - 1; b <= cy + 1; b++)
         for (int64_t c = cz - 1; c <= cz + 1; c++) {
-          auto it = grid.cells.find(EndGrid::key(a, b, c));
-          if (it == grid.cells.end()) continue;
-          for (int64_t code : it->second) {
+          const auto rg = grid.find(EndGrid::key(a, b, c));
+          for (int64_t q = rg.first; q < rg.second; q++) {
+            const int64_t code = grid.order[q];
             const int64_t ic = code >> 1;
             if (ic == i) continue;
             const int end = (int)(code & 1);
@@ -534,17 +609,56 @@ void Geometry::check_overlaps() {
   };
   double thr_max = 0.0;
   for (auto& e : ends) thr_max = std::max(thr_max, e.thr);
-  {
-    int ax = axis_of(ends);
-    std::stable_sort(ends.begin(), ends.end(), [&](const End& l, const End& r) {
-      return coord(l.p, ax) < coord(r.p, ax);
-    });
-    for (size_t a = 0; a < ends.size(); a++)
-      for (size_t p = a + 1; p < ends.size() && coord(ends[p].p, ax) - coord(ends[a].p, ax) <= thr_max; p++) {
+  // Candidate pairs come from a grid of cubes no smaller than the largest
+  // interaction distance, so each item meets only the items of its own and
+  // the 26 neighbouring cubes (every pair within that distance is among
+  // them); without a usable cube size, from a sweep along the widest axis.
+  auto grid_pairs = [&](size_t count, auto pos, double reach, auto visit) {
+    if (std::isfinite(reach) && reach > 0.0 && count > 256) {
+      FlatGrid grid;
+      grid.build(count, reach, pos);
+      const double r2 = reach * reach * 3.0;
+      for (size_t i = 0; i < count; i++) {
+        const V3 v = pos(i);
+        const int64_t cx = EndGrid::idx(v.x, reach), cy = EndGrid::idx(v.y, reach), cz = EndGrid::idx(v.z, reach);
+        for (int64_t a = cx - 1; a <= cx + 1; a++)
+          for (int64_t b = cy - 1; b <= cy + 1; b++)
+            for (int64_t c = cz - 1; c <= cz + 1; c++) {
+              const auto rg = grid.find(EndGrid::key(a, b, c));
+              for (int64_t q = rg.first; q < rg.second; q++) {
+                const int64_t j = grid.order[q];
+                if ((size_t)j <= i) continue;
+                const V3 w = pos((size_t)j);
+                const double dx = w.x - v.x, dy = w.y - v.y, dz = w.z - v.z;
+                if (dx * dx + dy * dy + dz * dz > r2) continue;  // farther than any pair of interest
+                visit(i, (size_t)j);
+              }
+            }
+      }
+      return;
+    }
+    std::vector<size_t> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    std::vector<V3> pts(count);
+    for (size_t i = 0; i < count; i++) pts[i] = pos(i);
+    struct P {
+      V3 p;
+    };
+    std::vector<P> tmp(count);
+    for (size_t i = 0; i < count; i++) tmp[i].p = pts[i];
+    const int ax = count ? axis_of(tmp) : 0;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t l, size_t r) { return coord(pts[l], ax) < coord(pts[r], ax); });
+    for (size_t a = 0; a < count; a++)
+      for (size_t p = a + 1; p < count && coord(pts[order[p]], ax) - coord(pts[order[a]], ax) <= reach; p++)
+        visit(std::min(order[a], order[p]), std::max(order[a], order[p]));
+  };
+  grid_pairs(
+      ends.size(), [&](size_t i) { return ends[i].p; }, thr_max,
+      [&](size_t a, size_t p) {
         double t = std::max(ends[a].thr, ends[p].thr);
         if (norm_l1(sub(ends[a].p, ends[p].p)) <= t) parent[root(ends[p].idx)] = root(ends[a].idx);
-      }
-  }
+      });
   std::vector<std::pair<int64_t, int64_t>> nodes(n);
   for (int64_t i = 0; i < n; i++) nodes[i] = {root(2 * i), root(2 * i + 1)};
   auto one_node = [&](int64_t s, int64_t t) {
@@ -567,19 +681,9 @@ void Geometry::check_overlaps() {
   };
   double reach = 0.0;
   for (auto& v : views) reach = std::max(reach, 0.5 * norm3(sub(v.b, v.a)) + v.r);
-  // views carry their centre in .c; sort along the widest axis of the centres
-  struct P {
-    V3 p;
-  };
-  std::vector<P> cen(views.size());
-  for (size_t i = 0; i < views.size(); i++) cen[i].p = views[i].c;
-  int ax = axis_of(cen);
-  std::stable_sort(views.begin(), views.end(), [&](const View& l, const View& r) {
-    return coord(l.c, ax) < coord(r.c, ax);
-  });
-  for (size_t a = 0; a < views.size(); a++)
-    for (size_t p = a + 1; p < views.size() && coord(views[p].c, ax) - coord(views[a].c, ax) <= reach; p++) {
-      if (one_node(views[a].idx, views[p].idx)) continue;
+  // a centre inside a segment lies within `reach` of that segment's centre
+  grid_pairs(views.size(), [&](size_t i) { return views[i].c; }, reach, [&](size_t a, size_t p) {
+      if (one_node(views[a].idx, views[p].idx)) return;
       const View* pairs[2][2] = {{&views[a], &views[p]}, {&views[p], &views[a]}};
       for (auto& pr : pairs) {
         const View& inside = *pr[0];
@@ -596,7 +700,7 @@ void Geometry::check_overlaps() {
           throw nec_error(buf);
         }
       }
-    }
+  });
 }
 
 // geometry_complete, c_geometry.cpp:454-612 (wire part).

@@ -30,6 +30,7 @@ class Geometry {
             double yw2, double zw2, double rad, double rdel, double rrad);
   void helix(int tag, int nseg, double s, double hl, double a1, double b1,
              double a2, double b2, double rad);
+  void arc(int tag, int nseg, double rada, double ang1, double ang2, double rad);
   void move(double rox, double roy, double roz, double xs, double ys, double zs,
             int its, int nrpt, int itgi);
   void scale(double factor);
