@@ -361,12 +361,15 @@ void Geometry::build_connections(int ignd) {
   // first match in the cyclic order i+1, i+2, ..., i-1 (start before end of
   // the same segment): returns 2 * segment + end, or -1
   auto grid_first = [&](int64_t i, const V3& v, double slen) -> int64_t {
-    const int64_t cx = EndGrid::idx(v.x, grid.cell), cy = EndGrid::idx(v.y, grid.cell),
-                  cz = EndGrid::idx(v.z, grid.cell);
+    // ends within L1 distance slen lie in the cubes the box v +- slen meets
+    const double cell = grid.cell;
+    const int64_t x0 = EndGrid::idx(v.x - slen, cell), x1 = EndGrid::idx(v.x + slen, cell);
+    const int64_t y0 = EndGrid::idx(v.y - slen, cell), y1 = EndGrid::idx(v.y + slen, cell);
+    const int64_t z0 = EndGrid::idx(v.z - slen, cell), z1 = EndGrid::idx(v.z + slen, cell);
     int64_t best = -1, best_rank = INT64_MAX;
-    for (int64_t a = cx - 1; a <= cx + 1; a++)
-      for (int64_t b = cy - 1; b <= cy + 1; b++)
-        for (int64_t c = cz - 1; c <= cz + 1; c++) {
+    for (int64_t a = x0; a <= x1; a++)
+      for (int64_t b = y0; b <= y1; b++)
+        for (int64_t c = z0; c <= z1; c++) {
           const auto rg = grid.find(EndGrid::key(a, b, c));
           for (int64_t q = rg.first; q < rg.second; q++) {
             const int64_t code = grid.order[q];
@@ -615,15 +618,20 @@ void Geometry::check_overlaps() {
   // them); without a usable cube size, from a sweep along the widest axis.
   auto grid_pairs = [&](size_t count, auto pos, double reach, auto visit) {
     if (std::isfinite(reach) && reach > 0.0 && count > 256) {
+      // cubes of edge 2 * reach: the box of half-width reach around a point
+      // meets at most two cubes along each axis
       FlatGrid grid;
-      grid.build(count, reach, pos);
+      const double cell = 2.0 * reach;
+      grid.build(count, cell, pos);
       const double r2 = reach * reach * 3.0;
       for (size_t i = 0; i < count; i++) {
         const V3 v = pos(i);
-        const int64_t cx = EndGrid::idx(v.x, reach), cy = EndGrid::idx(v.y, reach), cz = EndGrid::idx(v.z, reach);
-        for (int64_t a = cx - 1; a <= cx + 1; a++)
-          for (int64_t b = cy - 1; b <= cy + 1; b++)
-            for (int64_t c = cz - 1; c <= cz + 1; c++) {
+        const int64_t x0 = EndGrid::idx(v.x - reach, cell), x1 = EndGrid::idx(v.x + reach, cell);
+        const int64_t y0 = EndGrid::idx(v.y - reach, cell), y1 = EndGrid::idx(v.y + reach, cell);
+        const int64_t z0 = EndGrid::idx(v.z - reach, cell), z1 = EndGrid::idx(v.z + reach, cell);
+        for (int64_t a = x0; a <= x1; a++)
+          for (int64_t b = y0; b <= y1; b++)
+            for (int64_t c = z0; c <= z1; c++) {
               const auto rg = grid.find(EndGrid::key(a, b, c));
               for (int64_t q = rg.first; q < rg.second; q++) {
                 const int64_t j = grid.order[q];
