@@ -12,11 +12,9 @@
 // MP, NX, EN, XT.  Cards outside this build (GR, GX, SP, SM, SC, GF, GD, CP,
 // PL, WG) stop the run with a message, as any card error does.
 #include <cctype>
-#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
-#include <cstring>
 #include <fstream>
 #include <iostream>
 #include <memory>
