@@ -117,6 +117,7 @@ struct necgpu_engine {
   cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
   bool lookahead = true;
   int lookahead_sms = 48;
+  bool trsm8 = true;  // U12 panel solves with eight warps per vector block (else one thread per vector)
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
   double2* d_zload = nullptr;  // impedance loading per segment (null: unloaded)
@@ -799,6 +800,35 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm_panel_smem<T>()));
+  CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm8_smem<T>()));
+  CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm8_smem<T>()));
+  // panel solve: vectors [sbeg, nend) against the 64 x 64 block at k0
+  // (LEFT: columns of U12, else rows of L21); kind and flop count for timing
+  auto trsm = [&](bool left, int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind) -> int {
+    const int64_t cnt = nend - sbeg;
+    if (cnt <= 0) return 0;
+    const double fl = 4.0 * (double)kBlk * kBlk * cnt;
+    // eight warps per vector block pay off for the U12 columns; the L21 rows
+    // (long panels, a triangle load per 32 vectors) stay one per thread
+    if (e->trsm8 && left) {
+      const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
+      const unsigned sm = (unsigned)trsm8_smem<T>();
+      if (left)
+        KLAUNCH(kind, fl, trsm8_panel_kernel<T, true><<<g, 256, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
+      else
+        KLAUNCH(kind, fl, trsm8_panel_kernel<T, false><<<g, 256, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
+      return 0;
+    }
+    const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);
+    const unsigned sm = (unsigned)trsm_panel_smem<T>();
+    if (left)
+      KLAUNCH(kind, fl, trsm_panel_kernel<T, true><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
+    else
+      KLAUNCH(kind, fl, trsm_panel_kernel<T, false><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
+    return 0;
+  };
   // gemm_grid: CTAs the persistent tensor-core update may take (fewer while
   // a far update runs beside the panel work)
   int gemm_grid = e->nsm;
@@ -820,7 +850,6 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                                                                                kb, e->d_piv));
     return 0;
   };
-  const unsigned smem = (unsigned)trsm_panel_smem<T>();
   // Outer blocks of e->outer columns (a multiple of 64) factored with 64-wide
   // inner panels whose updates stay inside the outer block's columns; the
   // outer block's U12 rows are brought up to date left-looking, and one
@@ -852,14 +881,10 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
       const int64_t r0 = k0 + kb, rest = n - r0;
       if (rest <= 0) continue;
-      KLAUNCH(NECGPU_K_PANEL, 4.0 * (double)kb * kb * rest,
-              trsm_panel_kernel<T, false><<<(unsigned)((rest + kTrsmW - 1) / kTrsmW), kTrsmW, smem, e->stream>>>(
-                  M, ld, n, k0, r0, dinv));
+      TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL));
       const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
       if (pc > 0) {
-        KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kb * kb * pc,
-                trsm_panel_kernel<T, true><<<(unsigned)((pc + kTrsmW - 1) / kTrsmW), kTrsmW, smem, e->stream>>>(
-                    M, ld, KE, k0, r0, dinv));
+        TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
         TRY(gemm(r0, r0, k0, rest, pc, kb));
       }
     }
@@ -876,9 +901,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     // U12 of the outer row block: rows [K0, KE), columns [KE, n)
     for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
       TRY(gemm(k0, KE, K0, kBlk, rest, (int)(k0 - K0)));
-      KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)kBlk * kBlk * rest,
-              trsm_panel_kernel<T, true><<<(unsigned)((rest + kTrsmW - 1) / kTrsmW), kTrsmW, smem, e->stream>>>(
-                  M, ld, n, k0, KE, e->d_dinv + k0));
+      TRY(trsm(true, k0, KE, n, e->d_dinv + k0, NECGPU_K_TRSM));
     }
     // trailing update with K = outer
     const int kk = (int)(KE - K0);
@@ -1392,6 +1415,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_FLAG_SWEEP")) e->inv_sweep = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_NO_DMMA")) e->use_dmma = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD")) e->lookahead = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_TRSM1")) e->trsm8 = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD_SMS")) {
     const int v = std::atoi(s);
     if (v >= 1 && v < 128) e->lookahead_sms = v;

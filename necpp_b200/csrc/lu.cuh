@@ -609,6 +609,95 @@ __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, in
   }
 }
 
+// The same panel solves with the 64 unknowns of a vector spread over eight
+// warps: warp g holds block g (8 unknowns) of 32 vectors, one per lane.  In
+// stage Q warp Q finishes its block (the 8 x 8 triangle, in registers) and
+// posts it to shared memory; after one barrier every warp g > Q subtracts
+// its contribution (64 complex multiply-adds per lane).  Eight stages
+// replace the 64-step chain of one thread per vector.  The triangle is kept
+// column-block-major with an odd stride per block so that the eight warps
+// of a stage read distinct banks.  kb = 64 (callers solve full blocks).
+constexpr int kTrsm8Vec = 32;  // vectors per CTA
+constexpr int kTrsm8TriStride = kBlk * 9 + 1;
+template <typename T>
+constexpr size_t trsm8_smem() {
+  return (size_t)(8 * kTrsm8TriStride + 8 * kTrsm8Vec * 9 + kBlk) * sizeof(T);
+}
+
+template <typename T, bool LEFT>
+__global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
+                                                          const T* dinv) {
+  constexpr int NB = kBlk, V = kTrsm8Vec;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Tri = reinterpret_cast<T*>(smem_raw);             // element (i, j) at (j>>3)*stride + i*9 + (j&7)
+  T* Xs = Tri + 8 * kTrsm8TriStride;                   // finished blocks: (Q * V + lane) * 9 + i
+  T* di = Xs + 8 * V * 9;
+  const int t = threadIdx.x, lane = t & 31, g = t >> 5;
+  const int64_t vec = sbeg + (int64_t)blockIdx.x * V + lane;
+  const bool valid = vec < n;
+  // triangle (RIGHT: U11 upper; LEFT: L11 transposed, strictly upper)
+  for (int e = t; e < NB * NB; e += 256) {
+    const int r = e / NB, c = e % NB;
+    const T v = M[(k0 + r) * ld + k0 + c];
+    if (LEFT)
+      Tri[(r >> 3) * kTrsm8TriStride + c * 9 + (r & 7)] = r > c ? v : czero<T>();
+    else
+      Tri[(c >> 3) * kTrsm8TriStride + r * 9 + (c & 7)] = v;
+  }
+  if (!LEFT && t < NB) di[t] = dinv[t];
+  // this thread's block of its vector
+  T acc[8];
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int c = g * 8 + j;
+    acc[j] = valid ? (LEFT ? M[(k0 + c) * ld + vec] : M[vec * ld + k0 + c]) : czero<T>();
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int Q = 0; Q < 8; Q++) {
+    if (g == Q) {
+      // the diagonal 8 x 8 triangle of block Q
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        if (!LEFT) acc[i] = cmul(acc[i], di[Q * 8 + i]);
+#pragma unroll
+        for (int j = i + 1; j < 8; j++) {
+          const T u = Tri[Q * kTrsm8TriStride + (Q * 8 + i) * 9 + j];
+          acc[j].x -= acc[i].x * u.x - acc[i].y * u.y;
+          acc[j].y -= acc[i].x * u.y + acc[i].y * u.x;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++) Xs[(Q * V + lane) * 9 + i] = acc[i];
+    }
+    __syncthreads();
+    if (g > Q) {
+      const T* xq = Xs + (Q * V + lane) * 9;
+      const T* tb = Tri + g * kTrsm8TriStride + (Q * 8) * 9;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const T x = xq[i];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const T u = tb[i * 9 + j];
+          acc[j].x -= x.x * u.x - x.y * u.y;
+          acc[j].y -= x.x * u.y + x.y * u.x;
+        }
+      }
+    }
+  }
+  if (valid) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int c = g * 8 + j;
+      if (LEFT)
+        M[(k0 + c) * ld + vec] = acc[j];
+      else
+        M[vec * ld + k0 + c] = acc[j];
+    }
+  }
+}
+
 // Row interchanges of a block-pivoted panel: the kb <= 64 exchanges stay
 // inside rows [k0, k0+kb), so each column is one gather of those rows.  A
 // CTA covers 32 columns of [c_lo, c_hi) with 8 row groups; all reads finish
