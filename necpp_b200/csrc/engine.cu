@@ -800,8 +800,6 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm_panel_smem<T>()));
-  CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)trsm8_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm8_smem<T>()));
   // panel solve: vectors [sbeg, nend) against the 64 x 64 block at k0
@@ -810,15 +808,13 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
     const double fl = 4.0 * (double)kBlk * kBlk * cnt;
-    // eight warps per vector block pay off for the U12 columns; the L21 rows
-    // (long panels, a triangle load per 32 vectors) stay one per thread
+    // eight warps per block of 32 vectors pay off for the U12 columns
+    // (coalesced along the row); the L21 rows stay one per thread, which
+    // measured faster than the eight-warp form with 32 or 128 rows per CTA
     if (e->trsm8 && left) {
       const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
-      const unsigned sm = (unsigned)trsm8_smem<T>();
-      if (left)
-        KLAUNCH(kind, fl, trsm8_panel_kernel<T, true><<<g, 256, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
-      else
-        KLAUNCH(kind, fl, trsm8_panel_kernel<T, false><<<g, 256, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
+      KLAUNCH(kind, fl, trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), e->stream>>>(
+                            M, ld, nend, k0, sbeg, dinv));
       return 0;
     }
     const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);

@@ -617,24 +617,23 @@ __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, in
 // replace the 64-step chain of one thread per vector.  The triangle is kept
 // column-block-major with an odd stride per block so that the eight warps
 // of a stage read distinct banks.  kb = 64 (callers solve full blocks).
-constexpr int kTrsm8Vec = 32;  // vectors per CTA
+constexpr int kTrsm8Vec = 32;  // vectors per CTA per lane slot
 constexpr int kTrsm8TriStride = kBlk * 9 + 1;
-template <typename T>
+template <typename T, int VPL = 1>
 constexpr size_t trsm8_smem() {
-  return (size_t)(8 * kTrsm8TriStride + 8 * kTrsm8Vec * 9 + kBlk) * sizeof(T);
+  return (size_t)(8 * kTrsm8TriStride + 8 * VPL * kTrsm8Vec * 9 + kBlk) * sizeof(T);
 }
 
-template <typename T, bool LEFT>
+// VPL vectors per lane: 32 * VPL vectors per CTA share one triangle load.
+template <typename T, bool LEFT, int VPL = 1>
 __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
                                                           const T* dinv) {
-  constexpr int NB = kBlk, V = kTrsm8Vec;
+  constexpr int NB = kBlk, V = kTrsm8Vec * VPL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Tri = reinterpret_cast<T*>(smem_raw);             // element (i, j) at (j>>3)*stride + i*9 + (j&7)
-  T* Xs = Tri + 8 * kTrsm8TriStride;                   // finished blocks: (Q * V + lane) * 9 + i
+  T* Xs = Tri + 8 * kTrsm8TriStride;                   // finished blocks: (Q * V + vector) * 9 + i
   T* di = Xs + 8 * V * 9;
   const int t = threadIdx.x, lane = t & 31, g = t >> 5;
-  const int64_t vec = sbeg + (int64_t)blockIdx.x * V + lane;
-  const bool valid = vec < n;
   // triangle (RIGHT: U11 upper; LEFT: L11 transposed, strictly upper)
   for (int e = t; e < NB * NB; e += 256) {
     const int r = e / NB, c = e % NB;
@@ -645,12 +644,19 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
       Tri[(c >> 3) * kTrsm8TriStride + r * 9 + (c & 7)] = v;
   }
   if (!LEFT && t < NB) di[t] = dinv[t];
-  // this thread's block of its vector
-  T acc[8];
+  // this thread's block of its vectors (vector slot s = lane + 32 * w)
+  T acc[VPL][8];
+  int64_t vec[VPL];
+  bool valid[VPL];
 #pragma unroll
-  for (int j = 0; j < 8; j++) {
-    const int c = g * 8 + j;
-    acc[j] = valid ? (LEFT ? M[(k0 + c) * ld + vec] : M[vec * ld + k0 + c]) : czero<T>();
+  for (int w = 0; w < VPL; w++) {
+    vec[w] = sbeg + (int64_t)blockIdx.x * V + lane + 32 * w;
+    valid[w] = vec[w] < n;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+      const int c = g * 8 + j;
+      acc[w][j] = valid[w] ? (LEFT ? M[(k0 + c) * ld + vec[w]] : M[vec[w] * ld + k0 + c]) : czero<T>();
+    }
   }
   __syncthreads();
 #pragma unroll 1
@@ -659,41 +665,55 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
       // the diagonal 8 x 8 triangle of block Q
 #pragma unroll
       for (int i = 0; i < 8; i++) {
-        if (!LEFT) acc[i] = cmul(acc[i], di[Q * 8 + i]);
+        const T dq = LEFT ? czero<T>() : di[Q * 8 + i];
+#pragma unroll
+        for (int w = 0; w < VPL; w++)
+          if (!LEFT) acc[w][i] = cmul(acc[w][i], dq);
 #pragma unroll
         for (int j = i + 1; j < 8; j++) {
           const T u = Tri[Q * kTrsm8TriStride + (Q * 8 + i) * 9 + j];
-          acc[j].x -= acc[i].x * u.x - acc[i].y * u.y;
-          acc[j].y -= acc[i].x * u.y + acc[i].y * u.x;
+#pragma unroll
+          for (int w = 0; w < VPL; w++) {
+            acc[w][j].x -= acc[w][i].x * u.x - acc[w][i].y * u.y;
+            acc[w][j].y -= acc[w][i].x * u.y + acc[w][i].y * u.x;
+          }
         }
       }
 #pragma unroll
-      for (int i = 0; i < 8; i++) Xs[(Q * V + lane) * 9 + i] = acc[i];
+      for (int w = 0; w < VPL; w++)
+#pragma unroll
+        for (int i = 0; i < 8; i++) Xs[(Q * V + lane + 32 * w) * 9 + i] = acc[w][i];
     }
     __syncthreads();
     if (g > Q) {
-      const T* xq = Xs + (Q * V + lane) * 9;
       const T* tb = Tri + g * kTrsm8TriStride + (Q * 8) * 9;
 #pragma unroll
       for (int i = 0; i < 8; i++) {
-        const T x = xq[i];
+        T x[VPL];
+#pragma unroll
+        for (int w = 0; w < VPL; w++) x[w] = Xs[(Q * V + lane + 32 * w) * 9 + i];
 #pragma unroll
         for (int j = 0; j < 8; j++) {
           const T u = tb[i * 9 + j];
-          acc[j].x -= x.x * u.x - x.y * u.y;
-          acc[j].y -= x.x * u.y + x.y * u.x;
+#pragma unroll
+          for (int w = 0; w < VPL; w++) {
+            acc[w][j].x -= x[w].x * u.x - x[w].y * u.y;
+            acc[w][j].y -= x[w].x * u.y + x[w].y * u.x;
+          }
         }
       }
     }
   }
-  if (valid) {
+#pragma unroll
+  for (int w = 0; w < VPL; w++) {
+    if (!valid[w]) continue;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
       const int c = g * 8 + j;
       if (LEFT)
-        M[(k0 + c) * ld + vec] = acc[j];
+        M[(k0 + c) * ld + vec[w]] = acc[w][j];
       else
-        M[vec * ld + k0 + c] = acc[j];
+        M[vec[w] * ld + k0 + c] = acc[w][j];
     }
   }
 }
