@@ -1400,11 +1400,15 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (device < 0 || device >= count) return fail(e, NECGPU_ERR_ARG, "device index out of range");
   e->device = device;
   CUDA_TRY(cudaSetDevice(device));
-  cudaDeviceProp prop;
-  CUDA_TRY(cudaGetDeviceProperties(&prop, device));
-  if (prop.major < 10) return fail(e, NECGPU_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
-  if (!prop.cooperativeLaunch) return fail(e, NECGPU_ERR_NO_DEVICE, "device lacks cooperative launch");
-  e->nsm = prop.multiProcessorCount;
+  // three attributes instead of the whole property block (which costs
+  // milliseconds per context)
+  int major = 0, coop = 0, nsm = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  if (major < 10) return fail(e, NECGPU_ERR_NO_DEVICE, "this build targets sm_100a (B200)");
+  if (!coop) return fail(e, NECGPU_ERR_NO_DEVICE, "device lacks cooperative launch");
+  e->nsm = nsm;
   if (const char* s = std::getenv("NECPP_B200_NO_TC")) e->use_tc = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_BLOCKED_TRSV")) e->sweep_trsv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
+#include <thread>
 #include <unordered_map>
 #include <cstdint>
 #include <climits>
@@ -613,36 +614,51 @@ void Geometry::check_overlaps() {
   double thr_max = 0.0;
   for (auto& e : ends) thr_max = std::max(thr_max, e.thr);
   // Candidate pairs come from a grid of cubes no smaller than the largest
-  // interaction distance, so each item meets only the items of its own and
-  // the 26 neighbouring cubes (every pair within that distance is among
-  // them); without a usable cube size, from a sweep along the widest axis.
-  auto grid_pairs = [&](size_t count, auto pos, double reach, auto visit) {
+  // interaction distance: the box of half-width `reach` around an item meets
+  // at most two cubes along each axis, and every pair within that distance
+  // is among the items found there.  Without a usable cube size the pairs
+  // come from a sweep along the widest axis.  visit(worker, a, p) sees each
+  // candidate pair once, a < p; with the grid the items are split over
+  // worker threads, each visiting the pairs of its own items.
+  const int nworkers = std::max(1, std::min(8, (int)std::thread::hardware_concurrency()));
+  auto grid_pairs = [&](size_t count, auto pos, double reach, int workers, auto visit) {
     if (std::isfinite(reach) && reach > 0.0 && count > 256) {
-      // cubes of edge 2 * reach: the box of half-width reach around a point
-      // meets at most two cubes along each axis
       FlatGrid grid;
       const double cell = 2.0 * reach;
       grid.build(count, cell, pos);
       const double r2 = reach * reach * 3.0;
-      for (size_t i = 0; i < count; i++) {
-        const V3 v = pos(i);
-        const int64_t x0 = EndGrid::idx(v.x - reach, cell), x1 = EndGrid::idx(v.x + reach, cell);
-        const int64_t y0 = EndGrid::idx(v.y - reach, cell), y1 = EndGrid::idx(v.y + reach, cell);
-        const int64_t z0 = EndGrid::idx(v.z - reach, cell), z1 = EndGrid::idx(v.z + reach, cell);
-        for (int64_t a = x0; a <= x1; a++)
-          for (int64_t b = y0; b <= y1; b++)
-            for (int64_t c = z0; c <= z1; c++) {
-              const auto rg = grid.find(EndGrid::key(a, b, c));
-              for (int64_t q = rg.first; q < rg.second; q++) {
-                const int64_t j = grid.order[q];
-                if ((size_t)j <= i) continue;
-                const V3 w = pos((size_t)j);
-                const double dx = w.x - v.x, dy = w.y - v.y, dz = w.z - v.z;
-                if (dx * dx + dy * dy + dz * dz > r2) continue;  // farther than any pair of interest
-                visit(i, (size_t)j);
+      auto range = [&](int w, size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; i++) {
+          const V3 v = pos(i);
+          const int64_t x0 = EndGrid::idx(v.x - reach, cell), x1 = EndGrid::idx(v.x + reach, cell);
+          const int64_t y0 = EndGrid::idx(v.y - reach, cell), y1 = EndGrid::idx(v.y + reach, cell);
+          const int64_t z0 = EndGrid::idx(v.z - reach, cell), z1 = EndGrid::idx(v.z + reach, cell);
+          for (int64_t a = x0; a <= x1; a++)
+            for (int64_t b = y0; b <= y1; b++)
+              for (int64_t c = z0; c <= z1; c++) {
+                const auto rg = grid.find(EndGrid::key(a, b, c));
+                for (int64_t q = rg.first; q < rg.second; q++) {
+                  const int64_t j = grid.order[q];
+                  if ((size_t)j <= i) continue;
+                  const V3 u = pos((size_t)j);
+                  const double dx = u.x - v.x, dy = u.y - v.y, dz = u.z - v.z;
+                  if (dx * dx + dy * dy + dz * dz > r2) continue;  // farther than any pair of interest
+                  visit(w, i, (size_t)j);
+                }
               }
-            }
+        }
+      };
+      if (workers <= 1 || count < 4096) {
+        range(0, 0, count);
+        return;
       }
+      std::vector<std::thread> pool;
+      const size_t chunk = (count + workers - 1) / workers;
+      for (int w = 0; w < workers; w++) {
+        const size_t i0 = std::min(count, w * chunk), i1 = std::min(count, (w + 1) * chunk);
+        pool.emplace_back(range, w, i0, i1);
+      }
+      for (auto& th : pool) th.join();
       return;
     }
     std::vector<size_t> order(count);
@@ -659,14 +675,19 @@ void Geometry::check_overlaps() {
                      [&](size_t l, size_t r) { return coord(pts[l], ax) < coord(pts[r], ax); });
     for (size_t a = 0; a < count; a++)
       for (size_t p = a + 1; p < count && coord(pts[order[p]], ax) - coord(pts[order[a]], ax) <= reach; p++)
-        visit(std::min(order[a], order[p]), std::max(order[a], order[p]));
+        visit(0, std::min(order[a], order[p]), std::max(order[a], order[p]));
   };
-  grid_pairs(
-      ends.size(), [&](size_t i) { return ends[i].p; }, thr_max,
-      [&](size_t a, size_t p) {
-        double t = std::max(ends[a].thr, ends[p].thr);
-        if (norm_l1(sub(ends[a].p, ends[p].p)) <= t) parent[root(ends[p].idx)] = root(ends[a].idx);
-      });
+  // node classes: pairs of ends in contact, collected per worker, then joined
+  {
+    std::vector<std::vector<std::pair<size_t, size_t>>> touch(nworkers);
+    grid_pairs(ends.size(), [&](size_t i) { return ends[i].p; }, thr_max, nworkers,
+               [&](int w, size_t a, size_t p) {
+                 double t = std::max(ends[a].thr, ends[p].thr);
+                 if (norm_l1(sub(ends[a].p, ends[p].p)) <= t) touch[w].push_back({a, p});
+               });
+    for (auto& lst : touch)
+      for (auto& pr : lst) parent[root(ends[pr.second].idx)] = root(ends[pr.first].idx);
+  }
   std::vector<std::pair<int64_t, int64_t>> nodes(n);
   for (int64_t i = 0; i < n; i++) nodes[i] = {root(2 * i), root(2 * i + 1)};
   auto one_node = [&](int64_t s, int64_t t) {
@@ -679,7 +700,6 @@ void Geometry::check_overlaps() {
   auto axis_distance = [](const View& w, const V3& q) {
     double a0x = w.a.x, a0y = w.a.y, a0z = w.a.z, a1x = w.b.x, a1y = w.b.y, a1z = w.b.z;
     double sq = (a1x - a0x) * (a1x - a0x) + (a1y - a0y) * (a1y - a0y) + (a1z - a0z) * (a1z - a0z);
-    if (sq == 0.0) fail("nec_wire::axis_distance(): zero-length wire");
     double sa = (a1x * q.x + a1y * q.y + a1z * q.z - a0x * a1x - a0x * q.x - a0y * a1y - a0y * q.y -
                  a0z * a1z - a0z * q.z + a0x * a0x + a0y * a0y + a0z * a0z) / sq;
     if (sa < 0) sa = 0.0;
@@ -687,28 +707,48 @@ void Geometry::check_overlaps() {
     V3 pt{a0x + (a1x - a0x) * sa, a0y + (a1y - a0y) * sa, a0z + (a1z - a0z) * sa};
     return norm3(sub(pt, q));
   };
+  for (auto& v : views) {
+    const V3 d = sub(v.b, v.a);
+    if (d.x * d.x + d.y * d.y + d.z * d.z == 0.0) fail("nec_wire::axis_distance(): zero-length wire");
+  }
   double reach = 0.0;
   for (auto& v : views) reach = std::max(reach, 0.5 * norm3(sub(v.b, v.a)) + v.r);
-  // a centre inside a segment lies within `reach` of that segment's centre
-  grid_pairs(views.size(), [&](size_t i) { return views[i].c; }, reach, [&](size_t a, size_t p) {
-      if (one_node(views[a].idx, views[p].idx)) return;
-      const View* pairs[2][2] = {{&views[a], &views[p]}, {&views[p], &views[a]}};
-      for (auto& pr : pairs) {
-        const View& inside = *pr[0];
-        const View& container = *pr[1];
-        double d = axis_distance(container, inside.c);
-        if (d > container.r) continue;
-        if (overlap_fatal_) {
-          char buf[256];
-          snprintf(buf, sizeof(buf),
-                   "GEOMETRY DATA ERROR -- SEGMENT #%lld (TAG ID #%d) MIDPOINT LIES WITHIN "
-                   "SEGMENT #%lld (TAG ID #%d) AT DISTANCE %.5f RADIUS %.5f",
-                   (long long)(inside.idx + 1), inside.tag, (long long)(container.idx + 1),
-                   container.tag, d, container.r);
-          throw nec_error(buf);
-        }
-      }
+  // a centre inside a segment lies within `reach` of that segment's centre;
+  // each worker keeps its first violation, the lowest (inside, container)
+  // segment pair is reported
+  struct Hit {
+    int64_t inside = -1, container = -1;
+    double d = 0;
+  };
+  std::vector<Hit> hits(nworkers);
+  grid_pairs(views.size(), [&](size_t i) { return views[i].c; }, reach, nworkers, [&](int w, size_t a, size_t p) {
+    if (!overlap_fatal_ || one_node(views[a].idx, views[p].idx)) return;
+    const View* pairs[2][2] = {{&views[a], &views[p]}, {&views[p], &views[a]}};
+    for (auto& pr : pairs) {
+      const View& inside = *pr[0];
+      const View& container = *pr[1];
+      double d = axis_distance(container, inside.c);
+      if (d > container.r) continue;
+      Hit& h = hits[w];
+      if (h.inside < 0 || std::make_pair(inside.idx, container.idx) < std::make_pair(h.inside, h.container))
+        h = Hit{inside.idx, container.idx, d};
+    }
   });
+  const Hit* first = nullptr;
+  for (auto& h : hits)
+    if (h.inside >= 0 && (!first || std::make_pair(h.inside, h.container) < std::make_pair(first->inside, first->container)))
+      first = &h;
+  if (first) {
+    const View& inside = views[first->inside];
+    const View& container = views[first->container];
+    char buf[256];
+    snprintf(buf, sizeof(buf),
+             "GEOMETRY DATA ERROR -- SEGMENT #%lld (TAG ID #%d) MIDPOINT LIES WITHIN "
+             "SEGMENT #%lld (TAG ID #%d) AT DISTANCE %.5f RADIUS %.5f",
+             (long long)(inside.idx + 1), inside.tag, (long long)(container.idx + 1), container.tag, first->d,
+             container.r);
+    throw nec_error(buf);
+  }
 }
 
 // geometry_complete, c_geometry.cpp:454-612 (wire part).
