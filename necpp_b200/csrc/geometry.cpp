@@ -294,38 +294,44 @@ struct FlatGrid {
   std::vector<uint64_t> slot_key;              // table: key + 1 (0 = empty)
   std::vector<std::pair<int64_t, int64_t>> slot_range;
   uint64_t mask = 0;
-  static uint64_t hash(uint64_t k) {
-    k ^= k >> 33;
-    k *= 0xff51afd7ed558ccdULL;
-    k ^= k >> 33;
+  static uint64_t hash(uint64_t k) {  // splitmix64 finaliser
+    k ^= k >> 30;
+    k *= 0xbf58476d1ce4e5b9ULL;
+    k ^= k >> 27;
+    k *= 0x94d049bb133111ebULL;
+    k ^= k >> 31;
     return k;
   }
   template <typename Pos>
   void build(size_t count, double c, Pos pos) {
     cell = c;
-    std::vector<uint64_t> keys(count);
-    for (size_t i = 0; i < count; i++) {
-      const V3 v = pos(i);
-      keys[i] = EndGrid::key(EndGrid::idx(v.x, c), EndGrid::idx(v.y, c), EndGrid::idx(v.z, c));
-    }
-    order.resize(count);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int64_t l, int64_t r) { return keys[l] < keys[r]; });
+    // counting sort by cell: the table gives each distinct key a slot, the
+    // slots' counts become ranges, and the items are scattered in item
+    // order, so each cell lists its items in ascending order
     size_t cap = 16;
     while (cap < 2 * count) cap *= 2;
     mask = cap - 1;
     slot_key.assign(cap, 0);
     slot_range.assign(cap, {0, 0});
-    for (size_t b = 0; b < count;) {
-      size_t e = b;
-      const uint64_t k = keys[order[b]];
-      while (e < count && keys[order[e]] == k) e++;
+    std::vector<uint32_t> slot_of(count);
+    for (size_t i = 0; i < count; i++) {
+      const V3 v = pos(i);
+      const uint64_t k = EndGrid::key(EndGrid::idx(v.x, c), EndGrid::idx(v.y, c), EndGrid::idx(v.z, c));
       uint64_t h = hash(k) & mask;
-      while (slot_key[h]) h = (h + 1) & mask;
+      while (slot_key[h] && slot_key[h] != k + 1) h = (h + 1) & mask;
       slot_key[h] = k + 1;
-      slot_range[h] = {(int64_t)b, (int64_t)e};
-      b = e;
+      slot_range[h].second++;
+      slot_of[i] = (uint32_t)h;
     }
+    int64_t at = 0;
+    for (size_t h = 0; h < cap; h++) {
+      if (!slot_key[h]) continue;
+      const int64_t cnt = slot_range[h].second;
+      slot_range[h] = {at, at};
+      at += cnt;
+    }
+    order.resize(count);
+    for (size_t i = 0; i < count; i++) order[slot_range[slot_of[i]].second++] = (int64_t)i;
   }
   // the range in `order` of the cell with key k (empty if none)
   std::pair<int64_t, int64_t> find(uint64_t k) const {
@@ -388,7 +394,31 @@ void Geometry::build_connections(int ignd) {
         }
     return best;
   };
-  for (int64_t i = 0; i < n; i++) {
+  if (use_grid) {
+    // no ground: the searches only read the coordinates, so the segments
+    // are split over worker threads
+    auto search = [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; i++) {
+        const V3 v1{x[i], y[i], z[i]}, v2{x2[i], y2[i], z2[i]};
+        const double slen = norm3(sub(v2, v1)) * kSmin;
+        int64_t m = grid_first(i, v1, slen);
+        icon1[i] = m < 0 ? 0 : ((m & 1) == 0 ? -(int)((m >> 1) + 1) : (int)((m >> 1) + 1));
+        m = grid_first(i, v2, slen);
+        icon2[i] = m < 0 ? 0 : ((m & 1) == 0 ? (int)((m >> 1) + 1) : -(int)((m >> 1) + 1));
+      }
+    };
+    const int workers = n >= 4096 ? std::max(1, std::min(8, (int)std::thread::hardware_concurrency())) : 1;
+    if (workers == 1) {
+      search(0, n);
+    } else {
+      std::vector<std::thread> pool;
+      const int64_t chunk = (n + workers - 1) / workers;
+      for (int w = 0; w < workers; w++)
+        pool.emplace_back(search, std::min<int64_t>(n, w * chunk), std::min<int64_t>(n, (w + 1) * chunk));
+      for (auto& th : pool) th.join();
+    }
+  }
+  for (int64_t i = 0; i < n && !use_grid; i++) {
     int64_t iz = i + 1;
     double zi1 = z[i], zi2 = z2[i];
     V3 v1{x[i], y[i], z[i]}, v2{x2[i], y2[i], z2[i]};
@@ -403,10 +433,7 @@ void Geometry::build_connections(int ignd) {
         on_ground = true;
       }
     }
-    if (!on_ground && use_grid) {
-      const int64_t m = grid_first(i, v1, slen);
-      icon1[i] = m < 0 ? 0 : ((m & 1) == 0 ? -(int)((m >> 1) + 1) : (int)((m >> 1) + 1));
-    } else if (!on_ground) {
+    if (!on_ground) {
       int64_t ic = i;
       bool found = false;
       for (int64_t j = 1; j < n; j++) {
@@ -436,11 +463,6 @@ void Geometry::build_connections(int ignd) {
     }
     v1 = V3{x[i], y[i], z[i]};
     v2 = V3{x2[i], y2[i], z2[i]};
-    if (use_grid) {
-      const int64_t m = grid_first(i, v2, slen);
-      icon2[i] = m < 0 ? 0 : ((m & 1) == 0 ? (int)((m >> 1) + 1) : -(int)((m >> 1) + 1));
-      continue;
-    }
     int64_t ic = i;
     bool found = false;
     for (int64_t j = 1; j < n; j++) {
