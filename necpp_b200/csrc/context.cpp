@@ -2,6 +2,7 @@
 // Follows nec_context (src/nec_context.cpp, line ranges per function); the
 // fill, factor, solve and far-field sum run on the GPU via necgpu.h.
 #include "context.h"
+#include "host_parallel.h"
 
 #include <algorithm>
 #include <cmath>
@@ -1276,110 +1277,117 @@ void Context::far_field() {
                             reinterpret_cast<double*>(eph.data())));
   }
 
-  double pint = 0.0;
+  if (ndir > 0 && (rp_norm < 0 || rp_norm > 5)) fail("Unknown Gain Normalization Encountered.");
   const double delta_phi_rad = degrees_to_rad(dph);
   const double tmp2 = 0.5 * degrees_to_rad(dth);
-  for (int d = 0; d < ndir; d++) {
-    const int cell = cell_list[d];
-    const int kth = cell % nth, kph = cell / nth;
-    const double tha = tha_list[d];
-    double ethm2 = std::norm(eth[d]);
-    double ethm = std::sqrt(ethm2);
-    double etha = rad_to_degrees(std::arg(eth[d]));
-    double ephm2 = std::norm(eph[d]);
-    double ephm = std::sqrt(ephm2);
-    double epha = rad_to_degrees(std::arg(eph[d]));
-    double tilta, emajr2, eminr2, axrat;
-    int sense;
-    if (ethm2 <= 1.0e-20 && ephm2 <= 1.0e-20) {
-      tilta = 0.;
-      emajr2 = 0.;
-      eminr2 = 0.;
-      axrat = 0.;
-      sense = 3;
-    } else {
-      double dfaz = epha - etha;
-      double dfaz2 = (epha >= 0.) ? dfaz - 360. : dfaz + 360.;
-      if (std::fabs(dfaz) > std::fabs(dfaz2)) dfaz = dfaz2;
-      double cdfaz = std::cos(degrees_to_rad(dfaz));
-      double tstor1 = ethm2 - ephm2;
-      double tstor2 = 2. * ephm * ethm * cdfaz;
-      tilta = .5 * std::atan2(tstor2, tstor1);
-      double stilta = std::sin(tilta);
-      tstor1 = tstor1 * stilta * stilta;
-      tstor2 = tstor2 * stilta * std::cos(tilta);
-      emajr2 = -tstor1 + tstor2 + ethm2;
-      eminr2 = tstor1 - tstor2 + ephm2;
-      if (eminr2 < 0.) eminr2 = 0.;
-      axrat = std::sqrt(eminr2 / emajr2);
-      tilta = rad_to_degrees(tilta);
-      if (axrat <= 1.0e-5)
-        sense = 0;  // linear
-      else if (dfaz <= 0.)
-        sense = 1;  // right
-      else
-        sense = 2;  // left
+  // per-direction gains and polarisation over worker threads; the averaging
+  // integral's terms are kept per direction and summed in direction order
+  std::vector<double> pint_d(iavp != 0 ? ndir : 0);
+  auto analyze = [&](int, int64_t d0, int64_t d1) {
+    for (int64_t d = d0; d < d1; d++) {
+      const int cell = cell_list[d];
+      const int kth = cell % nth, kph = cell / nth;
+      const double tha = tha_list[d];
+      double ethm2 = std::norm(eth[d]);
+      double ethm = std::sqrt(ethm2);
+      double etha = rad_to_degrees(std::arg(eth[d]));
+      double ephm2 = std::norm(eph[d]);
+      double ephm = std::sqrt(ephm2);
+      double epha = rad_to_degrees(std::arg(eph[d]));
+      double tilta, emajr2, eminr2, axrat;
+      int sense;
+      if (ethm2 <= 1.0e-20 && ephm2 <= 1.0e-20) {
+        tilta = 0.;
+        emajr2 = 0.;
+        eminr2 = 0.;
+        axrat = 0.;
+        sense = 3;
+      } else {
+        double dfaz = epha - etha;
+        double dfaz2 = (epha >= 0.) ? dfaz - 360. : dfaz + 360.;
+        if (std::fabs(dfaz) > std::fabs(dfaz2)) dfaz = dfaz2;
+        double cdfaz = std::cos(degrees_to_rad(dfaz));
+        double tstor1 = ethm2 - ephm2;
+        double tstor2 = 2. * ephm * ethm * cdfaz;
+        tilta = .5 * std::atan2(tstor2, tstor1);
+        double stilta = std::sin(tilta);
+        tstor1 = tstor1 * stilta * stilta;
+        tstor2 = tstor2 * stilta * std::cos(tilta);
+        emajr2 = -tstor1 + tstor2 + ethm2;
+        eminr2 = tstor1 - tstor2 + ephm2;
+        if (eminr2 < 0.) eminr2 = 0.;
+        axrat = std::sqrt(eminr2 / emajr2);
+        tilta = rad_to_degrees(tilta);
+        if (axrat <= 1.0e-5)
+          sense = 0;  // linear
+        else if (dfaz <= 0.)
+          sense = 1;  // right
+        else
+          sense = 2;  // left
+      }
+      double gnmj = db10(gcon * emajr2);
+      double gnmn = db10(gcon * eminr2);
+      double gnv = db10(gcon * ethm2);
+      double gnh = db10(gcon * ephm2);
+      double gtot = db10(gcon * (ethm2 + ephm2));
+      double g;
+      switch (rp_norm) {
+        case 0: g = gtot; break;
+        case 1: g = gnmj; break;
+        case 2: g = gnmn; break;
+        case 3: g = gnv; break;
+        case 4: g = gnh; break;
+        default: g = gtot; break;  // 5
+      }
+      rp.gain[cell] = g;
+      if (iavp != 0) {
+        double tstor1 = gcop * (ethm2 + ephm2);
+        double tmp3 = tha - tmp2, tmp4 = tha + tmp2;
+        if (kth == 0)
+          tmp3 = tha;
+        else if (kth == nth - 1)
+          tmp4 = tha;
+        double da = std::fabs(delta_phi_rad * (std::cos(tmp3) - std::cos(tmp4)));
+        if (kph == 0 || kph == nph - 1) da *= .5;
+        pint_d[d] = tstor1 * da;
+        if (iavp == 2) continue;
+      }
+      if (rp_fmt != 1) {
+        rp.gain_vert[cell] = gnmj;
+        rp.gain_horiz[cell] = gnmn;
+      } else {
+        rp.gain_vert[cell] = gnv;
+        rp.gain_horiz[cell] = gnh;
+      }
+      ethm *= wavelength_;
+      ephm *= wavelength_;
+      if (rfld >= 1.0e-20) {
+        ethm = ethm * exrm;
+        etha = etha + exra;
+        ephm = ephm * exrm;
+        epha = epha + exra;
+      }
+      rp.e_theta[cell] = std::polar(ethm, degrees_to_rad(etha));
+      rp.e_phi[cell] = std::polar(ephm, degrees_to_rad(epha));
+      rp.gain_tot[cell] = gtot;
+      {
+        double a = axrat;
+        if (sense == 1) a = -a;
+        double gain = from_db10(gtot);
+        double lhcp_f = (1 + 2 * a + a * a) / (2 * (1 + a * a));
+        double rhcp_f = (1 - 2 * a + a * a) / (2 * (1 + a * a));
+        rp.gain_rhcp[cell] = db10(gain * rhcp_f);
+        rp.gain_lhcp[cell] = db10(gain * lhcp_f);
+      }
+      rp.axial_ratio[cell] = axrat;
+      rp.tilt[cell] = tilta;
+      rp.sense[cell] = sense;
+      rp.avg_scale[cell] = (std::sin(tha) * (nth - 1) / nth) + 1.0 / nth;
     }
-    double gnmj = db10(gcon * emajr2);
-    double gnmn = db10(gcon * eminr2);
-    double gnv = db10(gcon * ethm2);
-    double gnh = db10(gcon * ephm2);
-    double gtot = db10(gcon * (ethm2 + ephm2));
-    double g;
-    switch (rp_norm) {
-      case 0: g = gtot; break;
-      case 1: g = gnmj; break;
-      case 2: g = gnmn; break;
-      case 3: g = gnv; break;
-      case 4: g = gnh; break;
-      case 5: g = gtot; break;
-      default: fail("Unknown Gain Normalization Encountered.");
-    }
-    rp.gain[cell] = g;
-    if (iavp != 0) {
-      double tstor1 = gcop * (ethm2 + ephm2);
-      double tmp3 = tha - tmp2, tmp4 = tha + tmp2;
-      if (kth == 0)
-        tmp3 = tha;
-      else if (kth == nth - 1)
-        tmp4 = tha;
-      double da = std::fabs(delta_phi_rad * (std::cos(tmp3) - std::cos(tmp4)));
-      if (kph == 0 || kph == nph - 1) da *= .5;
-      pint += tstor1 * da;
-      if (iavp == 2) continue;
-    }
-    if (rp_fmt != 1) {
-      rp.gain_vert[cell] = gnmj;
-      rp.gain_horiz[cell] = gnmn;
-    } else {
-      rp.gain_vert[cell] = gnv;
-      rp.gain_horiz[cell] = gnh;
-    }
-    ethm *= wavelength_;
-    ephm *= wavelength_;
-    if (rfld >= 1.0e-20) {
-      ethm = ethm * exrm;
-      etha = etha + exra;
-      ephm = ephm * exrm;
-      epha = epha + exra;
-    }
-    rp.e_theta[cell] = std::polar(ethm, degrees_to_rad(etha));
-    rp.e_phi[cell] = std::polar(ephm, degrees_to_rad(epha));
-    rp.gain_tot[cell] = gtot;
-    {
-      double a = axrat;
-      if (sense == 1) a = -a;
-      double gain = from_db10(gtot);
-      double lhcp_f = (1 + 2 * a + a * a) / (2 * (1 + a * a));
-      double rhcp_f = (1 - 2 * a + a * a) / (2 * (1 + a * a));
-      rp.gain_rhcp[cell] = db10(gain * rhcp_f);
-      rp.gain_lhcp[cell] = db10(gain * lhcp_f);
-    }
-    rp.axial_ratio[cell] = axrat;
-    rp.tilt[cell] = tilta;
-    rp.sense[cell] = sense;
-    rp.avg_scale[cell] = (std::sin(tha) * (nth - 1) / nth) + 1.0 / nth;
-  }
+  };
+  parallel_chunks(ndir, host_workers(ndir, 512), analyze);
+  double pint = 0.0;
+  for (double v : pint_d) pint += v;
   if (iavp != 0) {
     double th0r = degrees_to_rad(thets);
     double th_range = degrees_to_rad(dth) * static_cast<double>(nth - 1);

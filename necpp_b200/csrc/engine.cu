@@ -1105,10 +1105,13 @@ int refine(necgpu_engine* e, int* iters, double* rel_out) {
     KLAUNCH(NECGPU_K_RESID, (double)n * n * sizeof(double2),
             residual_kernel<<<gr, 256, 0, e->stream>>>(e->Z64, e->ld, n, e->d_x, e->d_b, e->d_r, e->d_rn2));
     double rn2[2] = {0, 0};
+    int st = 0;
     CUDA_TRY(cudaMemcpyAsync(rn2, e->d_rn2, 2 * sizeof(double), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(&st, e->d_status, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
-    e->stats.d2h_bytes += 2 * sizeof(double);
+    e->stats.d2h_bytes += 2 * sizeof(double) + sizeof(int);
     kflush(e);
+    if (st & (1 << 9)) return fail(e, NECGPU_ERR_CUDA, "refinement: triangular sweep gave up waiting on a block");
     const double bn = std::sqrt(rn2[1]);
     rel = bn > 0 ? std::sqrt(rn2[0]) / bn : 0.0;
     if (!std::isfinite(rel)) {

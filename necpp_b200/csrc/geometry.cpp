@@ -3,6 +3,7 @@
 // function); the code is organised around per-segment precomputed terms
 // instead of the reference's recomputation inside every sbf/tbf call.
 #include "geometry.h"
+#include "host_parallel.h"
 
 #include <algorithm>
 #include <cmath>
@@ -397,7 +398,7 @@ void Geometry::build_connections(int ignd) {
   if (use_grid) {
     // no ground: the searches only read the coordinates, so the segments
     // are split over worker threads
-    auto search = [&](int64_t i0, int64_t i1) {
+    auto search = [&](int, int64_t i0, int64_t i1) {
       for (int64_t i = i0; i < i1; i++) {
         const V3 v1{x[i], y[i], z[i]}, v2{x2[i], y2[i], z2[i]};
         const double slen = norm3(sub(v2, v1)) * kSmin;
@@ -407,16 +408,7 @@ void Geometry::build_connections(int ignd) {
         icon2[i] = m < 0 ? 0 : ((m & 1) == 0 ? (int)((m >> 1) + 1) : -(int)((m >> 1) + 1));
       }
     };
-    const int workers = n >= 4096 ? std::max(1, std::min(8, (int)std::thread::hardware_concurrency())) : 1;
-    if (workers == 1) {
-      search(0, n);
-    } else {
-      std::vector<std::thread> pool;
-      const int64_t chunk = (n + workers - 1) / workers;
-      for (int w = 0; w < workers; w++)
-        pool.emplace_back(search, std::min<int64_t>(n, w * chunk), std::min<int64_t>(n, (w + 1) * chunk));
-      for (auto& th : pool) th.join();
-    }
+    parallel_chunks(n, host_workers(n, 512), search);
   }
   for (int64_t i = 0; i < n && !use_grid; i++) {
     int64_t iz = i + 1;
@@ -642,7 +634,7 @@ void Geometry::check_overlaps() {
   // come from a sweep along the widest axis.  visit(worker, a, p) sees each
   // candidate pair once, a < p; with the grid the items are split over
   // worker threads, each visiting the pairs of its own items.
-  const int nworkers = std::max(1, std::min(8, (int)std::thread::hardware_concurrency()));
+  const int nworkers = host_workers(2 * n, 512);
   auto grid_pairs = [&](size_t count, auto pos, double reach, int workers, auto visit) {
     if (std::isfinite(reach) && reach > 0.0 && count > 256) {
       FlatGrid grid;
@@ -670,17 +662,8 @@ void Geometry::check_overlaps() {
               }
         }
       };
-      if (workers <= 1 || count < 4096) {
-        range(0, 0, count);
-        return;
-      }
-      std::vector<std::thread> pool;
-      const size_t chunk = (count + workers - 1) / workers;
-      for (int w = 0; w < workers; w++) {
-        const size_t i0 = std::min(count, w * chunk), i1 = std::min(count, (w + 1) * chunk);
-        pool.emplace_back(range, w, i0, i1);
-      }
-      for (auto& th : pool) th.join();
+      parallel_chunks((int64_t)count, count < 4096 ? 1 : workers,
+                      [&](int w, int64_t i0, int64_t i1) { range(w, (size_t)i0, (size_t)i1); });
       return;
     }
     std::vector<size_t> order(count);

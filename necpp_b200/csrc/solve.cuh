@@ -433,29 +433,45 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
 }
 
 constexpr int kInvSweepThreads = 256;
+constexpr int kInvSweepChunk = 16;                  // solved blocks staged per pass
+constexpr unsigned long long kSweepWaitNs = 4000000000ull;  // 4 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 // LOWER: x = L^-1 b (unit lower); !LOWER: x = U^-1 b.  counter must be 0 at
-// launch.  On a wait that runs out the kernel sets bit 9 of *status and
-// every CTA returns.
+// launch; it counts the completed positions of the sweep order.
+//
+// CTA s owns block row v(s) and accumulates M[v][u] x_u over the positions
+// before it.  Thread 0 alone polls the counter, sleeping longer the further
+// the row is from the sweep front, and the solved blocks known to be
+// complete (up to 16 at a time) are staged in shared memory with one load
+// per element, so the CTAs waiting at the front do not all poll and re-read
+// the same few L2 lines.  Each thread holds the next tile row quarter in
+// registers while it multiplies the current one.  A wait that runs out sets
+// bit 9 of *status; every CTA then returns.
 template <bool LOWER>
 __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float2* M, int64_t ld, int64_t n,
                                                                      const float2* tinv, const float2* b, float2* x,
                                                                      unsigned* counter, int* status) {
-  constexpr int NB = kBlk, QW = NB / 4;  // four column quarters of 16
+  constexpr int NB = kBlk, QW = NB / 4, KX = kInvSweepChunk;  // four column quarters of 16
   __shared__ float2 part[4][NB];
   __shared__ float2 sv[NB];
-  __shared__ volatile int s_abort;
-  const int t = threadIdx.x, lane = t & 31;
+  __shared__ float2 sx[KX * NB];
+  __shared__ int s_avail;
+  const int t = threadIdx.x;
   const int r = t & (NB - 1), q = t >> 6;  // row in the block, column quarter
   const int nblk = (int)((n + NB - 1) / NB);
-  if (t == 0) s_abort = 0;
-  __syncthreads();
   for (int s = blockIdx.x; s < nblk; s += gridDim.x) {  // s: position in sweep order
     const int v = LOWER ? s : nblk - 1 - s;
     const int64_t r0 = (int64_t)v * NB;
     const int bs = (int)min((int64_t)NB, n - r0);
     const bool rowok = r < bs;
-    // this thread's 16 entries of row r of inv(T_vv)
+    // independent of the sweep: this thread's 16 entries of row r of
+    // inv(T_vv), and the right-hand side of the block
     float2 inv[QW];
     {
       const float4* ip =
@@ -467,13 +483,11 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
         inv[2 * k + 1] = make_float2(w.z, w.w);
       }
     }
-    float accr = 0.f, acci = 0.f;
-    int done = 0;  // sweep positions known to be complete
-    for (int i = 0; i < s; i++) {
+    const float2 bb = t < bs ? b[r0 + t] : make_float2(0.f, 0.f);
+    // the quarter row of the tile at sweep position i
+    auto load_tile = [&](float2 (&m)[QW], int i) {
       const int u = LOWER ? i : nblk - 1 - i;
       const int64_t c0 = (int64_t)u * NB + q * QW;
-      // the tile row is independent of x: in flight before the wait
-      float2 m[QW];
       if (rowok && c0 + QW <= n) {
         const float4* mp = reinterpret_cast<const float4*>(M + (r0 + r) * ld + c0);
 #pragma unroll
@@ -487,39 +501,65 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
         for (int k = 0; k < QW; k++)
           m[k] = (rowok && c0 + k < n) ? M[(r0 + r) * ld + c0 + k] : make_float2(0.f, 0.f);
       }
-      if (i >= done) {
-        int seen = 0;
-        if (lane == 0) {
+    };
+    float2 m[QW];
+    if (s > 0) load_tile(m, 0);
+    float accr = 0.f, acci = 0.f;
+    int avail = 0;  // positions known complete (the same in every thread)
+    for (int i0 = 0; i0 < s;) {
+      if (avail <= i0) {
+        if (t == 0) {
+          const unsigned long long t0 = global_ns();
           long long spins = 0;
-          unsigned c = ld_acquire_u32(counter);
-          while ((int)c <= i) {
-            if (s_abort || ++spins > kSweepSpinLimit) {
-              if (!s_abort) atomicOr(status, 1 << 9);
-              s_abort = 1;
+          int c = (int)ld_acquire_u32(counter);
+          while (c <= i0) {
+            if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+                global_ns() - t0 > kSweepWaitNs) {
+              atomicOr(status, 1 << 9);
+              c = -1;
               break;
             }
-            __nanosleep(32);
-            c = ld_acquire_u32(counter);
+            // the row needs position s - 1 only after s - 1 - c more blocks
+            const int ahead = s - 1 - c;
+            __nanosleep(ahead <= 0 ? 20u : (unsigned)min(ahead * 128, 2048));
+            c = (int)ld_acquire_u32(counter);
           }
-          seen = (int)c > i ? (int)c : -1;
+          s_avail = c;
         }
-        done = __shfl_sync(0xffffffffu, seen, 0);  // the same decision in every lane
-        __syncwarp();                               // x reads below are ordered after the acquire
-        if (done < 0) break;
+        __syncthreads();  // orders thread 0's acquire before the x reads below
+        avail = s_avail;
+        if (avail < 0) return;
       }
+      const int i1 = min(s, min(avail, i0 + KX));
+      for (int e = t; e < (i1 - i0) * NB; e += kInvSweepThreads) {
+        const int i = i0 + e / NB;
+        const int64_t col = (int64_t)(LOWER ? i : nblk - 1 - i) * NB + (e % NB);
+        sx[e] = col < n ? __ldcg(x + col) : make_float2(0.f, 0.f);
+      }
+      __syncthreads();
+      for (int i = i0; i < i1; i++) {
+        float2 mn[QW];
+        if (i + 1 < s) load_tile(mn, i + 1);  // in flight during this tile's products
+        const float2* xs = sx + (i - i0) * NB + q * QW;
 #pragma unroll
-      for (int k = 0; k < QW; k++) {
-        const float2 xv = c0 + k < n ? __ldcg(x + c0 + k) : make_float2(0.f, 0.f);
-        accr += m[k].x * xv.x - m[k].y * xv.y;
-        acci += m[k].x * xv.y + m[k].y * xv.x;
+        for (int k = 0; k < QW; k++) {
+          const float2 xv = xs[k];
+          accr += m[k].x * xv.x - m[k].y * xv.y;
+          acci += m[k].x * xv.y + m[k].y * xv.x;
+        }
+        if (i + 1 < s) {
+#pragma unroll
+          for (int k = 0; k < QW; k++) m[k] = mn[k];
+        }
       }
+      __syncthreads();  // sx is reused by the next pass
+      i0 = i1;
     }
     part[q][r] = make_float2(accr, acci);
     __syncthreads();
     if (t < NB) {
       float2 a = make_float2(0.f, 0.f);
       if (t < bs) {
-        const float2 bb = b[r0 + t];
         a.x = bb.x - (part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x);
         a.y = bb.y - (part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
       }
@@ -536,13 +576,12 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
     }
     part[q][r] = make_float2(accr, acci);
     __syncthreads();
-    if (t < bs && !s_abort) {
+    if (t < bs) {
       x[r0 + t] = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
                               part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
       __threadfence();
     }
     __syncthreads();
-    if (s_abort) return;
     if (t == 0) st_release_u32(counter, (unsigned)(s + 1));
   }
 }
