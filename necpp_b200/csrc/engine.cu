@@ -62,6 +62,7 @@ struct necgpu_engine {
   int factored = -1;  // precision of the factors held, -1 none
   bool filled = false;
   int* d_piv = nullptr;
+  int* d_src = nullptr;  // block-pivoted LU: gather order of each diagonal block's rows
   int* d_perm = nullptr;
 
   double* d_cand_val = nullptr;
@@ -331,6 +332,7 @@ void free_all(necgpu_engine* e) {
   e->pw_cap = 0;
   dfree(e, e->Z32);
   dfree(e, e->d_piv);
+  dfree(e, e->d_src);
   dfree(e, e->d_perm);
   dfree(e, e->d_cand_val);
   dfree(e, e->d_cand_valf);
@@ -795,6 +797,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   const int64_t n = e->n, ld = e->ld;
   const int64_t nblk = (n + kBlk - 1) / kBlk;
   if (!e->d_piv) TRY(dalloc(e, e->d_piv, (size_t)n));
+  if (!e->d_src) TRY(dalloc(e, e->d_src, (size_t)n));
   if (!e->d_dinv) TRY(dalloc(e, e->d_dinv, (size_t)nblk * kBlk));
   CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm_panel_smem<T>()));
@@ -843,7 +846,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     if (c_hi <= c_lo) return 0;
     KLAUNCH(NECGPU_K_LASWP, 0.0,
             laswp_block_kernel<T><<<(unsigned)((c_hi - c_lo + 31) / 32), 256, 0, e->stream>>>(M, ld, c_lo, c_hi, k0,
-                                                                                               kb, e->d_piv));
+                                                                                               kb, e->d_src));
     return 0;
   };
   // Outer blocks of e->outer columns (a multiple of 64) factored with 64-wide
@@ -873,7 +876,8 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       const int kb = (int)std::min<int64_t>(kBlk, n - k0);
       T* dinv = e->d_dinv + k0;
       KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
-              diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, dinv, e->d_status));
+              diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_src, dinv,
+                                                                   e->d_status));
       if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
       const int64_t r0 = k0 + kb, rest = n - r0;
       if (rest <= 0) continue;

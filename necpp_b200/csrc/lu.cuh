@@ -281,7 +281,6 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs<R> A) {
 // back to full partial pivoting if the refinement does not converge.
 
 constexpr int kBlk = 64;  // diagonal block edge
-constexpr int kDiagThreads = 256;
 
 template <typename T>
 __device__ __forceinline__ T czero() {
@@ -310,24 +309,34 @@ __device__ __forceinline__ T crecip(T b) {  // 1 / b, Smith's algorithm
 
 // LU with partial pivoting inside the kb x kb diagonal block at (k0, k0)
 // (kb <= 64), in place.  piv[k0 + c] receives the global row exchanged with
-// row k0 + c (exchanges applied in order, as LAPACK's ipiv); dinv[c]
-// receives 1 / U[c][c].
+// row k0 + c (exchanges applied in order, as LAPACK's ipiv), src[k0 + r]
+// the block row that ends up in row r (the same permutation as a gather),
+// dinv[c] 1 / U[c][c].
 //
-// Warp w owns columns w, w+8, ..., and its lanes are rows, so column access
-// is free of bank conflicts.  Step c, between two barriers: every warp
-// applies the exchange (c, p_c) to its columns and updates its columns q > c
-// with the published multipliers of column c; the owner of column c+1
-// updates that column first, then finds its pivot, exchanges and scales it,
-// and publishes p_{c+1} and the multipliers of column c+1 in the other half
-// of a double buffer.  One barrier per column.
+// Rows are not moved while factoring: the pivot of column c is chosen among
+// the rows not yet used as pivots (largest |v|^2, lowest row on ties), rows
+// already used are left alone by later updates, and the block is written
+// out in pivot order at the end, which gives the same L and U as exchanging
+// rows at every step.  The block is factored in panels of 8 columns.  Warp
+// 0 holds a 64 x 8 panel in registers (lane l: rows l and l+32) and factors
+// it with shuffles only, while the other warps apply the previous panel's
+// update to the columns beyond the current panel (lookahead).  Then all
+// warps form the panel's 8 U rows on the trailing columns (forward
+// substitution, one column per thread) and apply the K = 8 update to the
+// next panel's columns.  Three barriers per panel.
+constexpr int kDiagThreads = 256;
+constexpr int kDiagPanel = 8;
+
 template <typename T>
 __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(T* M, int64_t ld, int64_t k0, int kb, int* piv,
-                                                               T* dinv, int* status) {
+                                                               int* src, T* dinv, int* status) {
   using R = decltype(T{}.x);
-  constexpr int NB = kBlk, PER = NB * NB / kDiagThreads, NW = kDiagThreads / 32;
+  constexpr int NB = kBlk, PER = NB * NB / kDiagThreads, W = kDiagPanel;
+  constexpr unsigned FULL = 0xffffffffu;
   __shared__ T D[NB][NB + 1];
-  __shared__ T Lc[2][NB];  // multipliers of the current / next column
-  __shared__ int s_p[2];
+  __shared__ int s_seq[NB];                // physical row of pivot c
+  __shared__ int s_row_at[NB], s_pos[NB];  // interchange bookkeeping
+  __shared__ unsigned char s_used[2][NB];  // after panel j (buffer j & 1): row outside the block or a pivot
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   {
     T v[PER];  // all loads in flight before the first shared-memory store
@@ -342,152 +351,184 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(T* M, int64_t ld,
       D[e / NB][e % NB] = v[i];
     }
   }
+  if (t < NB) {
+    s_row_at[t] = t;
+    s_pos[t] = t;
+  }
   __syncthreads();
-
-  // pivot of column q over rows [q, kb), exchange within column q, scale:
-  // run by the warp that owns column q once the column is up to date
-  auto pivot_column = [&](int q) {
-    const int r0 = q + lane, r1 = q + 32 + lane;
-    R best = (R)-1;
-    int brow = q;
-    if (r0 < kb) {
-      const T v = D[r0][q];
-      const R a = v.x * v.x + v.y * v.y;
-      if (a > best) {
-        best = a;
-        brow = r0;
+  // the LAPACK interchange of pivot c, recorded in order of c by one thread
+  auto record = [&](int c) {
+    const int p = s_seq[c];
+    const int i = s_pos[p], rc = s_row_at[c];
+    piv[k0 + c] = (int)(k0 + i);
+    s_row_at[c] = p;
+    s_row_at[i] = rc;
+    s_pos[p] = c;
+    s_pos[rc] = i;
+  };
+  // columns [qa, qb) of the rows not in `used` -= (panel at pj0, width pw)
+  // times its U rows: one column and every G-th row per thread, four rows
+  // at a time
+  auto update = [&](int tid, int nthr, int pj0, int pw, const unsigned char* used, int qa, int qb) {
+    const int nq = qb - qa;
+    if (nq <= 0) return;
+    const int G = max(1, nthr / nq);
+    if (tid >= G * nq) return;
+    const int q = qa + tid % nq, g = tid / nq;
+    T u[W];
+#pragma unroll
+    for (int k = 0; k < W; k++) u[k] = k < pw ? D[s_seq[pj0 + k]][q] : czero<T>();
+    for (int r0 = g; r0 < kb; r0 += 4 * G) {
+      T acc[4];
+      bool act[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = r0 + i * G;
+        act[i] = r < kb && !used[r];
+        acc[i] = act[i] ? D[r][q] : czero<T>();
       }
-    }
-    if (r1 < kb) {
-      const T v = D[r1][q];
-      const R a = v.x * v.x + v.y * v.y;
-      if (a > best) {  // NaN never wins
-        best = a;
-        brow = r1;
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          if (act[i]) {
+            const T l = D[r0 + i * G][pj0 + k];
+            acc[i].x -= l.x * u[k].x - l.y * u[k].y;
+            acc[i].y -= l.x * u[k].y + l.y * u[k].x;
+          }
+        }
       }
-    }
-    // warp argmax: |v|^2 >= 0 orders like its bit pattern (-1: no row);
-    // the lowest lane holding the maximum supplies the row
-    const unsigned key = best >= (R)0 ? __float_as_uint((float)best) : 0u;
-    const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
-    const int src = __ffs(__ballot_sync(0xffffffffu, key == kmax && best >= (R)0)) - 1;
-    brow = src >= 0 ? __shfl_sync(0xffffffffu, brow, src) : q;
-    if (!(kmax > 0u)) {  // all zero, or no finite candidate
-      if (lane == 0) atomicOr(status, src >= 0 ? kLuStatSingular : kLuStatNonFinite);
-      brow = q;
-    }
-    const T pv = D[brow][q];  // every lane reads the pivot before the exchange
-    __syncwarp();
-    if (lane == 0 && brow != q) {
-      D[brow][q] = D[q][q];
-      D[q][q] = pv;
-    }
-    __syncwarp();
-    // 1/pv = conj(pv) / |pv|^2, with Smith's division outside the safe range
-    const R d2 = pv.x * pv.x + pv.y * pv.y;
-    T pinv;
-    if (d2 > (R)1e-30 && d2 < (R)1e30) {
-      const R rr = (R)1 / d2;
-      pinv.x = pv.x * rr;
-      pinv.y = -pv.y * rr;
-    } else {
-      pinv = crecip(pv);
-    }
-    T* L = Lc[q & 1];
-    if (r0 > q && r0 < kb) {
-      const T l = cmul(D[r0][q], pinv);
-      D[r0][q] = l;
-      L[r0] = l;
-    }
-    if (r1 < kb) {
-      const T l = cmul(D[r1][q], pinv);
-      D[r1][q] = l;
-      L[r1] = l;
-    }
-    if (lane == 0) {
-      s_p[q & 1] = brow;
-      dinv[q] = pinv;
-      piv[k0 + q] = (int)(k0 + brow);
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        if (act[i]) D[r0 + i * G][q] = acc[i];
     }
   };
-
-  if (warp == 0) pivot_column(0);
-  __syncthreads();
-  for (int c = 0; c < kb; c++) {
-    const int pc = s_p[c & 1];
-    const T* L = Lc[c & 1];
-    // 1. the exchange (c, pc) on this warp's columns (the owner of c did its own)
-    if (pc != c && lane < NB / NW) {
-      const int q = warp + NW * lane;
-      if (q < kb && q != c) {
-        const T a = D[c][q];
-        D[c][q] = D[pc][q];
-        D[pc][q] = a;
-      }
-    }
-    __syncwarp();
-    // 2. rank-1 update of this warp's columns q > c: the owner of c+1 does
-    //    that column first and pivots it, then all columns in one batch
-    const int r0 = c + 1 + lane, r1 = c + 33 + lane;
-    const T l0 = r0 < kb ? L[r0] : czero<T>();
-    const T l1 = r1 < kb ? L[r1] : czero<T>();
-    const int first = c + 1;
-    int q0 = warp;  // this warp's first column beyond c
-    if (q0 < first) q0 += (first - q0 + NW - 1) / NW * NW;
-    if (first < kb && q0 == first) {
-      const T u = D[c][first];
-      if (r0 < kb) {
-        T a = D[r0][first];
-        a.x -= l0.x * u.x - l0.y * u.y;
-        a.y -= l0.x * u.y + l0.y * u.x;
-        D[r0][first] = a;
-      }
-      if (r1 < kb) {
-        T a = D[r1][first];
-        a.x -= l1.x * u.x - l1.y * u.y;
-        a.y -= l1.x * u.y + l1.y * u.x;
-        D[r1][first] = a;
-      }
-      __syncwarp();
-      pivot_column(first);
-      q0 += NW;
-    }
-    {
-      constexpr int J = NB / NW;
-      T u[J], a0[J], a1[J];
+  // warp 0's view of the used rows: bit h for row lane + 32 h
+  unsigned used = (lane >= kb ? 1u : 0u) | (lane + 32 >= kb ? 2u : 0u);
+  for (int j0 = 0, j = 0; j0 < kb; j0 += W, j++) {
+    const int w = min(W, kb - j0);
+    if (warp == 0) {
+      T P[W][2];
 #pragma unroll
-      for (int j = 0; j < J; j++) {
-        const int q = q0 + NW * j;
-        if (q < kb) {
-          u[j] = D[c][q];
-          if (r0 < kb) a0[j] = D[r0][q];
-          if (r1 < kb) a1[j] = D[r1][q];
+      for (int k = 0; k < W; k++) {
+        P[k][0] = D[lane][j0 + k];
+        P[k][1] = D[lane + 32][j0 + k];
+      }
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        if (k >= w) break;
+        const T v0 = P[k][0], v1 = P[k][1];
+        const R m0 = v0.x * v0.x + v0.y * v0.y, m1 = v1.x * v1.x + v1.y * v1.y;
+        const bool ok0 = !(used & 1u) && m0 >= (R)0, ok1 = !(used & 2u) && m1 >= (R)0;  // NaN never wins
+        // |v|^2 >= 0 orders like its bit pattern
+        const unsigned key0 = ok0 ? __float_as_uint((float)m0) : 0u;
+        const unsigned key1 = ok1 ? __float_as_uint((float)m1) : 0u;
+        const unsigned kmax = __reduce_max_sync(FULL, key0 > key1 ? key0 : key1);
+        int p;
+        if (kmax > 0u) {
+          const unsigned b0 = __ballot_sync(FULL, ok0 && key0 == kmax);
+          const unsigned b1 = __ballot_sync(FULL, ok1 && key1 == kmax);
+          p = b0 ? __ffs(b0) - 1 : 32 + __ffs(b1) - 1;
+        } else {  // all zero, or no finite candidate: go on with the first free row
+          const unsigned any = __ballot_sync(FULL, ok0 || ok1);
+          if (lane == 0) atomicOr(status, any ? kLuStatSingular : kLuStatNonFinite);
+          const unsigned f0 = __ballot_sync(FULL, !(used & 1u)), f1 = __ballot_sync(FULL, !(used & 2u));
+          p = f0 ? __ffs(f0) - 1 : 32 + __ffs(f1) - 1;
+        }
+        const int pl = p & 31;
+        const bool ph = p >= 32;
+        // the pivot and the pivot row's later panel entries, from lane pl
+        const T ps = ph ? v1 : v0;
+        T pv, u[W];
+        pv.x = __shfl_sync(FULL, ps.x, pl);
+        pv.y = __shfl_sync(FULL, ps.y, pl);
+#pragma unroll
+        for (int k2 = k + 1; k2 < W; k2++) {
+          const T us = ph ? P[k2][1] : P[k2][0];
+          u[k2].x = __shfl_sync(FULL, us.x, pl);
+          u[k2].y = __shfl_sync(FULL, us.y, pl);
+        }
+        if (lane == pl) used |= ph ? 2u : 1u;
+        // 1/pv = conj(pv) / |pv|^2, with Smith's division outside the safe range
+        const R d2 = pv.x * pv.x + pv.y * pv.y;
+        T pinv;
+        if (d2 > (R)1e-30 && d2 < (R)1e30) {
+          const R rr = (R)1 / d2;
+          pinv.x = pv.x * rr;
+          pinv.y = -pv.y * rr;
+        } else {
+          pinv = crecip(pv);
+        }
+        if (!(used & 1u)) P[k][0] = cmul(v0, pinv);
+        if (!(used & 2u)) P[k][1] = cmul(v1, pinv);
+#pragma unroll
+        for (int k2 = k + 1; k2 < W; k2++) {
+          if (!(used & 1u)) {
+            P[k2][0].x -= P[k][0].x * u[k2].x - P[k][0].y * u[k2].y;
+            P[k2][0].y -= P[k][0].x * u[k2].y + P[k][0].y * u[k2].x;
+          }
+          if (!(used & 2u)) {
+            P[k2][1].x -= P[k][1].x * u[k2].x - P[k][1].y * u[k2].y;
+            P[k2][1].y -= P[k][1].x * u[k2].y + P[k][1].y * u[k2].x;
+          }
+        }
+        if (lane == 0) {
+          s_seq[j0 + k] = p;
+          dinv[j0 + k] = pinv;
         }
       }
 #pragma unroll
-      for (int j = 0; j < J; j++) {
-        const int q = q0 + NW * j;
-        if (q < kb) {
-          if (r0 < kb) {
-            a0[j].x -= l0.x * u[j].x - l0.y * u[j].y;
-            a0[j].y -= l0.x * u[j].y + l0.y * u[j].x;
-            D[r0][q] = a0[j];
-          }
-          if (r1 < kb) {
-            a1[j].x -= l1.x * u[j].x - l1.y * u[j].y;
-            a1[j].y -= l1.x * u[j].y + l1.y * u[j].x;
-            D[r1][q] = a1[j];
-          }
+      for (int k = 0; k < W; k++) {
+        if (k < w) {
+          D[lane][j0 + k] = P[k][0];
+          D[lane + 32][j0 + k] = P[k][1];
         }
+      }
+      s_used[j & 1][lane] = (unsigned char)(used & 1u);
+      s_used[j & 1][lane + 32] = (unsigned char)((used >> 1) & 1u);
+    } else if (j > 0) {
+      // lookahead: the previous panel's update of the columns beyond this
+      // panel, and its interchanges
+      update(t - 32, kDiagThreads - 32, j0 - W, W, s_used[(j - 1) & 1], j0 + W, kb);
+      if (t == kDiagThreads - 32)
+        for (int c = j0 - W; c < j0; c++) record(c);
+    }
+    __syncthreads();
+    const int q0 = j0 + w, nq = kb - q0;  // trailing columns
+    if (nq <= 0) continue;
+    // U rows of the panel's pivots on the trailing columns
+    if (t < nq) {
+      const int q = q0 + t;
+      T u[W];
+#pragma unroll
+      for (int i = 0; i < W; i++) {
+        if (i >= w) break;
+        const int pr = s_seq[j0 + i];
+        T v = D[pr][q];
+#pragma unroll
+        for (int k = 0; k < i; k++) {
+          const T l = D[pr][j0 + k];
+          v.x -= l.x * u[k].x - l.y * u[k].y;
+          v.y -= l.x * u[k].y + l.y * u[k].x;
+        }
+        u[i] = v;
+        D[pr][q] = v;
       }
     }
     __syncthreads();
+    // this panel's update of the next panel's columns
+    update(t, kDiagThreads, j0, w, s_used[j & 1], q0, min(kb, q0 + W));
+    __syncthreads();
   }
+  if (t == 0)
+    for (int c = (kb - 1) / W * W; c < kb; c++) record(c);  // the last panel's interchanges
+  if (t < kb) src[k0 + t] = s_seq[t];
   for (int c = kb + t; c < NB; c += kDiagThreads) dinv[c] = czero<T>();
+  // row c of the factors is physical row s_seq[c]
 #pragma unroll
   for (int i = 0; i < PER; i++) {
     const int e = t + i * kDiagThreads, r = e / NB, c = e % NB;
-    if (r < kb && c < kb) M[(k0 + r) * ld + k0 + c] = D[r][c];
+    if (r < kb && c < kb) M[(k0 + r) * ld + k0 + c] = D[s_seq[r]][c];
   }
 }
 
@@ -719,29 +760,17 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
 }
 
 // Row interchanges of a block-pivoted panel: the kb <= 64 exchanges stay
-// inside rows [k0, k0+kb), so each column is one gather of those rows.  A
-// CTA covers 32 columns of [c_lo, c_hi) with 8 row groups; all reads finish
-// (barrier) before any write.  Columns [k0, k0+kb) (the diagonal block) are
-// skipped.
+// inside rows [k0, k0+kb), so each column is one gather of those rows
+// (src[k0 + r]: the block row that ends up in row r).  A CTA covers 32
+// columns of [c_lo, c_hi) with 8 row groups; all reads finish (barrier)
+// before any write.  Columns [k0, k0+kb) (the diagonal block) are skipped.
 template <typename T>
 __global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int64_t c_lo, int64_t c_hi, int64_t k0,
-                                                          int kb, const int* piv) {
+                                                          int kb, const int* src_rows) {
   constexpr int NB = kBlk, RG = 8, PER = NB / RG;
-  __shared__ int sp[NB];
   __shared__ int src[NB];
   const int t = threadIdx.x, tx = t & 31, g = t >> 5;
-  if (t < NB) sp[t] = t < kb ? piv[k0 + t] - (int)k0 : t;
-  __syncthreads();
-  if (t == 0) {
-    // src[r]: the original row that ends up in row r
-    for (int i = 0; i < NB; i++) src[i] = i;
-    for (int c = 0; c < kb; c++) {
-      const int p = min(max(sp[c], 0), NB - 1);
-      const int a = src[c];
-      src[c] = src[p];
-      src[p] = a;
-    }
-  }
+  if (t < NB) src[t] = t < kb ? min(max(src_rows[k0 + t], 0), NB - 1) : t;
   __syncthreads();
   const int64_t col = c_lo + (int64_t)blockIdx.x * 32 + tx;
   const bool act = col < c_hi && !(col >= k0 && col < k0 + kb);
