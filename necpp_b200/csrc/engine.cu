@@ -116,6 +116,9 @@ struct necgpu_engine {
   // stream2 with lookahead_sms SMs left free for the next panel
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
+  // stream3: each inner panel's U12 solve beside its L21 solve
+  cudaStream_t stream3 = nullptr;
+  cudaEvent_t ev_u12a = nullptr, ev_u12b = nullptr;
   bool lookahead = true;
   int lookahead_sms = 48;
   bool trsm8 = true;  // U12 panel solves with eight warps per vector block (else one thread per vector)
@@ -828,6 +831,22 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       KLAUNCH(kind, fl, trsm_panel_kernel<T, false><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
     return 0;
   };
+  // U12 of an inner panel (eight-warp form) on stream st
+  auto trsm_left_on = [&](int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind, cudaStream_t st) -> int {
+    const int64_t cnt = nend - sbeg;
+    if (cnt <= 0) return 0;
+    const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
+    const int kt = kbegin(e, st);
+    trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv);
+    kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st);
+    LAUNCHED();
+    return 0;
+  };
+  if (e->trsm8 && !e->stream3) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->stream3, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_u12a, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_u12b, cudaEventDisableTiming));
+  }
   // gemm_grid: CTAs the persistent tensor-core update may take (fewer while
   // a far update runs beside the panel work)
   int gemm_grid = e->nsm;
@@ -881,10 +900,23 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
       const int64_t r0 = k0 + kb, rest = n - r0;
       if (rest <= 0) continue;
-      TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL));
       const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
+      // U12 (rows of the block, columns [r0, KE)) and L21 (rows [r0, n),
+      // the block's columns) touch disjoint parts of M: U12 runs on stream3
+      // beside L21, and the update after them waits for both
+      const bool fork = pc > 0 && e->trsm8 && e->stream3;
+      if (fork) {
+        CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
+        CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
+        TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3));
+        CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
+      }
+      TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL));
       if (pc > 0) {
-        TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
+        if (fork)
+          CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
+        else
+          TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
         TRY(gemm(r0, r0, k0, rest, pc, kb));
       }
     }
@@ -1469,6 +1501,12 @@ int necgpu_destroy(necgpu_engine* e) {
   }
   if (e->ev_fork) cudaEventDestroy(e->ev_fork);
   if (e->ev_far) cudaEventDestroy(e->ev_far);
+  if (e->stream3) {
+    cudaStreamSynchronize(e->stream3);
+    cudaStreamDestroy(e->stream3);
+  }
+  if (e->ev_u12a) cudaEventDestroy(e->ev_u12a);
+  if (e->ev_u12b) cudaEventDestroy(e->ev_u12b);
   if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return NECGPU_OK;
