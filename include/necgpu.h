@@ -300,6 +300,15 @@ int necgpu_batch_solve(necgpu_engine* e, int nprob, const necgpu_structure* stru
 int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, double* max_abs_diff,
                          double* max_abs_ref);
 
+/* Self-check of the block-pivoted complex64 LU of the mixed path: factors a
+ * seeded random n x n matrix (n <= 4096) on the engine's buffers and reports
+ * the componentwise backward error max |P A - L U|_ij / (|L| |U|)_ij, max |A|
+ * and how many of the n interchanges moved a row.  The engine must hold no
+ * structure, and holds none afterwards.  Test support; it has no counterpart
+ * in the reference. */
+int necgpu_check_block_lu(necgpu_engine* e, int n, unsigned seed, double* backward_err, double* max_abs,
+                          int* interchanges);
+
 #ifdef __cplusplus
 }
 #endif

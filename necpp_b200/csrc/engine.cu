@@ -1839,6 +1839,74 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
   return rc;
 }
 
+// Componentwise backward error of the factors F of P A (L unit lower, U
+// upper; P A row i = A row perm[i]): max over i, j of
+// |(P A - L U)_ij| / sum_k |L_ik| |U_kj| (|.|: |re| + |im|), and max |A|.
+__global__ void lu_residual_kernel(const float2* A, const float2* F, const int* perm, int64_t ld, int64_t n,
+                                   float* out) {
+  float mx = 0.f, ref = 0.f;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e / n, j = e - i * n;
+    const int64_t kend = i < j ? i : j;
+    float sr = 0.f, si = 0.f, sa = 0.f;
+    for (int64_t k = 0; k <= kend; k++) {
+      const float2 l = k == i ? make_float2(1.f, 0.f) : F[i * ld + k];
+      const float2 u = F[k * ld + j];
+      sr += l.x * u.x - l.y * u.y;
+      si += l.x * u.y + l.y * u.x;
+      sa += (fabsf(l.x) + fabsf(l.y)) * (fabsf(u.x) + fabsf(u.y));
+    }
+    const float2 a = A[(int64_t)perm[i] * ld + j];
+    const float d = fabsf(a.x - sr) + fabsf(a.y - si);
+    if (sa > 0.f) mx = fmaxf(mx, d / sa);
+    ref = fmaxf(ref, fabsf(a.x) + fabsf(a.y));
+  }
+  atomicMax((int*)out, __float_as_int(mx));
+  atomicMax((int*)out + 1, __float_as_int(ref));
+}
+
+int necgpu_check_block_lu(necgpu_engine* e, int n, unsigned seed, double* backward_err, double* max_abs,
+                          int* interchanges) {
+  if (!e || n < 1 || n > 4096 || !backward_err || !max_abs || !interchanges) return NECGPU_ERR_ARG;
+  if (e->n > 0) return fail(e, NECGPU_ERR_ARG, "check_block_lu: needs an engine without a structure");
+  CUDA_TRY(cudaSetDevice(e->device));
+  // the factorisation runs on the engine's own buffers, as for a structure
+  // of n unknowns; the engine is left without a structure afterwards
+  e->n = n;
+  e->ld = (n + 63) / 64 * 64;
+  const int64_t ld = e->ld, cnt = (int64_t)n * ld;
+  float2* A = nullptr;
+  float* d = nullptr;
+  int rc = dalloc(e, e->Z32, (size_t)cnt);
+  if (!rc) rc = dalloc(e, A, (size_t)cnt);
+  if (!rc) rc = dalloc(e, d, 2);
+  if (!rc) {
+    fill_random_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(e->Z32, cnt, seed);
+    cudaMemcpyAsync(A, e->Z32, cnt * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream);
+    cudaMemsetAsync(d, 0, 2 * sizeof(float), e->stream);
+    cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream);
+    rc = run_lu_blockpiv(e, e->Z32);
+    if (!rc) {
+      lu_residual_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(A, e->Z32, e->d_perm, ld, n, d);
+      float h[2] = {0, 0};
+      std::vector<int> piv(n);
+      cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, e->stream);
+      cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream);
+      const cudaError_t ce = cudaStreamSynchronize(e->stream);
+      if (ce != cudaSuccess) rc = fail(e, NECGPU_ERR_CUDA, cudaGetErrorString(ce));
+      int moved = 0;
+      for (int k = 0; k < n; k++) moved += piv[k] != k;
+      *backward_err = h[0];
+      *max_abs = h[1];
+      *interchanges = moved;
+    }
+  }
+  dfree(e, A);
+  dfree(e, d);
+  free_all(e);
+  return rc;
+}
+
 int necgpu_set_loads(necgpu_engine* e, const double* zload) {
   if (!e) return NECGPU_ERR_ARG;
   if (e->n <= 0) return fail(e, NECGPU_ERR_ARG, "set_loads: no structure set");

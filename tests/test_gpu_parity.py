@@ -284,6 +284,32 @@ def test_excitation_only_resolve_and_pattern_reuse(nb, api, oracle):
     nb.nec_delete(c2)
 
 
+@pytest.mark.parametrize("n,seed", [(64, 1), (200, 2), (333, 3), (700, 4), (1100, 5)])
+def test_block_pivoted_lu_backward_error(nb, n, seed):
+    """The mixed path's block-pivoted complex64 LU on seeded random matrices
+    (pivoting inside every diagonal block; n not a multiple of 64; n > 256
+    brings in the outer blocks, the far update beside the panels and the U12
+    solves beside L21): P A = L U with a componentwise backward error at the
+    FP32 / split-BF16 level, against O(1) for a wrong interchange or update."""
+    import ctypes as C
+    from gpu_helpers import Engine
+    L = nb.lib
+    L.necgpu_check_block_lu.argtypes = [C.c_void_p, C.c_int, C.c_uint, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    e = Engine(L)
+    try:
+        berr, amax, moved = C.c_double(), C.c_double(), C.c_int()
+        rc = L.necgpu_check_block_lu(e.h, n, seed, C.byref(berr), C.byref(amax), C.byref(moved))
+        assert rc == 0, e.err()
+        assert amax.value > 0.1
+        assert moved.value > n // 4  # random blocks: most pivots come from another row
+        assert berr.value <= 5e-4, berr.value
+        # the engine holds no structure afterwards
+        assert L.necgpu_fill(e.h) != 0 and "no structure" in e.err()
+    finally:
+        e.close()
+
+
 def test_engine_rejects_bad_calls(nb):
     from gpu_helpers import Engine
     e = Engine(nb.lib)
