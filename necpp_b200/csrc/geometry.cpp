@@ -294,6 +294,7 @@ struct FlatGrid {
   std::vector<int64_t> order;                  // item ids sorted by cell key
   std::vector<uint64_t> slot_key;              // table: key + 1 (0 = empty)
   std::vector<std::pair<int64_t, int64_t>> slot_range;
+  std::vector<uint32_t> slot_of, used;  // build scratch: each item's slot, the occupied slots
   uint64_t mask = 0;
   static uint64_t hash(uint64_t k) {  // splitmix64 finaliser
     k ^= k >> 30;
@@ -314,19 +315,20 @@ struct FlatGrid {
     mask = cap - 1;
     slot_key.assign(cap, 0);
     slot_range.assign(cap, {0, 0});
-    std::vector<uint32_t> slot_of(count);
+    slot_of.resize(count);
+    used.clear();
     for (size_t i = 0; i < count; i++) {
       const V3 v = pos(i);
       const uint64_t k = EndGrid::key(EndGrid::idx(v.x, c), EndGrid::idx(v.y, c), EndGrid::idx(v.z, c));
       uint64_t h = hash(k) & mask;
       while (slot_key[h] && slot_key[h] != k + 1) h = (h + 1) & mask;
+      if (!slot_key[h]) used.push_back((uint32_t)h);
       slot_key[h] = k + 1;
       slot_range[h].second++;
       slot_of[i] = (uint32_t)h;
     }
     int64_t at = 0;
-    for (size_t h = 0; h < cap; h++) {
-      if (!slot_key[h]) continue;
+    for (const uint32_t h : used) {
       const int64_t cnt = slot_range[h].second;
       slot_range[h] = {at, at};
       at += cnt;
@@ -360,7 +362,11 @@ void Geometry::build_connections(int ignd) {
   for (int64_t i = 0; i < n; i++)
     max_slen = std::max(max_slen, norm3(sub(V3{x2[i], y2[i], z2[i]}, V3{x[i], y[i], z[i]})) * kSmin);
   const bool use_grid = ignd == 0 && n > 256 && std::isfinite(max_slen) && max_slen > 0.0;
-  FlatGrid grid;
+  // kept per thread between calls: a new structure reuses the mapped buffers.
+  // Worker threads reach it through the reference (naming the thread_local
+  // inside their lambdas would give them their own, empty, instances).
+  static thread_local FlatGrid tl_grid;
+  FlatGrid& grid = tl_grid;
   if (use_grid)
     grid.build((size_t)(2 * n), 2.0 * max_slen, [&](size_t code) {
       const int64_t i = (int64_t)(code >> 1);
@@ -637,7 +643,10 @@ void Geometry::check_overlaps() {
   const int nworkers = host_workers(2 * n, 512);
   auto grid_pairs = [&](size_t count, auto pos, double reach, int workers, auto visit) {
     if (std::isfinite(reach) && reach > 0.0 && count > 256) {
-      FlatGrid grid;
+      // reused by the two searches and by later structures; workers use the
+      // reference, not the thread_local name
+      static thread_local FlatGrid tl_pair_grid;
+      FlatGrid& grid = tl_pair_grid;
       const double cell = 2.0 * reach;
       grid.build(count, cell, pos);
       const double r2 = reach * reach * 3.0;
