@@ -592,8 +592,16 @@ void Geometry::check_overlaps() {
     double r;
     int tag;
   };
-  std::vector<End> ends;
-  std::vector<View> views;
+  // per-thread scratch kept between structures (the pages stay mapped);
+  // worker threads reach it through these references
+  static thread_local std::vector<End> tl_ends;
+  static thread_local std::vector<View> tl_views;
+  static thread_local std::vector<int64_t> tl_parent;
+  static thread_local std::vector<std::pair<int64_t, int64_t>> tl_nodes;
+  std::vector<End>& ends = tl_ends;
+  std::vector<View>& views = tl_views;
+  ends.clear();
+  views.clear();
   ends.reserve(2 * n);
   views.reserve(n);
   for (int64_t i = 0; i < n; i++) {
@@ -622,7 +630,8 @@ void Geometry::check_overlaps() {
   auto coord = [](const V3& v, int ax) { return ax == 0 ? v.x : (ax == 1 ? v.y : v.z); };
 
   // node classes (union-find over ends)
-  std::vector<int64_t> parent(2 * n);
+  std::vector<int64_t>& parent = tl_parent;
+  parent.resize(2 * n);
   std::iota(parent.begin(), parent.end(), 0);
   auto root = [&](int64_t e) {
     while (parent[e] != e) {
@@ -702,7 +711,8 @@ void Geometry::check_overlaps() {
     for (auto& lst : touch)
       for (auto& pr : lst) parent[root(ends[pr.second].idx)] = root(ends[pr.first].idx);
   }
-  std::vector<std::pair<int64_t, int64_t>> nodes(n);
+  std::vector<std::pair<int64_t, int64_t>>& nodes = tl_nodes;
+  nodes.resize(n);
   for (int64_t i = 0; i < n; i++) nodes[i] = {root(2 * i), root(2 * i + 1)};
   auto one_node = [&](int64_t s, int64_t t) {
     auto& A = nodes[s];
