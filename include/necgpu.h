@@ -230,17 +230,25 @@ int necgpu_read_resident(necgpu_engine* e, double* cur, double* eth, double* eph
  * its inner loop, where a cudaMalloc can fail or fragment that pool and a
  * cudaFree waits for the whole device, stalling the caller's other streams.
  *
+ * Each buffer must lie inside one device allocation: one that runs past the
+ * end of its allocation is rejected with NECGPU_ERR_ARG.  A sub-allocation of
+ * a caching allocator (PyTorch's, say) can only be checked against the end of
+ * the segment that holds it, so the lengths above stay the caller's duty.
+ *
  * The first call on a device does the set-up, with that device current:
  * it looks up the static array, zeroes the sweep flag words (they must start
- * at zero; nothing else in the array needs to), and sets the kernels'
+ * at zero; nothing else in the array needs to), loads every kernel the call
+ * can launch in either precision (under CUDA's lazy module loading a kernel
+ * takes device memory when it is first loaded), and sets the kernels'
  * attributes.  Make that first call before any stream capture.  The work
  * runs on the engine's stream; the call returns when it has finished
  * (mixed refinement also waits once per refinement step).  The engine's own
  * solution (for necgpu_pattern) is left as it was.
  *
- * All engines on one device share the one array: calls that overlap in time
- * on the same device (from two threads, or two engines on different
- * streams) race on it and give wrong results.  Serialise them.
+ * All engines on one device share the one array and its host-side sweep
+ * counter: calls that overlap in time on the same device (from two threads,
+ * or two engines on different streams) race on the array and give wrong
+ * results.  Serialise them.
  *
  * If the mixed refinement stalls on block-pivoted factors, the call fails
  * with NECGPU_ERR_REFINE instead of refactoring (which would allocate);

@@ -2622,10 +2622,43 @@ struct NoAllocDevice {
 NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 std::mutex g_noalloc_mutex;
 
+// Every kernel the allocation-free solve can launch, FP64 and mixed.  With
+// CUDA's lazy module loading (the default since CUDA 12.2) a kernel's code is
+// loaded, and device memory taken for it, on its first launch; querying its
+// attributes loads it, so the set-up touches each of them once.
+int noalloc_preload(necgpu_engine* e) {
+  const void* kernels[] = {
+      (const void*)trsv_sweep_kernel<float2, true>,  (const void*)trsv_sweep_kernel<float2, false>,
+      (const void*)trsv_sweep_kernel<double2, true>, (const void*)trsv_sweep_kernel<double2, false>,
+      (const void*)permute_kernel<double2, double2>, (const void*)permute_kernel<float2, double2>,
+      (const void*)norm2_kernel,                     (const void*)axpy_kernel<float2>,
+      (const void*)residual_kernel,                  (const void*)coeff_kernel};
+  for (const void* k : kernels) {
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k));
+  }
+  return 0;
+}
+
+// The driver's cuMemGetAddressRange (base and size of the allocation that
+// holds a device address), looked up once through the runtime.
+typedef CUresult (*AddressRangeFn)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddressRangeFn address_range() {
+  static AddressRangeFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (AddressRangeFn)p;
+  }
+  return fn;
+}
+
 // Once per device, with that device current: look up the scratch array,
 // zero its flag words (a sweep waits for a flag equal to its epoch, and the
-// first epoch is 1), set the sweep kernels' shared-memory limits and size
-// their cooperative grids.
+// first epoch is 1), load every kernel of the path, set the sweep kernels'
+// shared-memory limits and size their cooperative grids.
 int noalloc_setup(necgpu_engine* e, NoAllocDevice** out) {
   if (e->device < 0 || e->device >= kNoAllocMaxDevices)
     return fail(e, NECGPU_ERR_ARG, "solve_noalloc: device index beyond the per-device table");
@@ -2651,6 +2684,8 @@ int noalloc_setup(necgpu_engine* e, NoAllocDevice** out) {
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], trsv_sweep_kernel<double2, true>,
                                                            kSweepThreads, dsm64));
     if (per_sm[0] < 1 || per_sm[1] < 1) return fail(e, NECGPU_ERR_CUDA, "solve_noalloc: sweep kernel cannot be resident");
+    TRY(noalloc_preload(e));
+    if (!address_range()) return fail(e, NECGPU_ERR_CUDA, "solve_noalloc: cuMemGetAddressRange unavailable");
     unsigned char* base = static_cast<unsigned char*>(p);
     CUDA_TRY(cudaMemsetAsync(base + kNoAllocOffFlags, 0, kNoAllocFlagBytes, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
@@ -2678,7 +2713,11 @@ int noalloc_sweeps(necgpu_engine* e, NoAllocDevice& d, const T* M, T* rhs, T* so
     d.epoch = 0;
   }
   for (int pass = 0; pass < 2; pass++) {
-    int epoch = ++d.epoch;
+    int epoch;
+    {
+      std::lock_guard<std::mutex> lock(g_noalloc_mutex);  // the epoch counter is shared by the device's engines
+      epoch = ++d.epoch;
+    }
     const T* src = pass == 0 ? rhs : sol;
     T* dst = pass == 0 ? sol : rhs;
     void* args[] = {(void*)&M, (void*)&ld, (void*)&n, (void*)&src, (void*)&dst, (void*)&flags, (void*)&epoch,
@@ -2699,7 +2738,15 @@ int noalloc_device_buffer(necgpu_engine* e, const void* p, size_t bytes, size_t 
   CUDA_TRY(cudaPointerGetAttributes(&at, p));
   if ((at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged) || at.device != e->device)
     return fail(e, NECGPU_ERR_ARG, std::string("solve_noalloc: ") + what + " is not device memory of the engine's device");
-  (void)bytes;
+  // the buffer must end inside the allocation that holds its start (a
+  // caching allocator's sub-allocation is checked against its segment only)
+  CUdeviceptr base = 0;
+  size_t size = 0;
+  if (address_range()(&base, &size, (CUdeviceptr)p) != CUDA_SUCCESS)
+    return fail(e, NECGPU_ERR_ARG, std::string("solve_noalloc: ") + what + " is not inside a device allocation");
+  if ((CUdeviceptr)p - base + bytes > size)
+    return fail(e, NECGPU_ERR_ARG, std::string("solve_noalloc: ") + what + " ends beyond its allocation (needs " +
+                                       std::to_string(bytes) + " bytes)");
   return 0;
 }
 
@@ -2723,6 +2770,8 @@ int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_de
   if (e->factored != NECGPU_FP64 && e->factored != NECGPU_MIXED)
     return fail(e, NECGPU_ERR_ARG, "solve_noalloc: no factorisation held");
   CUDA_TRY(cudaSetDevice(e->device));
+  NoAllocDevice* d = nullptr;
+  TRY(noalloc_setup(e, &d));
   const size_t vec = (size_t)n * sizeof(double2);
   TRY(noalloc_device_buffer(e, rhs_dev, vec, 16, "rhs"));
   TRY(noalloc_device_buffer(e, cur_dev, vec, 16, "cur"));
@@ -2730,8 +2779,6 @@ int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_de
   if (overlaps(rhs_dev, vec, cur_dev, vec) || (abc_dev && (overlaps(abc_dev, 48 * (size_t)n, rhs_dev, vec) ||
                                                            overlaps(abc_dev, 48 * (size_t)n, cur_dev, vec))))
     return fail(e, NECGPU_ERR_ARG, "solve_noalloc: rhs, cur and abc must not overlap");
-  NoAllocDevice* d = nullptr;
-  TRY(noalloc_setup(e, &d));
   unsigned char* base = d->base;
   double2* x = reinterpret_cast<double2*>(base + kNoAllocOffX);
   double2* r = reinterpret_cast<double2*>(base + kNoAllocOffR);

@@ -77,7 +77,8 @@ def helix_geometry():
     return a, s, 6.0 * s
 
 
-def helix_array(api, ctx, k=8, seed=0, nseg=180, pattern=PATTERN_91x72, freq_mhz=1000.0):
+def helix_array(api, ctx, k=8, seed=0, nseg=180, pattern=PATTERN_91x72, freq_mhz=1000.0, execute=True):
+    """execute=False stops after the EX cards (no XQ or RP card)."""
     c = lambda r, w: _check(api, ctx, r, w)
     a, s, hl = helix_geometry()
     c(api.helix(ctx, 1, nseg, s, hl, a, a, a, a, 1e-3), "helix")
@@ -89,6 +90,8 @@ def helix_array(api, ctx, k=8, seed=0, nseg=180, pattern=PATTERN_91x72, freq_mhz
     phases = np.random.default_rng(seed).uniform(0.0, 2.0 * math.pi, size=k * k)
     for t in range(k * k):
         c(api.nec_ex_card(ctx, 0, t + 1, 1, 0, math.cos(phases[t]), math.sin(phases[t]), 0.0, 0.0, 0.0, 0.0), "ex")
+    if not execute:
+        return k * k * nseg
     if pattern is not None:
         c(api.nec_rp_card(ctx, *pattern), "rp")
     else:

@@ -238,3 +238,25 @@ CASES = {
     "yagi_fields_reflection": (_yagi_fields_reflection, (10, 4)),
     "yagi_fields_perfect": (_yagi_fields_perfect, (10, 4)),
 }
+
+
+def _helix_array_8x8(api, ctx):
+    """The benchmark workload: 8 x 8 axial-mode helix array, N = 11520,
+    1 GHz, 64 feeds with seeded phases (seed 0), 91 x 72 pattern."""
+    W.helix_array(api, ctx, k=8, seed=0)
+    return 1000.0
+
+
+def _wire_mesh_41(api, ctx):
+    """Square wire mesh, 41 + 41 wires of 40 segments (N = 3280, 4-way
+    junctions at the crossings), 150 MHz, plane wave at theta 30 deg,
+    theta-polarised, bistatic 181 x 72 pattern."""
+    W.wire_mesh(api, ctx)
+    return 150.0
+
+
+# full-size workloads: compact fixtures (no full Z, no host tables)
+LARGE_CASES = {
+    "helix_array_8x8": (_helix_array_8x8, (91, 72)),
+    "wire_mesh_41": (_wire_mesh_41, (181, 72)),
+}

@@ -9,9 +9,11 @@ coefficients, and the unfactored interaction matrix (full for N <= 200,
 otherwise a seeded sample of elements).
 
     make -C oracle ref && python tests/golden/make_golden.py
+    python tests/golden/make_golden.py helix_array_8x8 wire_mesh_41   # full size
 """
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -20,18 +22,25 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
+from oracle import refwrap  # noqa: E402
 from oracle.refwrap import RefAPI  # noqa: E402
-from cases import CASES  # noqa: E402
+from cases import CASES, LARGE_CASES  # noqa: E402
 
 
-def collect(ref, name, builder, grid):
+def collect(ref, name, builder, grid, compact=False):
+    """compact (the full-size workloads): no segment arrays, basis tables or
+    current coefficients (the host tables are compared with the live
+    reference by the CPU tests), Z as a sample plus its diagonal."""
     ctx = ref.nec_create()
+    t0 = time.perf_counter()
     builder(ref, ctx)
+    t_solve = time.perf_counter() - t0
     out = {}
     seg = ref.segments(ctx)
     n = len(seg["x"])
-    for k, v in seg.items():
-        out["seg_" + k] = v
+    if not compact:
+        for k, v in seg.items():
+            out["seg_" + k] = v
     out["wavelength"] = np.array(ref.ref_wavelength(ctx))
     # antenna inputs
     zin = []
@@ -74,17 +83,18 @@ def collect(ref, name, builder, grid):
     # last solution
     cur, abc = ref.currents(ctx)
     out["current_vector"] = cur
-    out["abc"] = abc
-    # trio tables at the last frequency scaling
-    ptr, basis, coef = [0], [], []
-    for j in range(1, n + 1):
-        jco, ax, bx, cx = ref.trio(ctx, j)
-        basis.extend(jco.tolist())
-        coef.extend(zip(ax, bx, cx))
-        ptr.append(len(basis))
-    out["trio_ptr"] = np.array(ptr, dtype=np.int32)
-    out["trio_basis"] = np.array(basis, dtype=np.int32)
-    out["trio_abc"] = np.array(coef, dtype=np.float64).reshape(-1, 3)
+    if not compact:
+        out["abc"] = abc
+        # trio tables at the last frequency scaling
+        ptr, basis, coef = [0], [], []
+        for j in range(1, n + 1):
+            jco, ax, bx, cx = ref.trio(ctx, j)
+            basis.extend(jco.tolist())
+            coef.extend(zip(ax, bx, cx))
+            ptr.append(len(basis))
+        out["trio_ptr"] = np.array(ptr, dtype=np.int32)
+        out["trio_basis"] = np.array(basis, dtype=np.int32)
+        out["trio_abc"] = np.array(coef, dtype=np.float64).reshape(-1, 3)
     # Sommerfeld tables of the last frequency (zero when the case has none)
     tab, eps = ref.somm_tables(ctx)
     if np.any(tab != 0):
@@ -93,7 +103,9 @@ def collect(ref, name, builder, grid):
     # interaction matrix (refilled by the reference's cmset, its table
     # interpolation cache reset to the state of a new context)
     ref.ref_somm_interp_reset(ctx)
+    t0 = time.perf_counter()
     z = ref.fill(ctx)
+    t_fill = time.perf_counter() - t0
     if n <= 200:
         out["Z"] = z
     else:
@@ -104,15 +116,23 @@ def collect(ref, name, builder, grid):
         out["Z_diag"] = np.diag(z).copy()
     out["n"] = np.array(n)
     ref.nec_delete(ctx)
+    print("  %s: reference solve %.1f s, refill %.1f s" % (name, t_solve, t_fill), flush=True)
     return out
 
 
 def main():
-    ref = RefAPI()
-    names = sys.argv[1:] or list(CASES)
-    for name in names:
-        builder, grid = CASES[name]
-        out = collect(ref, name, builder, grid)
+    # the full-size workloads run the reference's OpenMP build (Eigen's LU
+    # over all cores); its results agree with the one-thread build to
+    # rounding, far inside the parity tolerances
+    args = sys.argv[1:]
+    large = [a for a in args if a in LARGE_CASES]
+    names = [a for a in args if a not in LARGE_CASES] if args else list(CASES)
+    jobs = [(nm, CASES[nm], False) for nm in names] + [(nm, LARGE_CASES[nm], True) for nm in large]
+    refs = {}
+    for name, (builder, grid), compact in jobs:
+        if compact not in refs:
+            refs[compact] = RefAPI(omp=compact and refwrap.available(omp=True))
+        out = collect(refs[compact], name, builder, grid, compact=compact)
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **out)
         print("%-22s N=%-5d zin=%s -> %s (%d KB)" % (name, int(out["n"]), out["zin"].shape,

@@ -6,6 +6,9 @@ sweep epochs, so a stale flag word or an uncleared vector shows up as a
 mismatch.  The file is named to be collected last, and also runs alone.
 """
 import ctypes as C
+import os
+import subprocess
+import sys
 
 import numpy as np
 import pytest
@@ -104,3 +107,85 @@ def test_noalloc_rejects_beyond_static_limit(nb, engine):
     rc = _noalloc(engine, rhs_t, cur_t, None)
     assert rc == 2
     assert "16384" in engine.err()
+
+
+def test_noalloc_rejects_buffer_past_its_allocation(nb, engine):
+    """A right-hand side that runs 16 bytes past the end of its cudaMalloc
+    allocation is refused (the extent comes from cuMemGetAddressRange)."""
+    import torch
+    ctx, st, rhs, _ = host_case(nb, CASES["helix2"][0])
+    n = st["n"]
+    engine.set_structure(st)
+    engine.fill()
+    engine.factor(0)
+    torch.cuda.init()
+    rt = C.CDLL("libcudart.so.12")  # the runtime torch has loaded
+    rt.cudaMalloc.argtypes = [C.POINTER(C.c_void_p), C.c_size_t]
+    rt.cudaFree.argtypes = [C.c_void_p]
+    size = 2 << 20
+    vec = 16 * n
+    base = C.c_void_p()
+    assert rt.cudaMalloc(C.byref(base), size) == 0
+    try:
+        cur = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        inside = base.value + size - vec
+        rc = engine.lib.necgpu_solve_noalloc(engine.h, C.c_void_p(inside), C.c_void_p(cur.data_ptr()), None)
+        assert rc == 0, engine.err()
+        rc = engine.lib.necgpu_solve_noalloc(engine.h, C.c_void_p(inside + 16), C.c_void_p(cur.data_ptr()), None)
+        assert rc == 2 and "beyond its allocation" in engine.err()
+    finally:
+        torch.cuda.synchronize()
+        rt.cudaFree(base)
+    nb.nec_delete(ctx)
+
+
+_FRESH = r"""
+import ctypes as C, sys
+import numpy as np, torch
+import necpp_b200 as nb
+from cases import CASES
+from gpu_helpers import Engine
+from helpers import host_case
+e = Engine(nb.lib)
+nb.lib.necgpu_solve_noalloc.argtypes = [C.c_void_p] * 4
+ctx, st, rhs, _ = host_case(nb, CASES["helix2"][0])
+n = st["n"]
+rhs_t = torch.from_numpy(np.ascontiguousarray(rhs, dtype=np.complex128).view(np.float64)).cuda()
+cur_t = torch.zeros(2 * n, dtype=torch.float64, device="cuda")
+abc_t = torch.zeros(6 * n, dtype=torch.float64, device="cuda")
+def call():
+    torch.cuda.synchronize()
+    rc = nb.lib.necgpu_solve_noalloc(e.h, rhs_t.data_ptr(), cur_t.data_ptr(), abc_t.data_ptr())
+    assert rc == 0, e.err()
+e.set_structure(st)
+e.fill()
+e.factor(0)
+call()                      # first call on the device: the set-up
+e.factor(1)                 # mixed factors; no mixed solve has run in this process
+torch.cuda.synchronize()
+free0, reserved0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+call()                      # mixed refinement kernels, loaded by the set-up
+free1, reserved1 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
+assert free1 == free0, ("device memory taken by the second call", free0 - free1)
+assert reserved1 == reserved0
+c = cur_t.cpu().numpy()
+cur_ref, _ = e.solve(rhs)
+err = np.max(np.abs(c[0::2] + 1j * c[1::2] - cur_ref)) / np.max(np.abs(cur_ref))
+assert err <= 1e-10, err
+print("fresh-process noalloc ok", err)
+"""
+
+
+def test_noalloc_allocates_nothing_after_the_first_call():
+    """In a fresh process (lazy module loading as by default): FP64 factors,
+    the first call (set-up), then mixed factors with no mixed solve run
+    before; the second call must leave the device's free memory and
+    PyTorch's reserved memory unchanged and match necgpu_solve."""
+    here = os.path.dirname(os.path.abspath(__file__))
+    env = dict(os.environ)
+    env["PYTHONPATH"] = os.pathsep.join([os.path.dirname(here), here, env.get("PYTHONPATH", "")])
+    env.pop("CUDA_MODULE_LOADING", None)
+    r = subprocess.run([sys.executable, "-c", _FRESH], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    assert "fresh-process noalloc ok" in r.stdout
