@@ -429,6 +429,7 @@ def run_b200(args):
     L.necgpu_last_error.restype = C.c_char_p
     L.necgpu_last_error.argtypes = [C.c_void_p]
     L.necgpu_read_resident.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.necgpu_measure_peak.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double)]
 
     class API:
         def __getattr__(self, k):
@@ -518,6 +519,20 @@ def run_b200(args):
         ms_f_max = max_over_ranks(ms_f)
         _, st_f, _, _ = timed(eng_f, 0, 1, 0, None, level=2)
         out["fp64_kernels_ms_per_step"] = {K_NAMES[i]: st_f.k_ms[i] for i in range(9) if st_f.k_launches[i]}
+        # measured FP64 peaks (register-only loops) and the FP64 path's update against them
+        pk = {}
+        for kind, nm in ((0, "fp64_fma"), (1, "fp64_tensor_mma")):
+            v = C.c_double(0.0)
+            check(eng_f, L.necgpu_measure_peak(eng_f, kind, C.byref(v)))
+            pk[nm] = v.value
+        out["fp64_peaks_tflops"] = pk
+        gi = K_NAMES.index("lu_gemm")
+        if st_f.k_launches[gi]:
+            ach = st_f.k_flops[gi] / (st_f.k_ms[gi] * 1e-3) / 1e12
+            out["fp64_roofline"] = {"kernel": "gemm_dmma_kernel (FP64 trailing update)", "achieved": ach,
+                                    "peak": pk["fp64_tensor_mma"], "unit": "TFLOP/s",
+                                    "frac": ach / pk["fp64_tensor_mma"],
+                                    "peak_source": "measured here: mma.sync m8n8k4 f64 register loop"}
         nb.nec_delete(ctx_f)
 
     # ---- end to end through the C API (host buffers)

@@ -308,6 +308,54 @@ int necgpu_batch_solve(necgpu_engine* e, int nprob, const necgpu_structure* stru
 int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, double* max_abs_diff,
                          double* max_abs_ref);
 
+/* ---- tuning of the mixed-precision LU (no counterpart in the reference,
+ * whose Eigen LU has fixed blocking, src/matrix_algebra.cpp:243-251) ----
+ *
+ * outer          columns per outer block of the block-pivoted LU: 64-wide
+ *                inner panels inside it, one tensor-core trailing update of
+ *                inner dimension `outer` per block (multiple of 64, 64..1024)
+ * lookahead_sms  SMs kept for the next outer block's panels while the far
+ *                part of the trailing update runs beside them (0: no
+ *                lookahead; at most 127)
+ * gemm_group     m-tiles per band of the tensor-core update's tile walk
+ *                (1..1024)
+ *
+ * The values a factorisation uses are, in order of precedence: the
+ * environment (NECPP_B200_OUTER, NECPP_B200_LOOKAHEAD_SMS,
+ * NECPP_B200_LOOKAHEAD=0, NECPP_B200_GEMM_GROUP), an explicit
+ * necgpu_set_tuning, the row of the tuning table for the precision and n,
+ * the built-in defaults (256, 48, 16).  The tuning table is the text file
+ * tuning.tsv beside the library (written by the autotuner,
+ * necpp_b200/tune.py), or the file named by NECPP_B200_TUNING ("none": no
+ * table).  Its rows are "precision n_max outer lookahead_sms gemm_group
+ * [measurement]" with precision "mixed" or "fp64"; a size uses the row with
+ * the smallest n_max >= n, else the row with the largest n_max. */
+typedef struct necgpu_tuning {
+  int outer;
+  int lookahead_sms;
+  int gemm_group;
+} necgpu_tuning;
+
+/* Fix the engine's tuning (NULL: back to the table and defaults). */
+int necgpu_set_tuning(necgpu_engine* e, const necgpu_tuning* t);
+
+/* The tuning a factorisation of n unknowns in `precision` would use now. */
+int necgpu_get_tuning(const necgpu_engine* e, int precision, int64_t n, necgpu_tuning* out);
+
+/* Host-only lookup in a tuning table (path NULL: the library's table, as
+ * above).  Returns 0 and fills *out when a row applies, NECGPU_ERR_ARG when
+ * the table is missing, unreadable, malformed or has no row for the
+ * precision (out then holds the defaults).  Needs no device. */
+int necgpu_tuning_lookup(const char* path, int precision, int64_t n, necgpu_tuning* out);
+
+/* Measured FP64 throughput of this device in TFLOP/s, the denominator of the
+ * FP64 kernels' rooflines: kind 0 = FP64 FMA on the CUDA cores (the fill and
+ * pattern arithmetic), kind 1 = FP64 tensor-core MMA (mma.sync m8n8k4, the
+ * FP64 LU's trailing update).  A register-only loop over 4 CTAs per SM, best
+ * of three timed launches.  Measurement support; no counterpart in the
+ * reference. */
+int necgpu_measure_peak(necgpu_engine* e, int kind, double* tflops);
+
 /* Self-check of the block-pivoted complex64 LU of the mixed path: factors a
  * seeded random n x n matrix (n <= 4096) on the engine's buffers and reports
  * the componentwise backward error max |P A - L U|_ij / (|L| |U|)_ij, max |A|

@@ -2,6 +2,7 @@
 // include/necgpu.h.  One engine per nec_context; all work goes to one
 // stream.  There is no CPU fallback: every compute step is a kernel.
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -26,6 +27,7 @@
 #include "batch.cuh"
 #include "somm.cuh"
 #include "nearfield.cuh"
+#include "peak.cuh"
 
 using namespace necb;
 
@@ -119,8 +121,15 @@ struct necgpu_engine {
   // stream3: each inner panel's U12 solve beside its L21 solve
   cudaStream_t stream3 = nullptr;
   cudaEvent_t ev_u12a = nullptr, ev_u12b = nullptr;
+  // tuning in effect for the current factorisation (select_tuning)
   bool lookahead = true;
   int lookahead_sms = 48;
+  // m-tiles per band of the tensor-core update's tile walk
+  int gemm_group = 16;
+  bool tuning_explicit = false;  // necgpu_set_tuning
+  necgpu_tuning tuning_set{};
+  // environment overrides read at creation (0 / -1: not given)
+  int env_outer = 0, env_lookahead_sms = 0, env_lookahead = -1, env_group = 0;
   bool trsm8 = true;  // U12 panel solves with eight warps per vector block (else one thread per vector)
   CUtensorMap tmA{}, tmB{};
   float2* d_dinv = nullptr;  // reciprocal diagonal of U (block-pivoted mixed LU)
@@ -634,7 +643,9 @@ int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int 
   const int n_tiles = (int)((2 * ncols + tc::BN - 1) / tc::BN);
   const int grid = std::max(1, std::min(m_tiles * n_tiles, grid_max));
   const int kt = kbegin(e, st);
-  tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(tmA, tmB, tmC, (int)m, (int)ncols, kdim, e->d_status);
+  const int group = std::max(1, std::min(e->gemm_group, m_tiles));
+  tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(tmA, tmB, tmC, (int)m, (int)ncols, kdim, group,
+                                                               e->d_status);
   kend(e, kt, NECGPU_K_GEMM, 8.0 * (double)m * ncols * kb, st);
   LAUNCHED();
   return 0;
@@ -1312,8 +1323,111 @@ int ensure_pattern(necgpu_engine* e, int ndir) {
   return 0;
 }
 
+// ---------------- tuning table ----------------
+constexpr necgpu_tuning kDefaultTuning = {256, 48, 16};
+
+struct TuningRow {
+  int precision;
+  int64_t nmax;
+  necgpu_tuning t;
+};
+
+bool tuning_valid(const necgpu_tuning& t) {
+  return t.outer >= 64 && t.outer <= 1024 && t.outer % 64 == 0 && t.lookahead_sms >= 0 && t.lookahead_sms < 128 &&
+         t.gemm_group >= 1 && t.gemm_group <= 1024;
+}
+
+// "precision n_max outer lookahead_sms gemm_group [anything]" per line; '#'
+// starts a comment line.  False when the file cannot be read or a row is
+// malformed.
+bool parse_tuning(const char* path, std::vector<TuningRow>& rows) {
+  FILE* f = std::fopen(path, "r");
+  if (!f) return false;
+  char line[512];
+  bool ok = true;
+  while (std::fgets(line, sizeof line, f)) {
+    const char* p = line;
+    while (*p == ' ' || *p == '\t') p++;
+    if (*p == '#' || *p == '\n' || *p == '\r' || *p == 0) continue;
+    char prec[16] = {0};
+    long long nmax = 0;
+    necgpu_tuning t{};
+    if (std::sscanf(p, "%15s %lld %d %d %d", prec, &nmax, &t.outer, &t.lookahead_sms, &t.gemm_group) != 5) {
+      ok = false;
+      break;
+    }
+    const int pr = !std::strcmp(prec, "mixed") ? NECGPU_MIXED : !std::strcmp(prec, "fp64") ? NECGPU_FP64 : -1;
+    if (pr < 0 || nmax < 1 || !tuning_valid(t)) {
+      ok = false;
+      break;
+    }
+    rows.push_back({pr, (int64_t)nmax, t});
+  }
+  std::fclose(f);
+  return ok;
+}
+
+// The row for (precision, n): smallest n_max >= n, else the largest n_max.
+bool tuning_row(const std::vector<TuningRow>& rows, int precision, int64_t n, necgpu_tuning* out) {
+  const TuningRow* best = nullptr;
+  const TuningRow* largest = nullptr;
+  for (const TuningRow& r : rows) {
+    if (r.precision != precision) continue;
+    if (r.nmax >= n && (!best || r.nmax < best->nmax)) best = &r;
+    if (!largest || r.nmax > largest->nmax) largest = &r;
+  }
+  if (!best) best = largest;
+  if (!best) return false;
+  *out = best->t;
+  return true;
+}
+
+// Path of the library's table: NECPP_B200_TUNING, else tuning.tsv in the
+// directory of the shared library holding this code ("" for none).
+std::string library_tuning_path() {
+  if (const char* s = std::getenv("NECPP_B200_TUNING")) return std::strcmp(s, "none") ? std::string(s) : "";
+  Dl_info info;
+  if (!dladdr(reinterpret_cast<const void*>(&library_tuning_path), &info) || !info.dli_fname) return "";
+  std::string p(info.dli_fname);
+  const size_t slash = p.rfind('/');
+  return (slash == std::string::npos ? std::string(".") : p.substr(0, slash)) + "/tuning.tsv";
+}
+
+const std::vector<TuningRow>& library_tuning() {
+  static std::vector<TuningRow> rows;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    const std::string path = library_tuning_path();
+    if (path.empty() || !parse_tuning(path.c_str(), rows)) rows.clear();
+  });
+  return rows;
+}
+
+necgpu_tuning effective_tuning(const necgpu_engine* e, int precision, int64_t n) {
+  necgpu_tuning t = kDefaultTuning;
+  necgpu_tuning r;
+  if (e->tuning_explicit)
+    t = e->tuning_set;
+  else if (tuning_row(library_tuning(), precision, n, &r))
+    t = r;
+  if (e->env_outer) t.outer = e->env_outer;
+  if (e->env_lookahead_sms) t.lookahead_sms = e->env_lookahead_sms;
+  if (e->env_lookahead == 0) t.lookahead_sms = 0;
+  if (e->env_group) t.gemm_group = e->env_group;
+  return t;
+}
+
+void select_tuning(necgpu_engine* e, int precision) {
+  const necgpu_tuning t = effective_tuning(e, precision, e->n);
+  e->outer = t.outer;
+  e->lookahead = t.lookahead_sms > 0;
+  if (t.lookahead_sms > 0) e->lookahead_sms = t.lookahead_sms;
+  e->gemm_group = t.gemm_group;
+}
+
 int run_factor(necgpu_engine* e, int precision) {
   if (!e->filled) return fail(e, NECGPU_ERR_ARG, "factor: matrix not filled");
+  select_tuning(e, precision);
   if (precision == NECGPU_FP64) {
     TRY(run_lu<double>(e, e->Z64));
     e->filled = false;  // Z64 now holds the factors
@@ -1453,16 +1567,20 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_PARTIAL_PIVOT")) e->prefer_blockpiv = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_FLAG_SWEEP")) e->inv_sweep = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_NO_DMMA")) e->use_dmma = (s[0] == '0');
-  if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD")) e->lookahead = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD")) e->env_lookahead = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_TRSM1")) e->trsm8 = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_GEMM_GROUP")) {
+    const int v = std::atoi(s);
+    if (v >= 1 && v <= 1024) e->env_group = v;
+  }
   if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD_SMS")) {
     const int v = std::atoi(s);
-    if (v >= 1 && v < 128) e->lookahead_sms = v;
+    if (v >= 1 && v < 128) e->env_lookahead_sms = v;
   }
   CUDA_TRY(cudaFuncSetAttribute(gemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DmmaSmem)));
   if (const char* s = std::getenv("NECPP_B200_OUTER")) {
     const int64_t v = std::atoll(s);
-    if (v >= 64 && v % 64 == 0 && v <= 1024) e->outer = v;
+    if (v >= 64 && v % 64 == 0 && v <= 1024) e->env_outer = (int)v;
   }
   CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
   e->own_stream = true;
@@ -1865,6 +1983,73 @@ __global__ void lu_residual_kernel(const float2* A, const float2* F, const int* 
   atomicMax((int*)out + 1, __float_as_int(ref));
 }
 
+int necgpu_set_tuning(necgpu_engine* e, const necgpu_tuning* t) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (!t) {
+    e->tuning_explicit = false;
+    return NECGPU_OK;
+  }
+  if (!tuning_valid(*t))
+    return fail(e, NECGPU_ERR_ARG,
+                "set_tuning: outer must be a multiple of 64 in [64, 1024], lookahead_sms in [0, 127], gemm_group "
+                "in [1, 1024]");
+  e->tuning_set = *t;
+  e->tuning_explicit = true;
+  return NECGPU_OK;
+}
+
+int necgpu_get_tuning(const necgpu_engine* e, int precision, int64_t n, necgpu_tuning* out) {
+  if (!e || !out || (precision != NECGPU_FP64 && precision != NECGPU_MIXED) || n < 1) return NECGPU_ERR_ARG;
+  *out = effective_tuning(e, precision, n);
+  return NECGPU_OK;
+}
+
+int necgpu_tuning_lookup(const char* path, int precision, int64_t n, necgpu_tuning* out) {
+  if (!out || (precision != NECGPU_FP64 && precision != NECGPU_MIXED) || n < 1) return NECGPU_ERR_ARG;
+  *out = kDefaultTuning;
+  std::vector<TuningRow> rows;
+  const std::string p = path ? std::string(path) : library_tuning_path();
+  if (p.empty() || !parse_tuning(p.c_str(), rows)) return NECGPU_ERR_ARG;
+  return tuning_row(rows, precision, n, out) ? NECGPU_OK : NECGPU_ERR_ARG;
+}
+
+int necgpu_measure_peak(necgpu_engine* e, int kind, double* tflops) {
+  if (!e || !tflops || kind < 0 || kind > 1) return NECGPU_ERR_ARG;
+  CUDA_TRY(cudaSetDevice(e->device));
+  const int ctas = 4 * e->nsm;
+  double* sink = nullptr;
+  TRY(dalloc(e, sink, (size_t)ctas * peak::kThreads));
+  // a few milliseconds per launch; the best of three timed launches after one warm-up
+  const int iters = kind == 0 ? 65536 : 16384;
+  const double flops = kind == 0 ? (double)ctas * peak::kThreads * iters * 2.0 * peak::kChains
+                                 : (double)ctas * (peak::kThreads / 32) * iters * 4.0 * 512.0;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  int rc = 0;
+  float best = 0.f;
+  if (cudaEventCreate(&t0) != cudaSuccess || cudaEventCreate(&t1) != cudaSuccess) rc = NECGPU_ERR_CUDA;
+  for (int rep = 0; rep < 4 && !rc; rep++) {
+    cudaEventRecord(t0, e->stream);
+    if (kind == 0)
+      peak::dfma_peak_kernel<<<ctas, peak::kThreads, 0, e->stream>>>(sink, iters);
+    else
+      peak::dmma_peak_kernel<<<ctas, peak::kThreads, 0, e->stream>>>(sink, iters);
+    cudaEventRecord(t1, e->stream);
+    const cudaError_t ce = cudaEventSynchronize(t1);
+    if (ce != cudaSuccess) {
+      rc = fail(e, NECGPU_ERR_CUDA, cudaGetErrorString(ce));
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t0, t1);
+    if (rep > 0 && (best == 0.f || ms < best)) best = ms;
+  }
+  if (t0) cudaEventDestroy(t0);
+  if (t1) cudaEventDestroy(t1);
+  dfree(e, sink);
+  if (!rc) *tflops = flops / (best * 1e-3) / 1e12;
+  return rc;
+}
+
 int necgpu_check_block_lu(necgpu_engine* e, int n, unsigned seed, double* backward_err, double* max_abs,
                           int* interchanges) {
   if (!e || n < 1 || n > 4096 || !backward_err || !max_abs || !interchanges) return NECGPU_ERR_ARG;
@@ -1874,6 +2059,7 @@ int necgpu_check_block_lu(necgpu_engine* e, int n, unsigned seed, double* backwa
   // of n unknowns; the engine is left without a structure afterwards
   e->n = n;
   e->ld = (n + 63) / 64 * 64;
+  select_tuning(e, NECGPU_MIXED);
   const int64_t ld = e->ld, cnt = (int64_t)n * ld;
   float2* A = nullptr;
   float* d = nullptr;

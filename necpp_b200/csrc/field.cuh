@@ -28,7 +28,11 @@ enum : int {
 struct SrcSeg {
   double x, y, z, s, b, cab, sab, salp;
   int ind1, ind2;
+  double sfac;  // far_sfac(s): set by whoever builds the SrcSeg
 };
+
+// sin(pi s) / pi of efld_compute's far branch (2815), once per source
+__device__ __forceinline__ double far_sfac(double s) { return sin(kPiD * s) / kPiD; }
 
 struct FieldParams {
   double rkh;
@@ -365,25 +369,31 @@ __device__ double efld_compute(const SrcSeg& J, double xij, double yij, double a
     rhoy = 0.0;
     rhoz = 0.0;
   } else {
-    rhox /= rh;
-    rhoy /= rh;
-    rhoz /= rh;
+    // one reciprocal for the three components (the FP64 divide is the
+    // costliest operation of a far pair)
+    const double rhinv = 1.0 / rh;
+    rhox *= rhinv;
+    rhoy *= rhinv;
+    rhoz *= rhinv;
   }
   double r = sqrt(zp * zp + rh * rh);
   if (r >= P.rkh) {
-    // lumped current element, 2798-2819
+    // lumped current element, 2798-2819, with the divisions by r, rmag and
+    // py = 2 pi r^2 folded into two reciprocals
+    const double rinv = 1.0 / r;
     double rmag = kTwoPiD * r;
-    double cth = zp / r;
-    double px = rh / r;
+    double cth = zp * rinv;
+    double px = rh * rinv;
     double sn, cs;
     sincos(rmag, &sn, &cs);
     cplx e0 = mk(cs, -sn);
-    double py = kTwoPiD * r * r;
-    cplx e1 = P.eta * cth * e0 * mk(1.0, -1.0 / rmag) / py;
-    cplx e2 = P.eta * px * e0 * mk(1.0, rmag - 1.0 / rmag) / (2. * py);
+    const double rminv = 1.0 / rmag;
+    const double pyinv = rminv * rinv;  // 1 / py
+    cplx e1 = (P.eta * cth * pyinv) * e0 * mk(1.0, -rminv);
+    cplx e2 = (0.5 * P.eta * px * pyinv) * e0 * mk(1.0, rmag - rminv);
     tezk = e1 * cth - e2 * px;
     terk = e1 * px + e2 * cth;
-    double sfac = sin(kPiD * J.s) / kPiD;
+    const double sfac = J.sfac;
     tezc = tezk * sfac;
     terc = terk * sfac;
     tezk = tezk * J.s;

@@ -72,9 +72,19 @@ __device__ __forceinline__ void fill_tile(const FillArgs& A, const ContractArgs&
   }
   int status = 0;
   const int sbeg = A.tile_src_ptr[tile], send = A.tile_src_ptr[tile + 1];
+  // the far-pair factor sin(pi s)/pi of the tile's sources, computed once per
+  // source by the CTA in chunks of kFillTI instead of once per pair
+  __shared__ double sfac[kFillTI];
   for (int sidx = sbeg; sidx < send; sidx++) {
+    if ((sidx - sbeg) % kFillTI == 0) {
+      __syncthreads();  // the previous chunk's factors are no longer read
+      const int q = sidx + tid;
+      if (q < send) sfac[tid] = far_sfac(__ldg(A.s + __ldg(A.tsrc + q)));
+      __syncthreads();
+    }
     const int j = __ldg(A.tsrc + sidx);
     SrcSeg J;
+    J.sfac = sfac[(sidx - sbeg) % kFillTI];
     J.x = __ldg(A.x + j);
     J.y = __ldg(A.y + j);
     J.z = __ldg(A.z + j);

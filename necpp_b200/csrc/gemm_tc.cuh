@@ -205,11 +205,27 @@ __global__ void __launch_bounds__(256) pack_b_kernel(const float2* B, int64_t ld
 }
 
 // ---- the GEMM -----------------------------------------------------------
+// Tile order of the persistent loop: bands of `group` m-tiles; inside a band
+// the walk goes down the band's m-tiles for one n-tile, then to the next
+// n-tile.  The CTAs resident at one time then share a few B' tiles (each is
+// read from DRAM once per band and by the band's other CTAs from L2) and
+// the band's A' tiles stay in L2 while the band sweeps n, instead of every
+// m-row of tiles sweeping all of B' while the C traffic evicts it.
+__device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, int group, int& mt, int& nt) {
+  const int per_band = group * n_tiles;
+  const int band = tile / per_band;
+  const int m0 = band * group;
+  const int gm = min(group, m_tiles - m0);  // m-tiles in this band (the last may be short)
+  const int local = tile - band * per_band;
+  mt = m0 + local % gm;
+  nt = local / gm;
+}
+
 // C (m x n complex, row-major; tmC views it as m rows x 2n FP32 with 32 x 32
 // boxes, 128B swizzle) -= D, D = A' B'^T, K' = kdim (multiple of 64)
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                   const __grid_constant__ CUtensorMap tmC, int m, int n, int kdim, int* status) {
+                   const __grid_constant__ CUtensorMap tmC, int m, int n, int kdim, int group, int* status) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   uint8_t* epi = smem + STAGES * STAGE_BYTES;  // 1 KB aligned (the swizzle atom)
@@ -258,7 +274,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (lane == 0) {
       int it = 0;
       for (int tile = blockIdx.x; tile < total && !*abort_flag; tile += gridDim.x) {
-        const int mt = tile / n_tiles, nt = tile - mt * n_tiles;
+        int mt, nt;
+      tile_coords(tile, m_tiles, n_tiles, group, mt, nt);
         for (int kb = 0; kb < kblocks; kb++, it++) {
           const int s = it % STAGES;
           const uint32_t ph = (it / STAGES) & 1;
@@ -335,7 +352,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         break;
       }
       tc_fence_after();
-      const int mt = tile / n_tiles, nt = tile - mt * n_tiles;
+      int mt, nt;
+      tile_coords(tile, m_tiles, n_tiles, group, mt, nt);
       const int y = mt * BM + q * 32;  // first C row of this warp's quarter
       const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN);
 #pragma unroll 1

@@ -43,6 +43,7 @@ __device__ __forceinline__ SrcSeg load_seg(const NearFieldArgs& A, int64_t i, bo
   J.sab = A.sab[i];
   J.salp = A.salp[i];
   J.ind1 = exk ? A.ind1[i] : 0;
+  J.sfac = far_sfac(J.s);
   J.ind2 = exk ? A.ind2[i] : 0;
   return J;
 }

@@ -998,6 +998,7 @@ __global__ void __launch_bounds__(64) near_ground_kernel(FillArgs A, const cplx*
     J.salp = A.salp[j];
     J.ind1 = EXK ? A.ind1[j] : 0;
     J.ind2 = EXK ? A.ind2[j] : 0;
+    J.sfac = far_sfac(J.s);
     for (int64_t i = 0; i < n; i++) {
       const double xi = A.x[i], yi = A.y[i], zi = A.z[i];
       if (image_r2(xi - J.x, yi - J.y, zi + J.z) > .95) continue;

@@ -86,3 +86,41 @@ def test_batch_rejects_oversized_problem(nb):
     nb.nec_delete(ctx)
     with pytest.raises(RuntimeError, match="640"):
         B.sweep([prob])
+
+
+@pytest.mark.gpu
+def test_batch_matches_reference_sweep(nb):
+    """Twelve problems of the seeded 256 x 32 Yagi sweep (seed 0), spread
+    over its range of N, solved in one batched call and compared with the
+    reference's own solves of the same problems (tests/golden/yagi_sweep.npz,
+    made by make_sweep_golden.py): Zin within 1e-9 relative, the float32
+    gain grid within 1e-4 dB where the gain is within 60 dB of its peak."""
+    import os
+    from necpp_b200 import batch as B
+    from necpp_b200 import workloads as W
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "yagi_sweep.npz"))
+    rng = np.random.default_rng(0)
+    params = [W.yagi_params(rng) for _ in range(256)]
+    freqs = np.linspace(140.0, 160.0, 32)
+    problems = []
+    for v, fi in g["pick"]:
+        half, xs, rad, segs = params[v]
+        ctx = nb.nec_create()
+        for e in range(len(half)):
+            assert nb.nec_wire(ctx, e + 1, int(segs[e]), float(xs[e]), 0.0, -float(half[e]), float(xs[e]), 0.0,
+                               float(half[e]), float(rad[e]), 1.0, 1.0) == 0
+        nb.nec_geometry_complete(ctx, 0)
+        nb.nec_ex_card(ctx, 0, 2, (int(segs[1]) + 1) // 2, 0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+        feed = int(segs[0]) + (int(segs[1]) + 1) // 2 - 1
+        problems.append(B.host_problem(ctx, float(freqs[fi]), feed))
+        nb.nec_delete(ctx)
+    assert [p[0]["n"] for p in problems] == list(g["n"])
+    th, ph = B.pattern_grid()
+    res = B.sweep(problems, th, ph)
+    assert np.all(res["status"] == 0), res["status"]
+    rel = np.abs(res["zin"] - g["zin"]) / np.abs(g["zin"])
+    assert np.max(rel) <= 1e-9, rel
+    for k in range(len(problems)):
+        ref = g["gain"][k].astype(np.float64)
+        strong = ref > np.max(ref) - 60.0
+        assert np.max(np.abs(res["gain"][k][strong] - ref[strong])) <= 1e-4, k
