@@ -54,6 +54,9 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-gradient", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--trace", default=None,
+                   help="write a launch trace (every kernel with its stream, start and end) of one mixed step "
+                        "to this JSON file")
     return p.parse_args()
 
 
@@ -401,6 +404,32 @@ def reference_sweep_sample(problems, labels, k):
                       % (k, problems[pick[0]][0]["n"], problems[pick[-1]][0]["n"])}
 
 
+class TraceRec(C.Structure):
+    _fields_ = [("cls", C.c_int), ("stream", C.c_int), ("start_ms", C.c_float), ("end_ms", C.c_float),
+                ("work", C.c_double), ("name", C.c_char * 48)]
+
+
+def write_trace(L, eng, path, check):
+    """One resident mixed step at timing level 3: every launch with its
+    class, stream, start and end (ms from the step's first launch).  The
+    events around each launch slow the step; the order and overlap of the
+    launches are what the trace is for."""
+    L.necgpu_get_trace.argtypes = [C.c_void_p, C.POINTER(TraceRec), C.c_int]
+    check(eng, L.necgpu_enable_timing(eng, 3))
+    check(eng, L.necgpu_step_resident(eng, 1))  # warm
+    L.necgpu_reset_kernel_stats(eng)
+    check(eng, L.necgpu_step_resident(eng, 1))
+    cnt = L.necgpu_get_trace(eng, None, 0)
+    buf = (TraceRec * cnt)()
+    L.necgpu_get_trace(eng, buf, cnt)
+    L.necgpu_enable_timing(eng, 0)
+    recs = [{"cls": K_NAMES[r.cls] if 0 <= r.cls < len(K_NAMES) else r.cls, "stream": r.stream,
+             "start_ms": r.start_ms, "end_ms": r.end_ms, "work": r.work,
+             "name": r.name.decode(errors="replace").split("<<<")[0]} for r in buf]
+    with open(path, "w") as f:
+        json.dump(recs, f)
+
+
 def run_b200(args):
     import torch
     import torch.distributed as dist
@@ -508,6 +537,9 @@ def run_b200(args):
     ms_m_max = secs * 1e3 / args.steps
     # the same steps again with per-launch events, for the per-kernel roofline
     ms_inst, st_m, _, _ = timed(eng_m, 1, args.steps, 1, None, level=2)
+
+    if args.trace:
+        write_trace(L, eng_m, args.trace, check)
 
     # ---- plain FP64
     ms_f_max, z_fp64 = None, None

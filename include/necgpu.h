@@ -189,9 +189,27 @@ typedef struct necgpu_stats {
 int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out);
 /* 1: time each stage (fill / factor / solve / pattern) with CUDA events.
    2: additionally time every kernel launch by class (events around each
-      launch on the engine's stream; accumulated into k_ms / k_launches). */
+      launch on the stream it runs on; accumulated into k_ms / k_launches).
+   3: additionally keep a trace of every timed launch (necgpu_get_trace). */
 int necgpu_enable_timing(necgpu_engine* e, int on);
+/* Clears the per-class sums and the trace; the next traced launch sets the
+   trace's time origin. */
 int necgpu_reset_kernel_stats(necgpu_engine* e);
+
+/* One launch of the trace: class (necgpu_kernel_class), stream (0 the
+   engine's, 2 the lookahead's far update, 3 the U12 panel solves, 1 other),
+   start and end in ms after the trace origin, its algorithmic work (the unit
+   of its class) and the launch expression (truncated). */
+typedef struct necgpu_trace_rec {
+  int cls;
+  int stream;
+  float start_ms, end_ms;
+  double work;
+  char name[48];
+} necgpu_trace_rec;
+/* Copies up to cap records of the trace (timing level 3, read after the
+   stages have synchronised) and returns how many there are. */
+int necgpu_get_trace(necgpu_engine* e, necgpu_trace_rec* out, int cap);
 /* Make the last right-hand side and direction list passed to necgpu_solve /
    necgpu_pattern the resident inputs of necgpu_step_resident. */
 int necgpu_reuse_last_inputs(necgpu_engine* e);
@@ -307,6 +325,22 @@ int necgpu_batch_solve(necgpu_engine* e, int nprob, const necgpu_structure* stru
  * FP32 kernel; report max |difference| and max |reference| over C. */
 int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, double* max_abs_diff,
                          double* max_abs_ref);
+
+/* Dense complex solve of a caller's matrix, without a structure: the
+ * replacement of factrs + solves (src/matrix_algebra.cpp:319-338, 351-503)
+ * for a matrix that does not come from the fill.  z: n x n complex
+ * (interleaved re, im), row-major, z[i*n + j] the coefficient of x_j in
+ * equation i; b: n complex; x: n complex out.  NECGPU_FP64 factors with
+ * partial pivoting; NECGPU_MIXED factors the complex64 copy (block-local
+ * pivoting, with the partial-pivot refactor when a diagonal block has no
+ * usable pivot or the refinement stalls) and refines in FP64 against z.
+ * residual (may be NULL) receives the final relative residual of the mixed
+ * refinement (0 for FP64).  An exactly singular matrix fails with
+ * NECGPU_ERR_SINGULAR (or NECGPU_ERR_NONFINITE), never with a non-finite x.
+ * Any structure the engine held is dropped, and the engine holds none
+ * afterwards.  n <= 65536. */
+int necgpu_matrix_solve(necgpu_engine* e, int64_t n, const double* z, const double* b, int precision, double* x,
+                        double* residual);
 
 /* ---- tuning of the mixed-precision LU (no counterpart in the reference,
  * whose Eigen LU has fixed blocking, src/matrix_algebra.cpp:243-251) ----

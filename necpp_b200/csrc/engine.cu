@@ -94,7 +94,14 @@ struct necgpu_engine {
   struct PendingK {
     int cls, ev;
     double flops;
+    int stream;        // 0 engine stream, 2 / 3 the lookahead and U12 streams, 1 other
+    const char* name;  // launch expression (static storage) or null
   };
+  // timing level 3: every timed launch with its start and end on a common
+  // time origin (necgpu_get_trace)
+  cudaEvent_t trace_base = nullptr;
+  bool trace_based = false;
+  std::vector<necgpu_trace_rec> trace;
   std::vector<cudaEvent_t> kev;
   int kev_used = 0;
   std::vector<PendingK> kpend;
@@ -126,6 +133,7 @@ struct necgpu_engine {
   int lookahead_sms = 48;
   // m-tiles per band of the tensor-core update's tile walk
   int gemm_group = 16;
+  bool matrix_only = false;      // necgpu_matrix_solve: a caller's matrix, no structure tables
   bool tuning_explicit = false;  // necgpu_set_tuning
   necgpu_tuning tuning_set{};
   // environment overrides read at creation (0 / -1: not given)
@@ -227,6 +235,12 @@ int fail(necgpu_engine* e, int code, const std::string& msg) {
 // kernel of a class, resolved after the next stream synchronisation.
 int kbegin(necgpu_engine* e, cudaStream_t st = nullptr) {
   if (e->timing_level < 2) return -1;
+  if (e->timing_level >= 3 && !e->trace_based) {
+    // the trace's time origin: recorded before the first traced launch
+    if (!e->trace_base && cudaEventCreate(&e->trace_base) != cudaSuccess) return -1;
+    cudaEventRecord(e->trace_base, e->stream);
+    e->trace_based = true;
+  }
   while ((int)e->kev.size() < e->kev_used + 2) {
     cudaEvent_t ev;
     if (cudaEventCreate(&ev) != cudaSuccess) return -1;
@@ -237,10 +251,12 @@ int kbegin(necgpu_engine* e, cudaStream_t st = nullptr) {
   cudaEventRecord(e->kev[i], st ? st : e->stream);
   return i;
 }
-void kend(necgpu_engine* e, int i, int cls, double flops, cudaStream_t st = nullptr) {
+void kend(necgpu_engine* e, int i, int cls, double flops, cudaStream_t st = nullptr, const char* name = nullptr) {
   if (i < 0) return;
-  cudaEventRecord(e->kev[i + 1], st ? st : e->stream);
-  e->kpend.push_back({cls, i, flops});
+  cudaStream_t s = st ? st : e->stream;
+  cudaEventRecord(e->kev[i + 1], s);
+  const int sid = s == e->stream ? 0 : s == e->stream2 ? 2 : s == e->stream3 ? 3 : 1;
+  e->kpend.push_back({cls, i, flops, sid, name});
 }
 void kflush(necgpu_engine* e) {  // call after the stream has synchronised
   for (auto& p : e->kpend) {
@@ -249,6 +265,18 @@ void kflush(necgpu_engine* e) {  // call after the stream has synchronised
       e->stats.k_ms[p.cls] += ms;
       e->stats.k_launches[p.cls] += 1;
       e->stats.k_flops[p.cls] += p.flops;
+      float t0 = 0.f;
+      if (e->timing_level >= 3 && e->trace_based &&
+          cudaEventElapsedTime(&t0, e->trace_base, e->kev[p.ev]) == cudaSuccess && e->trace.size() < (1u << 20)) {
+        necgpu_trace_rec r;
+        r.cls = p.cls;
+        r.stream = p.stream;
+        r.start_ms = t0;
+        r.end_ms = t0 + ms;
+        r.work = p.flops;
+        std::snprintf(r.name, sizeof r.name, "%s", p.name ? p.name : "");
+        e->trace.push_back(r);
+      }
     }
   }
   e->kpend.clear();
@@ -256,12 +284,12 @@ void kflush(necgpu_engine* e) {  // call after the stream has synchronised
 }
 
 // launch a kernel of class cls (algorithmic work 'flops') and check it
-#define KLAUNCH(cls, flops, ...)        \
-  do {                                  \
-    const int _kt = kbegin(e);          \
-    __VA_ARGS__;                        \
-    kend(e, _kt, (cls), (flops));       \
-    LAUNCHED();                         \
+#define KLAUNCH(cls, flops, ...)                         \
+  do {                                                   \
+    const int _kt = kbegin(e);                           \
+    __VA_ARGS__;                                         \
+    kend(e, _kt, (cls), (flops), nullptr, #__VA_ARGS__); \
+    LAUNCHED();                                          \
   } while (0)
 
 // Device buffers are stream-ordered allocations from the device's default
@@ -646,7 +674,7 @@ int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int 
   const int group = std::max(1, std::min(e->gemm_group, m_tiles));
   tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(tmA, tmB, tmC, (int)m, (int)ncols, kdim, group,
                                                                e->d_status);
-  kend(e, kt, NECGPU_K_GEMM, 8.0 * (double)m * ncols * kb, st);
+  kend(e, kt, NECGPU_K_GEMM, 8.0 * (double)m * ncols * kb, st, "tc::gemm_tc_kernel");
   LAUNCHED();
   return 0;
 }
@@ -744,7 +772,7 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
       const int kt = kbegin(e);
       CUDA_TRY(cudaLaunchCooperativeKernel((const void*)panel_kernel<R, kNB>, dim3(P), dim3(kPanelThreads),
                                            args, smem, e->stream));
-      kend(e, kt, NECGPU_K_PANEL, 4.0 * (double)m * kb * kb);
+      kend(e, kt, NECGPU_K_PANEL, 4.0 * (double)m * kb * kb, nullptr, "trsm_panel_kernel");
       LAUNCHED();
     }
     if (n > kb)
@@ -849,7 +877,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
     const int kt = kbegin(e, st);
     trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv);
-    kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st);
+    kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm8_panel_kernel");
     LAUNCHED();
     return 0;
   };
@@ -1013,7 +1041,7 @@ int run_trsv(necgpu_engine* e, const typename cvec<R>::T* M, typename cvec<R>::T
       CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)trsv_sweep_kernel<T, true>
                                                      : (const void*)trsv_sweep_kernel<T, false>,
                                            dim3(grid), dim3(kSweepThreads), args, dsm, e->stream));
-      kend(e, kt, NECGPU_K_TRSV, tri_bytes);
+      kend(e, kt, NECGPU_K_TRSV, tri_bytes, nullptr, "trsv_sweep_kernel");
       LAUNCHED();
     }
     // the backward pass wrote the solution into rhs; return it in sol
@@ -1097,7 +1125,7 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
     CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)inv_sweep_kernel<true>
                                                    : (const void*)inv_sweep_kernel<false>,
                                          dim3(grid), dim3(kInvSweepThreads), args, 0, e->stream));
-    kend(e, kt, NECGPU_K_TRSV, tri_bytes);
+    kend(e, kt, NECGPU_K_TRSV, tri_bytes, nullptr, "inv_sweep_kernel");
     LAUNCHED();
   }
   // the backward pass wrote the solution into rhs
@@ -1278,9 +1306,10 @@ int run_solve(necgpu_engine* e, bool sync_checks) {
   } else {
     return fail(e, NECGPU_ERR_ARG, "solve: no factorisation held");
   }
-  KLAUNCH(NECGPU_K_OTHER, 0.0,
-          coeff_kernel<<<g1, 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc,
-                                                  e->d_ccoef + 2 * e->nc, e->d_x, e->d_abc, e->d_cur));
+  if (!e->matrix_only)
+    KLAUNCH(NECGPU_K_OTHER, 0.0,
+            coeff_kernel<<<g1, 256, 0, e->stream>>>(n, e->d_cptr, e->d_cbasis, e->d_ccoef, e->d_ccoef + e->nc,
+                                                    e->d_ccoef + 2 * e->nc, e->d_x, e->d_abc, e->d_cur));
   if (sync_checks) CUDA_TRY(cudaStreamSynchronize(e->stream));
   e->have_solution = true;
   return 0;
@@ -1656,8 +1685,17 @@ int necgpu_enable_timing(necgpu_engine* e, int on) {
   return NECGPU_OK;
 }
 
+int necgpu_get_trace(necgpu_engine* e, necgpu_trace_rec* out, int cap) {
+  if (!e || cap < 0) return -NECGPU_ERR_ARG;
+  const int cnt = (int)std::min<size_t>(e->trace.size(), (size_t)cap);
+  if (out) std::copy(e->trace.begin(), e->trace.begin() + cnt, out);
+  return (int)e->trace.size();
+}
+
 int necgpu_reset_kernel_stats(necgpu_engine* e) {
   if (!e) return NECGPU_ERR_ARG;
+  e->trace.clear();
+  e->trace_based = false;
   for (int k = 0; k < NECGPU_K_COUNT; k++) {
     e->stats.k_ms[k] = 0;
     e->stats.k_launches[k] = 0;
@@ -1717,6 +1755,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   e->filled = false;
   e->have_solution = false;
   e->adj_ready = false;
+  e->matrix_only = false;
   dfree(e, e->d_zload);  // loads belong to one structure: set them after it
   e->somm_ready = false;   // so do the Sommerfeld tables (they follow the frequency)
   dfree(e, e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
@@ -1981,6 +2020,50 @@ __global__ void lu_residual_kernel(const float2* A, const float2* F, const int* 
   }
   atomicMax((int*)out, __float_as_int(mx));
   atomicMax((int*)out + 1, __float_as_int(ref));
+}
+
+int necgpu_matrix_solve(necgpu_engine* e, int64_t n, const double* z, const double* b, int precision, double* x,
+                        double* residual) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (!z || !b || !x || n < 1 || n > 65536) return fail(e, NECGPU_ERR_ARG, "matrix_solve: bad arguments");
+  if (precision != NECGPU_FP64 && precision != NECGPU_MIXED)
+    return fail(e, NECGPU_ERR_ARG, "matrix_solve: unknown precision");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  free_all(e);  // a structure held before is dropped
+  e->n = n;
+  e->ld = (n + 63) / 64 * 64;
+  e->matrix_only = true;
+  int rc = dalloc(e, e->Z64, (size_t)n * e->ld);
+  if (!rc) rc = ensure_vectors(e);
+  if (!rc) {
+    if (cudaMemcpy2DAsync(e->Z64, e->ld * sizeof(double2), z, n * sizeof(double2), n * sizeof(double2), n,
+                          cudaMemcpyHostToDevice, e->stream) != cudaSuccess ||
+        cudaMemcpyAsync(e->d_b, b, n * sizeof(double2), cudaMemcpyHostToDevice, e->stream) != cudaSuccess ||
+        cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream) != cudaSuccess)
+      rc = fail(e, NECGPU_ERR_CUDA, "matrix_solve: upload failed");
+    e->stats.h2d_bytes += (n * n + n) * sizeof(double2);
+  }
+  if (!rc) {
+    e->filled = true;
+    e->factored = -1;
+    rc = run_factor(e, precision);
+  }
+  if (!rc) rc = run_solve(e, true);
+  if (!rc) {
+    if (cudaMemcpyAsync(x, e->d_x, n * sizeof(double2), cudaMemcpyDeviceToHost, e->stream) != cudaSuccess ||
+        cudaStreamSynchronize(e->stream) != cudaSuccess)
+      rc = fail(e, NECGPU_ERR_CUDA, "matrix_solve: download failed");
+    e->stats.d2h_bytes += n * sizeof(double2);
+    if (residual) *residual = e->stats.refine_residual;
+    for (int64_t i = 0; !rc && i < 2 * n; i++)
+      if (!std::isfinite(x[i])) rc = fail(e, NECGPU_ERR_NONFINITE, "matrix_solve: non-finite solution");
+  }
+  kflush(e);
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  free_all(e);  // the engine holds no structure or matrix afterwards
+  e->matrix_only = false;
+  return rc;
 }
 
 int necgpu_set_tuning(necgpu_engine* e, const necgpu_tuning* t) {

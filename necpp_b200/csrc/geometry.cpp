@@ -600,6 +600,19 @@ void Geometry::check_overlaps() {
   static thread_local std::vector<std::pair<int64_t, int64_t>> tl_nodes;
   std::vector<End>& ends = tl_ends;
   std::vector<View>& views = tl_views;
+  // a structure much smaller than the largest one seen returns the memory
+  // (one large structure would otherwise stay mapped in this thread)
+  const size_t nseg = (size_t)n;
+  auto trim = [nseg](auto& v, size_t per) {
+    if (v.capacity() > 4096 && v.capacity() > 8 * per * nseg) {
+      v.clear();
+      v.shrink_to_fit();
+    }
+  };
+  trim(ends, 2);
+  trim(views, 1);
+  trim(tl_parent, 2);
+  trim(tl_nodes, 2);
   ends.clear();
   views.clear();
   ends.reserve(2 * n);

@@ -46,8 +46,17 @@ def whole_job_rate(units, seconds, device="cpu"):
 
 def partition_by_cost(costs, world, rank):
     """Indices of the units this rank solves when independent units of
-    uneven cost (e.g. N^3 of each problem of a batched sweep) are dealt
-    round-robin in order of decreasing cost; every rank gets a near-equal
-    share of the total cost."""
+    uneven cost (e.g. N^3 of each problem of a batched sweep) are shared
+    out: largest first, each to the rank whose total is smallest so far
+    (ties to the lowest rank).  The most loaded rank then exceeds the
+    average by less than the cost of one unit.  Every rank computes the
+    same assignment, so no exchange is needed."""
     order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
-    return [i for k, i in enumerate(order) if k % world == rank]
+    loads = [0.0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (loads[q], q))
+        loads[r] += float(costs[i])
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)

@@ -70,3 +70,6 @@ def test_partition_by_cost_covers_all_units_evenly():
     assert allidx == list(range(1000))
     shares = [cost[p].sum() / cost.sum() for p in parts]
     assert max(shares) - min(shares) < 0.02
+    # the largest total exceeds the average by less than one unit's cost
+    loads = [cost[p].sum() for p in parts]
+    assert max(loads) - cost.sum() / 4 < cost.max()
