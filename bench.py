@@ -320,6 +320,30 @@ def gradient_cost(nb, W, reps=5):
             % reps}
 
 
+def gradient_population_cost(nb, W, rank, world, replicas, m=64):
+    """The population check of the adjoint workload: m seeded designs
+    (yagi_ground_params(seed), seeds 0..m-1), shared out over the ranks.
+    adjoint_s: wall clock of this rank's adjoint gradients (27 x 3 each);
+    batched_fd_s: the same designs' central differences, all m x 55 base
+    and perturbed structures in one batched solve; agreement: the largest
+    |adjoint - difference| over each output's largest derivative."""
+    from necpp_b200 import adjoint
+    build = lambda ctx, q: W.yagi_ground_cards(nb, ctx, q)
+    P = np.array([W.yagi_ground_params(s) for s in range(m)])
+    t0 = time.perf_counter()
+    idx, vals, jacs = adjoint.gradient_population(build, P, 145.0, 80.0, 0.0, world=world, rank=rank)
+    t_adj = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    _, fd = adjoint.batched_fd(build, P[idx], 145.0, 80.0, 0.0)
+    t_fd = time.perf_counter() - t0
+    err = max(float(np.max(np.max(np.abs(jacs[k] - fd[k]), axis=1) / np.max(np.abs(fd[k]), axis=1)))
+              for k in range(len(idx)))
+    rate, total, slowest = replicas.whole_job_rate(len(idx), t_adj, device="cuda")
+    return {"designs": int(total), "adjoint_s": slowest, "gradients_per_s": rate, "batched_fd_s": t_fd,
+            "batched_fd_structures": len(idx) * 55, "max_rel_err_vs_batched_fd": err,
+            "partition": "%d design(s) on rank %d of %d" % (len(idx), rank, world)}
+
+
 def batched_sweep(nb, rank, world, replicas, reps=3, ref_sample=16):
     """The batched sweep: 256 seeded Yagi-Uda variants x 32 frequencies
     (140-160 MHz) = 8192 solves of fill, LU, FP64-refined solve, currents
@@ -653,6 +677,10 @@ def run_b200(args):
 
     if rank == 0 and not args.no_gradient:
         line["gradient"] = gradient_cost(nb, W)
+    if not args.no_gradient:
+        pop = gradient_population_cost(nb, W, rank, world, replicas)
+        if rank == 0:
+            line.setdefault("gradient", {})["population"] = pop
     if not args.no_sweep:
         sw = batched_sweep(nb, rank, world, replicas, ref_sample=0 if args.no_cpu_baseline else 16)
         if rank == 0:

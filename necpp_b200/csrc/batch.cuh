@@ -503,6 +503,7 @@ __global__ void __launch_bounds__(kPatDirs * 32) batch_pattern_kernel(BatchPatte
           g.bii = A.abc[3 * T + i];
           g.cir = A.abc[4 * T + i];
           g.cii = A.abc[5 * T + i];
+          seg_pat_el(g);
           seg[t] = g;
         }
       }

@@ -156,6 +156,8 @@ struct necgpu_engine {
   int* d_near_cols = nullptr;
   int64_t near_cap = 0;
   float2* d_tinv = nullptr;  // inverted 64 x 64 diagonal blocks of the complex64 factors
+  float2* d_wnext = nullptr;  // their products with the neighbouring tile (next_tile_kernel)
+  float2* d_wnextT = nullptr;  // the same for the transposed factors (adjoint solves)
   // adjoint solves: transposed factors, matrix and block inverses
   float2* ZT32 = nullptr;
   double2* ZT64 = nullptr;
@@ -354,6 +356,8 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->ZT32);
   dfree(e, e->ZT64);
   dfree(e, e->d_tinvT);
+  dfree(e, e->d_wnext);
+  dfree(e, e->d_wnextT);
   dfree(e, e->d_adj_phi);
   dfree(e, e->d_adj_w);
   dfree(e, e->d_adj_r);
@@ -1100,12 +1104,17 @@ int invert_diag_blocks(necgpu_engine* e, bool force = false) {
   CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_inv_smem()));
   KLAUNCH(NECGPU_K_OTHER, 0.0,
           tri_inv_kernel<<<(unsigned)nblk, 128, tri_inv_smem(), e->stream>>>(e->Z32, e->ld, e->n, e->d_tinv));
+  if (!e->d_wnext) TRY(dalloc(e, e->d_wnext, (size_t)nblk * 2 * kBlk * kBlk));
+  KLAUNCH(NECGPU_K_OTHER, 0.0,
+          next_tile_kernel<<<dim3((unsigned)nblk, 2), 256, 0, e->stream>>>(e->Z32, e->ld, e->n, e->d_tinv,
+                                                                           e->d_wnext));
   return 0;
 }
 
 // sol = U^-1 L^-1 rhs on the complex64 factors with inverted diagonal
 // blocks (rhs is overwritten): two persistent sweeps
-int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_blocks, float2* rhs, float2* sol) {
+int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_blocks, const float2* wnext_blocks,
+                    float2* rhs, float2* sol) {
   const int64_t n = e->n, ld = e->ld;
   const int nblk = (int)((n + kBlk - 1) / kBlk);
   int per_sm = 0;
@@ -1117,10 +1126,11 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
     const float2* src = pass == 0 ? rhs : sol;
     float2* dst = pass == 0 ? sol : rhs;
     const float2* tinv = tinv_blocks;
+    const float2* wnext = wnext_blocks;
     unsigned* counter = e->d_sweep_ctr;
     CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), e->stream));
-    void* args[] = {(void*)&Mf, (void*)&ld, (void*)&n, (void*)&tinv, (void*)&src, (void*)&dst, (void*)&counter,
-                    (void*)&e->d_status};
+    void* args[] = {(void*)&Mf,  (void*)&ld,  (void*)&n,       (void*)&tinv,       (void*)&wnext,
+                    (void*)&src, (void*)&dst, (void*)&counter, (void*)&e->d_status};
     const int kt = kbegin(e);
     CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)inv_sweep_kernel<true>
                                                    : (const void*)inv_sweep_kernel<false>,
@@ -1132,7 +1142,9 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
   CUDA_TRY(cudaMemcpyAsync(sol, rhs, n * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream));
   return 0;
 }
-int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) { return run_trsv_inv_on(e, e->Z32, e->d_tinv, rhs, sol); }
+int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
+  return run_trsv_inv_on(e, e->Z32, e->d_tinv, e->d_wnext, rhs, sol);
+}
 
 // Mixed-precision factorisation of the FP64 matrix: demote to complex64, then
 // LU with block-local pivoting (blockpiv) or full partial pivoting.
@@ -1222,6 +1234,9 @@ int ensure_adjoint(necgpu_engine* e) {
   KLAUNCH(NECGPU_K_OTHER, 0.0, transpose_kernel<float2><<<g, 256, 0, e->stream>>>(e->Z32, ld, e->ZT32, ld, n));
   KLAUNCH(NECGPU_K_OTHER, 0.0, transpose_kernel<double2><<<g, 256, 0, e->stream>>>(e->Z64, ld, e->ZT64, ld, n));
   KLAUNCH(NECGPU_K_OTHER, 0.0, tinv_transpose_kernel<<<(unsigned)nblk, 256, 0, e->stream>>>(e->d_tinv, e->d_tinvT));
+  if (!e->d_wnextT) TRY(dalloc(e, e->d_wnextT, (size_t)nblk * 2 * kBlk * kBlk));
+  KLAUNCH(NECGPU_K_OTHER, 0.0,
+          next_tile_kernel<<<dim3((unsigned)nblk, 2), 256, 0, e->stream>>>(e->ZT32, ld, n, e->d_tinvT, e->d_wnextT));
   e->adj_ready = true;
   return 0;
 }
@@ -1243,7 +1258,7 @@ int refine_T(necgpu_engine* e, const double2* phi, double2* w, int* iters, doubl
   int it = 0;
   for (; it <= e->refine_max; it++) {
     KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<g1, 256, 0, e->stream>>>(r, w1, n));
-    TRY(run_trsv_inv_on(e, e->ZT32, e->d_tinvT, w1, w2));
+    TRY(run_trsv_inv_on(e, e->ZT32, e->d_tinvT, e->d_wnextT, w1, w2));
     KLAUNCH(NECGPU_K_OTHER, 0.0, axpy_scatter_kernel<<<g1, 256, 0, e->stream>>>(w, w2, e->d_perm, n));
     CUDA_TRY(cudaMemsetAsync(e->d_rn2, 0, sizeof(double), e->stream));
     KLAUNCH(NECGPU_K_RESID, (double)n * n * sizeof(double2),

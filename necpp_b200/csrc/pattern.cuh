@@ -3,9 +3,10 @@
 //
 // One warp per direction; a CTA of PAT_DIRS warps stages segment data and
 // current coefficients through shared memory in chunks so each datum is read
-// from L2 once per CTA.  Per (direction, segment) the work is four sines and
-// one sincos: the segment shape factors a, b, c of the sine/cosine/constant
-// current components and the phase exp(j 2pi r.r_i).
+// from L2 once per CTA.  Per (direction, segment) the work is two sincos:
+// the segment shape factors a, b, c of the sine/cosine/constant current
+// components (sin(pi s (1 +- omega)) from the staged sin and cos of pi s by
+// the addition formula) and the phase exp(j 2pi r.r_i).
 #pragma once
 #include <cstdint>
 
@@ -31,7 +32,14 @@ struct PatternArgs {
 
 struct SegPat {
   double x, y, z, s, cab, sab, salp, air, aii, bir, bii, cir, cii;
+  double sel, cel;  // sin and cos of el = pi s (per segment, set when staged)
 };
+
+// the per-segment part of a SegPat's shape factors
+__device__ __forceinline__ void seg_pat_el(SegPat& g) {
+  const double pi = 3.1415926536;
+  sincos(pi * g.s, &g.sel, &g.cel);
+}
 
 __device__ __forceinline__ void seg_term(const SegPat& g, double rox, double roy, double roz,
                                          cplx* exa) {
@@ -41,17 +49,20 @@ __device__ __forceinline__ void seg_term(const SegPat& g, double rox, double roy
   double sill = omega * el;
   double top = el + sill;
   double bot = el - sill;
+  // one sincos per term: sin(el +- sill) from the segment's sin / cos of el
+  double ssill, csill;
+  sincos(sill, &ssill, &csill);
   double a, too, boo;
   if (fabs(omega) >= 1.0e-7)
-    a = 2. * sin(sill) / omega;
+    a = 2. * ssill / omega;
   else
     a = (2. - omega * omega * el * el / 3.) * el;
   if (fabs(top) >= 1.0e-7)
-    too = sin(top) / top;
+    too = (g.sel * csill + g.cel * ssill) / top;
   else
     too = 1. - top * top / 6.;
   if (fabs(bot) >= 1.0e-7)
-    boo = sin(bot) / bot;
+    boo = (g.sel * csill - g.cel * ssill) / bot;
   else
     boo = 1. - bot * bot / 6.;
   double b = el * (boo - too);
@@ -105,6 +116,7 @@ __global__ void __launch_bounds__(kPatDirs * 32) pattern_kernel(PatternArgs A) {
           g.bii = A.abc[3 * A.n + i];
           g.cir = A.abc[4 * A.n + i];
           g.cii = A.abc[5 * A.n + i];
+          seg_pat_el(g);
           seg[t] = g;
         }
       }

@@ -442,25 +442,69 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
+// The product of each diagonal-block inverse with the tile next to it in the
+// sweep order, for the last step of each block:
+//   W[2v]   = inv(L_vv) L_{v,v-1}   (v >= 1; zero for v = 0)
+//   W[2v+1] = inv(U_vv) U_{v,v+1}   (v < nblk - 1; zero for the last block)
+// 64 x 64 row-major each, zero outside the matrix.  grid (nblk, 2), 256
+// threads; blockIdx.y selects the lower (0) or upper (1) product.
+__global__ void __launch_bounds__(256) next_tile_kernel(const float2* M, int64_t ld, int64_t n, const float2* tinv,
+                                                       float2* W) {
+  constexpr int NB = kBlk;
+  __shared__ float2 Tm[NB][NB + 1];
+  const int t = threadIdx.x;
+  const int nblk = (int)((n + NB - 1) / NB);
+  const int v = blockIdx.x, side = blockIdx.y;
+  const int u = side == 0 ? v - 1 : v + 1;
+  float2* out = W + ((int64_t)v * 2 + side) * NB * NB;
+  if (u < 0 || u >= nblk) {
+    for (int e = t; e < NB * NB; e += 256) out[e] = make_float2(0.f, 0.f);
+    return;
+  }
+  const float2* inv = tinv + ((int64_t)v * 2 + side) * NB * NB;
+  const int64_t r0 = (int64_t)v * NB, c0 = (int64_t)u * NB;
+  for (int e = t; e < NB * NB; e += 256) {
+    const int r = e / NB, c = e % NB;
+    Tm[r][c] = (r0 + r < n && c0 + c < n) ? M[(r0 + r) * ld + c0 + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int e = t; e < NB * NB; e += 256) {
+    const int r = e / NB, c = e % NB;  // a warp shares r: the inverse's row is a broadcast load
+    float sr = 0.f, si = 0.f;
+    for (int k = 0; k < NB; k++) {
+      const float2 a = __ldg(inv + r * NB + k), b = Tm[k][c];
+      sr += a.x * b.x - a.y * b.y;
+      si += a.x * b.y + a.y * b.x;
+    }
+    out[e] = make_float2(sr, si);
+  }
+}
+
 // LOWER: x = L^-1 b (unit lower); !LOWER: x = U^-1 b.  counter must be 0 at
 // launch; it counts the completed positions of the sweep order.
 //
-// CTA s owns block row v(s) and accumulates M[v][u] x_u over the positions
-// before it.  Thread 0 alone polls the counter, sleeping longer the further
-// the row is from the sweep front, and the solved blocks known to be
-// complete (up to 16 at a time) are staged in shared memory with one load
-// per element, so the CTAs waiting at the front do not all poll and re-read
-// the same few L2 lines.  Each thread holds the next tile row quarter in
-// registers while it multiplies the current one.  A wait that runs out sets
-// bit 9 of *status; every CTA then returns.
+// CTA s owns block row v(s).  Before the block at the previous position is
+// done it folds in every earlier one, M[v][u] x_u over the positions before
+// s - 1, and forms c = inv(T_vv) (b_v - that sum).  What is left once the
+// previous block arrives is one 64 x 64 product with its precomputed
+// W = inv(T_vv) T_{v,prev} (next_tile_kernel): x_v = c - W x_prev, the only
+// work between two blocks of the sweep besides the counter hand-off.
+// Thread 0 alone polls the counter, sleeping longer the further the row is
+// from the sweep front, and solved blocks known to be complete (up to 16 at a
+// time) are staged in shared memory with one load per element.  Each thread
+// holds the next tile row quarter in registers while it multiplies the
+// current one.  A wait that runs out sets bit 9 of *status; every CTA then
+// returns.
 template <bool LOWER>
-__global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float2* M, int64_t ld, int64_t n,
-                                                                     const float2* tinv, const float2* b, float2* x,
-                                                                     unsigned* counter, int* status) {
+__global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const float2* M, int64_t ld, int64_t n,
+                                                                     const float2* tinv, const float2* wnext,
+                                                                     const float2* b, float2* x, unsigned* counter,
+                                                                     int* status) {
   constexpr int NB = kBlk, QW = NB / 4, KX = kInvSweepChunk;  // four column quarters of 16
   __shared__ float2 part[4][NB];
   __shared__ float2 sv[NB];
   __shared__ float2 sx[KX * NB];
+  __shared__ float2 sinv[NB][NB + 1];  // inv(T_vv), rows padded against bank conflicts
   __shared__ int s_avail;
   const int t = threadIdx.x;
   const int r = t & (NB - 1), q = t >> 6;  // row in the block, column quarter
@@ -470,19 +514,14 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
     const int64_t r0 = (int64_t)v * NB;
     const int bs = (int)min((int64_t)NB, n - r0);
     const bool rowok = r < bs;
-    // independent of the sweep: this thread's 16 entries of row r of
-    // inv(T_vv), and the right-hand side of the block
-    float2 inv[QW];
-    {
-      const float4* ip =
-          reinterpret_cast<const float4*>(tinv + ((int64_t)v * 2 + (LOWER ? 0 : 1)) * NB * NB + r * NB + q * QW);
-#pragma unroll
-      for (int k = 0; k < QW / 2; k++) {
-        const float4 w = ip[k];
-        inv[2 * k] = make_float2(w.x, w.y);
-        inv[2 * k + 1] = make_float2(w.z, w.w);
-      }
-    }
+    // independent of the sweep: inv(T_vv) into shared memory, this thread's
+    // row quarter of W (one 128-byte line, brought into L2 now and read once
+    // the tile loop has freed its registers), and the right-hand side
+    const int64_t bbase = ((int64_t)v * 2 + (LOWER ? 0 : 1)) * NB * NB;
+    const int64_t boff = bbase + r * NB + q * QW;
+    __syncthreads();  // the previous block's reads of sinv are done
+    for (int e = t; e < NB * NB; e += kInvSweepThreads) sinv[e / NB][e % NB] = tinv[bbase + e];
+    if (s > 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(wnext + boff));
     const float2 bb = t < bs ? b[r0 + t] : make_float2(0.f, 0.f);
     // the quarter row of the tile at sweep position i
     auto load_tile = [&](float2 (&m)[QW], int i) {
@@ -502,44 +541,49 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
           m[k] = (rowok && c0 + k < n) ? M[(r0 + r) * ld + c0 + k] : make_float2(0.f, 0.f);
       }
     };
-    float2 m[QW];
-    if (s > 0) load_tile(m, 0);
-    float accr = 0.f, acci = 0.f;
     int avail = 0;  // positions known complete (the same in every thread)
-    for (int i0 = 0; i0 < s;) {
-      if (avail <= i0) {
-        if (t == 0) {
-          const unsigned long long t0 = global_ns();
-          long long spins = 0;
-          int c = (int)ld_acquire_u32(counter);
-          while (c <= i0) {
-            if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
-                global_ns() - t0 > kSweepWaitNs) {
-              atomicOr(status, 1 << 9);
-              c = -1;
-              break;
-            }
-            // the row needs position s - 1 only after s - 1 - c more blocks
-            const int ahead = s - 1 - c;
-            __nanosleep(ahead <= 0 ? 20u : (unsigned)min(ahead * 128, 2048));
-            c = (int)ld_acquire_u32(counter);
+    // thread 0 waits until position `need` is complete; false when a wait ran out
+    auto wait_for = [&](int need) -> bool {
+      if (t == 0) {
+        const unsigned long long t0 = global_ns();
+        long long spins = 0;
+        int c = (int)ld_acquire_u32(counter);
+        while (c <= need) {
+          if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+              global_ns() - t0 > kSweepWaitNs) {
+            atomicOr(status, 1 << 9);
+            c = -1;
+            break;
           }
-          s_avail = c;
+          // the row needs position s - 1 only after s - 1 - c more blocks
+          const int ahead = s - 1 - c;
+          __nanosleep(ahead <= 0 ? 20u : (unsigned)min(ahead * 128, 2048));
+          c = (int)ld_acquire_u32(counter);
         }
-        __syncthreads();  // orders thread 0's acquire before the x reads below
-        avail = s_avail;
-        if (avail < 0) return;
+        s_avail = c;
       }
-      const int i1 = min(s, min(avail, i0 + KX));
+      __syncthreads();  // orders thread 0's acquire before the x reads that follow
+      avail = s_avail;
+      return avail >= 0;
+    };
+    const int lim = s - 1;  // positions folded in before the previous one arrives
+    float2 m[QW];
+    if (lim > 0) load_tile(m, 0);
+    float accr = 0.f, acci = 0.f;
+    bool ok = true;
+    for (int i0 = 0; i0 < lim;) {
+      if (avail <= i0 && !(ok = wait_for(i0))) break;
+      const int i1 = min(lim, min(avail, i0 + KX));
       for (int e = t; e < (i1 - i0) * NB; e += kInvSweepThreads) {
         const int i = i0 + e / NB;
         const int64_t col = (int64_t)(LOWER ? i : nblk - 1 - i) * NB + (e % NB);
         sx[e] = col < n ? __ldcg(x + col) : make_float2(0.f, 0.f);
       }
       __syncthreads();
+#pragma unroll 1
       for (int i = i0; i < i1; i++) {
         float2 mn[QW];
-        if (i + 1 < s) load_tile(mn, i + 1);  // in flight during this tile's products
+        if (i + 1 < lim) load_tile(mn, i + 1);  // in flight during this tile's products
         const float2* xs = sx + (i - i0) * NB + q * QW;
 #pragma unroll
         for (int k = 0; k < QW; k++) {
@@ -547,7 +591,7 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
           accr += m[k].x * xv.x - m[k].y * xv.y;
           acci += m[k].x * xv.y + m[k].y * xv.x;
         }
-        if (i + 1 < s) {
+        if (i + 1 < lim) {
 #pragma unroll
           for (int k = 0; k < QW; k++) m[k] = mn[k];
         }
@@ -555,6 +599,18 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
       __syncthreads();  // sx is reused by the next pass
       i0 = i1;
     }
+    if (!ok) return;
+    float2 wv[QW];
+    if (s > 0) {
+      const float4* wp = reinterpret_cast<const float4*>(wnext + boff);
+#pragma unroll
+      for (int k = 0; k < QW / 2; k++) {
+        const float4 w = wp[k];
+        wv[2 * k] = make_float2(w.x, w.y);
+        wv[2 * k + 1] = make_float2(w.z, w.w);
+      }
+    }
+    // c = inv(T_vv) (b_v - sum so far), row r held by thread r
     part[q][r] = make_float2(accr, acci);
     __syncthreads();
     if (t < NB) {
@@ -570,17 +626,42 @@ __global__ void __launch_bounds__(kInvSweepThreads) inv_sweep_kernel(const float
     acci = 0.f;
 #pragma unroll
     for (int k = 0; k < QW; k++) {
-      const float2 a = sv[q * QW + k];
-      accr += inv[k].x * a.x - inv[k].y * a.y;
-      acci += inv[k].x * a.y + inv[k].y * a.x;
+      const float2 a = sv[q * QW + k], w = sinv[r][q * QW + k];
+      accr += w.x * a.x - w.y * a.y;
+      acci += w.x * a.y + w.y * a.x;
     }
     part[q][r] = make_float2(accr, acci);
     __syncthreads();
-    if (t < bs) {
-      x[r0 + t] = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
-                              part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
-      __threadfence();
+    float2 c = make_float2(0.f, 0.f);
+    if (t < NB)
+      c = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
+                      part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
+    if (s > 0) {
+      // the previous position: x_v = c - W x_prev (the barrier in wait_for,
+      // or the one below, also ends the reads of part above)
+      if (avail < s) {
+        if (!wait_for(s - 1)) return;
+      } else {
+        __syncthreads();
+      }
+      const int64_t cp = (int64_t)(LOWER ? s - 1 : nblk - s) * NB + q * QW;
+      float pr = 0.f, pi = 0.f;
+#pragma unroll
+      for (int k = 0; k < QW; k++) {
+        const float2 xv = cp + k < n ? __ldcg(x + cp + k) : make_float2(0.f, 0.f);
+        pr += wv[k].x * xv.x - wv[k].y * xv.y;
+        pi += wv[k].x * xv.y + wv[k].y * xv.x;
+      }
+      part[q][r] = make_float2(pr, pi);
+      __syncthreads();
+      if (t < bs)
+        x[r0 + t] = make_float2(c.x - (part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x),
+                                c.y - (part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y));
+    } else if (t < bs) {
+      x[r0 + t] = c;
     }
+    // the block's stores are ordered before the counter by the barrier and
+    // thread 0's release at device scope
     __syncthreads();
     if (t == 0) st_release_u32(counter, (unsigned)(s + 1));
   }
