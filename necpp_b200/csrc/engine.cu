@@ -35,6 +35,22 @@ namespace {
 constexpr int kNB = 64;  // LU panel width
 }
 
+// What the launch sequence of a block-pivoted LU depends on: its size, its
+// tuning, its kernels' switches and every buffer and stream it names.
+struct LuGraphKey {
+  int64_t n = 0, ld = 0, outer = 0;
+  int la = 0, la_sms = 0, group = 0, use_tc = 0, trsm8 = 0, nsm = 0;
+  const void* ptr[12] = {};
+  bool operator==(const LuGraphKey& o) const {
+    if (n != o.n || ld != o.ld || outer != o.outer || la != o.la || la_sms != o.la_sms || group != o.group ||
+        use_tc != o.use_tc || trsm8 != o.trsm8 || nsm != o.nsm)
+      return false;
+    for (int i = 0; i < 12; i++)
+      if (ptr[i] != o.ptr[i]) return false;
+    return true;
+  }
+};
+
 struct necgpu_engine {
   int device = 0;
   int nsm = 0;
@@ -134,6 +150,11 @@ struct necgpu_engine {
   // m-tiles per band of the tensor-core update's tile walk
   int gemm_group = 16;
   bool matrix_only = false;      // necgpu_matrix_solve: a caller's matrix, no structure tables
+  // CUDA graph of the block-pivoted LU's launches (run_lu_blockpiv)
+  bool lu_graphs = true;
+  LuGraphKey lu_seen{}, lu_key{};
+  cudaGraphExec_t lu_exec = nullptr;
+  int64_t lu_exec_launches = 0;
   bool tuning_explicit = false;  // necgpu_set_tuning
   necgpu_tuning tuning_set{};
   // environment overrides read at creation (0 / -1: not given)
@@ -326,6 +347,12 @@ int upload(necgpu_engine* e, T*& p, const T* h, size_t count) {
 }
 
 void free_all(necgpu_engine* e) {
+  if (e->lu_exec) {
+    cudaGraphExecDestroy(e->lu_exec);
+    e->lu_exec = nullptr;
+  }
+  e->lu_seen = LuGraphKey{};
+  e->lu_key = LuGraphKey{};
   dfree(e, e->d_seg);
   dfree(e, e->d_ind);
   dfree(e, e->d_tile_ptr);
@@ -929,71 +956,127 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_far, cudaEventDisableTiming));
   }
-  bool far_pending = false;
-  for (int64_t K0 = 0; K0 < n; K0 += outer) {
-    const int64_t KE = std::min<int64_t>(n, K0 + outer);  // end of the outer block
-    const int64_t swap_hi = far_pending ? KE : n;          // columns the far update is not touching
-    gemm_grid = far_pending ? e->lookahead_sms : e->nsm;
-    for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
-      const int kb = (int)std::min<int64_t>(kBlk, n - k0);
-      T* dinv = e->d_dinv + k0;
-      KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
-              diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_src, dinv,
-                                                                   e->d_status));
-      if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
-      const int64_t r0 = k0 + kb, rest = n - r0;
+  // the whole factorisation on the device, as launches on the engine's
+  // stream (and stream2 / stream3, joined back into it)
+  auto issue = [&]() -> int {
+    bool far_pending = false;
+    for (int64_t K0 = 0; K0 < n; K0 += outer) {
+      const int64_t KE = std::min<int64_t>(n, K0 + outer);  // end of the outer block
+      const int64_t swap_hi = far_pending ? KE : n;          // columns the far update is not touching
+      gemm_grid = far_pending ? e->lookahead_sms : e->nsm;
+      for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
+        const int kb = (int)std::min<int64_t>(kBlk, n - k0);
+        T* dinv = e->d_dinv + k0;
+        KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
+                diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_src, dinv,
+                                                                     e->d_status));
+        if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
+        const int64_t r0 = k0 + kb, rest = n - r0;
+        if (rest <= 0) continue;
+        const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
+        // U12 (rows of the block, columns [r0, KE)) and L21 (rows [r0, n),
+        // the block's columns) touch disjoint parts of M: U12 runs on stream3
+        // beside L21, and the update after them waits for both
+        const bool fork = pc > 0 && e->trsm8 && e->stream3;
+        if (fork) {
+          CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
+          CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
+          TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3));
+          CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
+        }
+        TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL));
+        if (pc > 0) {
+          if (fork)
+            CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
+          else
+            TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
+          TRY(gemm(r0, r0, k0, rest, pc, kb));
+        }
+      }
+      gemm_grid = e->nsm;
+      if (far_pending) {
+        // the far update of the previous block is complete: its columns get
+        // this block's interchanges
+        CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
+        far_pending = false;
+        for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
+      }
+      const int64_t rest = n - KE;
       if (rest <= 0) continue;
-      const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
-      // U12 (rows of the block, columns [r0, KE)) and L21 (rows [r0, n),
-      // the block's columns) touch disjoint parts of M: U12 runs on stream3
-      // beside L21, and the update after them waits for both
-      const bool fork = pc > 0 && e->trsm8 && e->stream3;
-      if (fork) {
-        CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
-        CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
-        TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3));
-        CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
+      // U12 of the outer row block: rows [K0, KE), columns [KE, n)
+      for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
+        TRY(gemm(k0, KE, K0, kBlk, rest, (int)(k0 - K0)));
+        TRY(trsm(true, k0, KE, n, e->d_dinv + k0, NECGPU_K_TRSM));
       }
-      TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL));
-      if (pc > 0) {
-        if (fork)
-          CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
-        else
-          TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
-        TRY(gemm(r0, r0, k0, rest, pc, kb));
+      // trailing update with K = outer
+      const int kk = (int)(KE - K0);
+      if (la && rest > outer) {
+        TRY(tc_pack(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk));
+        TRY(tc_run(e, 1, rest, 0, outer, kk, M + KE * ld + KE, ld, e->stream, e->nsm));  // next outer block
+        CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
+        CUDA_TRY(cudaStreamWaitEvent(e->stream2, e->ev_fork, 0));
+        TRY(tc_run(e, 1, rest, outer, rest - outer, kk, M + KE * ld + KE + outer, ld, e->stream2,
+                   e->nsm - e->lookahead_sms));
+        CUDA_TRY(cudaEventRecord(e->ev_far, e->stream2));
+        far_pending = true;
+      } else {
+        TRY(gemm(KE, KE, K0, rest, rest, kk));
       }
     }
-    gemm_grid = e->nsm;
-    if (far_pending) {
-      // the far update of the previous block is complete: its columns get
-      // this block's interchanges
-      CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
-      far_pending = false;
-      for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
-    }
-    const int64_t rest = n - KE;
-    if (rest <= 0) continue;
-    // U12 of the outer row block: rows [K0, KE), columns [KE, n)
-    for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
-      TRY(gemm(k0, KE, K0, kBlk, rest, (int)(k0 - K0)));
-      TRY(trsm(true, k0, KE, n, e->d_dinv + k0, NECGPU_K_TRSM));
-    }
-    // trailing update with K = outer
-    const int kk = (int)(KE - K0);
-    if (la && rest > outer) {
-      TRY(tc_pack(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk));
-      TRY(tc_run(e, 1, rest, 0, outer, kk, M + KE * ld + KE, ld, e->stream, e->nsm));  // next outer block
-      CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
-      CUDA_TRY(cudaStreamWaitEvent(e->stream2, e->ev_fork, 0));
-      TRY(tc_run(e, 1, rest, outer, rest - outer, kk, M + KE * ld + KE + outer, ld, e->stream2,
-                 e->nsm - e->lookahead_sms));
-      CUDA_TRY(cudaEventRecord(e->ev_far, e->stream2));
-      far_pending = true;
-    } else {
-      TRY(gemm(KE, KE, K0, rest, rest, kk));
-    }
+    if (far_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
+    return 0;
+  };
+  // operand buffers at their largest sizes before any capture (no
+  // allocation happens inside the launches below)
+  if (e->use_tc) {
+    TRY(ensure_tc(e, 6 * (int)outer, n, 0));
+    if (la) TRY(ensure_tc(e, 6 * (int)outer, n, 1));
   }
-  if (far_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
+  // CUDA graph of the launch sequence: it depends only on the size, the
+  // tuning and the buffers, so the second factorisation with the same ones
+  // is captured and every later one replays the graph (no per-launch host
+  // submission, shorter gaps between the dependent launches of the panel
+  // chain).  Not while launches are timed, nor when the stream is the legacy
+  // default stream or is being captured by the caller.
+  LuGraphKey key{};
+  key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
+  key.group = e->gemm_group, key.use_tc = e->use_tc, key.trsm8 = e->trsm8, key.nsm = e->nsm;
+  key.ptr[0] = M, key.ptr[1] = e->d_piv, key.ptr[2] = e->d_src, key.ptr[3] = e->d_dinv;
+  key.ptr[4] = e->d_status, key.ptr[5] = e->d_Ap, key.ptr[6] = e->d_Bp, key.ptr[7] = e->d_Ap2;
+  key.ptr[8] = e->d_Bp2, key.ptr[9] = e->stream, key.ptr[10] = e->stream2, key.ptr[11] = e->stream3;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CUDA_TRY(cudaStreamIsCapturing(e->stream, &cap));
+  const bool graphs = e->lu_graphs && e->timing_level < 2 && e->stream && cap == cudaStreamCaptureStatusNone;
+  if (graphs && e->lu_exec && e->lu_key == key) {
+    CUDA_TRY(cudaGraphLaunch(e->lu_exec, e->stream));
+    e->launches += e->lu_exec_launches;
+  } else if (graphs && e->lu_seen == key) {
+    if (e->lu_exec) {
+      cudaGraphExecDestroy(e->lu_exec);
+      e->lu_exec = nullptr;
+    }
+    const int64_t l0 = e->launches;
+    CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeRelaxed));
+    const int rc = issue();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return rc ? rc : fail(e, NECGPU_ERR_CUDA, std::string("LU graph capture: ") + cudaGetErrorString(ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&e->lu_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      e->lu_exec = nullptr;
+      return fail(e, NECGPU_ERR_CUDA, std::string("LU graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    e->lu_key = key;
+    e->lu_exec_launches = e->launches - l0;
+    CUDA_TRY(cudaGraphLaunch(e->lu_exec, e->stream));
+  } else {
+    TRY(issue());
+    e->lu_seen = key;
+  }
   std::vector<int> piv(n), perm(n);
   CUDA_TRY(cudaMemcpyAsync(piv.data(), e->d_piv, n * sizeof(int), cudaMemcpyDeviceToHost, e->stream));
   e->stats.d2h_bytes += n * sizeof(int);
@@ -1613,6 +1696,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_NO_DMMA")) e->use_dmma = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD")) e->env_lookahead = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_TRSM1")) e->trsm8 = (s[0] == '0');
+  if (const char* s = std::getenv("NECPP_B200_LU_GRAPH")) e->lu_graphs = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_GEMM_GROUP")) {
     const int v = std::atoi(s);
     if (v >= 1 && v <= 1024) e->env_group = v;

@@ -118,3 +118,36 @@ def test_tuned_block_lu_backward_error(nb, tuning):
         assert be.value <= 5e-4 and moved.value > 1000
     finally:
         e.close()
+
+
+@pytest.mark.gpu
+def test_lu_graph_replay_matches_eager(nb, oracle):
+    """The block-pivoted LU runs eagerly the first time a size, tuning and
+    buffer set are seen, is captured as a CUDA graph the second time and
+    replayed after that: all three give the same currents bit for bit, and
+    they match the oracle."""
+    from gpu_helpers import Engine
+    from helpers import host_case
+    ctx, st, rhs, _ = host_case(nb, CASES["helix2"][0])
+    Zo, _ = oracle.fill(st)
+    x, _ = oracle.solve(Zo, rhs)
+    _, cur_o = oracle.coefficients(st, x)
+    e = Engine(nb.lib)
+    try:
+        e.set_structure(st)
+        curs, launches = [], []
+        for _ in range(4):
+            e.fill()
+            l0 = e.stats().launches
+            e.factor(1)
+            launches.append(e.stats().launches - l0)
+            cur, _ = e.solve(rhs)
+            curs.append(cur)
+        for c in curs[1:]:
+            assert np.array_equal(c, curs[0])
+        assert np.max(np.abs(curs[0] - cur_o)) / np.max(np.abs(cur_o)) <= 1e-9
+        # the replays account for the launches the graph holds
+        assert launches[2] == launches[1] == launches[3] and launches[0] >= launches[1] > 0
+    finally:
+        e.close()
+        nb.nec_delete(ctx)
