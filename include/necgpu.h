@@ -125,6 +125,13 @@ int necgpu_near_field(necgpu_engine* e, int magnetic, int npts, const double* pt
  * reference's cm layout). */
 int necgpu_fill(necgpu_engine* e);
 
+/* Announce the precision of the factorisations that follow the next fills
+ * (-1: unknown, the default).  With NECGPU_MIXED the fill also writes the
+ * complex64 copy the mixed LU factors, and the factorisation skips its
+ * demotion pass (not for loaded structures, whose loads are applied to the
+ * FP64 matrix after the fill).  Results are the same either way. */
+int necgpu_set_fill_precision(necgpu_engine* e, int precision);
+
 /* Replaces factrs/lu_decompose (src/matrix_algebra.cpp:217-266, 319-338):
  * LU with partial pivoting of the filled Z in the requested precision. */
 int necgpu_factor(necgpu_engine* e, int precision);

@@ -843,6 +843,7 @@ void Context::structure_loading() {
   // Sommerfeld tables of this frequency (calculate_antenna_environment,
   // src/nec_ground.cpp:204-209)
   if (tables.ground == NECGPU_GROUND_SOMMERFELD) check(e, necgpu_set_sommerfeld(e, tables.eps_re, tables.eps_im));
+  check(e, necgpu_set_fill_precision(e, precision_));
   check(e, necgpu_fill(e));
   check(e, necgpu_factor(e, precision_));
   have_factor_ = true;

@@ -150,6 +150,10 @@ struct necgpu_engine {
   // m-tiles per band of the tensor-core update's tile walk
   int gemm_group = 16;
   bool matrix_only = false;      // necgpu_matrix_solve: a caller's matrix, no structure tables
+  // the fill also writes the complex64 copy the mixed LU factors (skipping
+  // the demotion pass) when the next factorisation is announced as mixed
+  int fill_precision = -1;
+  bool z32_fresh = false;  // Z32 holds the demoted current Z64
   // CUDA graph of the block-pivoted LU's launches (run_lu_blockpiv)
   bool lu_graphs = true;
   LuGraphKey lu_seen{}, lu_key{};
@@ -1233,7 +1237,9 @@ int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
 // LU with block-local pivoting (blockpiv) or full partial pivoting.
 int factor_mixed(necgpu_engine* e, bool blockpiv) {
   if (!e->Z32) TRY(dalloc(e, e->Z32, (size_t)e->n * e->ld));
-  KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld));
+  if (!e->z32_fresh)
+    KLAUNCH(NECGPU_K_OTHER, 0.0, demote_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(e->Z64, e->Z32, e->n * e->ld));
+  e->z32_fresh = false;  // the factorisation overwrites it
   e->blockpiv = blockpiv;
   e->stats.pivoting = blockpiv ? 1 : 0;
   e->adj_ready = false;
@@ -1569,10 +1575,13 @@ int run_factor(necgpu_engine* e, int precision) {
 }
 
 int fill_checked(necgpu_engine* e, bool want32) {
+  // loads are applied to Z64 after the fill: their rows' copy would be stale
+  want32 = want32 && !e->d_zload;
   CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
   TRY(run_fill(e, true, want32));
   e->filled = true;
   e->factored = -1;
+  e->z32_fresh = want32;
   return 0;
 }
 
@@ -1855,6 +1864,7 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   e->have_solution = false;
   e->adj_ready = false;
   e->matrix_only = false;
+  e->z32_fresh = false;
   dfree(e, e->d_zload);  // loads belong to one structure: set them after it
   e->somm_ready = false;   // so do the Sommerfeld tables (they follow the frequency)
   dfree(e, e->Z32);  // re-derived from Z64 when a mixed factorisation is asked for
@@ -1922,11 +1932,19 @@ int necgpu_set_structure(necgpu_engine* e, const necgpu_structure* s) {
   return NECGPU_OK;
 }
 
+int necgpu_set_fill_precision(necgpu_engine* e, int precision) {
+  if (!e) return NECGPU_ERR_ARG;
+  if (precision != -1 && precision != NECGPU_FP64 && precision != NECGPU_MIXED)
+    return fail(e, NECGPU_ERR_ARG, "set_fill_precision: -1, NECGPU_FP64 or NECGPU_MIXED");
+  e->fill_precision = precision;
+  return NECGPU_OK;
+}
+
 int necgpu_fill(necgpu_engine* e) {
   if (!e) return NECGPU_ERR_ARG;
   CUDA_TRY(cudaSetDevice(e->device));
   tick(e);
-  TRY(fill_checked(e, false));
+  TRY(fill_checked(e, e->fill_precision == NECGPU_MIXED));
   e->stats.ms_fill = tock(e);
   int st = 0;
   TRY(sync_status(e, &st));
@@ -2034,7 +2052,7 @@ int necgpu_step_resident(necgpu_engine* e, int precision) {
   if (!e || !e->res_rhs) return e ? fail(e, NECGPU_ERR_ARG, "step: no resident inputs") : NECGPU_ERR_ARG;
   CUDA_TRY(cudaSetDevice(e->device));
   tick(e);
-  TRY(fill_checked(e, false));
+  TRY(fill_checked(e, precision == NECGPU_MIXED));
   e->stats.ms_fill = tock(e);
   tick(e);
   TRY(run_factor(e, precision));
