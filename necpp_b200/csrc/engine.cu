@@ -156,6 +156,7 @@ struct necgpu_engine {
   bool z32_fresh = false;  // Z32 holds the demoted current Z64
   // CUDA graph of the block-pivoted LU's launches (run_lu_blockpiv)
   bool lu_graphs = true;
+  bool u12_fused = true;  // the outer row block's U12 in one launch
   LuGraphKey lu_seen{}, lu_key{};
   cudaGraphExec_t lu_exec = nullptr;
   int64_t lu_exec_launches = 0;
@@ -960,6 +961,12 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_far, cudaEventDisableTiming));
   }
+  // the outer row block's U12 in one launch (u12_rows_kernel) when its
+  // finished rows fit in shared memory and its 64-row blocks are whole
+  const bool u12_fused = e->u12_fused && outer % kBlk == 0 && outer / kBlk <= kU12MaxBlocks;
+  if (u12_fused)
+    CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)u12_rows_smem((int)(outer / kBlk))));
   // the whole factorisation on the device, as launches on the engine's
   // stream (and stream2 / stream3, joined back into it)
   auto issue = [&]() -> int {
@@ -998,20 +1005,32 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         }
       }
       gemm_grid = e->nsm;
+      // the far columns still owe this block's interchanges when the far
+      // update of the previous block ran beside its panels
+      const bool swap_far = far_pending;
       if (far_pending) {
-        // the far update of the previous block is complete: its columns get
-        // this block's interchanges
         CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_far, 0));
         far_pending = false;
-        for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
       }
       const int64_t rest = n - KE;
-      if (rest <= 0) continue;
-      // U12 of the outer row block: rows [K0, KE), columns [KE, n)
-      for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
-        TRY(gemm(k0, KE, K0, kBlk, rest, (int)(k0 - K0)));
-        TRY(trsm(true, k0, KE, n, e->d_dinv + k0, NECGPU_K_TRSM));
+      const int nbo = (int)((KE - K0) / kBlk);
+      if (rest > 0 && u12_fused) {
+        // U12 of the outer row block, rows [K0, KE) x columns [KE, n), with
+        // the far columns' interchanges, in one launch
+        KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)(KE - K0) * (double)(KE - K0) * (double)rest,
+                u12_rows_kernel<<<(unsigned)((rest + 31) / 32), 256, (unsigned)u12_rows_smem(nbo), e->stream>>>(
+                    M, ld, K0, nbo, KE, n, e->d_src, swap_far ? 1 : 0));
+      } else {
+        if (swap_far)
+          for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
+        if (rest <= 0) continue;
+        // U12 of the outer row block: rows [K0, KE), columns [KE, n)
+        for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
+          TRY(gemm(k0, KE, K0, kBlk, rest, (int)(k0 - K0)));
+          TRY(trsm(true, k0, KE, n, e->d_dinv + k0, NECGPU_K_TRSM));
+        }
       }
+      if (rest <= 0) continue;
       // trailing update with K = outer
       const int kk = (int)(KE - K0);
       if (la && rest > outer) {
@@ -1044,7 +1063,8 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // default stream or is being captured by the caller.
   LuGraphKey key{};
   key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
-  key.group = e->gemm_group, key.use_tc = e->use_tc, key.trsm8 = e->trsm8, key.nsm = e->nsm;
+  key.group = e->gemm_group, key.use_tc = e->use_tc, key.trsm8 = e->trsm8 * 2 + (u12_fused ? 1 : 0);
+  key.nsm = e->nsm;
   key.ptr[0] = M, key.ptr[1] = e->d_piv, key.ptr[2] = e->d_src, key.ptr[3] = e->d_dinv;
   key.ptr[4] = e->d_status, key.ptr[5] = e->d_Ap, key.ptr[6] = e->d_Bp, key.ptr[7] = e->d_Ap2;
   key.ptr[8] = e->d_Bp2, key.ptr[9] = e->stream, key.ptr[10] = e->stream2, key.ptr[11] = e->stream3;
@@ -1706,6 +1726,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_LOOKAHEAD")) e->env_lookahead = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_TRSM1")) e->trsm8 = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_LU_GRAPH")) e->lu_graphs = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_U12_FUSED")) e->u12_fused = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_GEMM_GROUP")) {
     const int v = std::atoi(s);
     if (v >= 1 && v <= 1024) e->env_group = v;

@@ -788,6 +788,101 @@ __global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int6
   }
 }
 
+// U12 of an outer row block in one launch: rows [K0, K0 + nb*64), columns
+// [c_lo, c_hi) of M, in place.  With `swap`, each 64-row block first takes
+// the row order its diagonal LU chose (the gather of laswp_block_kernel,
+// src_rows[r0 + r] = the block row that ends up in row r).  Then
+// X = L^-1 A with the unit-lower diagonal block L = M[K0.., K0..] of the
+// outer block, left-looking by 64-row blocks:
+//     X_b = L_bb^-1 (A_b - sum_{j<b} L_bj X_j).
+// One CTA per 32 columns (lane = column), 8 warps; warp g holds rows
+// 8g..8g+7 of the current block in registers.  Finished rows stay in shared
+// memory for the later blocks; each L tile is staged once per CTA.  The
+// in-block solve runs in eight stages, one barrier each: warp Q finishes its
+// 8 x 8 triangle and posts its rows, warps g > Q fold them in.  This
+// replaces, per outer block, the deferred interchanges of the far columns
+// and a tensor-core update plus a panel solve for each 64-row block.
+constexpr int kU12MaxBlocks = 8;  // outer blocks up to 512 columns
+__host__ __device__ constexpr size_t u12_rows_smem(int nb) {
+  return (size_t)(nb * kBlk * 33 + kBlk * (kBlk + 1)) * sizeof(float2);
+}
+__global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, int64_t K0, int nb, int64_t c_lo,
+                                                       int64_t c_hi, const int* src_rows, int swap) {
+  constexpr int NB = kBlk;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2(*Xs)[33] = reinterpret_cast<float2(*)[33]>(smem_raw);           // nb*64 finished rows x 32 columns
+  float2(*Lt)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(Xs + nb * NB);  // one staged 64 x 64 tile of L
+  __shared__ int src[NB];
+  const int t = threadIdx.x, lane = t & 31, g = t >> 5;
+  const int64_t col = c_lo + (int64_t)blockIdx.x * 32 + lane;
+  const bool act = col < c_hi;
+  auto stage = [&](int64_t r0, int64_t cl0) {  // Lt = M[r0 .. r0+64, cl0 .. cl0+64)
+    __syncthreads();
+    for (int e = t; e < NB * NB; e += 256) Lt[e >> 6][e & 63] = M[(r0 + (e >> 6)) * ld + cl0 + (e & 63)];
+    __syncthreads();
+  };
+  for (int b = 0; b < nb; b++) {
+    const int64_t r0 = K0 + (int64_t)b * NB;
+    if (swap) {
+      __syncthreads();
+      if (t < NB) src[t] = min(max(src_rows[r0 + t], 0), NB - 1);
+      __syncthreads();
+    }
+    float2 x[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = 8 * g + i;
+      x[i] = act ? M[(r0 + (swap ? src[r] : r)) * ld + col] : make_float2(0.f, 0.f);
+    }
+    for (int j = 0; j < b; j++) {
+      stage(r0, K0 + (int64_t)j * NB);
+#pragma unroll 4
+      for (int k = 0; k < NB; k++) {
+        const float2 xv = Xs[j * NB + k][lane];
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          const float2 l = Lt[8 * g + i][k];
+          x[i].x -= l.x * xv.x - l.y * xv.y;
+          x[i].y -= l.x * xv.y + l.y * xv.x;
+        }
+      }
+    }
+    stage(r0, r0);  // the unit-lower diagonal block (its strict lower part is read)
+#pragma unroll 1
+    for (int Q = 0; Q < 8; Q++) {
+      if (g == Q) {
+#pragma unroll
+        for (int i = 1; i < 8; i++)
+#pragma unroll
+          for (int k = 0; k < i; k++) {
+            const float2 l = Lt[8 * Q + i][8 * Q + k];
+            x[i].x -= l.x * x[k].x - l.y * x[k].y;
+            x[i].y -= l.x * x[k].y + l.y * x[k].x;
+          }
+#pragma unroll
+        for (int i = 0; i < 8; i++) Xs[b * NB + 8 * Q + i][lane] = x[i];
+      }
+      __syncthreads();
+      if (g > Q) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const float2 xv = Xs[b * NB + 8 * Q + k][lane];
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            const float2 l = Lt[8 * g + i][8 * Q + k];
+            x[i].x -= l.x * xv.x - l.y * xv.y;
+            x[i].y -= l.x * xv.y + l.y * xv.x;
+          }
+        }
+      }
+    }
+    if (act) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) M[(r0 + 8 * g + i) * ld + col] = x[i];
+    }
+  }
+}
+
 // Row interchanges of one panel on the columns outside it.
 template <typename T>
 __global__ void laswp_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int kb, const int* piv) {

@@ -162,6 +162,7 @@ e.set_structure(st)
 e.fill()
 e.factor(0)
 call()                      # first call on the device: the set-up
+e.fill()                    # the FP64 factorisation overwrote Z
 e.factor(1)                 # mixed factors; no mixed solve has run in this process
 torch.cuda.synchronize()
 free0, reserved0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_reserved()
