@@ -157,6 +157,7 @@ struct necgpu_engine {
   // CUDA graph of the block-pivoted LU's launches (run_lu_blockpiv)
   bool lu_graphs = true;
   bool u12_fused = true;  // the outer row block's U12 in one launch
+  bool fused_pack = true;  // inner panel solves write the update's packed operands
   LuGraphKey lu_seen{}, lu_key{};
   cudaGraphExec_t lu_exec = nullptr;
   int64_t lu_exec_launches = 0;
@@ -666,7 +667,8 @@ int encode_operand(necgpu_engine* e, CUtensorMap* map, void* base, int kdim, int
 
 // Pack A (m x kb) and B (kb x n), complex64 row-major with leading
 // dimension ld, into operand set `set` (on the engine's stream).
-int tc_pack(necgpu_engine* e, int set, const float2* A, const float2* B, int64_t ld, int64_t m, int64_t n, int kb) {
+int tc_pack(necgpu_engine* e, int set, const float2* A, const float2* B, int64_t ld, int64_t m, int64_t n, int kb,
+            bool pack_b = true) {
   const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
   TRY(ensure_tc(e, 6 * kbp, std::max(m, n), set));
   __nv_bfloat16* Ap = set ? e->d_Ap2 : e->d_Ap;
@@ -674,6 +676,7 @@ int tc_pack(necgpu_engine* e, int set, const float2* A, const float2* B, int64_t
   const int64_t cnt = m * kbp;
   KLAUNCH(NECGPU_K_OTHER, 0.0,
           tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, Ap));
+  if (!pack_b) return 0;
   dim3 g((unsigned)((n + 31) / 32), (unsigned)(kbp / 64));
   KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, Bp));
   return 0;
@@ -885,7 +888,8 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm8_smem<T>()));
   // panel solve: vectors [sbeg, nend) against the 64 x 64 block at k0
   // (LEFT: columns of U12, else rows of L21); kind and flop count for timing
-  auto trsm = [&](bool left, int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind) -> int {
+  auto trsm = [&](bool left, int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind,
+                  __nv_bfloat16* Ap = nullptr, int64_t abase = 0) -> int {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
     const double fl = 4.0 * (double)kBlk * kBlk * cnt;
@@ -903,16 +907,18 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     if (left)
       KLAUNCH(kind, fl, trsm_panel_kernel<T, true><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
     else
-      KLAUNCH(kind, fl, trsm_panel_kernel<T, false><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
+      KLAUNCH(kind, fl,
+              trsm_panel_kernel<T, false><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv, Ap, abase));
     return 0;
   };
   // U12 of an inner panel (eight-warp form) on stream st
-  auto trsm_left_on = [&](int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind, cudaStream_t st) -> int {
+  auto trsm_left_on = [&](int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind, cudaStream_t st,
+                          __nv_bfloat16* Bp = nullptr, int64_t bbase = 0) -> int {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
     const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
     const int kt = kbegin(e, st);
-    trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv);
+    trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv, Bp, bbase);
     kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm8_panel_kernel");
     LAUNCHED();
     return 0;
@@ -964,6 +970,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // the outer row block's U12 in one launch (u12_rows_kernel) when its
   // finished rows fit in shared memory and its 64-row blocks are whole
   const bool u12_fused = e->u12_fused && outer % kBlk == 0 && outer / kBlk <= kU12MaxBlocks;
+  const bool fused_pack = e->fused_pack && e->use_tc;
   if (u12_fused)
     CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)u12_rows_smem((int)(outer / kBlk))));
@@ -989,19 +996,25 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         // the block's columns) touch disjoint parts of M: U12 runs on stream3
         // beside L21, and the update after them waits for both
         const bool fork = pc > 0 && e->trsm8 && e->stream3;
+        // the two panel solves write the update's packed BF16 operands
+        // (operand set 0) as they store their results: no packing passes
+        const bool emit = fork && fused_pack && kb == kBlk;
         if (fork) {
           CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
           CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
-          TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3));
+          TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3, emit ? e->d_Bp : nullptr, r0));
           CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
         }
-        TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL));
+        TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL, emit ? e->d_Ap : nullptr, r0));
         if (pc > 0) {
           if (fork)
             CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
           else
             TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
-          TRY(gemm(r0, r0, k0, rest, pc, kb));
+          if (emit)
+            TRY(tc_run(e, 0, rest, 0, pc, kb, M + r0 * ld + r0, ld, e->stream, gemm_grid));
+          else
+            TRY(gemm(r0, r0, k0, rest, pc, kb));
         }
       }
       gemm_grid = e->nsm;
@@ -1014,12 +1027,16 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       }
       const int64_t rest = n - KE;
       const int nbo = (int)((KE - K0) / kBlk);
+      // the fused U12 also writes the trailing update's packed B operand
+      // (set 1, free: the far update that read it has finished) when the
+      // lookahead path below is taken
+      const bool u12_emit = u12_fused && fused_pack && la && rest > outer && KE - K0 == outer;
       if (rest > 0 && u12_fused) {
         // U12 of the outer row block, rows [K0, KE) x columns [KE, n), with
         // the far columns' interchanges, in one launch
         KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)(KE - K0) * (double)(KE - K0) * (double)rest,
                 u12_rows_kernel<<<(unsigned)((rest + 31) / 32), 256, (unsigned)u12_rows_smem(nbo), e->stream>>>(
-                    M, ld, K0, nbo, KE, n, e->d_src, swap_far ? 1 : 0));
+                    M, ld, K0, nbo, KE, n, e->d_src, swap_far ? 1 : 0, u12_emit ? e->d_Bp2 : nullptr));
       } else {
         if (swap_far)
           for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
@@ -1034,7 +1051,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       // trailing update with K = outer
       const int kk = (int)(KE - K0);
       if (la && rest > outer) {
-        TRY(tc_pack(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk));
+        TRY(tc_pack(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk, !u12_emit));
         TRY(tc_run(e, 1, rest, 0, outer, kk, M + KE * ld + KE, ld, e->stream, e->nsm));  // next outer block
         CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
         CUDA_TRY(cudaStreamWaitEvent(e->stream2, e->ev_fork, 0));
@@ -1063,7 +1080,8 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // default stream or is being captured by the caller.
   LuGraphKey key{};
   key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
-  key.group = e->gemm_group, key.use_tc = e->use_tc, key.trsm8 = e->trsm8 * 2 + (u12_fused ? 1 : 0);
+  key.group = e->gemm_group, key.use_tc = e->use_tc;
+  key.trsm8 = e->trsm8 * 4 + (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
   key.nsm = e->nsm;
   key.ptr[0] = M, key.ptr[1] = e->d_piv, key.ptr[2] = e->d_src, key.ptr[3] = e->d_dinv;
   key.ptr[4] = e->d_status, key.ptr[5] = e->d_Ap, key.ptr[6] = e->d_Bp, key.ptr[7] = e->d_Ap2;
@@ -1727,6 +1745,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_TRSM1")) e->trsm8 = (s[0] == '0');
   if (const char* s = std::getenv("NECPP_B200_LU_GRAPH")) e->lu_graphs = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_U12_FUSED")) e->u12_fused = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_FUSED_PACK")) e->fused_pack = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_GEMM_GROUP")) {
     const int v = std::atoi(s);
     if (v >= 1 && v <= 1024) e->env_group = v;

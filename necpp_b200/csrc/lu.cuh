@@ -14,8 +14,11 @@
 // Pivots are global row indices (0-based); piv[k] = row swapped with k.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include <cuda_runtime.h>
+
+#include "gemm_tc.cuh"
 
 namespace necb {
 
@@ -546,9 +549,51 @@ constexpr size_t trsm_panel_smem() {
   return (size_t)(kBlk * (kBlk + 1) + kTrsmW * (kBlk + 1) + kBlk) * sizeof(T);
 }
 
+// The tensor-core update's packed BF16 operands (gemm_tc.cuh), written by
+// the panel solves that produce them instead of by separate packing passes.
+// kdim = 6 * 64 (one 64-wide panel): A' row i = [Ar_hi Ai_hi Ar_hi Ai_hi
+// Ar_lo Ai_lo]; B' rows 2j, 2j+1 = [Br_hi -Bi_hi Br_lo -Bi_lo Br_hi -Bi_hi],
+// [Bi_hi Br_hi Bi_lo Br_lo Bi_hi Br_hi] (the layouts of pack_a_kernel and
+// pack_b_kernel).
+__device__ __forceinline__ void emit_a(__nv_bfloat16* Ap, int64_t row, int k, float2 a) {
+  __nv_bfloat16 rh, rl, ih, il;
+  tc::split_bf16(a.x, rh, rl);
+  tc::split_bf16(a.y, ih, il);
+  __nv_bfloat16* p = Ap + row * (6 * kBlk) + k;
+  p[0 * kBlk] = rh;
+  p[1 * kBlk] = ih;
+  p[2 * kBlk] = rh;
+  p[3 * kBlk] = ih;
+  p[4 * kBlk] = rl;
+  p[5 * kBlk] = il;
+}
+// eight consecutive k (k0 a multiple of 8) of column j of B: 16-byte stores
+// (kbp: the operand's K per part, a multiple of 64)
+__device__ __forceinline__ void emit_b8(__nv_bfloat16* Bp, int64_t j, int k0, const float2 (&b)[8],
+                                        int kbp = kBlk) {
+  __align__(16) __nv_bfloat16 v[12][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    __nv_bfloat16 rh, rl, ih, il;
+    tc::split_bf16(b[i].x, rh, rl);
+    tc::split_bf16(b[i].y, ih, il);
+    const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
+    v[0][i] = rh, v[1][i] = nih, v[2][i] = rl, v[3][i] = nil, v[4][i] = rh, v[5][i] = nih;
+    v[6][i] = ih, v[7][i] = rh, v[8][i] = il, v[9][i] = rl, v[10][i] = ih, v[11][i] = rh;
+  }
+  __nv_bfloat16* re = Bp + (2 * j) * (6 * (int64_t)kbp) + k0;
+  __nv_bfloat16* im = re + 6 * kbp;
+#pragma unroll
+  for (int s = 0; s < 6; s++) {
+    *reinterpret_cast<uint4*>(re + s * kbp) = *reinterpret_cast<const uint4*>(v[s]);
+    *reinterpret_cast<uint4*>(im + s * kbp) = *reinterpret_cast<const uint4*>(v[6 + s]);
+  }
+}
+
 template <typename T, bool LEFT>
 __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
-                                                            const T* dinv) {
+                                                            const T* dinv, __nv_bfloat16* Ap = nullptr,
+                                                            int64_t abase = 0) {
   constexpr int NB = kBlk, W = kTrsmW, B = 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T(*Tri)[NB + 1] = reinterpret_cast<T(*)[NB + 1]>(smem_raw);
@@ -644,7 +689,12 @@ __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, in
         if (cc < cnt) M[(k0 + r) * ld + s0 + cc] = X[cc][r];
       } else {
         const int rr = e / NB, c = e % NB;
-        if (rr < cnt) M[(s0 + rr) * ld + k0 + c] = X[rr][c];
+        if (rr < cnt) {
+          M[(s0 + rr) * ld + k0 + c] = X[rr][c];
+          // L21 rows are the A operand of the update that follows
+          if constexpr (!LEFT && std::is_same<T, float2>::value)
+            if (Ap) emit_a(Ap, s0 + rr - abase, c, X[rr][c]);
+        }
       }
     }
   }
@@ -668,7 +718,8 @@ constexpr size_t trsm8_smem() {
 // VPL vectors per lane: 32 * VPL vectors per CTA share one triangle load.
 template <typename T, bool LEFT, int VPL = 1>
 __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
-                                                          const T* dinv) {
+                                                          const T* dinv, __nv_bfloat16* Bp = nullptr,
+                                                          int64_t bbase = 0) {
   constexpr int NB = kBlk, V = kTrsm8Vec * VPL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* Tri = reinterpret_cast<T*>(smem_raw);             // element (i, j) at (j>>3)*stride + i*9 + (j&7)
@@ -756,6 +807,9 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
       else
         M[vec[w] * ld + k0 + c] = acc[w][j];
     }
+    // U12 columns are the B operand of the update that follows
+    if constexpr (LEFT && std::is_same<T, float2>::value)
+      if (Bp) emit_b8(Bp, vec[w] - bbase, g * 8, acc[w]);
   }
 }
 
@@ -807,7 +861,8 @@ __host__ __device__ constexpr size_t u12_rows_smem(int nb) {
   return (size_t)(nb * kBlk * 33 + kBlk * (kBlk + 1)) * sizeof(float2);
 }
 __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, int64_t K0, int nb, int64_t c_lo,
-                                                       int64_t c_hi, const int* src_rows, int swap) {
+                                                       int64_t c_hi, const int* src_rows, int swap,
+                                                       __nv_bfloat16* Bp) {
   constexpr int NB = kBlk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2(*Xs)[33] = reinterpret_cast<float2(*)[33]>(smem_raw);           // nb*64 finished rows x 32 columns
@@ -879,6 +934,17 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
     if (act) {
 #pragma unroll
       for (int i = 0; i < 8; i++) M[(r0 + 8 * g + i) * ld + col] = x[i];
+    }
+  }
+  // the rows are the B operand of the trailing update (K = nb * 64): its
+  // packed BF16 form, eight k per store, columns relative to c_lo
+  // (every row of Xs was posted before the last stage's barrier)
+  if (Bp && act) {
+    for (int k8 = g; k8 < nb * 8; k8 += 8) {
+      float2 b[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) b[i] = Xs[k8 * 8 + i][lane];
+      emit_b8(Bp, col - c_lo, k8 * 8, b, nb * NB);
     }
   }
 }
