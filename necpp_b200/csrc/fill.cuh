@@ -20,7 +20,7 @@
 namespace necb {
 
 constexpr int kFillTI = 64;  // observation rows per CTA (= threads)
-constexpr int kFillTB = 32;  // basis columns per CTA
+constexpr int kFillTB = 16;  // basis columns per CTA
 
 struct FillArgs {
   int64_t n, ld;
@@ -143,20 +143,26 @@ __device__ __forceinline__ void fill_tile(const FillArgs& A, const ContractArgs&
     }
     return;
   }
-  // write out: one warp per row, lanes along the (contiguous) columns
-  const int64_t col = (int64_t)tile * kFillTB + lane;
-  for (int r = warp; r < kFillTI; r += kFillTI / 32) {
-    const int64_t row = row0 + r;
+  // write out: consecutive threads along a row's (contiguous) columns
+  (void)lane;
+  (void)warp;
+  const int64_t col0 = (int64_t)tile * kFillTB;
+  for (int e = tid; e < kFillTI * kFillTB; e += kFillTI) {
+    const int r = e / kFillTB, c = e % kFillTB;
+    const int64_t row = row0 + r, col = col0 + c;
     if (row < A.n && col < A.n) {
-      double2 v = acc[lane][r];
+      const double2 v = acc[c][r];
       if (A.Z64) A.Z64[row * A.ld + col] = v;
       if (A.Z32) A.Z32[row * A.ld + col] = make_float2((float)v.x, (float)v.y);
     }
   }
 }
 
+// Free space: registers capped so that eight 64-thread CTAs fit an SM (the
+// fill is latency-bound at six); the ground variants keep their registers
+// (their larger field code spills at the cap).
 template <int GROUND, bool EXK>
-__global__ void __launch_bounds__(kFillTI) fill_kernel(FillArgs A) {
+__global__ void __launch_bounds__(kFillTI, GROUND == 0 ? 8 : 1) fill_kernel(FillArgs A) {
   fill_tile<GROUND, EXK, false>(A, ContractArgs{}, blockIdx.y, (int64_t)blockIdx.x * kFillTI);
 }
 
