@@ -1035,7 +1035,8 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         // U12 of the outer row block, rows [K0, KE) x columns [KE, n), with
         // the far columns' interchanges, in one launch
         KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)(KE - K0) * (double)(KE - K0) * (double)rest,
-                u12_rows_kernel<<<(unsigned)((rest + 31) / 32), 256, (unsigned)u12_rows_smem(nbo), e->stream>>>(
+                u12_rows_kernel<<<(unsigned)((rest + kU12Cols - 1) / kU12Cols), 256, (unsigned)u12_rows_smem(nbo),
+                                  e->stream>>>(
                     M, ld, K0, nbo, KE, n, e->d_src, swap_far ? 1 : 0, u12_emit ? e->d_Bp2 : nullptr));
       } else {
         if (swap_far)
@@ -1254,6 +1255,9 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
     const float2* wnext = wnext_blocks;
     unsigned* counter = e->d_sweep_ctr;
     CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned), e->stream));
+    // every element of the solution starts as the sweep's unset marker
+    // (kSweepUnset in both halves), polled by the block after its owner
+    CUDA_TRY(cudaMemsetAsync(dst, 0xFF, n * sizeof(float2), e->stream));
     void* args[] = {(void*)&Mf,  (void*)&ld,  (void*)&n,       (void*)&tinv,       (void*)&wnext,
                     (void*)&src, (void*)&dst, (void*)&counter, (void*)&e->d_status};
     const int kt = kbegin(e);

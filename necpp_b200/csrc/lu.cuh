@@ -849,27 +849,34 @@ __global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int6
 // X = L^-1 A with the unit-lower diagonal block L = M[K0.., K0..] of the
 // outer block, left-looking by 64-row blocks:
 //     X_b = L_bb^-1 (A_b - sum_{j<b} L_bj X_j).
-// One CTA per 32 columns (lane = column), 8 warps; warp g holds rows
-// 8g..8g+7 of the current block in registers.  Finished rows stay in shared
-// memory for the later blocks; each L tile is staged once per CTA.  The
-// in-block solve runs in eight stages, one barrier each: warp Q finishes its
-// 8 x 8 triangle and posts its rows, warps g > Q fold them in.  This
+// One CTA per 16 columns, 8 warps; lane = column + 16 x half, and warp g
+// holds rows 8g..8g+7 of the current block in registers, four per half.
+// Finished rows stay in shared memory for the later blocks; each L tile is
+// staged once per CTA.  The in-block solve runs in eight stages, one barrier
+// each: warp Q finishes its 8 x 8 triangle (the upper half taking the lower
+// half's four rows by shuffle) and posts its rows, warps g > Q fold them
+// in.  Sixteen columns per CTA keep three CTAs on an SM and halve the
+// sequential work of each.  This
 // replaces, per outer block, the deferred interchanges of the far columns
 // and a tensor-core update plus a panel solve for each 64-row block.
 constexpr int kU12MaxBlocks = 8;  // outer blocks up to 512 columns
+constexpr int kU12Cols = 16;      // columns per CTA
 __host__ __device__ constexpr size_t u12_rows_smem(int nb) {
-  return (size_t)(nb * kBlk * 33 + kBlk * (kBlk + 1)) * sizeof(float2);
+  return (size_t)(nb * kBlk * (kU12Cols + 1) + kBlk * (kBlk + 1)) * sizeof(float2);
 }
 __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, int64_t K0, int nb, int64_t c_lo,
                                                        int64_t c_hi, const int* src_rows, int swap,
                                                        __nv_bfloat16* Bp) {
-  constexpr int NB = kBlk;
+  constexpr int NB = kBlk, CW = kU12Cols;
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2(*Xs)[33] = reinterpret_cast<float2(*)[33]>(smem_raw);           // nb*64 finished rows x 32 columns
+  float2(*Xs)[CW + 1] = reinterpret_cast<float2(*)[CW + 1]>(smem_raw);     // nb*64 finished rows x 16 columns
   float2(*Lt)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(Xs + nb * NB);  // one staged 64 x 64 tile of L
   __shared__ int src[NB];
   const int t = threadIdx.x, lane = t & 31, g = t >> 5;
-  const int64_t col = c_lo + (int64_t)blockIdx.x * 32 + lane;
+  const int cl = lane & (CW - 1), h = lane >> 4;  // column in the tile, half of the warp's eight rows
+  const int rb = 8 * g + 4 * h;                   // first of this thread's four rows
+  const int64_t col = c_lo + (int64_t)blockIdx.x * CW + cl;
   const bool act = col < c_hi;
   auto stage = [&](int64_t r0, int64_t cl0) {  // Lt = M[r0 .. r0+64, cl0 .. cl0+64)
     __syncthreads();
@@ -883,20 +890,20 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
       if (t < NB) src[t] = min(max(src_rows[r0 + t], 0), NB - 1);
       __syncthreads();
     }
-    float2 x[8];
+    float2 x[4];
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int r = 8 * g + i;
+    for (int i = 0; i < 4; i++) {
+      const int r = rb + i;
       x[i] = act ? M[(r0 + (swap ? src[r] : r)) * ld + col] : make_float2(0.f, 0.f);
     }
     for (int j = 0; j < b; j++) {
       stage(r0, K0 + (int64_t)j * NB);
 #pragma unroll 4
       for (int k = 0; k < NB; k++) {
-        const float2 xv = Xs[j * NB + k][lane];
+        const float2 xv = Xs[j * NB + k][cl];
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          const float2 l = Lt[8 * g + i][k];
+        for (int i = 0; i < 4; i++) {
+          const float2 l = Lt[rb + i][k];
           x[i].x -= l.x * xv.x - l.y * xv.y;
           x[i].y -= l.x * xv.y + l.y * xv.x;
         }
@@ -906,25 +913,54 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
 #pragma unroll 1
     for (int Q = 0; Q < 8; Q++) {
       if (g == Q) {
+        // the 8 x 8 triangle of rows 8Q..8Q+7: the lower half first solves
+        // its 4 x 4 triangle, the upper half takes those four values from
+        // the lane 16 below (same column) and then solves its own
+        if (h == 0) {
 #pragma unroll
-        for (int i = 1; i < 8; i++)
+          for (int i = 1; i < 4; i++)
 #pragma unroll
-          for (int k = 0; k < i; k++) {
-            const float2 l = Lt[8 * Q + i][8 * Q + k];
-            x[i].x -= l.x * x[k].x - l.y * x[k].y;
-            x[i].y -= l.x * x[k].y + l.y * x[k].x;
-          }
+            for (int k = 0; k < i; k++) {
+              const float2 l = Lt[rb + i][rb + k];
+              x[i].x -= l.x * x[k].x - l.y * x[k].y;
+              x[i].y -= l.x * x[k].y + l.y * x[k].x;
+            }
+        }
+        float2 y[4];
 #pragma unroll
-        for (int i = 0; i < 8; i++) Xs[b * NB + 8 * Q + i][lane] = x[i];
+        for (int k = 0; k < 4; k++) {
+          y[k].x = __shfl_sync(FULL, x[k].x, cl);
+          y[k].y = __shfl_sync(FULL, x[k].y, cl);
+        }
+        if (h == 1) {
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const float2 l = Lt[rb + i][8 * Q + k];
+              x[i].x -= l.x * y[k].x - l.y * y[k].y;
+              x[i].y -= l.x * y[k].y + l.y * y[k].x;
+            }
+#pragma unroll
+          for (int i = 1; i < 4; i++)
+#pragma unroll
+            for (int k = 0; k < i; k++) {
+              const float2 l = Lt[rb + i][rb + k];
+              x[i].x -= l.x * x[k].x - l.y * x[k].y;
+              x[i].y -= l.x * x[k].y + l.y * x[k].x;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++) Xs[b * NB + rb + i][cl] = x[i];
       }
       __syncthreads();
       if (g > Q) {
 #pragma unroll
         for (int k = 0; k < 8; k++) {
-          const float2 xv = Xs[b * NB + 8 * Q + k][lane];
+          const float2 xv = Xs[b * NB + 8 * Q + k][cl];
 #pragma unroll
-          for (int i = 0; i < 8; i++) {
-            const float2 l = Lt[8 * g + i][8 * Q + k];
+          for (int i = 0; i < 4; i++) {
+            const float2 l = Lt[rb + i][8 * Q + k];
             x[i].x -= l.x * xv.x - l.y * xv.y;
             x[i].y -= l.x * xv.y + l.y * xv.x;
           }
@@ -933,18 +969,18 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
     }
     if (act) {
 #pragma unroll
-      for (int i = 0; i < 8; i++) M[(r0 + 8 * g + i) * ld + col] = x[i];
+      for (int i = 0; i < 4; i++) M[(r0 + rb + i) * ld + col] = x[i];
     }
   }
   // the rows are the B operand of the trailing update (K = nb * 64): its
-  // packed BF16 form, eight k per store, columns relative to c_lo
-  // (every row of Xs was posted before the last stage's barrier)
+  // packed BF16 form, eight k per store, columns relative to c_lo (every
+  // row of Xs was posted before the last stage's barrier)
   if (Bp && act) {
-    for (int k8 = g; k8 < nb * 8; k8 += 8) {
-      float2 b[8];
+    for (int k8 = 2 * g + h; k8 < nb * 8; k8 += 16) {
+      float2 bv[8];
 #pragma unroll
-      for (int i = 0; i < 8; i++) b[i] = Xs[k8 * 8 + i][lane];
-      emit_b8(Bp, col - c_lo, k8 * 8, b, nb * NB);
+      for (int i = 0; i < 8; i++) bv[i] = Xs[k8 * 8 + i][cl];
+      emit_b8(Bp, col - c_lo, k8 * 8, bv, nb * NB);
     }
   }
 }

@@ -428,6 +428,16 @@ __global__ void __launch_bounds__(128) tri_inv_kernel(const float2* M, int64_t l
   }
 }
 
+// The sweeps' "not yet written" marker: every solution element starts as
+// this bit pattern (a NaN no arithmetic here produces from finite data), so
+// the CTA waiting on the previous block can poll the values themselves.
+constexpr unsigned kSweepUnset = 0xFFFFFFFFu;
+__device__ __forceinline__ float2 ld_relaxed_f2(const float2* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return make_float2(__uint_as_float((unsigned)v), __uint_as_float((unsigned)(v >> 32)));
+}
+
 __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -502,6 +512,7 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
                                                                      int* status) {
   constexpr int NB = kBlk, QW = NB / 4, KX = kInvSweepChunk;  // four column quarters of 16
   __shared__ float2 part[4][NB];
+  __shared__ float2 part2[4][NB];  // the last product's partial sums (part may still be read)
   __shared__ float2 sv[NB];
   __shared__ float2 sx[KX * NB];
   __shared__ float2 sinv[NB][NB + 1];  // inv(T_vv), rows padded against bank conflicts
@@ -637,26 +648,44 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
       c = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
                       part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
     if (s > 0) {
-      // the previous position: x_v = c - W x_prev (the barrier in wait_for,
-      // or the one below, also ends the reads of part above)
-      if (avail < s) {
-        if (!wait_for(s - 1)) return;
-      } else {
-        __syncthreads();
-      }
+      // the previous position: x_v = c - W x_prev.  Each thread polls its
+      // sixteen values of x_prev until none is still unset (x starts as
+      // kSweepUnset), which saves the counter's round trip on the chain
       const int64_t cp = (int64_t)(LOWER ? s - 1 : nblk - s) * NB + q * QW;
+      float2 xv[QW];
+      int timed_out = 0;
+      {
+        const unsigned long long t0 = global_ns();
+        long long spins = 0;
+        bool ready = false;
+        while (!ready) {
+          ready = true;
+#pragma unroll
+          for (int k = 0; k < QW; k++) {
+            xv[k] = cp + k < n ? ld_relaxed_f2(x + cp + k) : make_float2(0.f, 0.f);
+            ready = ready && __float_as_uint(xv[k].x) != kSweepUnset && __float_as_uint(xv[k].y) != kSweepUnset;
+          }
+          if (ready) break;
+          if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+              global_ns() - t0 > kSweepWaitNs) {
+            atomicOr(status, 1 << 9);
+            timed_out = 1;
+            break;
+          }
+          __nanosleep(20u);
+        }
+      }
       float pr = 0.f, pi = 0.f;
 #pragma unroll
       for (int k = 0; k < QW; k++) {
-        const float2 xv = cp + k < n ? __ldcg(x + cp + k) : make_float2(0.f, 0.f);
-        pr += wv[k].x * xv.x - wv[k].y * xv.y;
-        pi += wv[k].x * xv.y + wv[k].y * xv.x;
+        pr += wv[k].x * xv[k].x - wv[k].y * xv[k].y;
+        pi += wv[k].x * xv[k].y + wv[k].y * xv[k].x;
       }
-      part[q][r] = make_float2(pr, pi);
-      __syncthreads();
+      part2[q][r] = make_float2(pr, pi);
+      if (__syncthreads_or(timed_out)) return;  // a wait ran out: every thread leaves
       if (t < bs)
-        x[r0 + t] = make_float2(c.x - (part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x),
-                                c.y - (part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y));
+        x[r0 + t] = make_float2(c.x - (part2[0][t].x + part2[1][t].x + part2[2][t].x + part2[3][t].x),
+                                c.y - (part2[0][t].y + part2[1][t].y + part2[2][t].y + part2[3][t].y));
     } else if (t < bs) {
       x[r0 + t] = c;
     }
