@@ -204,7 +204,8 @@ int necgpu_enable_timing(necgpu_engine* e, int on);
 int necgpu_reset_kernel_stats(necgpu_engine* e);
 
 /* One launch of the trace: class (necgpu_kernel_class), stream (0 the
-   engine's, 2 the lookahead's far update, 3 the U12 panel solves, 1 other),
+   engine's, 2 the lookahead's far update, 3 the U12 panel solves, 4 the
+   panel solves and updates below the next panel's rows, 1 other),
    start and end in ms after the trace origin, its algorithmic work (the unit
    of its class) and the launch expression (truncated). */
 typedef struct necgpu_trace_rec {

@@ -40,12 +40,12 @@ constexpr int kNB = 64;  // LU panel width
 struct LuGraphKey {
   int64_t n = 0, ld = 0, outer = 0;
   int la = 0, la_sms = 0, group = 0, use_tc = 0, trsm8 = 0, nsm = 0;
-  const void* ptr[12] = {};
+  const void* ptr[14] = {};
   bool operator==(const LuGraphKey& o) const {
     if (n != o.n || ld != o.ld || outer != o.outer || la != o.la || la_sms != o.la_sms || group != o.group ||
         use_tc != o.use_tc || trsm8 != o.trsm8 || nsm != o.nsm)
       return false;
-    for (int i = 0; i < 12; i++)
+    for (int i = 0; i < 14; i++)
       if (ptr[i] != o.ptr[i]) return false;
     return true;
   }
@@ -110,7 +110,7 @@ struct necgpu_engine {
   struct PendingK {
     int cls, ev;
     double flops;
-    int stream;        // 0 engine stream, 2 / 3 the lookahead and U12 streams, 1 other
+    int stream;        // 0 engine stream, 2 / 3 / 4 the far update, U12 and bulk L21 streams, 1 other
     const char* name;  // launch expression (static storage) or null
   };
   // timing level 3: every timed launch with its start and end on a common
@@ -143,6 +143,14 @@ struct necgpu_engine {
   cudaEvent_t ev_fork = nullptr, ev_far = nullptr;
   // stream3: each inner panel's U12 solve beside its L21 solve
   cudaStream_t stream3 = nullptr;
+  // stream4: each inner panel's L21 solve and update below the next
+  // panel's rows, beside the next diagonal LU; its B operand alternates
+  // between d_Bp and d_Bp3
+  cudaStream_t stream4 = nullptr;
+  cudaEvent_t ev_diag = nullptr, ev_bulk = nullptr;
+  __nv_bfloat16* d_Bp3 = nullptr;
+  size_t bp3_elems = 0;
+  bool inner_split = true;
   cudaEvent_t ev_u12a = nullptr, ev_u12b = nullptr;
   // tuning in effect for the current factorisation (select_tuning)
   bool lookahead = true;
@@ -284,7 +292,7 @@ void kend(necgpu_engine* e, int i, int cls, double flops, cudaStream_t st = null
   if (i < 0) return;
   cudaStream_t s = st ? st : e->stream;
   cudaEventRecord(e->kev[i + 1], s);
-  const int sid = s == e->stream ? 0 : s == e->stream2 ? 2 : s == e->stream3 ? 3 : 1;
+  const int sid = s == e->stream ? 0 : s == e->stream2 ? 2 : s == e->stream3 ? 3 : s == e->stream4 ? 4 : 1;
   e->kpend.push_back({cls, i, flops, sid, name});
 }
 void kflush(necgpu_engine* e) {  // call after the stream has synchronised
@@ -382,6 +390,7 @@ void free_all(necgpu_engine* e) {
   e->near_cap = 0;
   dfree(e, e->d_Ap2);
   dfree(e, e->d_Bp2);
+  dfree(e, e->d_Bp3);
   e->tc_rows2 = 0;
   e->tc_kdim2 = 0;
   dfree(e, e->d_tinv);
@@ -685,11 +694,11 @@ int tc_pack(necgpu_engine* e, int set, const float2* A, const float2* B, int64_t
 // C (m x ncols) -= A' B'[columns j0, j0 + ncols) from operand set `set`, on
 // stream st with at most grid_max persistent CTAs.
 int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int kb, float2* C, int64_t ld,
-           cudaStream_t st, int grid_max) {
+           cudaStream_t st, int grid_max, int64_t a_row0 = 0, __nv_bfloat16* Bp_alt = nullptr) {
   const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
   const int kdim = 6 * kbp;
-  __nv_bfloat16* Ap = set ? e->d_Ap2 : e->d_Ap;
-  __nv_bfloat16* Bp = set ? e->d_Bp2 : e->d_Bp;
+  __nv_bfloat16* Ap = (set ? e->d_Ap2 : e->d_Ap) + a_row0 * kdim;
+  __nv_bfloat16* Bp = Bp_alt ? Bp_alt : set ? e->d_Bp2 : e->d_Bp;
   CUtensorMap tmA, tmB, tmC;
   TRY(encode_operand(e, &tmA, Ap, kdim, m, tc::BM));
   TRY(encode_operand(e, &tmB, Bp + 2 * j0 * kdim, kdim, 2 * ncols, tc::BN));
@@ -923,6 +932,19 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     LAUNCHED();
     return 0;
   };
+  // L21 rows [sbeg, nend) of the panel at k0 (one row per thread) on stream st
+  auto trsm_on = [&](int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind, cudaStream_t st,
+                     __nv_bfloat16* Ap, int64_t abase) -> int {
+    const int64_t cnt = nend - sbeg;
+    if (cnt <= 0) return 0;
+    const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);
+    const int kt = kbegin(e, st);
+    trsm_panel_kernel<T, false><<<g, kTrsmW, (unsigned)trsm_panel_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv, Ap,
+                                                                                   abase);
+    kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm_panel_kernel");
+    LAUNCHED();
+    return 0;
+  };
   if (e->trsm8 && !e->stream3) {
     CUDA_TRY(cudaStreamCreateWithFlags(&e->stream3, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_u12a, cudaEventDisableTiming));
@@ -971,6 +993,15 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // finished rows fit in shared memory and its 64-row blocks are whole
   const bool u12_fused = e->u12_fused && outer % kBlk == 0 && outer / kBlk <= kU12MaxBlocks;
   const bool fused_pack = e->fused_pack && e->use_tc;
+  // each inner panel's L21 solve and update split at the next panel's rows:
+  // the part that the next diagonal LU needs on the engine's stream, the
+  // rest on stream4 beside it
+  const bool split_inner = e->inner_split && fused_pack && e->trsm8;
+  if (split_inner && !e->stream4) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->stream4, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_diag, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->ev_bulk, cudaEventDisableTiming));
+  }
   if (u12_fused)
     CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)u12_rows_smem((int)(outer / kBlk))));
@@ -982,16 +1013,52 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       const int64_t KE = std::min<int64_t>(n, K0 + outer);  // end of the outer block
       const int64_t swap_hi = far_pending ? KE : n;          // columns the far update is not touching
       gemm_grid = far_pending ? e->lookahead_sms : e->nsm;
+      bool bulk_pending = false;  // stream4 holds the last panel's work below the next panel's rows
       for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
         const int kb = (int)std::min<int64_t>(kBlk, n - k0);
         T* dinv = e->d_dinv + k0;
         KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
                 diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_src, dinv,
                                                                      e->d_status));
-        if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
         const int64_t r0 = k0 + kb, rest = n - r0;
-        if (rest <= 0) continue;
         const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
+        const bool split = split_inner && kb == kBlk && pc > 0 && rest > 2 * kBlk;
+        if (split) CUDA_TRY(cudaEventRecord(e->ev_diag, e->stream));  // U11 and its reciprocal diagonal are ready
+        if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
+        if (rest <= 0) continue;
+        if (split) {
+          // Rows [r0, r0 + 64) (the next diagonal block's) take their L21
+          // rows and update on this stream; the rows below take theirs on
+          // stream4, beside the next diagonal LU.  The A operand's rows are
+          // split the same way; the B operand alternates between two
+          // buffers so that U12 of the next panel never overwrites the one
+          // the bulk update is reading.
+          const int p = (int)((k0 - K0) / kBlk);
+          __nv_bfloat16* Bsel = (p & 1) ? e->d_Bp3 : e->d_Bp;
+          CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
+          CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
+          TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3, Bsel, r0));
+          CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
+          // the bulk: L21 rows [r0 + 64, n) after the diagonal LU, then their update
+          CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_diag, 0));
+          TRY(trsm_on(k0, r0 + kBlk, n, dinv, NECGPU_K_PANEL, e->stream4, e->d_Ap, r0));
+          CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_u12b, 0));
+          TRY(tc_run(e, 0, rest - kBlk, 0, pc, kb, M + (r0 + kBlk) * ld + r0, ld, e->stream4, gemm_grid, kBlk,
+                     Bsel));
+          // the next diagonal block's rows: their L21 rows need the previous
+          // bulk update (it reached them), then their update
+          if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
+          TRY(trsm(false, k0, r0, r0 + kBlk, dinv, NECGPU_K_PANEL, e->d_Ap, r0));
+          CUDA_TRY(cudaEventRecord(e->ev_bulk, e->stream4));
+          bulk_pending = true;
+          CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
+          TRY(tc_run(e, 0, kBlk, 0, pc, kb, M + r0 * ld + r0, ld, e->stream, gemm_grid, 0, Bsel));
+          continue;
+        }
+        if (bulk_pending) {  // rows below this panel were last updated on stream4
+          CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
+          bulk_pending = false;
+        }
         // U12 (rows of the block, columns [r0, KE)) and L21 (rows [r0, n),
         // the block's columns) touch disjoint parts of M: U12 runs on stream3
         // beside L21, and the update after them waits for both
@@ -1017,6 +1084,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
             TRY(gemm(r0, r0, k0, rest, pc, kb));
         }
       }
+      if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
       gemm_grid = e->nsm;
       // the far columns still owe this block's interchanges when the far
       // update of the previous block ran beside its panels
@@ -1072,6 +1140,13 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   if (e->use_tc) {
     TRY(ensure_tc(e, 6 * (int)outer, n, 0));
     if (la) TRY(ensure_tc(e, 6 * (int)outer, n, 1));
+    if (split_inner) {
+      const size_t need = 2 * (size_t)e->tc_rows * (size_t)e->tc_kdim;
+      if (!e->d_Bp3 || e->bp3_elems < need) {
+        TRY(dalloc(e, e->d_Bp3, need));
+        e->bp3_elems = need;
+      }
+    }
   }
   // CUDA graph of the launch sequence: it depends only on the size, the
   // tuning and the buffers, so the second factorisation with the same ones
@@ -1082,11 +1157,12 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   LuGraphKey key{};
   key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
   key.group = e->gemm_group, key.use_tc = e->use_tc;
-  key.trsm8 = e->trsm8 * 4 + (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
+  key.trsm8 = e->trsm8 * 8 + (split_inner ? 4 : 0) + (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
   key.nsm = e->nsm;
   key.ptr[0] = M, key.ptr[1] = e->d_piv, key.ptr[2] = e->d_src, key.ptr[3] = e->d_dinv;
   key.ptr[4] = e->d_status, key.ptr[5] = e->d_Ap, key.ptr[6] = e->d_Bp, key.ptr[7] = e->d_Ap2;
   key.ptr[8] = e->d_Bp2, key.ptr[9] = e->stream, key.ptr[10] = e->stream2, key.ptr[11] = e->stream3;
+  key.ptr[12] = e->d_Bp3, key.ptr[13] = e->stream4;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CUDA_TRY(cudaStreamIsCapturing(e->stream, &cap));
   const bool graphs = e->lu_graphs && e->timing_level < 2 && e->stream && cap == cudaStreamCaptureStatusNone;
@@ -1750,6 +1826,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_LU_GRAPH")) e->lu_graphs = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_U12_FUSED")) e->u12_fused = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_FUSED_PACK")) e->fused_pack = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_INNER_SPLIT")) e->inner_split = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_GEMM_GROUP")) {
     const int v = std::atoi(s);
     if (v >= 1 && v <= 1024) e->env_group = v;
@@ -1806,6 +1883,12 @@ int necgpu_destroy(necgpu_engine* e) {
   }
   if (e->ev_u12a) cudaEventDestroy(e->ev_u12a);
   if (e->ev_u12b) cudaEventDestroy(e->ev_u12b);
+  if (e->stream4) {
+    cudaStreamSynchronize(e->stream4);
+    cudaStreamDestroy(e->stream4);
+  }
+  if (e->ev_diag) cudaEventDestroy(e->ev_diag);
+  if (e->ev_bulk) cudaEventDestroy(e->ev_bulk);
   if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return NECGPU_OK;

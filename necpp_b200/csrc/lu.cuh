@@ -878,11 +878,31 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
   const int rb = 8 * g + 4 * h;                   // first of this thread's four rows
   const int64_t col = c_lo + (int64_t)blockIdx.x * CW + cl;
   const bool act = col < c_hi;
-  auto stage = [&](int64_t r0, int64_t cl0) {  // Lt = M[r0 .. r0+64, cl0 .. cl0+64)
-    __syncthreads();
-    for (int e = t; e < NB * NB; e += 256) Lt[e >> 6][e & 63] = M[(r0 + (e >> 6)) * ld + cl0 + (e & 63)];
-    __syncthreads();
+  // The L tiles in the order they are used, (b, j) for j = 0..b (j == b:
+  // the diagonal tile), tile (b, j) = M[K0 + 64 b .., K0 + 64 j ..].  Each
+  // one is loaded into registers while the one before is in use, then
+  // posted to shared memory (stage).
+  float2 pf[NB * NB / 256];
+  auto fetch = [&](int tb, int tj) {
+    const float2* src_t = M + (K0 + (int64_t)tb * NB) * ld + K0 + (int64_t)tj * NB;
+#pragma unroll
+    for (int i = 0; i < NB * NB / 256; i++) {
+      const int e = t + i * 256;
+      pf[i] = src_t[(int64_t)(e >> 6) * ld + (e & 63)];
+    }
   };
+  auto stage = [&](int tb, int tj) {  // post the fetched tile, fetch the next one
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NB * NB / 256; i++) {
+      const int e = t + i * 256;
+      Lt[e >> 6][e & 63] = pf[i];
+    }
+    __syncthreads();
+    const int nb_ = tj < tb ? tb : tb + 1, nj = tj < tb ? tj + 1 : 0;
+    if (nb_ < nb) fetch(nb_, nj);
+  };
+  fetch(0, 0);
   for (int b = 0; b < nb; b++) {
     const int64_t r0 = K0 + (int64_t)b * NB;
     if (swap) {
@@ -897,7 +917,7 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
       x[i] = act ? M[(r0 + (swap ? src[r] : r)) * ld + col] : make_float2(0.f, 0.f);
     }
     for (int j = 0; j < b; j++) {
-      stage(r0, K0 + (int64_t)j * NB);
+      stage(b, j);
 #pragma unroll 4
       for (int k = 0; k < NB; k++) {
         const float2 xv = Xs[j * NB + k][cl];
@@ -909,7 +929,7 @@ __global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, in
         }
       }
     }
-    stage(r0, r0);  // the unit-lower diagonal block (its strict lower part is read)
+    stage(b, b);  // the unit-lower diagonal block (its strict lower part is read)
 #pragma unroll 1
     for (int Q = 0; Q < 8; Q++) {
       if (g == Q) {
