@@ -864,7 +864,7 @@ constexpr int kU12Cols = 16;      // columns per CTA
 __host__ __device__ constexpr size_t u12_rows_smem(int nb) {
   return (size_t)(nb * kBlk * (kU12Cols + 1) + kBlk * (kBlk + 1)) * sizeof(float2);
 }
-__global__ void __launch_bounds__(256) u12_rows_kernel(float2* M, int64_t ld, int64_t K0, int nb, int64_t c_lo,
+__global__ void __launch_bounds__(256, 3) u12_rows_kernel(float2* M, int64_t ld, int64_t K0, int nb, int64_t c_lo,
                                                        int64_t c_hi, const int* src_rows, int swap,
                                                        __nv_bfloat16* Bp) {
   constexpr int NB = kBlk, CW = kU12Cols;
