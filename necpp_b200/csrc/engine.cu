@@ -40,12 +40,12 @@ constexpr int kNB = 64;  // LU panel width
 struct LuGraphKey {
   int64_t n = 0, ld = 0, outer = 0;
   int la = 0, la_sms = 0, group = 0, use_tc = 0, trsm8 = 0, nsm = 0;
-  const void* ptr[14] = {};
+  const void* ptr[15] = {};
   bool operator==(const LuGraphKey& o) const {
     if (n != o.n || ld != o.ld || outer != o.outer || la != o.la || la_sms != o.la_sms || group != o.group ||
         use_tc != o.use_tc || trsm8 != o.trsm8 || nsm != o.nsm)
       return false;
-    for (int i = 0; i < 14; i++)
+    for (int i = 0; i < 15; i++)
       if (ptr[i] != o.ptr[i]) return false;
     return true;
   }
@@ -151,6 +151,13 @@ struct necgpu_engine {
   __nv_bfloat16* d_Bp3 = nullptr;
   size_t bp3_elems = 0;
   bool inner_split = true;
+  // the split path's next-block rows (L21, U12 and their update) in one
+  // launch (panel_top_kernel), the panel's interchanges on stream3
+  bool panel_top = true;
+  unsigned* d_top_cnt = nullptr;  // panel_top_kernel's arrival counters (zero between launches)
+  cudaEvent_t ev_swap = nullptr;
+  // launch priority of the panel chain's kernels (0: the streams' own)
+  int chain_prio = 0;
   cudaEvent_t ev_u12a = nullptr, ev_u12b = nullptr;
   // tuning in effect for the current factorisation (select_tuning)
   bool lookahead = true;
@@ -329,6 +336,24 @@ void kflush(necgpu_engine* e) {  // call after the stream has synchronised
     LAUNCHED();                                          \
   } while (0)
 
+// launch with a scheduling priority (0: the stream's own); a CUDA graph
+// captured from the stream keeps it on the kernel node
+template <typename... KArgs, typename... Args>
+cudaError_t launch_prio(int prio, void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                        Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributePriority;
+  attr[0].val.priority = prio;
+  cfg.attrs = attr;
+  cfg.numAttrs = prio ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Device buffers are stream-ordered allocations from the device's default
 // memory pool, whose release threshold necgpu_create raises: memory freed by
 // one engine (or one structure size) stays in the pool and serves the next
@@ -379,6 +404,7 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->d_ccoef);
   dfree(e, e->Z64);
   dfree(e, e->d_dinv);
+  dfree(e, e->d_top_cnt);
   dfree(e, e->d_zload);
   dfree(e, e->d_somm);
   dfree(e, e->d_near_g);
@@ -964,11 +990,17 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                                               M + r0 * ld + c0, ld, m, nc, kk));
     return 0;
   };
-  auto laswp = [&](int64_t k0, int kb, int64_t c_lo, int64_t c_hi) -> int {
+  // interchanges of the panel at k0 on columns [c_lo, c_hi) outside
+  // [k0, skip_hi) (default: the diagonal block), on stream st
+  auto laswp = [&](int64_t k0, int kb, int64_t c_lo, int64_t c_hi, cudaStream_t st = nullptr,
+                   int64_t skip_hi = -1) -> int {
     if (c_hi <= c_lo) return 0;
-    KLAUNCH(NECGPU_K_LASWP, 0.0,
-            laswp_block_kernel<T><<<(unsigned)((c_hi - c_lo + 31) / 32), 256, 0, e->stream>>>(M, ld, c_lo, c_hi, k0,
-                                                                                               kb, e->d_src));
+    cudaStream_t s = st ? st : e->stream;
+    const int kt = kbegin(e, s);
+    laswp_block_kernel<T><<<(unsigned)((c_hi - c_lo + 31) / 32), 256, 0, s>>>(M, ld, c_lo, c_hi, k0, kb, e->d_src,
+                                                                             skip_hi < 0 ? k0 + kb : skip_hi);
+    kend(e, kt, NECGPU_K_LASWP, 0.0, s, "laswp_block_kernel<T>");
+    LAUNCHED();
     return 0;
   };
   // Outer blocks of e->outer columns (a multiple of 64) factored with 64-wide
@@ -1002,6 +1034,14 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_diag, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&e->ev_bulk, cudaEventDisableTiming));
   }
+  // the split panels' next-block rows in one launch (panel_top_kernel),
+  // their interchanges on stream3
+  const bool panel_top = split_inner && e->panel_top && e->stream3 && (outer - kBlk) / kTopCols + 2 <= kTopCnt;
+  if (panel_top && !e->ev_swap) CUDA_TRY(cudaEventCreateWithFlags(&e->ev_swap, cudaEventDisableTiming));
+  if (panel_top && !e->d_top_cnt) {
+    TRY(dalloc(e, e->d_top_cnt, (size_t)kTopCnt));
+    CUDA_TRY(cudaMemsetAsync(e->d_top_cnt, 0, kTopCnt * sizeof(unsigned), e->stream));
+  }
   if (u12_fused)
     CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)u12_rows_smem((int)(outer / kBlk))));
@@ -1014,18 +1054,60 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       const int64_t swap_hi = far_pending ? KE : n;          // columns the far update is not touching
       gemm_grid = far_pending ? e->lookahead_sms : e->nsm;
       bool bulk_pending = false;  // stream4 holds the last panel's work below the next panel's rows
+      bool swap_pending = false;  // stream3 holds interchanges of this block's panels
       for (int64_t k0 = K0; k0 < KE; k0 += kBlk) {
         const int kb = (int)std::min<int64_t>(kBlk, n - k0);
         T* dinv = e->d_dinv + k0;
-        KLAUNCH(NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0,
-                diag_lu_kernel<T><<<1, kDiagThreads, 0, e->stream>>>(M, ld, k0, kb, e->d_piv, e->d_src, dinv,
-                                                                     e->d_status));
+        {
+          const int kt = kbegin(e);
+          CUDA_TRY(launch_prio(e->chain_prio, diag_lu_kernel<T>, dim3(1), dim3(kDiagThreads), 0, e->stream, M, ld, k0,
+                               kb, e->d_piv, e->d_src, dinv, e->d_status));
+          kend(e, kt, NECGPU_K_PANEL, 8.0 * (double)kb * kb * kb / 3.0, nullptr, "diag_lu_kernel<T>");
+          LAUNCHED();
+        }
         const int64_t r0 = k0 + kb, rest = n - r0;
         const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
         const bool split = split_inner && kb == kBlk && pc > 0 && rest > 2 * kBlk;
+        const bool top = split && panel_top;
         if (split) CUDA_TRY(cudaEventRecord(e->ev_diag, e->stream));  // U11 and its reciprocal diagonal are ready
-        if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
+        if (top) {
+          // the interchanges reach columns [r0, KE) through panel_top_kernel's
+          // gather; the others take them on stream3, off the panel chain
+          CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_diag, 0));
+          TRY(laswp(k0, kb, 0, swap_hi, e->stream3, KE));
+          swap_pending = true;
+        } else if (n > kb) {
+          TRY(laswp(k0, kb, 0, swap_hi));
+        }
         if (rest <= 0) continue;
+        if (top) {
+          // the bulk: L21 rows [r0 + 64, n) on stream4 after the diagonal LU;
+          // the next diagonal block's rows (their L21 rows, this panel's U12
+          // and their update) in one launch here, after the previous bulk
+          // update (it reached those rows); then the bulk's update with the
+          // U12 columns that launch wrote as its B operand
+          const int p = (int)((k0 - K0) / kBlk);
+          __nv_bfloat16* Bsel = (p & 1) ? e->d_Bp3 : e->d_Bp;
+          CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_diag, 0));
+          TRY(trsm_on(k0, r0 + kBlk, n, dinv, NECGPU_K_PANEL, e->stream4, e->d_Ap, r0));
+          if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
+          {
+            const dim3 tg((unsigned)((pc + kTopCols - 1) / kTopCols), (unsigned)(kBlk / kTopRows));
+            const int kt = kbegin(e);
+            CUDA_TRY(launch_prio(e->chain_prio, panel_top_kernel, tg, dim3(kTopThreads), 0, e->stream, M, ld, k0,
+                                 KE, (const int*)e->d_src, (const float2*)dinv, Bsel, e->d_top_cnt));
+            kend(e, kt, NECGPU_K_TRSM, 4.0 * (double)kBlk * kBlk * (double)(kBlk + pc) + 8.0 * kBlk * kBlk * pc,
+                 nullptr, "panel_top_kernel");
+            LAUNCHED();
+          }
+          CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream));
+          CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_u12b, 0));
+          TRY(tc_run(e, 0, rest - kBlk, 0, pc, kb, M + (r0 + kBlk) * ld + r0, ld, e->stream4, gemm_grid, kBlk,
+                     Bsel));
+          CUDA_TRY(cudaEventRecord(e->ev_bulk, e->stream4));
+          bulk_pending = true;
+          continue;
+        }
         if (split) {
           // Rows [r0, r0 + 64) (the next diagonal block's) take their L21
           // rows and update on this stream; the rows below take theirs on
@@ -1085,6 +1167,10 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         }
       }
       if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
+      if (swap_pending) {
+        CUDA_TRY(cudaEventRecord(e->ev_swap, e->stream3));
+        CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_swap, 0));
+      }
       gemm_grid = e->nsm;
       // the far columns still owe this block's interchanges when the far
       // update of the previous block ran beside its panels
@@ -1157,12 +1243,13 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   LuGraphKey key{};
   key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
   key.group = e->gemm_group, key.use_tc = e->use_tc;
-  key.trsm8 = e->trsm8 * 8 + (split_inner ? 4 : 0) + (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
+  key.trsm8 = (panel_top ? 32 : 0) + (e->chain_prio ? 16 : 0) + e->trsm8 * 8 + (split_inner ? 4 : 0) +
+              (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
   key.nsm = e->nsm;
   key.ptr[0] = M, key.ptr[1] = e->d_piv, key.ptr[2] = e->d_src, key.ptr[3] = e->d_dinv;
   key.ptr[4] = e->d_status, key.ptr[5] = e->d_Ap, key.ptr[6] = e->d_Bp, key.ptr[7] = e->d_Ap2;
   key.ptr[8] = e->d_Bp2, key.ptr[9] = e->stream, key.ptr[10] = e->stream2, key.ptr[11] = e->stream3;
-  key.ptr[12] = e->d_Bp3, key.ptr[13] = e->stream4;
+  key.ptr[12] = e->d_Bp3, key.ptr[13] = e->stream4, key.ptr[14] = e->d_top_cnt;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CUDA_TRY(cudaStreamIsCapturing(e->stream, &cap));
   const bool graphs = e->lu_graphs && e->timing_level < 2 && e->stream && cap == cudaStreamCaptureStatusNone;
@@ -1827,6 +1914,15 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_U12_FUSED")) e->u12_fused = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_FUSED_PACK")) e->fused_pack = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_INNER_SPLIT")) e->inner_split = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_PANEL_TOP")) e->panel_top = (s[0] != '0');
+  {
+    // the panel chain's launches take the device's greatest priority unless
+    // NECPP_B200_PRIORITY=0
+    int least = 0, greatest = 0;
+    const char* s = std::getenv("NECPP_B200_PRIORITY");
+    if ((!s || s[0] != '0') && cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess)
+      e->chain_prio = greatest;
+  }
   if (const char* s = std::getenv("NECPP_B200_GEMM_GROUP")) {
     const int v = std::atoi(s);
     if (v >= 1 && v <= 1024) e->env_group = v;

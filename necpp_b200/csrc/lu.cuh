@@ -813,21 +813,191 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
   }
 }
 
+// The next diagonal block's rows of a 64-wide inner panel, in one launch
+// (the split inner update).  For the panel at k0, whose LU is in
+// M[k0.., k0..] with its rows in pivot order and whose row order is
+// src_rows[k0 + r] (the block row that ends up in row r), and r0 = k0 + 64:
+//   L21 rows [r0, r0 + 64):  X = A[rows, k0..k0+64) U11^-1
+//   U12 columns J:            Y = L11^-1 A[k0.., J], the panel's rows taken
+//                             in pivot order (the gather of laswp_block_kernel)
+//   A[r0..r0+64, J] -= X Y
+// CTA (x, h) takes the 16 columns J = [r0 + 16x, ...) below c_hi and the 32
+// rows [r0 + 32h, ...).  Both solves run in the eight-stage form of
+// trsm8_panel_kernel side by side (warps 0-7: block g of the 32 L21 rows,
+// one per lane; warps 8-11: blocks 2w, 2w+1 of the 16 U12 columns, one per
+// half-warp lane), and the update is accumulated stage by stage from the
+// two blocks just finished, so it adds no pass of its own.  Each CTA solves
+// the L21 rows of its half and the U12 columns of its group; the results
+// are stored by the last CTA to finish among those that read the same
+// inputs (an arrival counter per L21 half and per column group, reset by
+// that CTA), so no CTA overwrites an input another CTA has yet to load.
+// The U12 columns also go out as the bulk update's packed B operand
+// (column j - r0).  The caller guarantees r0 + 64 <= n; cnt holds
+// 2 + gridDim.x zeroed counters.
+constexpr int kTopCols = 16, kTopRows = 32;
+constexpr int kTopThreads = 32 * 12;
+constexpr int kTopCnt = 128;  // counters the caller provides (2 + column groups)
+__global__ void __launch_bounds__(kTopThreads) panel_top_kernel(float2* M, int64_t ld, int64_t k0, int64_t c_hi,
+                                                                 const int* src_rows, const float2* dinv,
+                                                                 __nv_bfloat16* Bp, unsigned* cnt) {
+  constexpr int NB = kBlk;
+  __shared__ float2 D[NB][NB + 1];
+  __shared__ float2 XR[2][kTopRows][9];
+  __shared__ float2 XL[2][kTopCols][9];
+  __shared__ float2 di[NB];
+  __shared__ int s_last[2];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int64_t r0 = k0 + NB;
+  const int64_t j0 = r0 + (int64_t)blockIdx.x * kTopCols;
+  const int64_t row = r0 + (int64_t)blockIdx.y * kTopRows + lane;  // this lane's L21 row (warps 0-7)
+  const bool lrole = w < 8;
+  const int g = lrole ? w : 2 * (w - 8) + (lane >> 4);
+  const int jl = lane & 15;
+  const int64_t col = j0 + jl;  // this lane's U12 column (warps 8-11)
+  const bool cvalid = !lrole && col < c_hi;
+  // loads: the panel's LU block, this thread's vector block, and (L21
+  // threads) two entries of the block being updated
+  float4 dv[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const int e4 = t + i * kTopThreads;
+    if (e4 < NB * NB / 2) dv[i] = *reinterpret_cast<const float4*>(M + (k0 + e4 / 32) * ld + k0 + (e4 % 32) * 2);
+  }
+  float2 acc[8], cc[2];
+  if (lrole) {
+    const float4* p = reinterpret_cast<const float4*>(M + row * ld + k0 + g * 8);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const float4 v = p[i];
+      acc[2 * i] = make_float2(v.x, v.y);
+      acc[2 * i + 1] = make_float2(v.z, v.w);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int64_t c = j0 + 2 * g + m;
+      cc[m] = c < c_hi ? M[row * ld + c] : czero<float2>();
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int s = min(max(src_rows[k0 + g * 8 + i], 0), NB - 1);
+      acc[i] = cvalid ? M[(k0 + s) * ld + col] : czero<float2>();
+    }
+  }
+  if (t < NB) di[t] = dinv[t];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const int e4 = t + i * kTopThreads;
+    if (e4 < NB * NB / 2) {
+      D[e4 / 32][(e4 % 32) * 2] = make_float2(dv[i].x, dv[i].y);
+      D[e4 / 32][(e4 % 32) * 2 + 1] = make_float2(dv[i].z, dv[i].w);
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int Q = 0; Q < 8; Q++) {
+    const int b = Q & 1;
+    if (g == Q) {  // the diagonal 8 x 8 triangle of block Q, posted for the others
+      if (lrole) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          acc[i] = cmul(acc[i], di[Q * 8 + i]);
+#pragma unroll
+          for (int j = i + 1; j < 8; j++) {
+            const float2 u = D[Q * 8 + i][Q * 8 + j];
+            acc[j].x -= acc[i].x * u.x - acc[i].y * u.y;
+            acc[j].y -= acc[i].x * u.y + acc[i].y * u.x;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i++) XR[b][lane][i] = acc[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; i++)
+#pragma unroll
+          for (int j = i + 1; j < 8; j++) {
+            const float2 l = D[Q * 8 + j][Q * 8 + i];
+            acc[j].x -= acc[i].x * l.x - acc[i].y * l.y;
+            acc[j].y -= acc[i].x * l.y + acc[i].y * l.x;
+          }
+#pragma unroll
+        for (int i = 0; i < 8; i++) XL[b][jl][i] = acc[i];
+      }
+    }
+    __syncthreads();
+    if (g > Q) {  // fold block Q into this thread's block
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const float2 x = lrole ? XR[b][lane][i] : XL[b][jl][i];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const float2 u = lrole ? D[Q * 8 + i][g * 8 + j] : D[g * 8 + j][Q * 8 + i];
+          acc[j].x -= x.x * u.x - x.y * u.y;
+          acc[j].y -= x.x * u.y + x.y * u.x;
+        }
+      }
+    }
+    if (lrole) {  // the update's share of blocks Q: two entries per thread
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const float2 x = XR[b][lane][i];
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+          const float2 y = XL[b][2 * g + m][i];
+          cc[m].x -= x.x * y.x - x.y * y.y;
+          cc[m].y -= x.x * y.y + x.y * y.x;
+        }
+      }
+    }
+  }
+  // every load of this CTA is behind it: count it in, and learn whether
+  // this CTA is the last of its L21 half and of its column group
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    const unsigned a = atomicAdd(&cnt[blockIdx.y], 1u);
+    const unsigned c = atomicAdd(&cnt[2 + blockIdx.x], 1u);
+    s_last[0] = a == gridDim.x - 1;
+    s_last[1] = c == gridDim.y - 1;
+    if (s_last[0]) cnt[blockIdx.y] = 0;
+    if (s_last[1]) cnt[2 + blockIdx.x] = 0;
+    __threadfence();
+  }
+  __syncthreads();
+  if (lrole) {
+    if (s_last[0]) {
+      float4* p = reinterpret_cast<float4*>(M + row * ld + k0 + g * 8);
+#pragma unroll
+      for (int i = 0; i < 4; i++) p[i] = make_float4(acc[2 * i].x, acc[2 * i].y, acc[2 * i + 1].x, acc[2 * i + 1].y);
+    }
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int64_t c = j0 + 2 * g + m;
+      if (c < c_hi) M[row * ld + c] = cc[m];
+    }
+  } else if (s_last[1] && cvalid) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) M[(k0 + g * 8 + i) * ld + col] = acc[i];
+    if (Bp) emit_b8(Bp, col - r0, g * 8, acc);
+  }
+}
+
 // Row interchanges of a block-pivoted panel: the kb <= 64 exchanges stay
 // inside rows [k0, k0+kb), so each column is one gather of those rows
 // (src[k0 + r]: the block row that ends up in row r).  A CTA covers 32
 // columns of [c_lo, c_hi) with 8 row groups; all reads finish (barrier)
-// before any write.  Columns [k0, k0+kb) (the diagonal block) are skipped.
+// before any write.  Columns [k0, skip_hi) (the diagonal block, and the
+// columns panel_top_kernel gathers itself) are skipped.
 template <typename T>
 __global__ void __launch_bounds__(256) laswp_block_kernel(T* M, int64_t ld, int64_t c_lo, int64_t c_hi, int64_t k0,
-                                                          int kb, const int* src_rows) {
+                                                          int kb, const int* src_rows, int64_t skip_hi) {
   constexpr int NB = kBlk, RG = 8, PER = NB / RG;
   __shared__ int src[NB];
   const int t = threadIdx.x, tx = t & 31, g = t >> 5;
   if (t < NB) src[t] = t < kb ? min(max(src_rows[k0 + t], 0), NB - 1) : t;
   __syncthreads();
   const int64_t col = c_lo + (int64_t)blockIdx.x * 32 + tx;
-  const bool act = col < c_hi && !(col >= k0 && col < k0 + kb);
+  const bool act = col < c_hi && !(col >= k0 && col < skip_hi);
   T v[PER];
 #pragma unroll
   for (int i = 0; i < PER; i++) {
