@@ -40,12 +40,12 @@ constexpr int kNB = 64;  // LU panel width
 struct LuGraphKey {
   int64_t n = 0, ld = 0, outer = 0;
   int la = 0, la_sms = 0, group = 0, use_tc = 0, trsm8 = 0, nsm = 0;
-  const void* ptr[15] = {};
+  const void* ptr[16] = {};
   bool operator==(const LuGraphKey& o) const {
     if (n != o.n || ld != o.ld || outer != o.outer || la != o.la || la_sms != o.la_sms || group != o.group ||
         use_tc != o.use_tc || trsm8 != o.trsm8 || nsm != o.nsm)
       return false;
-    for (int i = 0; i < 15; i++)
+    for (int i = 0; i < 16; i++)
       if (ptr[i] != o.ptr[i]) return false;
     return true;
   }
@@ -155,6 +155,13 @@ struct necgpu_engine {
   // launch (panel_top_kernel), the panel's interchanges on stream3
   bool panel_top = true;
   unsigned* d_top_cnt = nullptr;  // panel_top_kernel's arrival counters (zero between launches)
+  __nv_bfloat16* d_Bpan = nullptr;  // its B operand slots, one per panel of an outer block
+  size_t bpan_elems = 0;
+  // L21 rows left-looking with a CTA per 32 rows (l21_rows_kernel) instead
+  // of one row per thread
+  bool l21_rows = true;
+  // CTAs of the rows-below-the-block work on stream4 (L21 solve and update)
+  int side_ctas = 32;
   cudaEvent_t ev_swap = nullptr;
   // launch priority of the panel chain's kernels (0: the streams' own)
   int chain_prio = 0;
@@ -405,6 +412,8 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->Z64);
   dfree(e, e->d_dinv);
   dfree(e, e->d_top_cnt);
+  dfree(e, e->d_Bpan);
+  e->bpan_elems = 0;
   dfree(e, e->d_zload);
   dfree(e, e->d_somm);
   dfree(e, e->d_near_g);
@@ -921,6 +930,10 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm8_smem<T>()));
+  CUDA_TRY(cudaFuncSetAttribute(panel_top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)panel_top_smem()));
+  CUDA_TRY(cudaFuncSetAttribute(l21_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)l21_rows_smem()));
   // panel solve: vectors [sbeg, nend) against the 64 x 64 block at k0
   // (LEFT: columns of U12, else rows of L21); kind and flop count for timing
   auto trsm = [&](bool left, int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind,
@@ -935,6 +948,12 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
       KLAUNCH(kind, fl, trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), e->stream>>>(
                             M, ld, nend, k0, sbeg, dinv));
+      return 0;
+    }
+    if (!left && e->l21_rows) {
+      const unsigned g = (unsigned)std::min<int64_t>((cnt + kL21Rows - 1) / kL21Rows, 4 * (int64_t)e->nsm);
+      KLAUNCH(kind, fl, l21_rows_kernel<<<g, 256, (unsigned)l21_rows_smem(), e->stream>>>(M, ld, nend, k0, sbeg, dinv,
+                                                                                            Ap, abase));
       return 0;
     }
     const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);
@@ -963,11 +982,18 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                      __nv_bfloat16* Ap, int64_t abase) -> int {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
-    const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);
     const int kt = kbegin(e, st);
-    trsm_panel_kernel<T, false><<<g, kTrsmW, (unsigned)trsm_panel_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv, Ap,
-                                                                                   abase);
-    kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm_panel_kernel");
+    if (e->l21_rows) {
+      // a capped persistent grid: this solve runs beside the panel chain
+      const unsigned g = (unsigned)std::min<int64_t>((cnt + kL21Rows - 1) / kL21Rows, e->side_ctas);
+      l21_rows_kernel<<<g, 256, (unsigned)l21_rows_smem(), st>>>(M, ld, nend, k0, sbeg, dinv, Ap, abase);
+      kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "l21_rows_kernel");
+    } else {
+      const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);
+      trsm_panel_kernel<T, false><<<g, kTrsmW, (unsigned)trsm_panel_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv,
+                                                                                     Ap, abase);
+      kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm_panel_kernel");
+    }
     LAUNCHED();
     return 0;
   };
@@ -1036,11 +1062,22 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   }
   // the split panels' next-block rows in one launch (panel_top_kernel),
   // their interchanges on stream3
-  const bool panel_top = split_inner && e->panel_top && e->stream3 && (outer - kBlk) / kTopCols + 2 <= kTopCnt;
+  const bool panel_top = split_inner && e->panel_top && e->stream3 && outer >= 2 * kBlk &&
+                         (outer - kBlk) / kTopRows <= kTopRowGroups &&
+                         kTopRowGroups + (outer - kBlk) / kTopCols <= kTopCnt;
+  // B operand slots of panel_top_kernel, one per panel of an outer block
+  const size_t bpan_slot = 2 * (size_t)(outer - kBlk) * 6 * kBlk;
   if (panel_top && !e->ev_swap) CUDA_TRY(cudaEventCreateWithFlags(&e->ev_swap, cudaEventDisableTiming));
   if (panel_top && !e->d_top_cnt) {
     TRY(dalloc(e, e->d_top_cnt, (size_t)kTopCnt));
     CUDA_TRY(cudaMemsetAsync(e->d_top_cnt, 0, kTopCnt * sizeof(unsigned), e->stream));
+  }
+  if (panel_top) {
+    const size_t need = (size_t)(outer / kBlk - 1) * bpan_slot;
+    if (!e->d_Bpan || e->bpan_elems < need) {
+      TRY(dalloc(e, e->d_Bpan, need));
+      e->bpan_elems = need;
+    }
   }
   if (u12_fused)
     CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1067,47 +1104,53 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         }
         const int64_t r0 = k0 + kb, rest = n - r0;
         const int64_t pc = KE - r0;  // panel columns of this outer block right of the inner panel
-        const bool split = split_inner && kb == kBlk && pc > 0 && rest > 2 * kBlk;
-        const bool top = split && panel_top;
-        if (split) CUDA_TRY(cudaEventRecord(e->ev_diag, e->stream));  // U11 and its reciprocal diagonal are ready
-        if (top) {
-          // the interchanges reach columns [r0, KE) through panel_top_kernel's
-          // gather; the others take them on stream3, off the panel chain
-          CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_diag, 0));
-          TRY(laswp(k0, kb, 0, swap_hi, e->stream3, KE));
-          swap_pending = true;
-        } else if (n > kb) {
-          TRY(laswp(k0, kb, 0, swap_hi));
-        }
-        if (rest <= 0) continue;
-        if (top) {
-          // the bulk: L21 rows [r0 + 64, n) on stream4 after the diagonal LU;
-          // the next diagonal block's rows (their L21 rows, this panel's U12
-          // and their update) in one launch here, after the previous bulk
-          // update (it reached those rows); then the bulk's update with the
-          // U12 columns that launch wrote as its B operand
-          const int p = (int)((k0 - K0) / kBlk);
-          __nv_bfloat16* Bsel = (p & 1) ? e->d_Bp3 : e->d_Bp;
-          CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_diag, 0));
-          TRY(trsm_on(k0, r0 + kBlk, n, dinv, NECGPU_K_PANEL, e->stream4, e->d_Ap, r0));
-          if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
-          {
-            const dim3 tg((unsigned)((pc + kTopCols - 1) / kTopCols), (unsigned)(kBlk / kTopRows));
-            const int kt = kbegin(e);
-            CUDA_TRY(launch_prio(e->chain_prio, panel_top_kernel, tg, dim3(kTopThreads), 0, e->stream, M, ld, k0,
-                                 KE, (const int*)e->d_src, (const float2*)dinv, Bsel, e->d_top_cnt));
-            kend(e, kt, NECGPU_K_TRSM, 4.0 * (double)kBlk * kBlk * (double)(kBlk + pc) + 8.0 * kBlk * kBlk * pc,
-                 nullptr, "panel_top_kernel");
-            LAUNCHED();
+        if (panel_top && kb == kBlk) {
+          // Block rows and columns on this stream, one launch per panel: the
+          // rest of the outer block's rows take their L21 rows, this panel's
+          // U12 (the interchanges gathered as it loads) and their update in
+          // panel_top_kernel.  The rows below the outer block take their L21
+          // rows and update on stream4, needed only by the trailing update;
+          // the panel's interchanges on the other columns go to stream3.
+          // Each panel of the block has its own B operand slot, so this
+          // stream never waits for stream4.
+          CUDA_TRY(cudaEventRecord(e->ev_diag, e->stream));  // U11, its reciprocal diagonal and the row order
+          if (n > kb) {
+            CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_diag, 0));
+            TRY(laswp(k0, kb, 0, swap_hi, e->stream3, KE));
+            swap_pending = true;
           }
-          CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream));
-          CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_u12b, 0));
-          TRY(tc_run(e, 0, rest - kBlk, 0, pc, kb, M + (r0 + kBlk) * ld + r0, ld, e->stream4, gemm_grid, kBlk,
-                     Bsel));
-          CUDA_TRY(cudaEventRecord(e->ev_bulk, e->stream4));
-          bulk_pending = true;
+          if (rest <= 0) continue;
+          const int64_t below = n - KE;
+          if (below > 0) {
+            CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_diag, 0));
+            TRY(trsm_on(k0, KE, n, dinv, NECGPU_K_PANEL, e->stream4, pc > 0 ? e->d_Ap : nullptr, KE));
+          }
+          if (pc > 0) {
+            __nv_bfloat16* Bsel = e->d_Bpan + (size_t)((k0 - K0) / kBlk) * bpan_slot;
+            const dim3 tg((unsigned)((pc + kTopCols - 1) / kTopCols), (unsigned)((pc + kTopRows - 1) / kTopRows));
+            const int kt = kbegin(e);
+            CUDA_TRY(launch_prio(e->chain_prio, panel_top_kernel, tg, dim3(kTopThreads), panel_top_smem(), e->stream,
+                                 M, ld, k0, KE, (const int*)e->d_src, (const float2*)dinv, Bsel, e->d_top_cnt));
+            kend(e, kt, NECGPU_K_TRSM, (4.0 * kBlk * kBlk + 8.0 * kBlk * (double)pc) * 2.0 * (double)pc, nullptr,
+                 "panel_top_kernel");
+            LAUNCHED();
+            if (below > 0) {
+              CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream));
+              CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_u12b, 0));
+              TRY(tc_run(e, 0, below, 0, pc, kb, M + KE * ld + r0, ld, e->stream4,
+                         std::min(gemm_grid, e->side_ctas), 0, Bsel));
+            }
+          }
+          if (below > 0) {
+            CUDA_TRY(cudaEventRecord(e->ev_bulk, e->stream4));
+            bulk_pending = true;
+          }
           continue;
         }
+        const bool split = split_inner && kb == kBlk && pc > 0 && rest > 2 * kBlk;
+        if (split) CUDA_TRY(cudaEventRecord(e->ev_diag, e->stream));  // U11 and its reciprocal diagonal are ready
+        if (n > kb) TRY(laswp(k0, kb, 0, swap_hi));
+        if (rest <= 0) continue;
         if (split) {
           // Rows [r0, r0 + 64) (the next diagonal block's) take their L21
           // rows and update on this stream; the rows below take theirs on
@@ -1166,7 +1209,9 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
             TRY(gemm(r0, r0, k0, rest, pc, kb));
         }
       }
-      if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
+      // (with panel_top_kernel the rows below the outer block are needed
+      // only by the trailing update, and U12 of the row block goes ahead)
+      if (bulk_pending && !panel_top) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
       if (swap_pending) {
         CUDA_TRY(cudaEventRecord(e->ev_swap, e->stream3));
         CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_swap, 0));
@@ -1203,6 +1248,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         }
       }
       if (rest <= 0) continue;
+      if (bulk_pending && panel_top) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
       // trailing update with K = outer
       const int kk = (int)(KE - K0);
       if (la && rest > outer) {
@@ -1243,13 +1289,14 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   LuGraphKey key{};
   key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
   key.group = e->gemm_group, key.use_tc = e->use_tc;
-  key.trsm8 = (panel_top ? 32 : 0) + (e->chain_prio ? 16 : 0) + e->trsm8 * 8 + (split_inner ? 4 : 0) +
+  key.trsm8 = (e->l21_rows ? 64 : 0) + (panel_top ? 32 : 0) + (e->chain_prio ? 16 : 0) + e->trsm8 * 8 + (split_inner ? 4 : 0) +
               (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
-  key.nsm = e->nsm;
+  key.nsm = e->nsm * 4096 + e->side_ctas;
   key.ptr[0] = M, key.ptr[1] = e->d_piv, key.ptr[2] = e->d_src, key.ptr[3] = e->d_dinv;
   key.ptr[4] = e->d_status, key.ptr[5] = e->d_Ap, key.ptr[6] = e->d_Bp, key.ptr[7] = e->d_Ap2;
   key.ptr[8] = e->d_Bp2, key.ptr[9] = e->stream, key.ptr[10] = e->stream2, key.ptr[11] = e->stream3;
   key.ptr[12] = e->d_Bp3, key.ptr[13] = e->stream4, key.ptr[14] = e->d_top_cnt;
+  key.ptr[15] = e->d_Bpan;
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   CUDA_TRY(cudaStreamIsCapturing(e->stream, &cap));
   const bool graphs = e->lu_graphs && e->timing_level < 2 && e->stream && cap == cudaStreamCaptureStatusNone;
@@ -1915,6 +1962,11 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_FUSED_PACK")) e->fused_pack = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_INNER_SPLIT")) e->inner_split = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_PANEL_TOP")) e->panel_top = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_L21_ROWS")) e->l21_rows = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_SIDE_CTAS")) {
+    const int v = std::atoi(s);
+    if (v >= 1 && v <= 1024) e->side_ctas = v;
+  }
   {
     // the panel chain's launches take the device's greatest priority unless
     // NECPP_B200_PRIORITY=0

@@ -310,6 +310,16 @@ __device__ __forceinline__ T crecip(T b) {  // 1 / b, Smith's algorithm
   return r;
 }
 
+// 1 / x for a pivot's |p|^2 in [1e-30, 1e30]: the hardware's approximate
+// reciprocal refined by one Newton-Raphson step (r <- r (2 - x r)), a few
+// ulp at most; the refinement of the solution absorbs it
+__device__ __forceinline__ float pivot_rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r * fmaf(-x, r, 2.f);
+}
+__device__ __forceinline__ double pivot_rcp(double x) { return 1.0 / x; }
+
 // LU with partial pivoting inside the kb x kb diagonal block at (k0, k0)
 // (kb <= 64), in place.  piv[k0 + c] receives the global row exchanged with
 // row k0 + c (exchanges applied in order, as LAPACK's ipiv), src[k0 + r]
@@ -424,14 +434,14 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(T* M, int64_t ld,
         const R m0 = v0.x * v0.x + v0.y * v0.y, m1 = v1.x * v1.x + v1.y * v1.y;
         const bool ok0 = !(used & 1u) && m0 >= (R)0, ok1 = !(used & 2u) && m1 >= (R)0;  // NaN never wins
         // |v|^2 >= 0 orders like its bit pattern
-        const unsigned key0 = ok0 ? __float_as_uint((float)m0) : 0u;
-        const unsigned key1 = ok1 ? __float_as_uint((float)m1) : 0u;
+        // |v|^2 >= 0 orders like its bit pattern; the row rides in the low
+        // six bits (63 - row: ties, to 2^-17 relative, go to the lowest row)
+        const unsigned key0 = ok0 ? (__float_as_uint((float)m0) & ~63u) | (unsigned)(63 - lane) : 0u;
+        const unsigned key1 = ok1 ? (__float_as_uint((float)m1) & ~63u) | (unsigned)(31 - lane) : 0u;
         const unsigned kmax = __reduce_max_sync(FULL, key0 > key1 ? key0 : key1);
         int p;
-        if (kmax > 0u) {
-          const unsigned b0 = __ballot_sync(FULL, ok0 && key0 == kmax);
-          const unsigned b1 = __ballot_sync(FULL, ok1 && key1 == kmax);
-          p = b0 ? __ffs(b0) - 1 : 32 + __ffs(b1) - 1;
+        if (kmax > 63u) {
+          p = 63 - (int)(kmax & 63u);
         } else {  // all zero, or no finite candidate: go on with the first free row
           const unsigned any = __ballot_sync(FULL, ok0 || ok1);
           if (lane == 0) atomicOr(status, any ? kLuStatSingular : kLuStatNonFinite);
@@ -456,7 +466,7 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(T* M, int64_t ld,
         const R d2 = pv.x * pv.x + pv.y * pv.y;
         T pinv;
         if (d2 > (R)1e-30 && d2 < (R)1e30) {
-          const R rr = (R)1 / d2;
+          const R rr = pivot_rcp(d2);
           pinv.x = pv.x * rr;
           pinv.y = -pv.y * rr;
         } else {
@@ -501,26 +511,54 @@ __global__ void __launch_bounds__(kDiagThreads) diag_lu_kernel(T* M, int64_t ld,
     if (nq <= 0) continue;
     // U rows of the panel's pivots on the trailing columns
     if (t < nq) {
+      // every load before the first store (the stores may alias the loads'
+      // rows for all the compiler knows)
       const int q = q0 + t;
+      int pr[W];
       T u[W];
 #pragma unroll
-      for (int i = 0; i < W; i++) {
-        if (i >= w) break;
-        const int pr = s_seq[j0 + i];
-        T v = D[pr][q];
+      for (int i = 0; i < W; i++) pr[i] = i < w ? s_seq[j0 + i] : 0;
+#pragma unroll
+      for (int i = 0; i < W; i++) u[i] = D[pr[i]][q];
+#pragma unroll
+      for (int i = 1; i < W; i++)
 #pragma unroll
         for (int k = 0; k < i; k++) {
-          const T l = D[pr][j0 + k];
-          v.x -= l.x * u[k].x - l.y * u[k].y;
-          v.y -= l.x * u[k].y + l.y * u[k].x;
+          const T lk = D[pr[i]][j0 + k];
+          u[i].x -= lk.x * u[k].x - lk.y * u[k].y;
+          u[i].y -= lk.x * u[k].y + lk.y * u[k].x;
         }
-        u[i] = v;
-        D[pr][q] = v;
-      }
+#pragma unroll
+      for (int i = 0; i < W; i++)
+        if (i < w) D[pr[i]][q] = u[i];
     }
     __syncthreads();
-    // this panel's update of the next panel's columns
-    update(t, kDiagThreads, j0, w, s_used[j & 1], q0, min(kb, q0 + W));
+    // this panel's update of the next panel's columns: column q0 + (t & 7),
+    // rows t >> 3 and (t >> 3) + 32
+    {
+      const int q = q0 + (t & 7), r = t >> 3;
+      if (q < kb && q < q0 + W) {
+        const unsigned char* used_j = s_used[j & 1];
+        int pr[W];
+        T u[W];
+#pragma unroll
+        for (int k = 0; k < W; k++) pr[k] = k < w ? s_seq[j0 + k] : 0;
+#pragma unroll
+        for (int k = 0; k < W; k++) u[k] = k < w ? D[pr[k]][q] : czero<T>();
+        const bool act_a = r < kb && !used_j[r], act_b = r + 32 < kb && !used_j[r + 32];
+        T a = D[r][q], b = D[r + 32][q];
+#pragma unroll
+        for (int k = 0; k < W; k++) {
+          const T la = D[r][j0 + k], lb = D[r + 32][j0 + k];
+          a.x -= la.x * u[k].x - la.y * u[k].y;
+          a.y -= la.x * u[k].y + la.y * u[k].x;
+          b.x -= lb.x * u[k].x - lb.y * u[k].y;
+          b.y -= lb.x * u[k].y + lb.y * u[k].x;
+        }
+        if (act_a) D[r][q] = a;
+        if (act_b) D[r + 32][q] = b;
+      }
+    }
     __syncthreads();
   }
   if (t == 0)
@@ -813,172 +851,373 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
   }
 }
 
-// The next diagonal block's rows of a 64-wide inner panel, in one launch
-// (the split inner update).  For the panel at k0, whose LU is in
-// M[k0.., k0..] with its rows in pivot order and whose row order is
-// src_rows[k0 + r] (the block row that ends up in row r), and r0 = k0 + 64:
-//   L21 rows [r0, r0 + 64):  X = A[rows, k0..k0+64) U11^-1
-//   U12 columns J:            Y = L11^-1 A[k0.., J], the panel's rows taken
-//                             in pivot order (the gather of laswp_block_kernel)
-//   A[r0..r0+64, J] -= X Y
-// CTA (x, h) takes the 16 columns J = [r0 + 16x, ...) below c_hi and the 32
-// rows [r0 + 32h, ...).  Both solves run in the eight-stage form of
-// trsm8_panel_kernel side by side (warps 0-7: block g of the 32 L21 rows,
-// one per lane; warps 8-11: blocks 2w, 2w+1 of the 16 U12 columns, one per
-// half-warp lane), and the update is accumulated stage by stage from the
-// two blocks just finished, so it adds no pass of its own.  Each CTA solves
-// the L21 rows of its half and the U12 columns of its group; the results
-// are stored by the last CTA to finish among those that read the same
-// inputs (an arrival counter per L21 half and per column group, reset by
-// that CTA), so no CTA overwrites an input another CTA has yet to load.
-// The U12 columns also go out as the bulk update's packed B operand
-// (column j - r0).  The caller guarantees r0 + 64 <= n; cnt holds
-// 2 + gridDim.x zeroed counters.
+// Row-block solves X <- X U11^-1 (L21 rows) and Y <- L11^-1 Y (U12
+// columns) against a 64 x 64 LU staged in shared memory, left-looking by
+// 8-column blocks with every thread on the current block.  The eight 8 x 8
+// diagonal blocks are inverted first (W_b = U_bb^-1 with the reciprocal
+// diagonal, V_b = L_bb^-1, one column per lane), so that a block is
+//   pair (row, j):  a_j = A_j - sum_{k < 8b} X_k U_kj        (dot product)
+//                   x_j = sum_{i <= j} a_i W_b[i][j]           (8-lane shuffles)
+// and one barrier separates two blocks.  The operands of the dot products
+// are stored with k contiguous (U transposed, U12 columns transposed) and
+// read two k at a time with 16-byte loads; rows of kS = 66 elements keep
+// those loads aligned and free of bank conflicts across eight rows.
+constexpr int kS = kBlk + 2;
+
+__device__ __forceinline__ void named_barrier(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+__device__ __forceinline__ float2 ld2(const float2* p) { return *p; }
+__device__ __forceinline__ void csub(float2& a, float2 x, float2 y) {  // a -= x y
+  a.x -= x.x * y.x - x.y * y.y;
+  a.y -= x.x * y.y + x.y * y.x;
+}
+__device__ __forceinline__ void cadd(float2& a, float2 x, float2 y) {  // a += x y
+  a.x += x.x * y.x - x.y * y.y;
+  a.y += x.x * y.y + x.y * y.x;
+}
+// a -= sum_{k < n2 * 2} p[k] q[k], both 16-byte aligned, two accumulators
+__device__ __forceinline__ float2 dot_sub(float2 a, const float2* p, const float2* q, int n2) {
+  float2 b = make_float2(0.f, 0.f);
+#pragma unroll 4
+  for (int k = 0; k < n2; k++) {
+    const float4 u = reinterpret_cast<const float4*>(p)[k], v = reinterpret_cast<const float4*>(q)[k];
+    csub(a, make_float2(u.x, u.y), make_float2(v.x, v.y));
+    csub(b, make_float2(u.z, u.w), make_float2(v.z, v.w));
+  }
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+// W_b = U_bb^-1 (U_ii^-1 = di[i]), column j = lane of warp b (lanes 0-7):
+// w_i = (delta_ij - sum_{i < m <= j} U_im w_m) di_i, for i = j down to 0.
+// Ut[j][k] = U[k][j]; W[(b * 8 + i) * 8 + j].
+__device__ __forceinline__ void invert_u_block(const float2* Ut, const float2* di, float2* W, int b, int j) {
+  float2 w[8];
+#pragma unroll
+  for (int i = 7; i >= 0; i--) {
+    float2 v = make_float2(i == j ? 1.f : 0.f, 0.f);
+#pragma unroll
+    for (int m = i + 1; m < 8; m++)
+      if (m <= j) csub(v, Ut[(8 * b + m) * kS + 8 * b + i], w[m]);
+    w[i] = i <= j ? cmul(v, di[8 * b + i]) : make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) W[(b * 8 + i) * 8 + j] = w[i];
+}
+// V_b = L_bb^-1 (unit lower), column m = lane - 8 of warp b (lanes 8-15):
+// v_m = 1, v_i = -sum_{m <= q < i} L_iq v_q.  Dl[i][k] = L[i][k];
+// V[(b * 8 + i) * 8 + m].
+__device__ __forceinline__ void invert_l_block(const float2* Dl, float2* V, int b, int m) {
+  float2 v[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    float2 a = make_float2(i == m ? 1.f : 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < i; q++)
+      if (q >= m) csub(a, Dl[(8 * b + i) * kS + 8 * b + q], v[q]);
+    v[i] = i >= m ? a : make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) V[(b * 8 + i) * 8 + m] = v[i];
+}
+// block b of an L21 row: pair (row r, column j = lane & 7); X rows of kS
+__device__ __forceinline__ void l21_step(float2* X, const float2* Ut, const float2* W, int b, int r, int lane) {
+  const int j = lane & 7;
+  const float2 a = dot_sub(X[r * kS + 8 * b + j], X + r * kS, Ut + (8 * b + j) * kS, 4 * b);
+  float2 x = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const float2 ai = make_float2(__shfl_sync(0xffffffffu, a.x, (lane & ~7) + i),
+                                  __shfl_sync(0xffffffffu, a.y, (lane & ~7) + i));
+    cadd(x, ai, W[(b * 8 + i) * 8 + j]);
+  }
+  X[r * kS + 8 * b + j] = x;
+}
+// staging of the panel's LU: element (r, c) into Ut[c][r] (r <= c) or
+// Dl[r][c] (r > c, when Dl is given); 16-byte loads of two columns
+__device__ __forceinline__ void stage_lu(const float2* M, int64_t ld, int64_t k0, float2* Ut, float2* Dl,
+                                         const float4* v, int t, int nthreads, int nv) {
+  for (int i = 0; i < nv; i++) {
+    const int e = t + i * nthreads;
+    if (e >= kBlk * kBlk / 2) break;
+    const int r = e / 32, c = (e % 32) * 2;
+    const float2 a0 = make_float2(v[i].x, v[i].y), a1 = make_float2(v[i].z, v[i].w);
+    if (r <= c) Ut[c * kS + r] = a0; else if (Dl) Dl[r * kS + c] = a0;
+    if (r <= c + 1) Ut[(c + 1) * kS + r] = a1; else if (Dl) Dl[r * kS + c + 1] = a1;
+  }
+}
+
+// The rest of an outer block's rows and columns for a 64-wide inner panel,
+// in one launch.  For the panel at k0, whose LU is in M[k0.., k0..] with
+// its rows in pivot order and whose row order is src_rows[k0 + r] (the
+// block row that ends up in row r), r0 = k0 + 64 and the outer block's end
+// c_hi:
+//   L21 rows [r0, c_hi):   X = A[rows, k0..k0+64) U11^-1
+//   U12 columns J:          Y = L11^-1 A[k0.., J], the panel's rows taken in
+//                           pivot order (the gather of laswp_block_kernel)
+//   A[rows, J] -= X Y
+// CTA (x, h) takes the 16 columns J = [r0 + 16x, ...) and the 32 rows
+// [r0 + 32h, ...), both below c_hi.  Warps 0-7 solve the L21 rows (pair =
+// row, column of the block), warps 8-11 the U12 columns (pair = column, row
+// of the block; the 8 rows of a column in consecutive lanes), and the
+// update is accumulated block by block as X and Y blocks are finished, two
+// entries per L21 thread.  Each CTA solves the L21 rows of its row group
+// and the U12 columns of its column group; the results are stored by the
+// last CTA to load among those that read the same inputs (an arrival
+// counter per row group and per column group, reset by that CTA), so no CTA
+// overwrites an input another CTA has yet to load.  Warp 12 counts the CTA
+// in once its loads are done, outside the solve's barriers.  The U12
+// columns also go out as the bulk update's packed B operand (column j -
+// r0).  The caller guarantees k0 + 64 <= n and c_hi <= n; cnt holds
+// kTopRowGroups + gridDim.x zeroed counters, gridDim.y <= kTopRowGroups.
 constexpr int kTopCols = 16, kTopRows = 32;
-constexpr int kTopThreads = 32 * 12;
-constexpr int kTopCnt = 128;  // counters the caller provides (2 + column groups)
+constexpr int kTopSolveThreads = 384;
+constexpr int kTopThreads = kTopSolveThreads + 32;
+constexpr int kTopRowGroups = 32;  // row groups of 32 (outer blocks up to 1088 columns)
+constexpr int kTopCnt = 128;       // counters the caller provides
+__host__ __device__ constexpr size_t panel_top_smem() {
+  return (size_t)(2 * kBlk * kS + kTopRows * kS + kTopCols * kS + 2 * 8 * 64 + kBlk) * sizeof(float2);
+}
 __global__ void __launch_bounds__(kTopThreads) panel_top_kernel(float2* M, int64_t ld, int64_t k0, int64_t c_hi,
                                                                  const int* src_rows, const float2* dinv,
                                                                  __nv_bfloat16* Bp, unsigned* cnt) {
-  constexpr int NB = kBlk;
-  __shared__ float2 D[NB][NB + 1];
-  __shared__ float2 XR[2][kTopRows][9];
-  __shared__ float2 XL[2][kTopCols][9];
-  __shared__ float2 di[NB];
+  constexpr int NB = kBlk, NT = kTopSolveThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* Ut = reinterpret_cast<float2*>(smem_raw);  // U11 transposed
+  float2* Dl = Ut + NB * kS;                         // L11
+  float2* X = Dl + NB * kS;                          // L21 rows
+  float2* Yt = X + kTopRows * kS;                    // U12 columns, transposed
+  float2* W = Yt + kTopCols * kS;                    // inverted diagonal blocks of U11
+  float2* V = W + 8 * 64;                            // and of L11
+  float2* di = V + 8 * 64;
   __shared__ int s_last[2];
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int64_t r0 = k0 + NB;
   const int64_t j0 = r0 + (int64_t)blockIdx.x * kTopCols;
-  const int64_t row = r0 + (int64_t)blockIdx.y * kTopRows + lane;  // this lane's L21 row (warps 0-7)
-  const bool lrole = w < 8;
-  const int g = lrole ? w : 2 * (w - 8) + (lane >> 4);
-  const int jl = lane & 15;
-  const int64_t col = j0 + jl;  // this lane's U12 column (warps 8-11)
-  const bool cvalid = !lrole && col < c_hi;
-  // loads: the panel's LU block, this thread's vector block, and (L21
-  // threads) two entries of the block being updated
-  float4 dv[6];
+  const int64_t row0 = r0 + (int64_t)blockIdx.y * kTopRows;
+  const int lr = t >> 3, lc = 2 * (t & 7);  // C pair (t < 256): row lr, columns lc, lc + 1
+  const bool crow = t < 256 && row0 + lr < c_hi;
+  float2 cc[2] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+  if (t < NT) {
+    // all loads in flight before the first shared-memory store
+    float4 dv[6], xv[3];
+    float2 yv[3];
 #pragma unroll
-  for (int i = 0; i < 6; i++) {
-    const int e4 = t + i * kTopThreads;
-    if (e4 < NB * NB / 2) dv[i] = *reinterpret_cast<const float4*>(M + (k0 + e4 / 32) * ld + k0 + (e4 % 32) * 2);
-  }
-  float2 acc[8], cc[2];
-  if (lrole) {
-    const float4* p = reinterpret_cast<const float4*>(M + row * ld + k0 + g * 8);
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const float4 v = p[i];
-      acc[2 * i] = make_float2(v.x, v.y);
-      acc[2 * i + 1] = make_float2(v.z, v.w);
+    for (int i = 0; i < 6; i++) {
+      const int e = t + i * NT;
+      if (e < NB * NB / 2) dv[i] = *reinterpret_cast<const float4*>(M + (k0 + e / 32) * ld + k0 + (e % 32) * 2);
     }
 #pragma unroll
-    for (int m = 0; m < 2; m++) {
-      const int64_t c = j0 + 2 * g + m;
-      cc[m] = c < c_hi ? M[row * ld + c] : czero<float2>();
+    for (int i = 0; i < 3; i++) {
+      const int e = t + i * NT;
+      if (e < kTopRows * NB / 2)
+        xv[i] = row0 + e / 32 < c_hi ? *reinterpret_cast<const float4*>(M + (row0 + e / 32) * ld + k0 + (e % 32) * 2)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int e = t + i * NT;
+      if (e < NB * kTopCols) {
+        const int s = min(max(src_rows[k0 + e / kTopCols], 0), NB - 1);
+        const int64_t c = j0 + e % kTopCols;
+        yv[i] = c < c_hi ? M[(k0 + s) * ld + c] : czero<float2>();
+      }
+    }
+    if (t < 256) {
+#pragma unroll
+      for (int m = 0; m < 2; m++) {
+        const int64_t c = j0 + lc + m;
+        cc[m] = crow && c < c_hi ? M[(row0 + lr) * ld + c] : czero<float2>();
+      }
+    }
+    if (t < NB) di[t] = dinv[t];
+    stage_lu(M, ld, k0, Ut, Dl, dv, t, NT, 6);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int e = t + i * NT;
+      if (e < kTopRows * NB / 2) {
+        X[(e / 32) * kS + (e % 32) * 2] = make_float2(xv[i].x, xv[i].y);
+        X[(e / 32) * kS + (e % 32) * 2 + 1] = make_float2(xv[i].z, xv[i].w);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int e = t + i * NT;
+      if (e < NB * kTopCols) Yt[(e % kTopCols) * kS + e / kTopCols] = yv[i];
+    }
+  }
+  __syncthreads();  // every load of this CTA is behind it
+  if (warp == NT / 32) {
+    // count the CTA in; learn whether it is the last of its row group and
+    // of its column group
+    if (lane == 0) {
+      __threadfence();
+      const unsigned a = atomicAdd(&cnt[blockIdx.y], 1u);
+      const unsigned c = atomicAdd(&cnt[kTopRowGroups + blockIdx.x], 1u);
+      s_last[0] = a == gridDim.x - 1;
+      s_last[1] = c == gridDim.y - 1;
+      if (s_last[0]) cnt[blockIdx.y] = 0;
+      if (s_last[1]) cnt[kTopRowGroups + blockIdx.x] = 0;
+      __threadfence();
     }
   } else {
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int s = min(max(src_rows[k0 + g * 8 + i], 0), NB - 1);
-      acc[i] = cvalid ? M[(k0 + s) * ld + col] : czero<float2>();
+    if (warp < 8) {
+      if (lane < 8)
+        invert_u_block(Ut, di, W, warp, lane);
+      else if (lane < 16)
+        invert_l_block(Dl, V, warp, lane - 8);
     }
-  }
-  if (t < NB) di[t] = dinv[t];
+    named_barrier(1, NT);
+    const int uc = (t - 256) >> 3, ui = t & 7;  // U12 pair (t >= 256): column uc, row ui of the block
+#pragma unroll 1
+    for (int b = 0; b < 8; b++) {
+      if (t < 256) {
+        if (b > 0) {  // C -= X_q Y_q for the block finished last
 #pragma unroll
-  for (int i = 0; i < 6; i++) {
-    const int e4 = t + i * kTopThreads;
-    if (e4 < NB * NB / 2) {
-      D[e4 / 32][(e4 % 32) * 2] = make_float2(dv[i].x, dv[i].y);
-      D[e4 / 32][(e4 % 32) * 2 + 1] = make_float2(dv[i].z, dv[i].w);
+          for (int k = 0; k < 8; k += 2) {
+            const float4 x = *reinterpret_cast<const float4*>(X + lr * kS + 8 * (b - 1) + k);
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+              const float4 y = *reinterpret_cast<const float4*>(Yt + (lc + m) * kS + 8 * (b - 1) + k);
+              csub(cc[m], make_float2(x.x, x.y), make_float2(y.x, y.y));
+              csub(cc[m], make_float2(x.z, x.w), make_float2(y.z, y.w));
+            }
+          }
+        }
+        l21_step(X, Ut, W, b, lr, lane);
+      } else {
+        const float2 a = dot_sub(Yt[uc * kS + 8 * b + ui], Dl + (8 * b + ui) * kS, Yt + uc * kS, 4 * b);
+        float2 y = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          const float2 am = make_float2(__shfl_sync(0xffffffffu, a.x, (lane & ~7) + m),
+                                        __shfl_sync(0xffffffffu, a.y, (lane & ~7) + m));
+          cadd(y, V[(b * 8 + ui) * 8 + m], am);
+        }
+        Yt[uc * kS + 8 * b + ui] = y;
+      }
+      named_barrier(1, NT);
+    }
+    if (t < 256) {
+#pragma unroll
+      for (int k = 0; k < 8; k += 2) {
+        const float4 x = *reinterpret_cast<const float4*>(X + lr * kS + 56 + k);
+#pragma unroll
+        for (int m = 0; m < 2; m++) {
+          const float4 y = *reinterpret_cast<const float4*>(Yt + (lc + m) * kS + 56 + k);
+          csub(cc[m], make_float2(x.x, x.y), make_float2(y.x, y.y));
+          csub(cc[m], make_float2(x.z, x.w), make_float2(y.z, y.w));
+        }
+      }
     }
   }
   __syncthreads();
+  if (s_last[0] && t < NT) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int e = t + i * NT;
+      if (e < kTopRows * NB / 2 && row0 + e / 32 < c_hi) {
+        const float2 a0 = X[(e / 32) * kS + (e % 32) * 2], a1 = X[(e / 32) * kS + (e % 32) * 2 + 1];
+        *reinterpret_cast<float4*>(M + (row0 + e / 32) * ld + k0 + (e % 32) * 2) = make_float4(a0.x, a0.y, a1.x, a1.y);
+      }
+    }
+  }
+  if (s_last[1] && t < NB * kTopCols / 8) {  // one column and eight rows per thread
+    const int c = t % kTopCols, g = t / kTopCols;
+    const int64_t col = j0 + c;
+    if (col < c_hi) {
+      float2 yb[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        yb[i] = Yt[c * kS + 8 * g + i];
+        M[(k0 + 8 * g + i) * ld + col] = yb[i];
+      }
+      if (Bp) emit_b8(Bp, col - r0, g * 8, yb);
+    }
+  }
+  if (crow) {
+#pragma unroll
+    for (int m = 0; m < 2; m++) {
+      const int64_t c = j0 + lc + m;
+      if (c < c_hi) M[(row0 + lr) * ld + c] = cc[m];
+    }
+  }
+}
+
+// L21 rows [sbeg, n_end) of the panel at k0 (x <- x U11^-1) in the form of
+// panel_top_kernel's L21 half, written back with the update's packed A'
+// rows (row - abase) when Ap is given.  Persistent: a CTA stages the
+// panel's U11 and its inverted diagonal blocks once and then takes 32-row
+// chunks blockIdx.x, blockIdx.x + gridDim.x, ...; the next chunk's rows are
+// loaded while the current one is written back.  A small grid keeps the
+// solve, which only the trailing update waits for, on a few SMs beside the
+// panel chain.
+constexpr int kL21Rows = 32;
+__host__ __device__ constexpr size_t l21_rows_smem() {
+  return (size_t)(kBlk * kS + kL21Rows * kS + 8 * 64 + kBlk) * sizeof(float2);
+}
+__global__ void __launch_bounds__(256) l21_rows_kernel(float2* M, int64_t ld, int64_t n_end, int64_t k0,
+                                                        int64_t sbeg, const float2* dinv, __nv_bfloat16* Ap,
+                                                        int64_t abase) {
+  constexpr int NB = kBlk;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* Ut = reinterpret_cast<float2*>(smem_raw);
+  float2* X = Ut + NB * kS;
+  float2* W = X + kL21Rows * kS;
+  float2* di = W + 8 * 64;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int64_t nchunks = (n_end - sbeg + kL21Rows - 1) / kL21Rows;
+  int64_t chunk = blockIdx.x;
+  float4 xv[4];
+  auto load_rows = [&](int64_t ch) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int e = t + i * 256;
+      const int64_t row = sbeg + ch * kL21Rows + e / 32;
+      xv[i] = ch < nchunks && row < n_end ? *reinterpret_cast<const float4*>(M + row * ld + k0 + (e % 32) * 2)
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  };
+  {
+    float4 dv[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int e = t + i * 256;
+      dv[i] = *reinterpret_cast<const float4*>(M + (k0 + e / 32) * ld + k0 + (e % 32) * 2);
+    }
+    load_rows(chunk);
+    if (t < NB) di[t] = dinv[t];
+    stage_lu(M, ld, k0, Ut, nullptr, dv, t, 256, 8);
+  }
+  __syncthreads();
+  if (lane < 8) invert_u_block(Ut, di, W, warp, lane);
+  for (; chunk < nchunks; chunk += gridDim.x) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int e = t + i * 256;
+      X[(e / 32) * kS + (e % 32) * 2] = make_float2(xv[i].x, xv[i].y);
+      X[(e / 32) * kS + (e % 32) * 2 + 1] = make_float2(xv[i].z, xv[i].w);
+    }
+    __syncthreads();
 #pragma unroll 1
-  for (int Q = 0; Q < 8; Q++) {
-    const int b = Q & 1;
-    if (g == Q) {  // the diagonal 8 x 8 triangle of block Q, posted for the others
-      if (lrole) {
+    for (int b = 0; b < 8; b++) {
+      l21_step(X, Ut, W, b, t >> 3, lane);
+      __syncthreads();
+    }
+    load_rows(chunk + gridDim.x);
+    // write back: element (r, k) with consecutive k across a warp (coalesced
+    // rows of M and of the packed A')
+    const int64_t row0 = sbeg + chunk * kL21Rows;
 #pragma unroll
-        for (int i = 0; i < 8; i++) {
-          acc[i] = cmul(acc[i], di[Q * 8 + i]);
-#pragma unroll
-          for (int j = i + 1; j < 8; j++) {
-            const float2 u = D[Q * 8 + i][Q * 8 + j];
-            acc[j].x -= acc[i].x * u.x - acc[i].y * u.y;
-            acc[j].y -= acc[i].x * u.y + acc[i].y * u.x;
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < 8; i++) XR[b][lane][i] = acc[i];
-      } else {
-#pragma unroll
-        for (int i = 0; i < 8; i++)
-#pragma unroll
-          for (int j = i + 1; j < 8; j++) {
-            const float2 l = D[Q * 8 + j][Q * 8 + i];
-            acc[j].x -= acc[i].x * l.x - acc[i].y * l.y;
-            acc[j].y -= acc[i].x * l.y + acc[i].y * l.x;
-          }
-#pragma unroll
-        for (int i = 0; i < 8; i++) XL[b][jl][i] = acc[i];
+    for (int i = 0; i < 8; i++) {
+      const int e = t + i * 256, r = e / NB, k = e % NB;
+      const int64_t row = row0 + r;
+      if (row < n_end) {
+        const float2 v = X[r * kS + k];
+        M[row * ld + k0 + k] = v;
+        if (Ap) emit_a(Ap, row - abase, k, v);
       }
     }
     __syncthreads();
-    if (g > Q) {  // fold block Q into this thread's block
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        const float2 x = lrole ? XR[b][lane][i] : XL[b][jl][i];
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-          const float2 u = lrole ? D[Q * 8 + i][g * 8 + j] : D[g * 8 + j][Q * 8 + i];
-          acc[j].x -= x.x * u.x - x.y * u.y;
-          acc[j].y -= x.x * u.y + x.y * u.x;
-        }
-      }
-    }
-    if (lrole) {  // the update's share of blocks Q: two entries per thread
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        const float2 x = XR[b][lane][i];
-#pragma unroll
-        for (int m = 0; m < 2; m++) {
-          const float2 y = XL[b][2 * g + m][i];
-          cc[m].x -= x.x * y.x - x.y * y.y;
-          cc[m].y -= x.x * y.y + x.y * y.x;
-        }
-      }
-    }
-  }
-  // every load of this CTA is behind it: count it in, and learn whether
-  // this CTA is the last of its L21 half and of its column group
-  __syncthreads();
-  if (t == 0) {
-    __threadfence();
-    const unsigned a = atomicAdd(&cnt[blockIdx.y], 1u);
-    const unsigned c = atomicAdd(&cnt[2 + blockIdx.x], 1u);
-    s_last[0] = a == gridDim.x - 1;
-    s_last[1] = c == gridDim.y - 1;
-    if (s_last[0]) cnt[blockIdx.y] = 0;
-    if (s_last[1]) cnt[2 + blockIdx.x] = 0;
-    __threadfence();
-  }
-  __syncthreads();
-  if (lrole) {
-    if (s_last[0]) {
-      float4* p = reinterpret_cast<float4*>(M + row * ld + k0 + g * 8);
-#pragma unroll
-      for (int i = 0; i < 4; i++) p[i] = make_float4(acc[2 * i].x, acc[2 * i].y, acc[2 * i + 1].x, acc[2 * i + 1].y);
-    }
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-      const int64_t c = j0 + 2 * g + m;
-      if (c < c_hi) M[row * ld + c] = cc[m];
-    }
-  } else if (s_last[1] && cvalid) {
-#pragma unroll
-    for (int i = 0; i < 8; i++) M[(k0 + g * 8 + i) * ld + col] = acc[i];
-    if (Bp) emit_b8(Bp, col - r0, g * 8, acc);
   }
 }
 
