@@ -154,6 +154,8 @@ struct necgpu_engine {
   // the split path's next-block rows (L21, U12 and their update) in one
   // launch (panel_top_kernel), the panel's interchanges on stream3
   bool panel_top = true;
+  // refinement sweeps in thread-block clusters (DSMEM hand-off)
+  bool sweep_cluster = true;
   unsigned* d_top_cnt = nullptr;  // panel_top_kernel's arrival counters (zero between launches)
   __nv_bfloat16* d_Bpan = nullptr;  // its B operand slots, one per panel of an outer block
   size_t bpan_elems = 0;
@@ -1458,6 +1460,35 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
   if (per_sm < 1) return fail(e, NECGPU_ERR_CUDA, "sweep kernel cannot be resident");
   const int grid = std::max(1, std::min(nblk, per_sm * e->nsm));
   const double tri_bytes = 0.5 * (double)n * (double)n * sizeof(float2);
+  // clusters of kSweepCluster CTAs, one position each, when every cluster
+  // can be resident at once (a cooperative launch)
+  constexpr int CS = kSweepCluster;
+  const int gridc = (nblk + CS - 1) / CS * CS;
+  cudaLaunchConfig_t ccfg = {};
+  cudaLaunchAttribute cattr[2];
+  ccfg.gridDim = dim3((unsigned)gridc);
+  ccfg.blockDim = dim3(kInvSweepThreads);
+  ccfg.stream = e->stream;
+  cattr[0].id = cudaLaunchAttributeClusterDimension;
+  cattr[0].val.clusterDim.x = CS;
+  cattr[0].val.clusterDim.y = 1;
+  cattr[0].val.clusterDim.z = 1;
+  cattr[1].id = cudaLaunchAttributeCooperative;
+  cattr[1].val.cooperative = 1;
+  ccfg.attrs = cattr;
+  ccfg.numAttrs = 2;
+  bool clustered = false;
+  if (e->sweep_cluster) {
+    int ncl = 0;
+    ccfg.numAttrs = 1;  // the occupancy query takes the cluster shape only
+    clustered = cudaOccupancyMaxActiveClusters(&ncl, inv_sweep_kernel<true, CS>, &ccfg) == cudaSuccess &&
+                (int64_t)ncl * CS >= gridc;
+    ccfg.numAttrs = 2;
+    if (!clustered) {
+      (void)cudaGetLastError();
+      e->sweep_cluster = false;
+    }
+  }
   for (int pass = 0; pass < 2; pass++) {
     const float2* src = pass == 0 ? rhs : sol;
     float2* dst = pass == 0 ? sol : rhs;
@@ -1471,10 +1502,20 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
     void* args[] = {(void*)&Mf,  (void*)&ld,  (void*)&n,       (void*)&tinv,       (void*)&wnext,
                     (void*)&src, (void*)&dst, (void*)&counter, (void*)&e->d_status};
     const int kt = kbegin(e);
-    CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)inv_sweep_kernel<true>
-                                                   : (const void*)inv_sweep_kernel<false>,
-                                         dim3(grid), dim3(kInvSweepThreads), args, 0, e->stream));
-    kend(e, kt, NECGPU_K_TRSV, tri_bytes, nullptr, "inv_sweep_kernel");
+    if (clustered) {
+      const cudaError_t le = cudaLaunchKernelEx(&ccfg, pass == 0 ? inv_sweep_kernel<true, CS> : inv_sweep_kernel<false, CS>,
+                                                Mf, ld, n, tinv, wnext, src, dst, counter, e->d_status);
+      if (le != cudaSuccess) {  // the configuration was refused: the launch below instead, from now on
+        (void)cudaGetLastError();
+        clustered = false;
+        e->sweep_cluster = false;
+      }
+    }
+    if (!clustered)
+      CUDA_TRY(cudaLaunchCooperativeKernel(pass == 0 ? (const void*)inv_sweep_kernel<true>
+                                                     : (const void*)inv_sweep_kernel<false>,
+                                           dim3(grid), dim3(kInvSweepThreads), args, 0, e->stream));
+    kend(e, kt, NECGPU_K_TRSV, tri_bytes, nullptr, clustered ? "inv_sweep_kernel (clusters)" : "inv_sweep_kernel");
     LAUNCHED();
   }
   // the backward pass wrote the solution into rhs
@@ -1962,6 +2003,7 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_FUSED_PACK")) e->fused_pack = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_INNER_SPLIT")) e->inner_split = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_PANEL_TOP")) e->panel_top = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_SWEEP_CLUSTER")) e->sweep_cluster = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_L21_ROWS")) e->l21_rows = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_SIDE_CTAS")) {
     const int v = std::atoi(s);

@@ -444,6 +444,7 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
 
 constexpr int kInvSweepThreads = 256;
 constexpr int kInvSweepChunk = 16;                  // solved blocks staged per pass
+constexpr int kSweepCluster = 8;                    // CTAs per cluster of the clustered sweep
 constexpr unsigned long long kSweepWaitNs = 4000000000ull;  // 4 s
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -490,6 +491,39 @@ __global__ void __launch_bounds__(256) next_tile_kernel(const float2* M, int64_t
   }
 }
 
+// Hand-off of a solved block to the next CTA of a thread-block cluster:
+// stores into its shared memory and a release-arrive on its mbarrier.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned peer_addr(unsigned local, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_peer_f2(unsigned addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void arrive_peer(unsigned bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool try_wait_parity(unsigned bar, unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
 // LOWER: x = L^-1 b (unit lower); !LOWER: x = U^-1 b.  counter must be 0 at
 // launch; it counts the completed positions of the sweep order.
 //
@@ -505,7 +539,16 @@ __global__ void __launch_bounds__(256) next_tile_kernel(const float2* M, int64_t
 // holds the next tile row quarter in registers while it multiplies the
 // current one.  A wait that runs out sets bit 9 of *status; every CTA then
 // returns.
-template <bool LOWER>
+//
+// CS > 0: launched in clusters of CS CTAs, one position per CTA (grid >=
+// the number of blocks).  A block whose predecessor in the sweep order is
+// in the same cluster receives x_prev in its own shared memory: the
+// predecessor stores it there and arrives on this CTA's mbarrier
+// (release / acquire at cluster scope), instead of the round trip through
+// L2.  The first block of each cluster polls x_prev in global memory as
+// without clusters.  All CTAs of a cluster meet at a cluster barrier before
+// they exit, so none exits while a peer may still write to it.
+template <bool LOWER, int CS = 0>
 __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const float2* M, int64_t ld, int64_t n,
                                                                      const float2* tinv, const float2* wnext,
                                                                      const float2* b, float2* x, unsigned* counter,
@@ -516,11 +559,23 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
   __shared__ float2 sv[NB];
   __shared__ float2 sx[KX * NB];
   __shared__ float2 sinv[NB][NB + 1];  // inv(T_vv), rows padded against bank conflicts
+  __shared__ float2 xin[NB];           // x_prev from the cluster peer (CS > 0)
+  __shared__ __align__(8) unsigned long long xbar;
   __shared__ int s_avail;
   const int t = threadIdx.x;
   const int r = t & (NB - 1), q = t >> 6;  // row in the block, column quarter
   const int nblk = (int)((n + NB - 1) / NB);
-  for (int s = blockIdx.x; s < nblk; s += gridDim.x) {  // s: position in sweep order
+  unsigned rank = 0;
+  if constexpr (CS > 0) {
+    rank = cluster_rank();
+    if (t == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&xbar)), "r"(NB) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    cluster_sync_all();
+  }
+  // one position of the sweep order; false when a wait ran out
+  auto position = [&](int s) -> bool {
     const int v = LOWER ? s : nblk - 1 - s;
     const int64_t r0 = (int64_t)v * NB;
     const int bs = (int)min((int64_t)NB, n - r0);
@@ -610,7 +665,7 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
       __syncthreads();  // sx is reused by the next pass
       i0 = i1;
     }
-    if (!ok) return;
+    if (!ok) return false;
     float2 wv[QW];
     if (s > 0) {
       const float4* wp = reinterpret_cast<const float4*>(wnext + boff);
@@ -647,14 +702,29 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
     if (t < NB)
       c = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
                       part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
+    float2 xval = c;  // x_v, row t (t < NB)
     if (s > 0) {
       // the previous position: x_v = c - W x_prev.  Each thread polls its
       // sixteen values of x_prev until none is still unset (x starts as
-      // kSweepUnset), which saves the counter's round trip on the chain
+      // kSweepUnset), which saves the counter's round trip on the chain;
+      // from a cluster peer it waits on the mbarrier the peer arrives on
       const int64_t cp = (int64_t)(LOWER ? s - 1 : nblk - s) * NB + q * QW;
       float2 xv[QW];
       int timed_out = 0;
-      {
+      if (CS > 0 && rank > 0) {
+        const unsigned long long t0 = global_ns();
+        long long spins = 0;
+        while (!try_wait_parity(smem_addr(&xbar), 0u)) {
+          if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+              global_ns() - t0 > kSweepWaitNs) {
+            atomicOr(status, 1 << 9);
+            timed_out = 1;
+            break;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < QW; k++) xv[k] = xin[q * QW + k];
+      } else {
         const unsigned long long t0 = global_ns();
         long long spins = 0;
         bool ready = false;
@@ -682,17 +752,31 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
         pi += wv[k].x * xv[k].y + wv[k].y * xv[k].x;
       }
       part2[q][r] = make_float2(pr, pi);
-      if (__syncthreads_or(timed_out)) return;  // a wait ran out: every thread leaves
-      if (t < bs)
-        x[r0 + t] = make_float2(c.x - (part2[0][t].x + part2[1][t].x + part2[2][t].x + part2[3][t].x),
-                                c.y - (part2[0][t].y + part2[1][t].y + part2[2][t].y + part2[3][t].y));
-    } else if (t < bs) {
-      x[r0 + t] = c;
+      if (__syncthreads_or(timed_out)) return false;  // a wait ran out: every thread leaves
+      if (t < NB)
+        xval = make_float2(c.x - (part2[0][t].x + part2[1][t].x + part2[2][t].x + part2[3][t].x),
+                           c.y - (part2[0][t].y + part2[1][t].y + part2[2][t].y + part2[3][t].y));
+    }
+    if (t < bs) x[r0 + t] = xval;
+    if constexpr (CS > 0) {
+      // the next position's CTA in this cluster takes x_v from here
+      if (t < NB && rank + 1 < (unsigned)CS && s + 1 < nblk) {
+        st_peer_f2(peer_addr(smem_addr(&xin[t]), rank + 1), t < bs ? xval : make_float2(0.f, 0.f));
+        arrive_peer(peer_addr(smem_addr(&xbar), rank + 1));
+      }
     }
     // the block's stores are ordered before the counter by the barrier and
     // thread 0's release at device scope
     __syncthreads();
     if (t == 0) st_release_u32(counter, (unsigned)(s + 1));
+    return true;
+  };
+  if constexpr (CS > 0) {
+    if ((int)blockIdx.x < nblk) position((int)blockIdx.x);
+    cluster_sync_all();
+  } else {
+    for (int s = blockIdx.x; s < nblk; s += gridDim.x)  // s: position in sweep order
+      if (!position(s)) return;
   }
 }
 
