@@ -621,7 +621,13 @@ def run_b200(args):
     # ---- roofline of the dominant kernel of the mixed step
     shares = {K_NAMES[i]: st_m.k_ms[i] for i in range(9) if st_m.k_launches[i]}
     tot = sum(shares.values()) or 1.0
-    dom = max(shares, key=shares.get)
+    # the roofline kernel: the largest class with a throughput bound (tensor
+    # or HBM).  The latency-bound panel classes run on side streams beside
+    # the updates; their summed time counts overlapped work and has no peak
+    # to be a fraction of, so the largest class by time is reported beside
+    dom_time = max(shares, key=shares.get)
+    thr = {k: v for k, v in shares.items() if K_BOUND[k][0] in ("tensor", "hbm")}
+    dom = max(thr, key=thr.get) if thr else dom_time
     di = K_NAMES.index(dom)
     avg_ms = st_m.k_ms[di] / st_m.k_launches[di]
     work = st_m.k_flops[di] / st_m.k_launches[di]
@@ -645,6 +651,8 @@ def run_b200(args):
                 "peak_source": peak_src + (" bf16 dense sustained" if unit != "GB/s" else " copy"),
                 "avg_launch_ms": avg_ms, "work_per_launch": work, "work_unit": unit_kind,
                 "launches_per_step": st_m.k_launches[di] / args.steps,
+                "largest_class_by_time": {"kernel": dom_time, "bound": K_BOUND[dom_time][0],
+                                          "share": round(shares[dom_time] / tot, 4)},
                 "share": {k: round(v / tot, 4) for k, v in sorted(shares.items(), key=lambda kv: -kv[1])},
                 "ms_per_step_by_kernel": {k: v / args.steps for k, v in shares.items()},
                 "ms_per_step_instrumented": ms_inst}

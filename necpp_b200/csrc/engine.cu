@@ -154,8 +154,9 @@ struct necgpu_engine {
   // the split path's next-block rows (L21, U12 and their update) in one
   // launch (panel_top_kernel), the panel's interchanges on stream3
   bool panel_top = true;
-  // refinement sweeps in thread-block clusters (DSMEM hand-off)
-  bool sweep_cluster = true;
+  // refinement sweeps in thread-block clusters of this many CTAs (16 or 8;
+  // 0: none), with the solved blocks handed over in shared memory
+  int sweep_cluster = 16;
   unsigned* d_top_cnt = nullptr;  // panel_top_kernel's arrival counters (zero between launches)
   __nv_bfloat16* d_Bpan = nullptr;  // its B operand slots, one per panel of an outer block
   size_t bpan_elems = 0;
@@ -1442,10 +1443,11 @@ int invert_diag_blocks(necgpu_engine* e, bool force = false) {
   CUDA_TRY(cudaFuncSetAttribute(tri_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_inv_smem()));
   KLAUNCH(NECGPU_K_OTHER, 0.0,
           tri_inv_kernel<<<(unsigned)nblk, 128, tri_inv_smem(), e->stream>>>(e->Z32, e->ld, e->n, e->d_tinv));
-  if (!e->d_wnext) TRY(dalloc(e, e->d_wnext, (size_t)nblk * 2 * kBlk * kBlk));
+  if (!e->d_wnext) TRY(dalloc(e, e->d_wnext, (size_t)nblk * 2 * kSweepDepth * kBlk * kBlk));
+  CUDA_TRY(cudaFuncSetAttribute(next_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)next_tile_smem()));
   KLAUNCH(NECGPU_K_OTHER, 0.0,
-          next_tile_kernel<<<dim3((unsigned)nblk, 2), 256, 0, e->stream>>>(e->Z32, e->ld, e->n, e->d_tinv,
-                                                                           e->d_wnext));
+          next_tile_kernel<<<dim3((unsigned)nblk, 2, kSweepDepth), 256, next_tile_smem(), e->stream>>>(
+              e->Z32, e->ld, e->n, e->d_tinv, e->d_wnext));
   return 0;
 }
 
@@ -1460,9 +1462,9 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
   if (per_sm < 1) return fail(e, NECGPU_ERR_CUDA, "sweep kernel cannot be resident");
   const int grid = std::max(1, std::min(nblk, per_sm * e->nsm));
   const double tri_bytes = 0.5 * (double)n * (double)n * sizeof(float2);
-  // clusters of kSweepCluster CTAs, one position each, when every cluster
-  // can be resident at once (a cooperative launch)
-  constexpr int CS = kSweepCluster;
+  // clusters of 16 (or 8) CTAs, one position each, when every cluster can be
+  // resident at once (a cooperative launch)
+  const int CS = e->sweep_cluster >= 16 ? 16 : 8;
   const int gridc = (nblk + CS - 1) / CS * CS;
   cudaLaunchConfig_t ccfg = {};
   cudaLaunchAttribute cattr[2];
@@ -1481,12 +1483,19 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
   if (e->sweep_cluster) {
     int ncl = 0;
     ccfg.numAttrs = 1;  // the occupancy query takes the cluster shape only
-    clustered = cudaOccupancyMaxActiveClusters(&ncl, inv_sweep_kernel<true, CS>, &ccfg) == cudaSuccess &&
-                (int64_t)ncl * CS >= gridc;
+    if (CS == 16) {
+      for (auto* k : {inv_sweep_kernel<true, 16>, inv_sweep_kernel<false, 16>})
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) ncl = -1;
+      clustered = ncl == 0 && cudaOccupancyMaxActiveClusters(&ncl, inv_sweep_kernel<true, 16>, &ccfg) == cudaSuccess &&
+                  (int64_t)ncl * CS >= gridc;
+    } else {
+      clustered = cudaOccupancyMaxActiveClusters(&ncl, inv_sweep_kernel<true, 8>, &ccfg) == cudaSuccess &&
+                  (int64_t)ncl * CS >= gridc;
+    }
     ccfg.numAttrs = 2;
     if (!clustered) {
       (void)cudaGetLastError();
-      e->sweep_cluster = false;
+      e->sweep_cluster = CS == 16 ? 8 : 0;  // the next solve tries eight, then none
     }
   }
   for (int pass = 0; pass < 2; pass++) {
@@ -1503,12 +1512,15 @@ int run_trsv_inv_on(necgpu_engine* e, const float2* Mf, const float2* tinv_block
                     (void*)&src, (void*)&dst, (void*)&counter, (void*)&e->d_status};
     const int kt = kbegin(e);
     if (clustered) {
-      const cudaError_t le = cudaLaunchKernelEx(&ccfg, pass == 0 ? inv_sweep_kernel<true, CS> : inv_sweep_kernel<false, CS>,
-                                                Mf, ld, n, tinv, wnext, src, dst, counter, e->d_status);
+      const cudaError_t le =
+          CS == 16 ? cudaLaunchKernelEx(&ccfg, pass == 0 ? inv_sweep_kernel<true, 16> : inv_sweep_kernel<false, 16>, Mf,
+                                        ld, n, tinv, wnext, src, dst, counter, e->d_status)
+                   : cudaLaunchKernelEx(&ccfg, pass == 0 ? inv_sweep_kernel<true, 8> : inv_sweep_kernel<false, 8>, Mf, ld,
+                                        n, tinv, wnext, src, dst, counter, e->d_status);
       if (le != cudaSuccess) {  // the configuration was refused: the launch below instead, from now on
         (void)cudaGetLastError();
         clustered = false;
-        e->sweep_cluster = false;
+        e->sweep_cluster = 0;
       }
     }
     if (!clustered)
@@ -1616,9 +1628,11 @@ int ensure_adjoint(necgpu_engine* e) {
   KLAUNCH(NECGPU_K_OTHER, 0.0, transpose_kernel<float2><<<g, 256, 0, e->stream>>>(e->Z32, ld, e->ZT32, ld, n));
   KLAUNCH(NECGPU_K_OTHER, 0.0, transpose_kernel<double2><<<g, 256, 0, e->stream>>>(e->Z64, ld, e->ZT64, ld, n));
   KLAUNCH(NECGPU_K_OTHER, 0.0, tinv_transpose_kernel<<<(unsigned)nblk, 256, 0, e->stream>>>(e->d_tinv, e->d_tinvT));
-  if (!e->d_wnextT) TRY(dalloc(e, e->d_wnextT, (size_t)nblk * 2 * kBlk * kBlk));
+  if (!e->d_wnextT) TRY(dalloc(e, e->d_wnextT, (size_t)nblk * 2 * kSweepDepth * kBlk * kBlk));
+  CUDA_TRY(cudaFuncSetAttribute(next_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)next_tile_smem()));
   KLAUNCH(NECGPU_K_OTHER, 0.0,
-          next_tile_kernel<<<dim3((unsigned)nblk, 2), 256, 0, e->stream>>>(e->ZT32, ld, n, e->d_tinvT, e->d_wnextT));
+          next_tile_kernel<<<dim3((unsigned)nblk, 2, kSweepDepth), 256, next_tile_smem(), e->stream>>>(
+              e->ZT32, ld, n, e->d_tinvT, e->d_wnextT));
   e->adj_ready = true;
   return 0;
 }
@@ -2003,7 +2017,10 @@ int necgpu_create(necgpu_engine** out, int device) {
   if (const char* s = std::getenv("NECPP_B200_FUSED_PACK")) e->fused_pack = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_INNER_SPLIT")) e->inner_split = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_PANEL_TOP")) e->panel_top = (s[0] != '0');
-  if (const char* s = std::getenv("NECPP_B200_SWEEP_CLUSTER")) e->sweep_cluster = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_SWEEP_CLUSTER")) {
+    const int v = std::atoi(s);
+    e->sweep_cluster = v >= 16 ? 16 : v >= 8 ? 8 : 0;
+  }
   if (const char* s = std::getenv("NECPP_B200_L21_ROWS")) e->l21_rows = (s[0] != '0');
   if (const char* s = std::getenv("NECPP_B200_SIDE_CTAS")) {
     const int v = std::atoi(s);

@@ -444,7 +444,6 @@ __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
 
 constexpr int kInvSweepThreads = 256;
 constexpr int kInvSweepChunk = 16;                  // solved blocks staged per pass
-constexpr int kSweepCluster = 8;                    // CTAs per cluster of the clustered sweep
 constexpr unsigned long long kSweepWaitNs = 4000000000ull;  // 4 s
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -453,21 +452,25 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// The product of each diagonal-block inverse with the tile next to it in the
-// sweep order, for the last step of each block:
-//   W[2v]   = inv(L_vv) L_{v,v-1}   (v >= 1; zero for v = 0)
-//   W[2v+1] = inv(U_vv) U_{v,v+1}   (v < nblk - 1; zero for the last block)
-// 64 x 64 row-major each, zero outside the matrix.  grid (nblk, 2), 256
-// threads; blockIdx.y selects the lower (0) or upper (1) product.
+// The products of each diagonal-block inverse with the tiles before it in
+// the sweep order, for the last kSweepDepth steps of each block:
+//   W[v][0][d] = inv(L_vv) L_{v,v-1-d}   (zero where v - 1 - d < 0)
+//   W[v][1][d] = inv(U_vv) U_{v,v+1+d}   (zero beyond the last block)
+// 64 x 64 row-major each, zero outside the matrix.  grid (nblk, 2,
+// kSweepDepth), 256 threads; blockIdx.y selects the lower (0) or upper (1)
+// product, blockIdx.z the distance d + 1.
+constexpr int kSweepDepth = 3;
 __global__ void __launch_bounds__(256) next_tile_kernel(const float2* M, int64_t ld, int64_t n, const float2* tinv,
                                                        float2* W) {
   constexpr int NB = kBlk;
-  __shared__ float2 Tm[NB][NB + 1];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2(*Tm)[NB + 1] = reinterpret_cast<float2(*)[NB + 1]>(smem_raw);  // the tile T_vu
+  float2(*Iv)[NB + 1] = Tm + NB;                                         // inv(T_vv)
   const int t = threadIdx.x;
   const int nblk = (int)((n + NB - 1) / NB);
-  const int v = blockIdx.x, side = blockIdx.y;
-  const int u = side == 0 ? v - 1 : v + 1;
-  float2* out = W + ((int64_t)v * 2 + side) * NB * NB;
+  const int v = blockIdx.x, side = blockIdx.y, d = blockIdx.z;
+  const int u = side == 0 ? v - 1 - d : v + 1 + d;
+  float2* out = W + (((int64_t)v * 2 + side) * kSweepDepth + d) * NB * NB;
   if (u < 0 || u >= nblk) {
     for (int e = t; e < NB * NB; e += 256) out[e] = make_float2(0.f, 0.f);
     return;
@@ -477,22 +480,32 @@ __global__ void __launch_bounds__(256) next_tile_kernel(const float2* M, int64_t
   for (int e = t; e < NB * NB; e += 256) {
     const int r = e / NB, c = e % NB;
     Tm[r][c] = (r0 + r < n && c0 + c < n) ? M[(r0 + r) * ld + c0 + c] : make_float2(0.f, 0.f);
+    Iv[r][c] = inv[e];
   }
   __syncthreads();
-  for (int e = t; e < NB * NB; e += 256) {
-    const int r = e / NB, c = e % NB;  // a warp shares r: the inverse's row is a broadcast load
-    float sr = 0.f, si = 0.f;
-    for (int k = 0; k < NB; k++) {
-      const float2 a = __ldg(inv + r * NB + k), b = Tm[k][c];
-      sr += a.x * b.x - a.y * b.y;
-      si += a.x * b.y + a.y * b.x;
+  // thread t: row t / 4, sixteen columns (t % 4) + 4 j (a warp reads 8 rows
+  // of the inverse and 4 runs of the tile per k)
+  const int r = t >> 2, cq = t & 3;
+  float2 acc[16];
+#pragma unroll
+  for (int j = 0; j < 16; j++) acc[j] = make_float2(0.f, 0.f);
+#pragma unroll 4
+  for (int k = 0; k < NB; k++) {
+    const float2 a = Iv[r][k];
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      const float2 b = Tm[k][cq + 4 * j];
+      acc[j].x += a.x * b.x - a.y * b.y;
+      acc[j].y += a.x * b.y + a.y * b.x;
     }
-    out[e] = make_float2(sr, si);
   }
+#pragma unroll
+  for (int j = 0; j < 16; j++) out[r * NB + cq + 4 * j] = acc[j];
 }
+constexpr size_t next_tile_smem() { return (size_t)2 * kBlk * (kBlk + 1) * sizeof(float2); }
 
-// Hand-off of a solved block to the next CTA of a thread-block cluster:
-// stores into its shared memory and a release-arrive on its mbarrier.
+// Hand-off of a solved block to the next CTAs of a thread-block cluster:
+// 64-bit stores into their shared memory.
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned cluster_rank() {
   unsigned r;
@@ -507,60 +520,62 @@ __device__ __forceinline__ unsigned peer_addr(unsigned local, unsigned rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
   return r;
 }
-__device__ __forceinline__ void st_peer_f2(unsigned addr, float2 v) {
-  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+__device__ __forceinline__ void st_peer_f2(unsigned addr, float2 v) {  // one 64-bit store
+  const unsigned long long u = (unsigned long long)__float_as_uint(v.x) | ((unsigned long long)__float_as_uint(v.y) << 32);
+  asm volatile("st.shared::cluster.u64 [%0], %1;" ::"r"(addr), "l"(u) : "memory");
 }
-__device__ __forceinline__ void arrive_peer(unsigned bar) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+// 16-byte load kept in program order with the waits around it (asm
+// volatile), so that the compiler does not move it to its first use
+__device__ __forceinline__ float4 ld_early_f4(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
 }
-__device__ __forceinline__ bool try_wait_parity(unsigned bar, unsigned parity) {
-  unsigned done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(done)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return done != 0;
+__device__ __forceinline__ float2 ld_volatile_shared_f2(const float2* p) {
+  unsigned long long u;
+  asm volatile("ld.volatile.shared.u64 %0, [%1];" : "=l"(u) : "r"(smem_addr(p)) : "memory");
+  return make_float2(__uint_as_float((unsigned)u), __uint_as_float((unsigned)(u >> 32)));
 }
 
 // LOWER: x = L^-1 b (unit lower); !LOWER: x = U^-1 b.  counter must be 0 at
 // launch; it counts the completed positions of the sweep order.
 //
-// CTA s owns block row v(s).  Before the block at the previous position is
-// done it folds in every earlier one, M[v][u] x_u over the positions before
-// s - 1, and forms c = inv(T_vv) (b_v - that sum).  What is left once the
-// previous block arrives is one 64 x 64 product with its precomputed
-// W = inv(T_vv) T_{v,prev} (next_tile_kernel): x_v = c - W x_prev, the only
-// work between two blocks of the sweep besides the counter hand-off.
-// Thread 0 alone polls the counter, sleeping longer the further the row is
-// from the sweep front, and solved blocks known to be complete (up to 16 at a
-// time) are staged in shared memory with one load per element.  Each thread
-// holds the next tile row quarter in registers while it multiplies the
-// current one.  A wait that runs out sets bit 9 of *status; every CTA then
+// CTA s owns block row v(s).  It folds in the positions before the last D =
+// kSweepDepth ones as they complete, M[v][u] x_u, and forms
+// c = inv(T_vv) (b_v - that sum).  The last D positions enter through the
+// precomputed products W_d = inv(T_vv) T_{v,u} (next_tile_kernel):
+// x_v = c - sum_d W_d x_{s-d}, each taken as soon as its block arrives, so
+// that only W_1 x_{s-1} lies between two blocks of the sweep and the fold-in
+// of the earlier positions, which goes through the completion counter, has
+// D steps of slack.  Thread 0 alone polls the counter, sleeping longer the
+// further the row is from what it needs, and solved blocks known to be
+// complete (up to 16 at a time) are staged in shared memory with one load
+// per element.  Each thread holds the next tile row quarter in registers
+// while it multiplies the current one.  A block x_{s-d} is taken by polling
+// its values in global memory until none is still unset (x starts as
+// kSweepUnset).  A wait that runs out sets bit 9 of *status; every CTA then
 // returns.
 //
 // CS > 0: launched in clusters of CS CTAs, one position per CTA (grid >=
-// the number of blocks).  A block whose predecessor in the sweep order is
-// in the same cluster receives x_prev in its own shared memory: the
-// predecessor stores it there and arrives on this CTA's mbarrier
-// (release / acquire at cluster scope), instead of the round trip through
-// L2.  The first block of each cluster polls x_prev in global memory as
-// without clusters.  All CTAs of a cluster meet at a cluster barrier before
-// they exit, so none exits while a peer may still write to it.
+// the number of blocks).  A block x_{s-d} whose CTA is in the same cluster
+// (rank >= d) arrives in this CTA's shared memory instead: its CTA stores
+// each value there with one 64-bit store and this CTA polls its own shared
+// memory for the unset marker, without the round trip through L2 and
+// without fences.  All CTAs of a cluster
+// meet at a cluster barrier before they exit, so none exits while a peer
+// may still write to it.
 template <bool LOWER, int CS = 0>
 __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const float2* M, int64_t ld, int64_t n,
                                                                      const float2* tinv, const float2* wnext,
                                                                      const float2* b, float2* x, unsigned* counter,
                                                                      int* status) {
-  constexpr int NB = kBlk, QW = NB / 4, KX = kInvSweepChunk;  // four column quarters of 16
+  constexpr int NB = kBlk, QW = NB / 4, KX = kInvSweepChunk, D = kSweepDepth;  // four column quarters of 16
   __shared__ float2 part[4][NB];
-  __shared__ float2 part2[4][NB];  // the last product's partial sums (part may still be read)
+  __shared__ float2 part2[4][NB];  // the last products' partial sums (part may still be read)
   __shared__ float2 sv[NB];
   __shared__ float2 sx[KX * NB];
   __shared__ float2 sinv[NB][NB + 1];  // inv(T_vv), rows padded against bank conflicts
-  __shared__ float2 xin[NB];           // x_prev from the cluster peer (CS > 0)
-  __shared__ __align__(8) unsigned long long xbar;
+  __shared__ float2 xin[D][NB];        // x_{s-d} from cluster peers (CS > 0), unset until written
   __shared__ int s_avail;
   const int t = threadIdx.x;
   const int r = t & (NB - 1), q = t >> 6;  // row in the block, column quarter
@@ -568,11 +583,9 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
   unsigned rank = 0;
   if constexpr (CS > 0) {
     rank = cluster_rank();
-    if (t == 0) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&xbar)), "r"(NB) : "memory");
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    cluster_sync_all();
+    for (int e = t; e < D * NB; e += kInvSweepThreads)
+      xin[e / NB][e % NB] = make_float2(__uint_as_float(kSweepUnset), __uint_as_float(kSweepUnset));
+    cluster_sync_all();  // no peer writes before every buffer is unset
   }
   // one position of the sweep order; false when a wait ran out
   auto position = [&](int s) -> bool {
@@ -580,14 +593,21 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
     const int64_t r0 = (int64_t)v * NB;
     const int bs = (int)min((int64_t)NB, n - r0);
     const bool rowok = r < bs;
-    // independent of the sweep: inv(T_vv) into shared memory, this thread's
-    // row quarter of W (one 128-byte line, brought into L2 now and read once
-    // the tile loop has freed its registers), and the right-hand side
+    // independent of the sweep: inv(T_vv) into shared memory and the
+    // right-hand side
     const int64_t bbase = ((int64_t)v * 2 + (LOWER ? 0 : 1)) * NB * NB;
-    const int64_t boff = bbase + r * NB + q * QW;
+    const int64_t wbase = ((int64_t)v * 2 + (LOWER ? 0 : 1)) * D * NB * NB + r * NB + q * QW;
     __syncthreads();  // the previous block's reads of sinv are done
     for (int e = t; e < NB * NB; e += kInvSweepThreads) sinv[e / NB][e % NB] = tinv[bbase + e];
-    if (s > 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(wnext + boff));
+    // this thread's row quarters of the W_d (128-byte lines) into L2, late
+    // enough that the tiles streamed meanwhile do not evict them: at the
+    // last pass of the fold-in, or now when there is none
+    auto prefetch_w = [&]() {
+#pragma unroll
+      for (int d = 1; d <= D; d++)
+        if (s >= d) asm volatile("prefetch.global.L2 [%0];" ::"l"(wnext + wbase + (d - 1) * NB * NB));
+    };
+    if (s - D <= 0) prefetch_w();
     const float2 bb = t < bs ? b[r0 + t] : make_float2(0.f, 0.f);
     // the quarter row of the tile at sweep position i
     auto load_tile = [&](float2 (&m)[QW], int i) {
@@ -607,7 +627,8 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
           m[k] = (rowok && c0 + k < n) ? M[(r0 + r) * ld + c0 + k] : make_float2(0.f, 0.f);
       }
     };
-    int avail = 0;  // positions known complete (the same in every thread)
+    const int lim = s - D;  // positions folded in through the counter: 0 .. lim - 1
+    int avail = 0;          // positions known complete (the same in every thread)
     // thread 0 waits until position `need` is complete; false when a wait ran out
     auto wait_for = [&](int need) -> bool {
       if (t == 0) {
@@ -621,9 +642,9 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
             c = -1;
             break;
           }
-          // the row needs position s - 1 only after s - 1 - c more blocks
-          const int ahead = s - 1 - c;
-          __nanosleep(ahead <= 0 ? 20u : (unsigned)min(ahead * 128, 2048));
+          // the row needs position lim - 1 only after lim - 1 - c more blocks
+          const int ahead = lim - 1 - c;
+          __nanosleep(ahead <= 1 ? 20u : (unsigned)min(ahead * 64, 1024));
           c = (int)ld_acquire_u32(counter);
         }
         s_avail = c;
@@ -632,7 +653,6 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
       avail = s_avail;
       return avail >= 0;
     };
-    const int lim = s - 1;  // positions folded in before the previous one arrives
     float2 m[QW];
     if (lim > 0) load_tile(m, 0);
     float accr = 0.f, acci = 0.f;
@@ -640,6 +660,7 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
     for (int i0 = 0; i0 < lim;) {
       if (avail <= i0 && !(ok = wait_for(i0))) break;
       const int i1 = min(lim, min(avail, i0 + KX));
+      if (i1 == lim) prefetch_w();
       for (int e = t; e < (i1 - i0) * NB; e += kInvSweepThreads) {
         const int i = i0 + e / NB;
         const int64_t col = (int64_t)(LOWER ? i : nblk - 1 - i) * NB + (e % NB);
@@ -666,15 +687,12 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
       i0 = i1;
     }
     if (!ok) return false;
-    float2 wv[QW];
+    // W_1's quarter row in registers ahead of the wait for x_{s-1}
+    float4 wv[QW / 2];
     if (s > 0) {
-      const float4* wp = reinterpret_cast<const float4*>(wnext + boff);
+      const float4* wp = reinterpret_cast<const float4*>(wnext + wbase);
 #pragma unroll
-      for (int k = 0; k < QW / 2; k++) {
-        const float4 w = wp[k];
-        wv[2 * k] = make_float2(w.x, w.y);
-        wv[2 * k + 1] = make_float2(w.z, w.w);
-      }
+      for (int k = 0; k < QW / 2; k++) wv[k] = ld_early_f4(wp + k);
     }
     // c = inv(T_vv) (b_v - sum so far), row r held by thread r
     part[q][r] = make_float2(accr, acci);
@@ -698,73 +716,97 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
     }
     part[q][r] = make_float2(accr, acci);
     __syncthreads();
-    float2 c = make_float2(0.f, 0.f);
+    float2 xval = make_float2(0.f, 0.f);  // x_v, row t (t < NB)
     if (t < NB)
-      c = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
-                      part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
-    float2 xval = c;  // x_v, row t (t < NB)
-    if (s > 0) {
-      // the previous position: x_v = c - W x_prev.  Each thread polls its
-      // sixteen values of x_prev until none is still unset (x starts as
-      // kSweepUnset), which saves the counter's round trip on the chain;
-      // from a cluster peer it waits on the mbarrier the peer arrives on
-      const int64_t cp = (int64_t)(LOWER ? s - 1 : nblk - s) * NB + q * QW;
-      float2 xv[QW];
-      int timed_out = 0;
-      if (CS > 0 && rank > 0) {
-        const unsigned long long t0 = global_ns();
-        long long spins = 0;
-        while (!try_wait_parity(smem_addr(&xbar), 0u)) {
-          if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
-              global_ns() - t0 > kSweepWaitNs) {
-            atomicOr(status, 1 << 9);
-            timed_out = 1;
-            break;
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < QW; k++) xv[k] = xin[q * QW + k];
-      } else {
-        const unsigned long long t0 = global_ns();
-        long long spins = 0;
-        bool ready = false;
-        while (!ready) {
-          ready = true;
+      xval = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
+                         part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
+    // this thread's quarter of x_{s-d} into xin[d - 1]: stored there by the
+    // cluster peer, or polled in global memory and copied there (each
+    // thread reads back only its own quarter)
+    float2* xq_base = &xin[0][q * QW];
+    auto acquire = [&](int d) -> bool {
+      const unsigned long long t0 = global_ns();
+      long long spins = 0;
+      float2* xq = xq_base + (d - 1) * NB;
+      if (CS > 0 && rank >= (unsigned)d) {
+        // the peer's 64-bit stores land in this CTA's shared memory: poll
+        // them until none is still unset
+        while (true) {
+          bool ready = true;
 #pragma unroll
           for (int k = 0; k < QW; k++) {
-            xv[k] = cp + k < n ? ld_relaxed_f2(x + cp + k) : make_float2(0.f, 0.f);
-            ready = ready && __float_as_uint(xv[k].x) != kSweepUnset && __float_as_uint(xv[k].y) != kSweepUnset;
+            const float2 v = ld_volatile_shared_f2(xq + k);
+            ready = ready && __float_as_uint(v.x) != kSweepUnset && __float_as_uint(v.y) != kSweepUnset;
           }
-          if (ready) break;
+          if (ready) return true;
           if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
               global_ns() - t0 > kSweepWaitNs) {
             atomicOr(status, 1 << 9);
-            timed_out = 1;
-            break;
+            return false;
           }
-          __nanosleep(20u);
         }
       }
-      float pr = 0.f, pi = 0.f;
+      const int sp = s - d;
+      const int64_t cp = (int64_t)(LOWER ? sp : nblk - 1 - sp) * NB + q * QW;
+      while (true) {
+        bool ready = true;
 #pragma unroll
-      for (int k = 0; k < QW; k++) {
-        pr += wv[k].x * xv[k].x - wv[k].y * xv[k].y;
-        pi += wv[k].x * xv[k].y + wv[k].y * xv[k].x;
+        for (int k = 0; k < QW; k++) {
+          const float2 v = cp + k < n ? ld_relaxed_f2(x + cp + k) : make_float2(0.f, 0.f);
+          ready = ready && __float_as_uint(v.x) != kSweepUnset && __float_as_uint(v.y) != kSweepUnset;
+          xq[k] = v;
+        }
+        if (ready) return true;
+        if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+            global_ns() - t0 > kSweepWaitNs) {
+          atomicOr(status, 1 << 9);
+          return false;
+        }
+        __nanosleep(20u);
       }
-      part2[q][r] = make_float2(pr, pi);
-      if (__syncthreads_or(timed_out)) return false;  // a wait ran out: every thread leaves
-      if (t < NB)
-        xval = make_float2(c.x - (part2[0][t].x + part2[1][t].x + part2[2][t].x + part2[3][t].x),
-                           c.y - (part2[0][t].y + part2[1][t].y + part2[2][t].y + part2[3][t].y));
+    };
+    // the last D positions, the oldest first: x_v = c - sum_d W_d x_{s-d}
+    float pr = 0.f, pi = 0.f;
+    int timed_out = 0;
+    for (int d = min(D, s); d >= 1 && !timed_out; d--) {
+      // W_d's quarter row (d >= 2) requested before the wait for its block
+      float4 wd[QW / 2];
+      if (d >= 2) {
+        const float4* wp = reinterpret_cast<const float4*>(wnext + wbase + (d - 1) * NB * NB);
+#pragma unroll
+        for (int k = 0; k < QW / 2; k++) wd[k] = ld_early_f4(wp + k);
+      }
+      if (!acquire(d)) {
+        timed_out = 1;
+        break;
+      }
+      const float4* xq = reinterpret_cast<const float4*>(xq_base + (d - 1) * NB);
+#pragma unroll
+      for (int k = 0; k < QW / 2; k++) {
+        const float4 w = d == 1 ? wv[k] : wd[k];
+        const float4 xx = xq[k];
+        pr += w.x * xx.x - w.y * xx.y + w.z * xx.z - w.w * xx.w;
+        pi += w.x * xx.y + w.y * xx.x + w.z * xx.w + w.w * xx.z;
+      }
+    }
+    part2[q][r] = make_float2(pr, pi);
+    if (__syncthreads_or(timed_out)) return false;  // a wait ran out: every thread leaves
+    if (t < NB && s > 0) {
+      xval.x -= part2[0][t].x + part2[1][t].x + part2[2][t].x + part2[3][t].x;
+      xval.y -= part2[0][t].y + part2[1][t].y + part2[2][t].y + part2[3][t].y;
+    }
+    if constexpr (CS > 0) {
+      // the next D positions' CTAs in this cluster take x_v from here, the
+      // nearest first (its CTA is waiting): each value is one 64-bit store
+      // that the receiver polls, so no fence is needed
+      if (t < NB) {
+        const float2 xo = t < bs ? xval : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int d = 1; d <= D; d++)
+          if (rank + d < (unsigned)CS && s + d < nblk) st_peer_f2(peer_addr(smem_addr(&xin[d - 1][t]), rank + d), xo);
+      }
     }
     if (t < bs) x[r0 + t] = xval;
-    if constexpr (CS > 0) {
-      // the next position's CTA in this cluster takes x_v from here
-      if (t < NB && rank + 1 < (unsigned)CS && s + 1 < nblk) {
-        st_peer_f2(peer_addr(smem_addr(&xin[t]), rank + 1), t < bs ? xval : make_float2(0.f, 0.f));
-        arrive_peer(peer_addr(smem_addr(&xbar), rank + 1));
-      }
-    }
     // the block's stores are ordered before the counter by the barrier and
     // thread 0's release at device scope
     __syncthreads();
