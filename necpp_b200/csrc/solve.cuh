@@ -720,9 +720,11 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
     if (t < NB)
       xval = make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
                          part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y);
-    // this thread's quarter of x_{s-d} into xin[d - 1]: stored there by the
-    // cluster peer, or polled in global memory and copied there (each
-    // thread reads back only its own quarter)
+    // this thread's quarter of x_{s-d} in xin[d - 1]: stored there by the
+    // cluster peer (each thread polls its quarter, read only), or polled in
+    // global memory by one thread per value, which stores it there, and a
+    // barrier before anyone reads them (that branch is the same in every
+    // thread of the CTA, and its iterations come before the peer ones)
     float2* xq_base = &xin[0][q * QW];
     auto acquire = [&](int d) -> bool {
       const unsigned long long t0 = global_ns();
@@ -746,24 +748,26 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
           }
         }
       }
-      const int sp = s - d;
-      const int64_t cp = (int64_t)(LOWER ? sp : nblk - 1 - sp) * NB + q * QW;
-      while (true) {
-        bool ready = true;
-#pragma unroll
-        for (int k = 0; k < QW; k++) {
-          const float2 v = cp + k < n ? ld_relaxed_f2(x + cp + k) : make_float2(0.f, 0.f);
-          ready = ready && __float_as_uint(v.x) != kSweepUnset && __float_as_uint(v.y) != kSweepUnset;
-          xq[k] = v;
+      bool ok = true;
+      if (r < QW) {  // value q * QW + r of x_{s-d}
+        const int sp = s - d;
+        const int64_t cp = (int64_t)(LOWER ? sp : nblk - 1 - sp) * NB + q * QW + r;
+        while (true) {
+          const float2 v = cp < n ? ld_relaxed_f2(x + cp) : make_float2(0.f, 0.f);
+          if (__float_as_uint(v.x) != kSweepUnset && __float_as_uint(v.y) != kSweepUnset) {
+            xq[r] = v;
+            break;
+          }
+          if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+              global_ns() - t0 > kSweepWaitNs) {
+            atomicOr(status, 1 << 9);
+            ok = false;
+            break;
+          }
+          __nanosleep(20u);
         }
-        if (ready) return true;
-        if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
-            global_ns() - t0 > kSweepWaitNs) {
-          atomicOr(status, 1 << 9);
-          return false;
-        }
-        __nanosleep(20u);
       }
+      return !__syncthreads_or(!ok);
     };
     // the last D positions, the oldest first: x_v = c - sum_d W_d x_{s-d}
     float pr = 0.f, pi = 0.f;

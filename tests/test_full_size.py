@@ -73,3 +73,25 @@ def test_full_size_fill_matches_reference(nb, name):
     assert np.max(np.abs(val - g["Z_val"])) <= 1e-12 * scale
     assert np.max(np.abs(diag - g["Z_diag"])) <= 1e-12 * scale
     nb.nec_delete(ctx)
+
+
+def test_full_size_unclustered_sweeps(nb, api, monkeypatch):
+    """The mixed path at N = 11,520 with the refinement sweeps launched
+    without clusters (the form taken when the clustered launch is refused;
+    every block of the sweep is then polled in global memory): the same
+    Zin as the reference within the mixed bound."""
+    monkeypatch.setenv("NECPP_B200_SWEEP_CLUSTER", "0")
+    name = "helix_array_8x8"
+    g = golden(name)
+    builder, _ = LARGE_CASES[name]
+    ctx = nb.nec_create()
+    assert nb.nec_set_precision(ctx, 1) == 0
+    builder(api, ctx)
+    zin = our_zin(nb, ctx)
+    ref = g["zin"]
+    for i, feeds in enumerate(zin):
+        rel = np.abs(np.array(feeds) - ref[i]) / np.abs(ref[i])
+        assert np.max(rel, initial=0) <= TOL_ZIN[1], (i, np.max(rel))
+    iters, resid = nb.last_refinement(ctx)
+    assert resid <= 1e-12 and 1 <= iters <= 10
+    nb.nec_delete(ctx)

@@ -151,3 +151,31 @@ def test_lu_graph_replay_matches_eager(nb, oracle):
     finally:
         e.close()
         nb.nec_delete(ctx)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("clusters", ["16", "8", "0"])
+@pytest.mark.parametrize("name", ["helix2", "mesh_small"])
+def test_sweep_forms_keep_parity(nb, oracle, name, clusters, monkeypatch):
+    """The refinement sweeps in clusters of 16 or 8 CTAs (blocks handed over
+    in shared memory) and without clusters (every block polled in global
+    memory, the form taken when the clustered launch is refused) refine to
+    the FP64 floor and match the oracle's currents to 1e-9."""
+    from gpu_helpers import Engine
+    from helpers import host_case
+    monkeypatch.setenv("NECPP_B200_SWEEP_CLUSTER", clusters)
+    ctx, st, rhs, _ = host_case(nb, CASES[name][0])
+    Zo, _ = oracle.fill(st)
+    x, _ = oracle.solve(Zo, rhs)
+    _, cur_o = oracle.coefficients(st, x)
+    e = Engine(nb.lib)
+    try:
+        e.set_structure(st)
+        e.fill()
+        e.factor(1)
+        cur, _ = e.solve(rhs)
+        assert e.stats().refine_residual <= 1e-12
+        assert np.max(np.abs(cur - cur_o)) / np.max(np.abs(cur_o)) <= 1e-9
+    finally:
+        e.close()
+        nb.nec_delete(ctx)
