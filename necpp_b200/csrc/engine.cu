@@ -2096,6 +2096,7 @@ int necgpu_destroy(necgpu_engine* e) {
   }
   if (e->ev_diag) cudaEventDestroy(e->ev_diag);
   if (e->ev_bulk) cudaEventDestroy(e->ev_bulk);
+  if (e->ev_swap) cudaEventDestroy(e->ev_swap);
   if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return NECGPU_OK;
