@@ -773,6 +773,7 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
     float pr = 0.f, pi = 0.f;
     int timed_out = 0;
     for (int d = min(D, s); d >= 1 && !timed_out; d--) {
+      if (CS > 0 && d >= 2 && rank >= (unsigned)d) continue;  // the peer sends W_d x_{s-d} itself
       // W_d's quarter row (d >= 2) requested before the wait for its block
       float4 wd[QW / 2];
       if (d >= 2) {
@@ -800,21 +801,66 @@ __global__ void __launch_bounds__(kInvSweepThreads, 2) inv_sweep_kernel(const fl
       xval.y -= part2[0][t].y + part2[1][t].y + part2[2][t].y + part2[3][t].y;
     }
     if constexpr (CS > 0) {
-      // the next D positions' CTAs in this cluster take x_v from here, the
-      // nearest first (its CTA is waiting): each value is one 64-bit store
-      // that the receiver polls, so no fence is needed
+      // W_d x_{s-d} (d >= 2) computed and sent by the peer: row t of it in
+      // xin[d - 1], polled until set
       if (t < NB) {
-        const float2 xo = t < bs ? xval : make_float2(0.f, 0.f);
-#pragma unroll
-        for (int d = 1; d <= D; d++)
-          if (rank + d < (unsigned)CS && s + d < nblk) st_peer_f2(peer_addr(smem_addr(&xin[d - 1][t]), rank + d), xo);
+        for (int d = 2; d <= min(D, s); d++) {
+          if (rank < (unsigned)d) continue;
+          const unsigned long long t0 = global_ns();
+          long long spins = 0;
+          while (true) {
+            const float2 y = ld_volatile_shared_f2(&xin[d - 1][t]);
+            if (__float_as_uint(y.x) != kSweepUnset && __float_as_uint(y.y) != kSweepUnset) {
+              xval.x -= y.x;
+              xval.y -= y.y;
+              break;
+            }
+            if (((++spins & 63) == 0 && (*(volatile int*)status & (1 << 9))) || spins > kSweepSpinLimit ||
+                global_ns() - t0 > kSweepWaitNs) {
+              atomicOr(status, 1 << 9);
+              break;
+            }
+          }
+        }
       }
+      // the next position's CTA in this cluster takes x_v from here: each
+      // value is one 64-bit store that the receiver polls, so no fence
+      if (t < NB && rank + 1 < (unsigned)CS && s + 1 < nblk)
+        st_peer_f2(peer_addr(smem_addr(&xin[0][t]), rank + 1), t < bs ? xval : make_float2(0.f, 0.f));
     }
     if (t < bs) x[r0 + t] = xval;
     // the block's stores are ordered before the counter by the barrier and
     // thread 0's release at device scope
     __syncthreads();
     if (t == 0) st_release_u32(counter, (unsigned)(s + 1));
+    if constexpr (CS > 0) {
+      // for the CTAs d = 2 .. D positions on in this cluster: W_d of their
+      // block times x_v, formed here after the block is out (its rows
+      // fetched now, off the chain) and stored into their xin[d - 1]
+      if (t < NB) sv[t] = t < bs ? xval : make_float2(0.f, 0.f);
+      __syncthreads();
+      for (int d = 2; d <= D; d++) {
+        if (rank + d >= (unsigned)CS || s + d >= nblk) continue;  // the same in every thread
+        const int vs = LOWER ? s + d : nblk - 1 - (s + d);
+        const float4* wp = reinterpret_cast<const float4*>(
+            wnext + (((int64_t)vs * 2 + (LOWER ? 0 : 1)) * D + (d - 1)) * NB * NB + r * NB + q * QW);
+        const float4* xs4 = reinterpret_cast<const float4*>(sv + q * QW);
+        float hr = 0.f, hi = 0.f;
+#pragma unroll
+        for (int k = 0; k < QW / 2; k++) {
+          const float4 w = wp[k], xx = xs4[k];
+          hr += w.x * xx.x - w.y * xx.y + w.z * xx.z - w.w * xx.w;
+          hi += w.x * xx.y + w.y * xx.x + w.z * xx.w + w.w * xx.z;
+        }
+        part[q][r] = make_float2(hr, hi);
+        __syncthreads();
+        if (t < NB)
+          st_peer_f2(peer_addr(smem_addr(&xin[d - 1][t]), rank + d),
+                     make_float2(part[0][t].x + part[1][t].x + part[2][t].x + part[3][t].x,
+                                 part[0][t].y + part[1][t].y + part[2][t].y + part[3][t].y));
+        __syncthreads();
+      }
+    }
     return true;
   };
   if constexpr (CS > 0) {
