@@ -433,6 +433,34 @@ class TraceRec(C.Structure):
                 ("work", C.c_double), ("name", C.c_char * 48)]
 
 
+def measure_tf32_peak(torch, n=8192, iters=300):
+    """Dense TF32 rate of this GPU: a cuBLAS FP32 GEMM with TF32 allowed
+    (n^3, about half a second of back-to-back launches), TFLOP/s.  The
+    tensor-core update's TF32 form is measured against it, as its split-BF16
+    form is against the measured BF16 GEMM rate."""
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    try:
+        g = torch.Generator(device="cuda").manual_seed(7)
+        a = torch.randn(n, n, device="cuda", generator=g)
+        b = torch.randn(n, n, device="cuda", generator=g)
+        c = torch.empty(n, n, device="cuda")
+        for _ in range(5):
+            torch.matmul(a, b, out=c)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(iters):
+            torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        secs = e0.elapsed_time(e1) * 1e-3
+        del a, b, c
+        return 2.0 * n ** 3 * iters / secs / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+
+
 def write_trace(L, eng, path, check):
     """One resident mixed step at timing level 3: every launch with its
     class, stream, start and end (ms from the step's first launch).  The
@@ -555,6 +583,8 @@ def run_b200(args):
     ctx_m, eng_m = prepare(1)
     z_mixed = zin_all(ctx_m)
     iters, resid = nb.last_refinement(ctx_m)
+    L.necgpu_update_format.argtypes = [C.c_void_p]
+    update_format = {1: "split_bf16x3", 2: "tf32"}.get(L.necgpu_update_format(eng_m), "none")
     sampler = ClockSampler(local)
     ms_m, _, launches_m, clocks = timed(eng_m, 1, args.steps, args.warmup, sampler)
     value, _, secs = replicas.whole_job_rate(args.steps, ms_m * args.steps / 1e3, device="cuda")
@@ -646,9 +676,16 @@ def run_b200(args):
     else:
         achieved = work / (avg_ms * 1e-3) / 1e12
         peak, unit = peaks["bf16_tflops_sustained"], "TFLOP/s"
+    peak_source = peak_src + (" bf16 dense sustained" if unit != "GB/s" else " copy")
+    extra = {}
+    if dom == "lu_gemm" and update_format == "tf32":
+        # the update computes in TF32, whose tensor-core rate is half of BF16's
+        extra["frac_of_bf16_peak"] = achieved / peak
+        peak = measure_tf32_peak(torch)
+        peak_source = "measured here: cuBLAS TF32 GEMM 8192^3 (torch.matmul, allow_tf32), 300 back-to-back launches"
     roofline = {"kernel": dom, "bound": "hbm" if bound == "hbm" else "tensor", "achieved": achieved,
-                "peak": peak, "unit": unit, "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
-                "peak_source": peak_src + (" bf16 dense sustained" if unit != "GB/s" else " copy"),
+                "peak": peak, "unit": unit, "frac": achieved / peak, **extra, "traffic": traffic,
+                "traffic_source": traffic_src, "peak_source": peak_source,
                 "avg_launch_ms": avg_ms, "work_per_launch": work, "work_unit": unit_kind,
                 "launches_per_step": st_m.k_launches[di] / args.steps,
                 "largest_class_by_time": {"kernel": dom_time, "bound": K_BOUND[dom_time][0],
@@ -664,7 +701,7 @@ def run_b200(args):
         "config": workload_config(args, world), "precision": "mixed",
         "gpu_launches": int(launches_m / args.steps * args.steps),
         "clocks": clocks,
-        "refine": {"iters": iters, "residual": resid},
+        "refine": {"iters": iters, "residual": resid, "update_format": update_format},
         "e2e": {"value": world * 1000.0 / e2e_ms_max, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": roofline,

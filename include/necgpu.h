@@ -160,6 +160,18 @@ int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter);
  * block) refactors with 0: partial pivoting over the whole column, the
  * reference's choice.  NECGPU_FP64 always uses partial pivoting. */
 int necgpu_set_pivoting(necgpu_engine* e, int mode);
+/* Operand format of the NECGPU_MIXED factorisation's tensor-core update.
+ * 1: complex64 operands split into BF16 hi/lo parts, three products per
+ * pair (~2^-16 relative); 2: one TF32 pass (~2^-11 relative, two thirds of
+ * the tensor-core time; the refinement takes a step or more extra);
+ * 0 (default): TF32 from 10,240 unknowns on (NECPP_B200_TF32_MIN_N), split
+ * BF16 below that and, for the rest of the engine's life, after a TF32
+ * factorisation whose refinement needed more than 5 steps or stalled (the
+ * solve then refactors with split BF16).  The environment variable
+ * NECPP_B200_TC_FORMAT (bf16x3, tf32, auto) sets it at engine creation. */
+int necgpu_set_update_format(necgpu_engine* e, int format);
+/* Format (1 or 2) of the held NECGPU_MIXED factors; 0 when none are held. */
+int necgpu_update_format(const necgpu_engine* e);
 
 /* Diagnostics of the last necgpu_solve / necgpu_factor. */
 enum necgpu_kernel_class {

@@ -127,16 +127,26 @@ struct necgpu_engine {
   bool sweep_trsv = true;
   int* d_flags = nullptr;
   int flag_epoch = 0;
-  // tensor-core trailing update of the FP32 LU: packed BF16 operands with
-  // tensor maps over the whole buffers (built once per size)
+  // tensor-core trailing update of the FP32 LU: packed operands (raw bytes,
+  // in the format of the factorisation: gemm_tc.cuh's SplitBf16 or Tf32)
   bool use_tc = true;
-  __nv_bfloat16 *d_Ap = nullptr, *d_Bp = nullptr;
+  unsigned char *d_Ap = nullptr, *d_Bp = nullptr;
   int64_t tc_rows = 0;
-  int tc_kdim = 0;
+  int64_t tc_kbytes = 0;  // bytes per operand row
   // second packed-operand set (the lookahead's far update)
-  __nv_bfloat16 *d_Ap2 = nullptr, *d_Bp2 = nullptr;
+  unsigned char *d_Ap2 = nullptr, *d_Bp2 = nullptr;
   int64_t tc_rows2 = 0;
-  int tc_kdim2 = 0;
+  int64_t tc_kbytes2 = 0;
+  unsigned tc_attr = 0;  // formats whose GEMM kernel has its shared-memory size set
+  // operand format of the mixed LU's update: 0 chooses (TF32 from
+  // tf32_min_n unknowns on, split BF16 below that or once a TF32
+  // factorisation needed more than tf32_max_iters refinement steps), 1 split
+  // BF16, 2 TF32; tc_format_used: the held factors' format
+  int tc_format = 0;
+  int tc_format_used = 0;
+  int64_t tf32_min_n = 10240;
+  int tf32_max_iters = 5;
+  bool tf32_demoted = false;
   // lookahead: the trailing update beyond the next outer block runs on
   // stream2 with lookahead_sms SMs left free for the next panel
   cudaStream_t stream2 = nullptr;
@@ -148,8 +158,8 @@ struct necgpu_engine {
   // between d_Bp and d_Bp3
   cudaStream_t stream4 = nullptr;
   cudaEvent_t ev_diag = nullptr, ev_bulk = nullptr;
-  __nv_bfloat16* d_Bp3 = nullptr;
-  size_t bp3_elems = 0;
+  unsigned char* d_Bp3 = nullptr;
+  size_t bp3_bytes = 0;
   bool inner_split = true;
   // the split path's next-block rows (L21, U12 and their update) in one
   // launch (panel_top_kernel), the panel's interchanges on stream3
@@ -158,8 +168,8 @@ struct necgpu_engine {
   // 0: none), with the solved blocks handed over in shared memory
   int sweep_cluster = 16;
   unsigned* d_top_cnt = nullptr;  // panel_top_kernel's arrival counters (zero between launches)
-  __nv_bfloat16* d_Bpan = nullptr;  // its B operand slots, one per panel of an outer block
-  size_t bpan_elems = 0;
+  unsigned char* d_Bpan = nullptr;  // its B operand slots, one per panel of an outer block
+  size_t bpan_bytes = 0;
   // L21 rows left-looking with a CTA per 32 rows (l21_rows_kernel) instead
   // of one row per thread
   bool l21_rows = true;
@@ -416,7 +426,7 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->d_dinv);
   dfree(e, e->d_top_cnt);
   dfree(e, e->d_Bpan);
-  e->bpan_elems = 0;
+  e->bpan_bytes = 0;
   dfree(e, e->d_zload);
   dfree(e, e->d_somm);
   dfree(e, e->d_near_g);
@@ -429,8 +439,9 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->d_Ap2);
   dfree(e, e->d_Bp2);
   dfree(e, e->d_Bp3);
+  e->bp3_bytes = 0;
   e->tc_rows2 = 0;
-  e->tc_kdim2 = 0;
+  e->tc_kbytes2 = 0;
   dfree(e, e->d_tinv);
   dfree(e, e->d_sweep_ctr);
   dfree(e, e->ZT32);
@@ -480,6 +491,7 @@ void free_all(necgpu_engine* e) {
   dfree(e, e->d_Ap);
   dfree(e, e->d_Bp);
   e->tc_rows = 0;
+  e->tc_kbytes = 0;
   e->pat_cap = 0;
   e->res_ndir = 0;
   e->res_rhs = false;
@@ -680,66 +692,83 @@ int launch_near_e(necgpu_engine* e, const NearFieldArgs& a) {
 }
 
 // ---------------- tensor-core trailing update ----------------
+template <class F>
+typename F::T* op(unsigned char* p) {
+  return reinterpret_cast<typename F::T*>(p);
+}
+
 // Packed-operand buffers (set 0 or 1) sized for `rows` rows of up to `kdim`
-// BF16 columns (grown, never shrunk); the tensor maps are encoded per update
-// for the update's own K'.
+// operand elements of format F (grown, never shrunk; sized in bytes, so
+// either format fits once the larger was needed); the tensor maps are
+// encoded per update for the update's own K'.
+template <class F>
 int ensure_tc(necgpu_engine* e, int kdim, int64_t rows, int set = 0) {
-  __nv_bfloat16*& Ap = set ? e->d_Ap2 : e->d_Ap;
-  __nv_bfloat16*& Bp = set ? e->d_Bp2 : e->d_Bp;
+  if (!(e->tc_attr & F::kFormat)) {
+    CUDA_TRY(cudaFuncSetAttribute(tc::gemm_tc_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    e->tc_attr |= F::kFormat;
+  }
+  unsigned char*& Ap = set ? e->d_Ap2 : e->d_Ap;
+  unsigned char*& Bp = set ? e->d_Bp2 : e->d_Bp;
   int64_t& trows = set ? e->tc_rows2 : e->tc_rows;
-  int& tkdim = set ? e->tc_kdim2 : e->tc_kdim;
-  if (Ap && trows >= rows && tkdim >= kdim) return 0;
+  int64_t& tkb = set ? e->tc_kbytes2 : e->tc_kbytes;
+  const int64_t kbytes = (int64_t)kdim * (int64_t)sizeof(typename F::T);
+  if (Ap && trows >= rows && tkb >= kbytes) return 0;
   if (!encode_tiled()) return fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   const int64_t r = std::max(rows, trows);
-  const int k = std::max(kdim, tkdim);
-  TRY(dalloc(e, Ap, (size_t)r * k));
-  TRY(dalloc(e, Bp, (size_t)2 * r * k));
-  CUDA_TRY(cudaFuncSetAttribute(tc::gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+  const int64_t k = std::max(kbytes, tkb);
+  TRY(dalloc(e, Ap, (size_t)(r * k)));
+  TRY(dalloc(e, Bp, (size_t)(2 * r * k)));
   trows = r;
-  tkdim = k;
+  tkb = k;
   return 0;
 }
 
-// K-major BF16 operand map: nrows rows of kdim elements, 64 x box_rows boxes
+// K-major operand map of format F: nrows rows of kdim elements, boxes of 128
+// bytes x box_rows
+template <class F>
 int encode_operand(necgpu_engine* e, CUtensorMap* map, void* base, int kdim, int64_t nrows, uint32_t box_rows) {
   cuuint64_t dims[2] = {(cuuint64_t)kdim, (cuuint64_t)nrows};
-  cuuint64_t strides[1] = {(cuuint64_t)kdim * 2};
-  cuuint32_t box[2] = {(cuuint32_t)tc::BK, box_rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kdim * sizeof(typename F::T)};
+  cuuint32_t box[2] = {(cuuint32_t)tc::bk<F>(), box_rows};
   cuuint32_t estr[2] = {1, 1};
-  CUresult r = encode_tiled()(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  const CUtensorMapDataType dt =
+      F::kFormat == 2 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+  CUresult r = encode_tiled()(map, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? 0 : fail(e, NECGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
 
 // Pack A (m x kb) and B (kb x n), complex64 row-major with leading
 // dimension ld, into operand set `set` (on the engine's stream).
+template <class F>
 int tc_pack(necgpu_engine* e, int set, const float2* A, const float2* B, int64_t ld, int64_t m, int64_t n, int kb,
             bool pack_b = true) {
-  const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
-  TRY(ensure_tc(e, 6 * kbp, std::max(m, n), set));
-  __nv_bfloat16* Ap = set ? e->d_Ap2 : e->d_Ap;
-  __nv_bfloat16* Bp = set ? e->d_Bp2 : e->d_Bp;
+  const int kbp = (kb + tc::KP - 1) / tc::KP * tc::KP;
+  TRY(ensure_tc<F>(e, F::kKMul * kbp, std::max(m, n), set));
+  typename F::T* Ap = op<F>(set ? e->d_Ap2 : e->d_Ap);
+  typename F::T* Bp = op<F>(set ? e->d_Bp2 : e->d_Bp);
   const int64_t cnt = m * kbp;
   KLAUNCH(NECGPU_K_OTHER, 0.0,
-          tc::pack_a_kernel<<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, Ap));
+          tc::pack_a_kernel<F><<<(unsigned)((cnt + 255) / 256), 256, 0, e->stream>>>(A, ld, (int)m, kb, kbp, Ap));
   if (!pack_b) return 0;
   dim3 g((unsigned)((n + 31) / 32), (unsigned)(kbp / 64));
-  KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, Bp));
+  KLAUNCH(NECGPU_K_OTHER, 0.0, tc::pack_b_kernel<F><<<g, 256, 0, e->stream>>>(B, ld, kb, kbp, (int)n, Bp));
   return 0;
 }
 
 // C (m x ncols) -= A' B'[columns j0, j0 + ncols) from operand set `set`, on
 // stream st with at most grid_max persistent CTAs.
+template <class F>
 int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int kb, float2* C, int64_t ld,
-           cudaStream_t st, int grid_max, int64_t a_row0 = 0, __nv_bfloat16* Bp_alt = nullptr) {
-  const int kbp = (kb + tc::BK - 1) / tc::BK * tc::BK;
-  const int kdim = 6 * kbp;
-  __nv_bfloat16* Ap = (set ? e->d_Ap2 : e->d_Ap) + a_row0 * kdim;
-  __nv_bfloat16* Bp = Bp_alt ? Bp_alt : set ? e->d_Bp2 : e->d_Bp;
+           cudaStream_t st, int grid_max, int64_t a_row0 = 0, typename F::T* Bp_alt = nullptr) {
+  const int kbp = (kb + tc::KP - 1) / tc::KP * tc::KP;
+  const int kdim = F::kKMul * kbp;
+  typename F::T* Ap = op<F>(set ? e->d_Ap2 : e->d_Ap) + a_row0 * kdim;
+  typename F::T* Bp = Bp_alt ? Bp_alt : op<F>(set ? e->d_Bp2 : e->d_Bp);
   CUtensorMap tmA, tmB, tmC;
-  TRY(encode_operand(e, &tmA, Ap, kdim, m, tc::BM));
-  TRY(encode_operand(e, &tmB, Bp + 2 * j0 * kdim, kdim, 2 * ncols, tc::BN));
+  TRY(encode_operand<F>(e, &tmA, Ap, kdim, m, tc::BM));
+  TRY(encode_operand<F>(e, &tmB, Bp + 2 * j0 * kdim, kdim, 2 * ncols, tc::BN));
   // C as m rows x 2 ncols FP32 (re, im interleaved), 32 x 32 boxes for the
   // reduce-add epilogue; TMA clips the boxes at the edges of C
   {
@@ -758,8 +787,8 @@ int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int 
   const int grid = std::max(1, std::min(m_tiles * n_tiles, grid_max));
   const int kt = kbegin(e, st);
   const int group = std::max(1, std::min(e->gemm_group, m_tiles));
-  tc::gemm_tc_kernel<<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(tmA, tmB, tmC, (int)m, (int)ncols, kdim, group,
-                                                               e->d_status);
+  tc::gemm_tc_kernel<F><<<grid, tc::THREADS, tc::SMEM_BYTES, st>>>(tmA, tmB, tmC, (int)m, (int)ncols, kdim,
+                                                                  group, e->d_status);
   kend(e, kt, NECGPU_K_GEMM, 8.0 * (double)m * ncols * kb, st, "tc::gemm_tc_kernel");
   LAUNCHED();
   return 0;
@@ -767,16 +796,18 @@ int tc_run(necgpu_engine* e, int set, int64_t m, int64_t j0, int64_t ncols, int 
 
 // C (m x n) -= A (m x kb) B (kb x n), complex64 row-major with leading
 // dimension ld, on the tensor cores (operand set 0, whole device).
+template <class F>
 int tc_gemm_sub(necgpu_engine* e, const float2* A, const float2* B, float2* C, int64_t ld, int64_t m, int64_t n,
                 int kb, int grid_max = 0) {
-  TRY(tc_pack(e, 0, A, B, ld, m, n, kb));
-  return tc_run(e, 0, m, 0, n, kb, C, ld, e->stream, grid_max > 0 ? grid_max : e->nsm);
+  TRY(tc_pack<F>(e, 0, A, B, ld, m, n, kb));
+  return tc_run<F>(e, 0, m, 0, n, kb, C, ld, e->stream, grid_max > 0 ? grid_max : e->nsm);
 }
 
 // trailing update of the FP32 LU for the panel at k0 of width kb
+template <class F>
 int tc_update(necgpu_engine* e, float2* M, int64_t k0, int kb) {
   const int64_t ld = e->ld, r0 = k0 + kb, rest = e->n - r0;
-  return tc_gemm_sub(e, M + r0 * ld + k0, M + k0 * ld + r0, M + r0 * ld + r0, ld, rest, rest, kb);
+  return tc_gemm_sub<F>(e, M + r0 * ld + k0, M + k0 * ld + r0, M + r0 * ld + r0, ld, rest, rest, kb);
 }
 
 __global__ void fill_random_kernel(float2* p, int64_t count, uint32_t seed) {
@@ -805,7 +836,7 @@ __global__ void max_diff_kernel(const float2* a, const float2* b, int64_t ld, in
 }
 
 // ---------------- LU ----------------
-template <typename R>
+template <typename R, class F = tc::SplitBf16>
 int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
   using T = typename cvec<R>::T;
   const int64_t n = e->n, ld = e->ld;
@@ -871,7 +902,7 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
       bool done = false;
       if constexpr (std::is_same<R, float>::value) {
         if (e->use_tc) {
-          TRY(tc_update(e, M, k0, kb));
+          TRY(tc_update<F>(e, M, k0, kb));
           done = true;
         }
       }
@@ -920,8 +951,10 @@ int run_lu(necgpu_engine* e, typename cvec<R>::T* M) {
 // CTA factors the diagonal block, the exchanges are a per-column gather
 // inside the block, L21 and U12 are row/column-parallel triangular solves,
 // and the trailing update runs on the tensor cores.
+template <class F>
 int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   using T = float2;
+  using Op = typename F::T;  // packed operand element
   const int64_t n = e->n, ld = e->ld;
   const int64_t nblk = (n + kBlk - 1) / kBlk;
   if (!e->d_piv) TRY(dalloc(e, e->d_piv, (size_t)n));
@@ -931,16 +964,20 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                                 (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm_panel_smem<T>()));
+  CUDA_TRY(cudaFuncSetAttribute(trsm_panel_kernel<T, false, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm_panel_smem<T>()));
   CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)trsm8_smem<T>()));
-  CUDA_TRY(cudaFuncSetAttribute(panel_top_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CUDA_TRY(cudaFuncSetAttribute(trsm8_panel_kernel<T, true, 1, F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)trsm8_smem<T>()));
+  CUDA_TRY(cudaFuncSetAttribute(panel_top_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)panel_top_smem()));
-  CUDA_TRY(cudaFuncSetAttribute(l21_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CUDA_TRY(cudaFuncSetAttribute(l21_rows_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)l21_rows_smem()));
   // panel solve: vectors [sbeg, nend) against the 64 x 64 block at k0
   // (LEFT: columns of U12, else rows of L21); kind and flop count for timing
   auto trsm = [&](bool left, int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind,
-                  __nv_bfloat16* Ap = nullptr, int64_t abase = 0) -> int {
+                  Op* Ap = nullptr, int64_t abase = 0) -> int {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
     const double fl = 4.0 * (double)kBlk * kBlk * cnt;
@@ -955,7 +992,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     }
     if (!left && e->l21_rows) {
       const unsigned g = (unsigned)std::min<int64_t>((cnt + kL21Rows - 1) / kL21Rows, 4 * (int64_t)e->nsm);
-      KLAUNCH(kind, fl, l21_rows_kernel<<<g, 256, (unsigned)l21_rows_smem(), e->stream>>>(M, ld, nend, k0, sbeg, dinv,
+      KLAUNCH(kind, fl, l21_rows_kernel<F><<<g, 256, (unsigned)l21_rows_smem(), e->stream>>>(M, ld, nend, k0, sbeg, dinv,
                                                                                             Ap, abase));
       return 0;
     }
@@ -965,36 +1002,37 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       KLAUNCH(kind, fl, trsm_panel_kernel<T, true><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv));
     else
       KLAUNCH(kind, fl,
-              trsm_panel_kernel<T, false><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv, Ap, abase));
+              trsm_panel_kernel<T, false, F><<<g, kTrsmW, sm, e->stream>>>(M, ld, nend, k0, sbeg, dinv, Ap, abase));
     return 0;
   };
   // U12 of an inner panel (eight-warp form) on stream st
   auto trsm_left_on = [&](int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind, cudaStream_t st,
-                          __nv_bfloat16* Bp = nullptr, int64_t bbase = 0) -> int {
+                          Op* Bp = nullptr, int64_t bbase = 0) -> int {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
     const unsigned g = (unsigned)((cnt + kTrsm8Vec - 1) / kTrsm8Vec);
     const int kt = kbegin(e, st);
-    trsm8_panel_kernel<T, true><<<g, 256, (unsigned)trsm8_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv, Bp, bbase);
+    trsm8_panel_kernel<T, true, 1, F><<<g, 256, (unsigned)trsm8_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv, Bp,
+                                                                                bbase);
     kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm8_panel_kernel");
     LAUNCHED();
     return 0;
   };
   // L21 rows [sbeg, nend) of the panel at k0 (one row per thread) on stream st
   auto trsm_on = [&](int64_t k0, int64_t sbeg, int64_t nend, const T* dinv, int kind, cudaStream_t st,
-                     __nv_bfloat16* Ap, int64_t abase) -> int {
+                     Op* Ap, int64_t abase) -> int {
     const int64_t cnt = nend - sbeg;
     if (cnt <= 0) return 0;
     const int kt = kbegin(e, st);
     if (e->l21_rows) {
       // a capped persistent grid: this solve runs beside the panel chain
       const unsigned g = (unsigned)std::min<int64_t>((cnt + kL21Rows - 1) / kL21Rows, e->side_ctas);
-      l21_rows_kernel<<<g, 256, (unsigned)l21_rows_smem(), st>>>(M, ld, nend, k0, sbeg, dinv, Ap, abase);
+      l21_rows_kernel<F><<<g, 256, (unsigned)l21_rows_smem(), st>>>(M, ld, nend, k0, sbeg, dinv, Ap, abase);
       kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "l21_rows_kernel");
     } else {
       const unsigned g = (unsigned)((cnt + kTrsmW - 1) / kTrsmW);
-      trsm_panel_kernel<T, false><<<g, kTrsmW, (unsigned)trsm_panel_smem<T>(), st>>>(M, ld, nend, k0, sbeg, dinv,
-                                                                                     Ap, abase);
+      trsm_panel_kernel<T, false, F><<<g, kTrsmW, (unsigned)trsm_panel_smem<T>(), st>>>(M, ld, nend, k0, sbeg,
+                                                                                        dinv, Ap, abase);
       kend(e, kt, kind, 4.0 * (double)kBlk * kBlk * cnt, st, "trsm_panel_kernel");
     }
     LAUNCHED();
@@ -1012,7 +1050,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
     // M[r0.., c0..] (m x nc) -= M[r0.., kc..kc+kk) M[kc..kc+kk, c0..)
     if (m <= 0 || nc <= 0 || kk <= 0) return 0;
     if (e->use_tc)
-      return tc_gemm_sub(e, M + r0 * ld + kc, M + kc * ld + c0, M + r0 * ld + c0, ld, m, nc, kk, gemm_grid);
+      return tc_gemm_sub<F>(e, M + r0 * ld + kc, M + kc * ld + c0, M + r0 * ld + c0, ld, m, nc, kk, gemm_grid);
     dim3 gg((unsigned)((nc + 63) / 64), (unsigned)((m + 63) / 64));
     KLAUNCH(NECGPU_K_GEMM, 8.0 * (double)m * nc * kk,
             gemm_sub_kernel<float><<<gg, 256, 0, e->stream>>>(M + r0 * ld + kc, ld, M + kc * ld + c0, ld,
@@ -1069,21 +1107,21 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
                          (outer - kBlk) / kTopRows <= kTopRowGroups &&
                          kTopRowGroups + (outer - kBlk) / kTopCols <= kTopCnt;
   // B operand slots of panel_top_kernel, one per panel of an outer block
-  const size_t bpan_slot = 2 * (size_t)(outer - kBlk) * 6 * kBlk;
+  const size_t bpan_slot = 2 * (size_t)(outer - kBlk) * F::kKMul * kBlk;  // elements
   if (panel_top && !e->ev_swap) CUDA_TRY(cudaEventCreateWithFlags(&e->ev_swap, cudaEventDisableTiming));
   if (panel_top && !e->d_top_cnt) {
     TRY(dalloc(e, e->d_top_cnt, (size_t)kTopCnt));
     CUDA_TRY(cudaMemsetAsync(e->d_top_cnt, 0, kTopCnt * sizeof(unsigned), e->stream));
   }
   if (panel_top) {
-    const size_t need = (size_t)(outer / kBlk - 1) * bpan_slot;
-    if (!e->d_Bpan || e->bpan_elems < need) {
+    const size_t need = (size_t)(outer / kBlk - 1) * bpan_slot * sizeof(Op);
+    if (!e->d_Bpan || e->bpan_bytes < need) {
       TRY(dalloc(e, e->d_Bpan, need));
-      e->bpan_elems = need;
+      e->bpan_bytes = need;
     }
   }
   if (u12_fused)
-    CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    CUDA_TRY(cudaFuncSetAttribute(u12_rows_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)u12_rows_smem((int)(outer / kBlk))));
   // the whole factorisation on the device, as launches on the engine's
   // stream (and stream2 / stream3, joined back into it)
@@ -1126,13 +1164,13 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
           const int64_t below = n - KE;
           if (below > 0) {
             CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_diag, 0));
-            TRY(trsm_on(k0, KE, n, dinv, NECGPU_K_PANEL, e->stream4, pc > 0 ? e->d_Ap : nullptr, KE));
+            TRY(trsm_on(k0, KE, n, dinv, NECGPU_K_PANEL, e->stream4, pc > 0 ? op<F>(e->d_Ap) : nullptr, KE));
           }
           if (pc > 0) {
-            __nv_bfloat16* Bsel = e->d_Bpan + (size_t)((k0 - K0) / kBlk) * bpan_slot;
+            Op* Bsel = op<F>(e->d_Bpan) + (size_t)((k0 - K0) / kBlk) * bpan_slot;
             const dim3 tg((unsigned)((pc + kTopCols - 1) / kTopCols), (unsigned)((pc + kTopRows - 1) / kTopRows));
             const int kt = kbegin(e);
-            CUDA_TRY(launch_prio(e->chain_prio, panel_top_kernel, tg, dim3(kTopThreads), panel_top_smem(), e->stream,
+            CUDA_TRY(launch_prio(e->chain_prio, panel_top_kernel<F>, tg, dim3(kTopThreads), panel_top_smem(), e->stream,
                                  M, ld, k0, KE, (const int*)e->d_src, (const float2*)dinv, Bsel, e->d_top_cnt));
             kend(e, kt, NECGPU_K_TRSM, (4.0 * kBlk * kBlk + 8.0 * kBlk * (double)pc) * 2.0 * (double)pc, nullptr,
                  "panel_top_kernel");
@@ -1140,7 +1178,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
             if (below > 0) {
               CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream));
               CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_u12b, 0));
-              TRY(tc_run(e, 0, below, 0, pc, kb, M + KE * ld + r0, ld, e->stream4,
+              TRY(tc_run<F>(e, 0, below, 0, pc, kb, M + KE * ld + r0, ld, e->stream4,
                          std::min(gemm_grid, e->side_ctas), 0, Bsel));
             }
           }
@@ -1162,25 +1200,25 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
           // buffers so that U12 of the next panel never overwrites the one
           // the bulk update is reading.
           const int p = (int)((k0 - K0) / kBlk);
-          __nv_bfloat16* Bsel = (p & 1) ? e->d_Bp3 : e->d_Bp;
+          Op* Bsel = op<F>((p & 1) ? e->d_Bp3 : e->d_Bp);
           CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
           CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
           TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3, Bsel, r0));
           CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
           // the bulk: L21 rows [r0 + 64, n) after the diagonal LU, then their update
           CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_diag, 0));
-          TRY(trsm_on(k0, r0 + kBlk, n, dinv, NECGPU_K_PANEL, e->stream4, e->d_Ap, r0));
+          TRY(trsm_on(k0, r0 + kBlk, n, dinv, NECGPU_K_PANEL, e->stream4, op<F>(e->d_Ap), r0));
           CUDA_TRY(cudaStreamWaitEvent(e->stream4, e->ev_u12b, 0));
-          TRY(tc_run(e, 0, rest - kBlk, 0, pc, kb, M + (r0 + kBlk) * ld + r0, ld, e->stream4, gemm_grid, kBlk,
+          TRY(tc_run<F>(e, 0, rest - kBlk, 0, pc, kb, M + (r0 + kBlk) * ld + r0, ld, e->stream4, gemm_grid, kBlk,
                      Bsel));
           // the next diagonal block's rows: their L21 rows need the previous
           // bulk update (it reached them), then their update
           if (bulk_pending) CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_bulk, 0));
-          TRY(trsm(false, k0, r0, r0 + kBlk, dinv, NECGPU_K_PANEL, e->d_Ap, r0));
+          TRY(trsm(false, k0, r0, r0 + kBlk, dinv, NECGPU_K_PANEL, op<F>(e->d_Ap), r0));
           CUDA_TRY(cudaEventRecord(e->ev_bulk, e->stream4));
           bulk_pending = true;
           CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
-          TRY(tc_run(e, 0, kBlk, 0, pc, kb, M + r0 * ld + r0, ld, e->stream, gemm_grid, 0, Bsel));
+          TRY(tc_run<F>(e, 0, kBlk, 0, pc, kb, M + r0 * ld + r0, ld, e->stream, gemm_grid, 0, Bsel));
           continue;
         }
         if (bulk_pending) {  // rows below this panel were last updated on stream4
@@ -1197,17 +1235,17 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         if (fork) {
           CUDA_TRY(cudaEventRecord(e->ev_u12a, e->stream));
           CUDA_TRY(cudaStreamWaitEvent(e->stream3, e->ev_u12a, 0));
-          TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3, emit ? e->d_Bp : nullptr, r0));
+          TRY(trsm_left_on(k0, r0, KE, dinv, NECGPU_K_TRSM, e->stream3, emit ? op<F>(e->d_Bp) : nullptr, r0));
           CUDA_TRY(cudaEventRecord(e->ev_u12b, e->stream3));
         }
-        TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL, emit ? e->d_Ap : nullptr, r0));
+        TRY(trsm(false, k0, r0, n, dinv, NECGPU_K_PANEL, emit ? op<F>(e->d_Ap) : nullptr, r0));
         if (pc > 0) {
           if (fork)
             CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_u12b, 0));
           else
             TRY(trsm(true, k0, r0, KE, dinv, NECGPU_K_TRSM));
           if (emit)
-            TRY(tc_run(e, 0, rest, 0, pc, kb, M + r0 * ld + r0, ld, e->stream, gemm_grid));
+            TRY(tc_run<F>(e, 0, rest, 0, pc, kb, M + r0 * ld + r0, ld, e->stream, gemm_grid));
           else
             TRY(gemm(r0, r0, k0, rest, pc, kb));
         }
@@ -1237,9 +1275,9 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
         // U12 of the outer row block, rows [K0, KE) x columns [KE, n), with
         // the far columns' interchanges, in one launch
         KLAUNCH(NECGPU_K_TRSM, 4.0 * (double)(KE - K0) * (double)(KE - K0) * (double)rest,
-                u12_rows_kernel<<<(unsigned)((rest + kU12Cols - 1) / kU12Cols), 256, (unsigned)u12_rows_smem(nbo),
+                u12_rows_kernel<F><<<(unsigned)((rest + kU12Cols - 1) / kU12Cols), 256, (unsigned)u12_rows_smem(nbo),
                                   e->stream>>>(
-                    M, ld, K0, nbo, KE, n, e->d_src, swap_far ? 1 : 0, u12_emit ? e->d_Bp2 : nullptr));
+                    M, ld, K0, nbo, KE, n, e->d_src, swap_far ? 1 : 0, u12_emit ? op<F>(e->d_Bp2) : nullptr));
       } else {
         if (swap_far)
           for (int64_t k0 = K0; k0 < KE; k0 += kBlk) TRY(laswp(k0, (int)std::min<int64_t>(kBlk, n - k0), KE, n));
@@ -1255,11 +1293,11 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
       // trailing update with K = outer
       const int kk = (int)(KE - K0);
       if (la && rest > outer) {
-        TRY(tc_pack(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk, !u12_emit));
-        TRY(tc_run(e, 1, rest, 0, outer, kk, M + KE * ld + KE, ld, e->stream, e->nsm));  // next outer block
+        TRY(tc_pack<F>(e, 1, M + KE * ld + K0, M + K0 * ld + KE, ld, rest, rest, kk, !u12_emit));
+        TRY(tc_run<F>(e, 1, rest, 0, outer, kk, M + KE * ld + KE, ld, e->stream, e->nsm));  // next outer block
         CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
         CUDA_TRY(cudaStreamWaitEvent(e->stream2, e->ev_fork, 0));
-        TRY(tc_run(e, 1, rest, outer, rest - outer, kk, M + KE * ld + KE + outer, ld, e->stream2,
+        TRY(tc_run<F>(e, 1, rest, outer, rest - outer, kk, M + KE * ld + KE + outer, ld, e->stream2,
                    e->nsm - e->lookahead_sms));
         CUDA_TRY(cudaEventRecord(e->ev_far, e->stream2));
         far_pending = true;
@@ -1273,13 +1311,13 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // operand buffers at their largest sizes before any capture (no
   // allocation happens inside the launches below)
   if (e->use_tc) {
-    TRY(ensure_tc(e, 6 * (int)outer, n, 0));
-    if (la) TRY(ensure_tc(e, 6 * (int)outer, n, 1));
+    TRY(ensure_tc<F>(e, F::kKMul * (int)outer, n, 0));
+    if (la) TRY(ensure_tc<F>(e, F::kKMul * (int)outer, n, 1));
     if (split_inner) {
-      const size_t need = 2 * (size_t)e->tc_rows * (size_t)e->tc_kdim;
-      if (!e->d_Bp3 || e->bp3_elems < need) {
+      const size_t need = 2 * (size_t)e->tc_rows * (size_t)e->tc_kbytes;
+      if (!e->d_Bp3 || e->bp3_bytes < need) {
         TRY(dalloc(e, e->d_Bp3, need));
-        e->bp3_elems = need;
+        e->bp3_bytes = need;
       }
     }
   }
@@ -1291,7 +1329,7 @@ int run_lu_blockpiv(necgpu_engine* e, float2* M) {
   // default stream or is being captured by the caller.
   LuGraphKey key{};
   key.n = n, key.ld = ld, key.outer = outer, key.la = la, key.la_sms = e->lookahead_sms;
-  key.group = e->gemm_group, key.use_tc = e->use_tc;
+  key.group = e->gemm_group, key.use_tc = e->use_tc + 2 * (int)F::kFormat;
   key.trsm8 = (e->l21_rows ? 64 : 0) + (panel_top ? 32 : 0) + (e->chain_prio ? 16 : 0) + e->trsm8 * 8 + (split_inner ? 4 : 0) +
               (u12_fused ? 2 : 0) + (fused_pack ? 1 : 0);
   key.nsm = e->nsm * 4096 + e->side_ctas;
@@ -1540,6 +1578,17 @@ int run_trsv_inv(necgpu_engine* e, float2* rhs, float2* sol) {
 
 // Mixed-precision factorisation of the FP64 matrix: demote to complex64, then
 // LU with block-local pivoting (blockpiv) or full partial pivoting.
+// Operand format of the next mixed factorisation.  TF32 saves a third of the
+// update's tensor-core time (~2 ms at 11,520 unknowns, growing as n^3) and
+// costs a refinement step or more (~1.2 ms there, growing as n to n^2), so
+// it is taken only for large systems, and no longer once a TF32
+// factorisation of this engine needed many refinement steps (a badly
+// conditioned structure, whose next frequencies would do the same).
+int pick_format(const necgpu_engine* e) {
+  if (e->tc_format) return e->tc_format;
+  return e->n >= e->tf32_min_n && !e->tf32_demoted ? 2 : 1;
+}
+
 int factor_mixed(necgpu_engine* e, bool blockpiv) {
   if (!e->Z32) TRY(dalloc(e, e->Z32, (size_t)e->n * e->ld));
   if (!e->z32_fresh)
@@ -1548,14 +1597,16 @@ int factor_mixed(necgpu_engine* e, bool blockpiv) {
   e->blockpiv = blockpiv;
   e->stats.pivoting = blockpiv ? 1 : 0;
   e->adj_ready = false;
+  const int fmt = pick_format(e);
+  e->tc_format_used = fmt;
   if (blockpiv) {
-    const int rc = run_lu_blockpiv(e, e->Z32);
+    const int rc = fmt == 2 ? run_lu_blockpiv<tc::Tf32>(e, e->Z32) : run_lu_blockpiv<tc::SplitBf16>(e, e->Z32);
     if (rc != NECGPU_ERR_SINGULAR && rc != NECGPU_ERR_NONFINITE) return rc ? rc : invert_diag_blocks(e);
     // a diagonal block without a usable pivot: full partial pivoting
     CUDA_TRY(cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream));
     return factor_mixed(e, false);
   }
-  TRY(run_lu<float>(e, e->Z32));
+  TRY((fmt == 2 ? run_lu<float, tc::Tf32>(e, e->Z32) : run_lu<float>(e, e->Z32)));
   return invert_diag_blocks(e);
 }
 
@@ -1702,9 +1753,13 @@ int run_solve(necgpu_engine* e, bool sync_checks) {
     int it = 0;
     double rel = 1.0;
     int rc = refine(e, &it, &rel);
-    if ((rc == NECGPU_ERR_NONFINITE || rel > kRefineFallback) && e->blockpiv) {
-      // block-local pivoting was not good enough for this matrix: refactor
-      // the FP32 copy with full partial pivoting and refine again
+    const bool tf32 = e->tc_format_used == 2;
+    if (!rc && tf32 && it > e->tf32_max_iters) e->tf32_demoted = true;
+    if ((rc == NECGPU_ERR_NONFINITE || rel > kRefineFallback) && (e->blockpiv || (tf32 && e->tc_format == 0))) {
+      // block-local pivoting (or the TF32 update) was not good enough for
+      // this matrix: refactor the FP32 copy with full partial pivoting (and
+      // split BF16 unless TF32 was asked for) and refine again
+      if (tf32) e->tf32_demoted = true;
       TRY(factor_mixed(e, false));
       int it2 = 0;
       rc = refine(e, &it2, &rel);
@@ -2022,6 +2077,12 @@ int necgpu_create(necgpu_engine** out, int device) {
     e->sweep_cluster = v >= 16 ? 16 : v >= 8 ? 8 : 0;
   }
   if (const char* s = std::getenv("NECPP_B200_L21_ROWS")) e->l21_rows = (s[0] != '0');
+  if (const char* s = std::getenv("NECPP_B200_TC_FORMAT"))
+    e->tc_format = !std::strcmp(s, "tf32") ? 2 : !std::strcmp(s, "bf16x3") ? 1 : 0;
+  if (const char* s = std::getenv("NECPP_B200_TF32_MIN_N")) {
+    const long long v = std::atoll(s);
+    if (v >= 1) e->tf32_min_n = v;
+  }
   if (const char* s = std::getenv("NECPP_B200_SIDE_CTAS")) {
     const int v = std::atoi(s);
     if (v >= 1 && v <= 1024) e->side_ctas = v;
@@ -2166,6 +2227,18 @@ int necgpu_set_pivoting(necgpu_engine* e, int mode) {
   if (!e || (mode != 0 && mode != 1)) return NECGPU_ERR_ARG;
   e->prefer_blockpiv = (mode == 1);
   return NECGPU_OK;
+}
+
+int necgpu_set_update_format(necgpu_engine* e, int format) {
+  if (!e || format < 0 || format > 2) return NECGPU_ERR_ARG;
+  e->tc_format = format;
+  e->tf32_demoted = false;
+  return NECGPU_OK;
+}
+
+int necgpu_update_format(const necgpu_engine* e) {
+  if (!e) return NECGPU_ERR_ARG;
+  return e->factored == NECGPU_MIXED ? e->tc_format_used : 0;
 }
 
 int necgpu_get_stats(const necgpu_engine* e, necgpu_stats* out) {
@@ -2424,7 +2497,8 @@ int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, 
     cudaMemsetAsync(d, 0, 2 * sizeof(float), e->stream);
     cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream);
     // X: tensor cores; Y: CUDA-core FP32 reference of the same update
-    rc = tc_gemm_sub(e, X + o * ld, X + o, X + o * ld + o, ld, m, n, kb);
+    rc = pick_format(e) == 2 ? tc_gemm_sub<tc::Tf32>(e, X + o * ld, X + o, X + o * ld + o, ld, m, n, kb)
+                             : tc_gemm_sub<tc::SplitBf16>(e, X + o * ld, X + o, X + o * ld + o, ld, m, n, kb);
     if (!rc) {
       dim3 g((unsigned)((n + 63) / 64), (unsigned)((m + 63) / 64));
       gemm_sub_kernel<float><<<g, 256, 0, e->stream>>>(Y + o * ld, ld, Y + o, ld, Y + o * ld + o, ld, m, n, kb);
@@ -2606,7 +2680,8 @@ int necgpu_check_block_lu(necgpu_engine* e, int n, unsigned seed, double* backwa
     cudaMemcpyAsync(A, e->Z32, cnt * sizeof(float2), cudaMemcpyDeviceToDevice, e->stream);
     cudaMemsetAsync(d, 0, 2 * sizeof(float), e->stream);
     cudaMemsetAsync(e->d_status, 0, 4 * sizeof(int), e->stream);
-    rc = run_lu_blockpiv(e, e->Z32);
+    e->tc_format_used = pick_format(e);
+    rc = e->tc_format_used == 2 ? run_lu_blockpiv<tc::Tf32>(e, e->Z32) : run_lu_blockpiv<tc::SplitBf16>(e, e->Z32);
     if (!rc) {
       lu_residual_kernel<<<8 * e->nsm, 256, 0, e->stream>>>(A, e->Z32, e->d_perm, ld, n, d);
       float h[2] = {0, 0};
@@ -3554,6 +3629,7 @@ int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_de
       }
       prev = rel;
     }
+    if (e->tc_format_used == 2 && iters > e->tf32_max_iters) e->tf32_demoted = true;
     if (e->blockpiv && rel > kRefineFallback)
       return fail(e, NECGPU_ERR_REFINE,
                   "solve_noalloc: refinement stalled on the block-pivoted factors; necgpu_solve refactors "

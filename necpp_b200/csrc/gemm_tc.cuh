@@ -1,21 +1,34 @@
 // Trailing update of the mixed-precision LU on the 5th-generation tensor
 // cores: C -= A * B for complex64 A (m x kb), B (kb x n), C (m x n), all
-// row-major, as ONE real BF16 GEMM with FP32 accumulation in TMEM.
+// row-major, as ONE real GEMM with FP32 accumulation in TMEM, in one of two
+// operand formats (the engine picks one per factorisation).
 //
-// Real formulation.  Each complex FP32 operand is split into BF16 hi/lo parts
-// (x = hi + lo + O(2^-16 x)); with K' = 6 * kbp (kbp = kb rounded up to 64):
+// Split BF16 (SplitBf16).  Each complex FP32 operand is split into BF16 hi/lo
+// parts (x = hi + lo + O(2^-16 x)); with K' = 6 * kbp (kbp = kb rounded up
+// to 64):
 //   A'[i]    = [ Ar_hi | Ai_hi | Ar_hi | Ai_hi | Ar_lo | Ai_lo ]          (m rows)
 //   B'[2j]   = [ Br_hi |-Bi_hi | Br_lo |-Bi_lo | Br_hi |-Bi_hi ]  -> Re(AB)_j
 //   B'[2j+1] = [ Bi_hi | Br_hi | Bi_lo | Br_lo | Bi_hi | Br_hi ]  -> Im(AB)_j
-// so D = A' B'^T (m x 2n) holds (Re, Im) of A*B interleaved per column: the
-// accumulator row of output row i is a contiguous run of complex values of
-// C's row i.  Products kept: hi*hi + hi*lo + lo*hi (the lo*lo term, ~2^-16
-// relative, is dropped); the FP64 refinement of the solve removes the rest.
+// Products kept: hi*hi + hi*lo + lo*hi (the lo*lo term, ~2^-16 relative, is
+// dropped).
+//
+// TF32 (Tf32).  One pass, K' = 2 * kbp, the operands rounded to
+// TF32 (10-bit mantissa, round to nearest) in FP32 containers:
+//   A'[i] = [ Ar | Ai ],  B'[2j] = [ Br | -Bi ],  B'[2j+1] = [ Bi | Br ].
+// TF32 runs at half the BF16 rate, so this issues 2/3 of the split form's
+// tensor cycles and moves 2/3 of its operand bytes; the factor's error is
+// ~2^-11 instead of ~2^-16, which costs the refinement a step.
+//
+// Either way D = A' B'^T (m x 2n) holds (Re, Im) of A*B interleaved per
+// column: the accumulator row of output row i is a contiguous run of
+// complex values of C's row i, and the FP64 refinement of the solve removes
+// the update's rounding.
 //
 // Kernel: persistent, one CTA per SM, 6 warps:
-//   warp 0  TMA producer: A' (128 x 64) and B' (256 x 64) tiles, 128B swizzle,
-//           into a 4-stage shared-memory ring (48 KB per stage);
-//   warp 1  MMA issuer: tcgen05.mma.cta_group::1.kind::f16, M=128 N=256 K=16,
+//   warp 0  TMA producer: A' (128 x 128 B) and B' (256 x 128 B) tiles, 128B
+//           swizzle, into a 4-stage shared-memory ring (48 KB per stage);
+//   warp 1  MMA issuer: tcgen05.mma.cta_group::1, M=128 N=256, four
+//           instructions of 32 B of K per stage (K=16 BF16 or K=8 TF32),
 //           accumulating in one of two 128 x 256 FP32 TMEM buffers;
 //   warps 2-5 epilogue: tcgen05.ld of the finished buffer (32 rows x 32
 //           columns per load), negated into a 128B-swizzled 4 KB staging
@@ -36,9 +49,27 @@
 namespace necb {
 namespace tc {
 
-constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;
-constexpr int A_BYTES = BM * BK * 2;            // 16 KB
-constexpr int B_BYTES = BN * BK * 2;            // 32 KB
+// The two operand formats: element type, K' per complex K (kKMul), the
+// instruction descriptor's A/B format code (1 = BF16, 2 = TF32)
+struct SplitBf16 {
+  using T = __nv_bfloat16;
+  static constexpr int kKMul = 6;
+  static constexpr uint32_t kFormat = 1;
+};
+struct Tf32 {
+  using T = float;  // TF32 values in FP32 containers
+  static constexpr int kKMul = 2;
+  static constexpr uint32_t kFormat = 2;
+};
+// BK: operand elements per 128-byte row of a stage; KP: the complex K of an
+// update is padded to a multiple of KP, and K' = F::kKMul * (padded K)
+template <class F>
+__host__ __device__ constexpr int bk() {
+  return 128 / (int)sizeof(typename F::T);
+}
+constexpr int BM = 128, BN = 256, KP = 64, STAGES = 4;
+constexpr int A_BYTES = BM * 128;               // 16 KB
+constexpr int B_BYTES = BN * 128;               // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;  // 48 KB
 constexpr int THREADS = 192;
 constexpr int EPI_WARPS = 4;
@@ -112,16 +143,31 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   d |= (uint64_t)2 << 61;          // SWIZZLE_128B
   return d;
 }
-// BF16 x BF16 -> FP32, both K-major, M = 128, N = 256
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// instruction descriptor: FP32 accumulator (bits 4-5 = 1), A and B format
+// (bits 7-9, 10-12: 1 = BF16, 2 = TF32), both K-major, N >> 3 at bit 17,
+// M >> 4 at bit 24; M = 128, N = 256
+template <class F>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4) | (F::kFormat << 7) | (F::kFormat << 10) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
-      : "memory");
+template <class F>
+__device__ __forceinline__ void mma_op(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  if constexpr (F::kFormat == 2)
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc<F>()), "r"(accumulate)
+        : "memory");
+  else
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc<F>()), "r"(accumulate)
+        : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -143,30 +189,77 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16& hi, __nv_bflo
   hi = __float2bfloat16_rn(x);
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
+// x rounded to TF32 (nearest, ties away), kept in an FP32 container
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// A' entries of one complex value a at column k of an A' row (kbp: the
+// padded complex K, so the parts sit kbp apart)
+template <class F>
+__device__ __forceinline__ void put_a(typename F::T* row, int kbp, int k, float2 a) {
+  if constexpr (F::kFormat == 2) {
+    row[k] = to_tf32(a.x);
+    row[kbp + k] = to_tf32(a.y);
+  } else {
+    __nv_bfloat16 rh, rl, ih, il;
+    split_bf16(a.x, rh, rl);
+    split_bf16(a.y, ih, il);
+    row[0 * kbp + k] = rh;
+    row[1 * kbp + k] = ih;
+    row[2 * kbp + k] = rh;
+    row[3 * kbp + k] = ih;
+    row[4 * kbp + k] = rl;
+    row[5 * kbp + k] = il;
+  }
+}
+// B' entries of one complex value b at column k of rows 2j (re) and 2j+1 (im)
+template <class F>
+__device__ __forceinline__ void put_b(typename F::T* re, typename F::T* im, int kbp, int k, float2 b) {
+  if constexpr (F::kFormat == 2) {
+    const float br = to_tf32(b.x), bi = to_tf32(b.y);
+    re[k] = br;
+    re[kbp + k] = -bi;
+    im[k] = bi;
+    im[kbp + k] = br;
+  } else {
+    __nv_bfloat16 rh, rl, ih, il;
+    split_bf16(b.x, rh, rl);
+    split_bf16(b.y, ih, il);
+    const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
+    re[0 * kbp + k] = rh;
+    re[1 * kbp + k] = nih;
+    re[2 * kbp + k] = rl;
+    re[3 * kbp + k] = nil;
+    re[4 * kbp + k] = rh;
+    re[5 * kbp + k] = nih;
+    im[0 * kbp + k] = ih;
+    im[1 * kbp + k] = rh;
+    im[2 * kbp + k] = il;
+    im[3 * kbp + k] = rl;
+    im[4 * kbp + k] = ih;
+    im[5 * kbp + k] = rh;
+  }
+}
 
 // A' from A (m x kb complex, row-major lda): one thread per (row, k)
-__global__ void pack_a_kernel(const float2* A, int64_t lda, int m, int kb, int kbp, __nv_bfloat16* Ap) {
+template <class F>
+__global__ void pack_a_kernel(const float2* A, int64_t lda, int m, int kb, int kbp, typename F::T* Ap) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)m * kbp) return;
   const int i = (int)(idx / kbp), k = (int)(idx - (int64_t)i * kbp);
-  float2 a = k < kb ? A[(int64_t)i * lda + k] : make_float2(0.f, 0.f);
-  __nv_bfloat16 rh, rl, ih, il;
-  split_bf16(a.x, rh, rl);
-  split_bf16(a.y, ih, il);
-  __nv_bfloat16* row = Ap + (int64_t)i * 6 * kbp;
-  row[0 * kbp + k] = rh;
-  row[1 * kbp + k] = ih;
-  row[2 * kbp + k] = rh;
-  row[3 * kbp + k] = ih;
-  row[4 * kbp + k] = rl;
-  row[5 * kbp + k] = il;
+  const float2 a = k < kb ? A[(int64_t)i * lda + k] : make_float2(0.f, 0.f);
+  put_a<F>(Ap + (int64_t)i * F::kKMul * kbp, kbp, k, a);
 }
 
 // B' from B (kb x n complex, row-major ldb): tile of 64 k x 32 columns
 // through shared memory so both the reads (along n) and the writes (along k)
 // are contiguous.
-__global__ void __launch_bounds__(256) pack_b_kernel(const float2* B, int64_t ldb, int kb, int kbp, int n,
-                                                     __nv_bfloat16* Bp) {
+template <class F>
+__global__ void __launch_bounds__(256)
+    pack_b_kernel(const float2* B, int64_t ldb, int kb, int kbp, int n, typename F::T* Bp) {
   __shared__ float2 t[64][33];
   const int j0 = blockIdx.x * 32, k0 = blockIdx.y * 64;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -175,32 +268,13 @@ __global__ void __launch_bounds__(256) pack_b_kernel(const float2* B, int64_t ld
     t[kk][tx] = (k < kb && j < n) ? B[(int64_t)k * ldb + j] : make_float2(0.f, 0.f);
   }
   __syncthreads();
-  const int64_t K2 = 6 * (int64_t)kbp;
+  const int64_t K2 = F::kKMul * (int64_t)kbp;
   // each warp writes rows (2j, 2j+1) for 4 columns j; lane covers k pairs
   for (int jj = ty; jj < 32; jj += 8) {
     const int j = j0 + jj;
     if (j >= n) continue;
-    __nv_bfloat16* re = Bp + (int64_t)(2 * j) * K2 + k0;
-    __nv_bfloat16* im = re + K2;
-    for (int kk = tx; kk < 64; kk += 32) {
-      float2 b = t[kk][jj];
-      __nv_bfloat16 rh, rl, ih, il;
-      split_bf16(b.x, rh, rl);
-      split_bf16(b.y, ih, il);
-      const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
-      re[0 * kbp + kk] = rh;
-      re[1 * kbp + kk] = nih;
-      re[2 * kbp + kk] = rl;
-      re[3 * kbp + kk] = nil;
-      re[4 * kbp + kk] = rh;
-      re[5 * kbp + kk] = nih;
-      im[0 * kbp + kk] = ih;
-      im[1 * kbp + kk] = rh;
-      im[2 * kbp + kk] = il;
-      im[3 * kbp + kk] = rl;
-      im[4 * kbp + kk] = ih;
-      im[5 * kbp + kk] = rh;
-    }
+    typename F::T* re = Bp + (int64_t)(2 * j) * K2 + k0;
+    for (int kk = tx; kk < 64; kk += 32) put_b<F>(re, re + K2, kbp, kk, t[kk][jj]);
   }
 }
 
@@ -223,6 +297,7 @@ __device__ __forceinline__ void tile_coords(int tile, int m_tiles, int n_tiles, 
 
 // C (m x n complex, row-major; tmC views it as m rows x 2n FP32 with 32 x 32
 // boxes, 128B swizzle) -= D, D = A' B'^T, K' = kdim (multiple of 64)
+template <class F>
 __global__ void __launch_bounds__(THREADS, 1)
     gemm_tc_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const __grid_constant__ CUtensorMap tmC, int m, int n, int kdim, int group, int* status) {
@@ -238,6 +313,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int m_tiles = (m + BM - 1) / BM;
   const int n_tiles = (2 * n + BN - 1) / BN;
   const int total = m_tiles * n_tiles;
+  constexpr int BK = bk<F>();
   const int kblocks = kdim / BK;
 
   auto bar = [&](int i) { return smem_u32(bars + i); };
@@ -324,8 +400,8 @@ __global__ void __launch_bounds__(THREADS, 1)
           const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
           const uint32_t b_addr = a_addr + A_BYTES;
 #pragma unroll
-          for (int k = 0; k < BK / 16; k++)
-            mma_bf16(d_tmem, smem_desc(a_addr + k * 32), smem_desc(b_addr + k * 32), (kb | k) != 0);
+          for (int k = 0; k < 4; k++)
+            mma_op<F>(d_tmem, smem_desc(a_addr + k * 32), smem_desc(b_addr + k * 32), (kb | k) != 0);
           mma_commit(bar(EMPTY + s));  // frees the stage once these MMAs retire
         }
         if (*abort_flag) break;

@@ -587,50 +587,56 @@ constexpr size_t trsm_panel_smem() {
   return (size_t)(kBlk * (kBlk + 1) + kTrsmW * (kBlk + 1) + kBlk) * sizeof(T);
 }
 
-// The tensor-core update's packed BF16 operands (gemm_tc.cuh), written by
-// the panel solves that produce them instead of by separate packing passes.
-// kdim = 6 * 64 (one 64-wide panel): A' row i = [Ar_hi Ai_hi Ar_hi Ai_hi
-// Ar_lo Ai_lo]; B' rows 2j, 2j+1 = [Br_hi -Bi_hi Br_lo -Bi_lo Br_hi -Bi_hi],
-// [Bi_hi Br_hi Bi_lo Br_lo Bi_hi Br_hi] (the layouts of pack_a_kernel and
-// pack_b_kernel).
-__device__ __forceinline__ void emit_a(__nv_bfloat16* Ap, int64_t row, int k, float2 a) {
-  __nv_bfloat16 rh, rl, ih, il;
-  tc::split_bf16(a.x, rh, rl);
-  tc::split_bf16(a.y, ih, il);
-  __nv_bfloat16* p = Ap + row * (6 * kBlk) + k;
-  p[0 * kBlk] = rh;
-  p[1 * kBlk] = ih;
-  p[2 * kBlk] = rh;
-  p[3 * kBlk] = ih;
-  p[4 * kBlk] = rl;
-  p[5 * kBlk] = il;
+// The tensor-core update's packed operands (gemm_tc.cuh, format F), written
+// by the panel solves that produce them instead of by separate packing
+// passes; kdim = F::kKMul * 64 (one 64-wide panel), the layouts of
+// pack_a_kernel and pack_b_kernel.
+template <class F>
+__device__ __forceinline__ void emit_a(typename F::T* Ap, int64_t row, int k, float2 a) {
+  tc::put_a<F>(Ap + row * (F::kKMul * kBlk), kBlk, k, a);
 }
 // eight consecutive k (k0 a multiple of 8) of column j of B: 16-byte stores
 // (kbp: the operand's K per part, a multiple of 64)
-__device__ __forceinline__ void emit_b8(__nv_bfloat16* Bp, int64_t j, int k0, const float2 (&b)[8],
-                                        int kbp = kBlk) {
-  __align__(16) __nv_bfloat16 v[12][8];
+template <class F>
+__device__ __forceinline__ void emit_b8(typename F::T* Bp, int64_t j, int k0, const float2 (&b)[8], int kbp = kBlk) {
+  typename F::T* re = Bp + (2 * j) * (F::kKMul * (int64_t)kbp) + k0;
+  typename F::T* im = re + F::kKMul * kbp;
+  if constexpr (F::kFormat == 2) {
+    __align__(16) float v[4][8];
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    __nv_bfloat16 rh, rl, ih, il;
-    tc::split_bf16(b[i].x, rh, rl);
-    tc::split_bf16(b[i].y, ih, il);
-    const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
-    v[0][i] = rh, v[1][i] = nih, v[2][i] = rl, v[3][i] = nil, v[4][i] = rh, v[5][i] = nih;
-    v[6][i] = ih, v[7][i] = rh, v[8][i] = il, v[9][i] = rl, v[10][i] = ih, v[11][i] = rh;
-  }
-  __nv_bfloat16* re = Bp + (2 * j) * (6 * (int64_t)kbp) + k0;
-  __nv_bfloat16* im = re + 6 * kbp;
+    for (int i = 0; i < 8; i++) {
+      const float br = tc::to_tf32(b[i].x), bi = tc::to_tf32(b[i].y);
+      v[0][i] = br, v[1][i] = -bi, v[2][i] = bi, v[3][i] = br;
+    }
 #pragma unroll
-  for (int s = 0; s < 6; s++) {
-    *reinterpret_cast<uint4*>(re + s * kbp) = *reinterpret_cast<const uint4*>(v[s]);
-    *reinterpret_cast<uint4*>(im + s * kbp) = *reinterpret_cast<const uint4*>(v[6 + s]);
+    for (int s = 0; s < 2; s++) {
+      *reinterpret_cast<uint4*>(re + s * kbp) = *reinterpret_cast<const uint4*>(&v[s][0]);
+      *reinterpret_cast<uint4*>(re + s * kbp + 4) = *reinterpret_cast<const uint4*>(&v[s][4]);
+      *reinterpret_cast<uint4*>(im + s * kbp) = *reinterpret_cast<const uint4*>(&v[2 + s][0]);
+      *reinterpret_cast<uint4*>(im + s * kbp + 4) = *reinterpret_cast<const uint4*>(&v[2 + s][4]);
+    }
+  } else {
+    __align__(16) __nv_bfloat16 v[12][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      __nv_bfloat16 rh, rl, ih, il;
+      tc::split_bf16(b[i].x, rh, rl);
+      tc::split_bf16(b[i].y, ih, il);
+      const __nv_bfloat16 nih = __hneg(ih), nil = __hneg(il);
+      v[0][i] = rh, v[1][i] = nih, v[2][i] = rl, v[3][i] = nil, v[4][i] = rh, v[5][i] = nih;
+      v[6][i] = ih, v[7][i] = rh, v[8][i] = il, v[9][i] = rl, v[10][i] = ih, v[11][i] = rh;
+    }
+#pragma unroll
+    for (int s = 0; s < 6; s++) {
+      *reinterpret_cast<uint4*>(re + s * kbp) = *reinterpret_cast<const uint4*>(v[s]);
+      *reinterpret_cast<uint4*>(im + s * kbp) = *reinterpret_cast<const uint4*>(v[6 + s]);
+    }
   }
 }
 
-template <typename T, bool LEFT>
+template <typename T, bool LEFT, class F = tc::SplitBf16>
 __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
-                                                            const T* dinv, __nv_bfloat16* Ap = nullptr,
+                                                            const T* dinv, typename F::T* Ap = nullptr,
                                                             int64_t abase = 0) {
   constexpr int NB = kBlk, W = kTrsmW, B = 8;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -731,7 +737,7 @@ __global__ void __launch_bounds__(kTrsmW) trsm_panel_kernel(T* M, int64_t ld, in
           M[(s0 + rr) * ld + k0 + c] = X[rr][c];
           // L21 rows are the A operand of the update that follows
           if constexpr (!LEFT && std::is_same<T, float2>::value)
-            if (Ap) emit_a(Ap, s0 + rr - abase, c, X[rr][c]);
+            if (Ap) emit_a<F>(Ap, s0 + rr - abase, c, X[rr][c]);
         }
       }
     }
@@ -754,9 +760,9 @@ constexpr size_t trsm8_smem() {
 }
 
 // VPL vectors per lane: 32 * VPL vectors per CTA share one triangle load.
-template <typename T, bool LEFT, int VPL = 1>
+template <typename T, bool LEFT, int VPL = 1, class F = tc::SplitBf16>
 __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int64_t n, int64_t k0, int64_t sbeg,
-                                                          const T* dinv, __nv_bfloat16* Bp = nullptr,
+                                                          const T* dinv, typename F::T* Bp = nullptr,
                                                           int64_t bbase = 0) {
   constexpr int NB = kBlk, V = kTrsm8Vec * VPL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -847,7 +853,7 @@ __global__ void __launch_bounds__(256) trsm8_panel_kernel(T* M, int64_t ld, int6
     }
     // U12 columns are the B operand of the update that follows
     if constexpr (LEFT && std::is_same<T, float2>::value)
-      if (Bp) emit_b8(Bp, vec[w] - bbase, g * 8, acc[w]);
+      if (Bp) emit_b8<F>(Bp, vec[w] - bbase, g * 8, acc[w]);
   }
 }
 
@@ -977,9 +983,10 @@ constexpr int kTopCnt = 128;       // counters the caller provides
 __host__ __device__ constexpr size_t panel_top_smem() {
   return (size_t)(2 * kBlk * kS + kTopRows * kS + kTopCols * kS + 2 * 8 * 64 + kBlk) * sizeof(float2);
 }
+template <class F>
 __global__ void __launch_bounds__(kTopThreads) panel_top_kernel(float2* M, int64_t ld, int64_t k0, int64_t c_hi,
                                                                  const int* src_rows, const float2* dinv,
-                                                                 __nv_bfloat16* Bp, unsigned* cnt) {
+                                                                 typename F::T* Bp, unsigned* cnt) {
   constexpr int NB = kBlk, NT = kTopSolveThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float2* Ut = reinterpret_cast<float2*>(smem_raw);  // U11 transposed
@@ -1131,7 +1138,7 @@ __global__ void __launch_bounds__(kTopThreads) panel_top_kernel(float2* M, int64
         yb[i] = Yt[c * kS + 8 * g + i];
         M[(k0 + 8 * g + i) * ld + col] = yb[i];
       }
-      if (Bp) emit_b8(Bp, col - r0, g * 8, yb);
+      if (Bp) emit_b8<F>(Bp, col - r0, g * 8, yb);
     }
   }
   if (crow) {
@@ -1155,8 +1162,9 @@ constexpr int kL21Rows = 32;
 __host__ __device__ constexpr size_t l21_rows_smem() {
   return (size_t)(kBlk * kS + kL21Rows * kS + 8 * 64 + kBlk) * sizeof(float2);
 }
+template <class F>
 __global__ void __launch_bounds__(256) l21_rows_kernel(float2* M, int64_t ld, int64_t n_end, int64_t k0,
-                                                        int64_t sbeg, const float2* dinv, __nv_bfloat16* Ap,
+                                                        int64_t sbeg, const float2* dinv, typename F::T* Ap,
                                                         int64_t abase) {
   constexpr int NB = kBlk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1214,7 +1222,7 @@ __global__ void __launch_bounds__(256) l21_rows_kernel(float2* M, int64_t ld, in
       if (row < n_end) {
         const float2 v = X[r * kS + k];
         M[row * ld + k0 + k] = v;
-        if (Ap) emit_a(Ap, row - abase, k, v);
+        if (Ap) emit_a<F>(Ap, row - abase, k, v);
       }
     }
     __syncthreads();
@@ -1273,9 +1281,10 @@ constexpr int kU12Cols = 16;      // columns per CTA
 __host__ __device__ constexpr size_t u12_rows_smem(int nb) {
   return (size_t)(nb * kBlk * (kU12Cols + 1) + kBlk * (kBlk + 1)) * sizeof(float2);
 }
+template <class F>
 __global__ void __launch_bounds__(256, 3) u12_rows_kernel(float2* M, int64_t ld, int64_t K0, int nb, int64_t c_lo,
                                                        int64_t c_hi, const int* src_rows, int swap,
-                                                       __nv_bfloat16* Bp) {
+                                                       typename F::T* Bp) {
   constexpr int NB = kBlk, CW = kU12Cols;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1409,7 +1418,7 @@ __global__ void __launch_bounds__(256, 3) u12_rows_kernel(float2* M, int64_t ld,
       float2 bv[8];
 #pragma unroll
       for (int i = 0; i < 8; i++) bv[i] = Xs[k8 * 8 + i][cl];
-      emit_b8(Bp, col - c_lo, k8 * 8, bv, nb * NB);
+      emit_b8<F>(Bp, col - c_lo, k8 * 8, bv, nb * NB);
     }
   }
 }

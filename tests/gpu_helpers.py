@@ -126,6 +126,13 @@ class Engine:
     def set_pivoting(self, mode):
         self.check(self.lib.necgpu_set_pivoting(self.h, mode))
 
+    def set_update_format(self, fmt):
+        """0: chosen by size, 1: split BF16, 2: TF32 (necgpu_set_update_format)."""
+        self.check(self.lib.necgpu_set_update_format(self.h, fmt))
+
+    def update_format(self):
+        return self.lib.necgpu_update_format(self.h)
+
     def stats(self):
         st = NecgpuStats()
         self.check(self.lib.necgpu_get_stats(self.h, C.byref(st)))

@@ -195,22 +195,31 @@ def test_mixed_pivoting_modes(nb, oracle, engine, name, mode):
     nb.nec_delete(ctx)
 
 
+@pytest.mark.parametrize("fmt", [1, 2])
 @pytest.mark.parametrize("m,n,kb", [(300, 200, 64), (1000, 517, 64), (129, 1, 13), (2500, 2500, 64),
                                     (777, 1500, 256), (64, 4000, 64)])
-def test_tensor_core_update_matches_fp32(nb, engine, m, n, kb):
-    """The tcgen05 split-BF16x3 trailing update C -= A B against the CUDA-core
-    FP32 update of the same seeded operands, including ragged edges (m, n
-    not multiples of the 128 x 128-complex tile)."""
+def test_tensor_core_update_matches_fp32(nb, engine, m, n, kb, fmt):
+    """The tcgen05 trailing update C -= A B in both operand formats (1: split
+    BF16, three products; 2: one TF32 pass) against the CUDA-core FP32
+    update of the same seeded operands, including ragged edges (m, n not
+    multiples of the 128 x 128-complex tile)."""
     import ctypes as C
     L = nb.lib
     L.necgpu_check_tc_gemm.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_uint,
                                        C.POINTER(C.c_double), C.POINTER(C.c_double)]
     diff, ref = C.c_double(), C.c_double()
-    rc = L.necgpu_check_tc_gemm(engine.h, m, n, kb, 1234, C.byref(diff), C.byref(ref))
+    engine.set_update_format(fmt)
+    try:
+        rc = L.necgpu_check_tc_gemm(engine.h, m, n, kb, 1234, C.byref(diff), C.byref(ref))
+    finally:
+        engine.set_update_format(0)
     assert rc == 0, engine.err()
     assert ref.value > 0.1
-    # dropped lo*lo products and BF16 rounding: ~2^-16 |a||b| per product
-    assert diff.value <= 2e-4 * math.sqrt(kb), (diff.value, ref.value)
+    # split BF16: dropped lo*lo products and BF16 rounding, ~2^-16 |a||b|
+    # per product; TF32: operands rounded to 11 significant bits, ~2^-11
+    # |a||b| per product (|a|, |b| <= 0.5, random signs)
+    tol = 2e-4 if fmt == 1 else 1e-3
+    assert diff.value <= tol * math.sqrt(kb), (diff.value, ref.value)
 
 
 def test_fill_is_deterministic(nb, engine):
@@ -284,8 +293,9 @@ def test_excitation_only_resolve_and_pattern_reuse(nb, api, oracle):
     nb.nec_delete(c2)
 
 
-@pytest.mark.parametrize("n,seed", [(64, 1), (200, 2), (333, 3), (700, 4), (1100, 5)])
-def test_block_pivoted_lu_backward_error(nb, n, seed):
+@pytest.mark.parametrize("n,seed,fmt", [(64, 1, 1), (200, 2, 1), (333, 3, 1), (700, 4, 1), (1100, 5, 1),
+                                        (333, 3, 2), (1100, 5, 2)])
+def test_block_pivoted_lu_backward_error(nb, n, seed, fmt):
     """The mixed path's block-pivoted complex64 LU on seeded random matrices
     (pivoting inside every diagonal block; n not a multiple of 64; n > 256
     brings in the outer blocks, the far update beside the panels and the U12
@@ -298,12 +308,14 @@ def test_block_pivoted_lu_backward_error(nb, n, seed):
                                         C.POINTER(C.c_double), C.POINTER(C.c_int)]
     e = Engine(L)
     try:
+        e.set_update_format(fmt)
         berr, amax, moved = C.c_double(), C.c_double(), C.c_int()
         rc = L.necgpu_check_block_lu(e.h, n, seed, C.byref(berr), C.byref(amax), C.byref(moved))
         assert rc == 0, e.err()
         assert amax.value > 0.1
         assert moved.value > n // 4  # random blocks: most pivots come from another row
-        assert berr.value <= 5e-4, berr.value
+        # FP32 / split BF16 level, or the TF32 update's ~2^-11
+        assert berr.value <= (5e-4 if fmt == 1 else 5e-3), berr.value
         # the engine holds no structure afterwards
         assert L.necgpu_fill(e.h) != 0 and "no structure" in e.err()
     finally:

@@ -179,3 +179,75 @@ def test_sweep_forms_keep_parity(nb, oracle, name, clusters, monkeypatch):
     finally:
         e.close()
         nb.nec_delete(ctx)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmt", [1, 2])
+@pytest.mark.parametrize("name", ["helix2", "mesh_small", "yagi_ground"])
+def test_update_formats_keep_parity(nb, oracle, name, fmt):
+    """Both operand formats of the mixed LU's tensor-core update (1: split
+    BF16, 2: TF32) refine to the FP64 floor and match the oracle's currents
+    to 1e-9; the held factors report the format they were made in."""
+    from gpu_helpers import Engine
+    from helpers import host_case
+    ctx, st, rhs, _ = host_case(nb, CASES[name][0])
+    Zo, _ = oracle.fill(st)
+    x, _ = oracle.solve(Zo, rhs)
+    _, cur_o = oracle.coefficients(st, x)
+    e = Engine(nb.lib)
+    try:
+        e.set_update_format(fmt)
+        e.set_structure(st)
+        e.fill()
+        assert e.update_format() == 0  # nothing factored yet
+        e.factor(1)
+        assert e.update_format() == fmt
+        cur, _ = e.solve(rhs)
+        assert e.stats().refine_residual <= 1e-12
+        assert np.max(np.abs(cur - cur_o)) / np.max(np.abs(cur_o)) <= 1e-9
+    finally:
+        e.close()
+        nb.nec_delete(ctx)
+
+
+@pytest.mark.gpu
+def test_update_format_choice_and_demotion(nb, monkeypatch):
+    """The engine's own choice: split BF16 below the TF32 threshold; with
+    the threshold lowered, TF32 first, and after a TF32 factorisation whose
+    refinement took more than five steps (the 41 + 41-wire mesh of 3,280
+    unknowns takes about twelve, against six with split BF16) split BF16
+    for the engine's later factorisations, with the same currents."""
+    from gpu_helpers import Engine
+    from helpers import host_case
+    from cases import LARGE_CASES
+    ctx, st, rhs, _ = host_case(nb, LARGE_CASES["wire_mesh_41"][0])
+    e = Engine(nb.lib)
+    try:
+        e.set_structure(st)
+        e.fill()
+        e.factor(1)
+        assert e.update_format() == 1  # 3,280 unknowns: below the threshold
+        cur_ref, _ = e.solve(rhs)
+        iters_bf16 = e.stats().refine_iters
+    finally:
+        e.close()
+    monkeypatch.setenv("NECPP_B200_TF32_MIN_N", "1000")
+    e = Engine(nb.lib)
+    try:
+        e.set_structure(st)
+        e.fill()
+        e.factor(1)
+        assert e.update_format() == 2
+        cur1, _ = e.solve(rhs)
+        s1 = e.stats()
+        assert s1.refine_residual <= 1e-12 and s1.refine_iters > max(5, iters_bf16)
+        e.fill()
+        e.factor(1)
+        assert e.update_format() == 1  # demoted for the rest of the engine's life
+        cur2, _ = e.solve(rhs)
+        assert e.stats().refine_iters == iters_bf16
+        for c in (cur1, cur2):
+            assert np.max(np.abs(c - cur_ref)) / np.max(np.abs(cur_ref)) <= 1e-9
+    finally:
+        e.close()
+        nb.nec_delete(ctx)
