@@ -78,6 +78,16 @@ typedef struct necgpu_engine necgpu_engine;
  * owned per nec_context and released by nec_delete (src/libNEC.cpp:40-42). */
 int necgpu_create(necgpu_engine** out, int device);
 int necgpu_destroy(necgpu_engine* e);
+/* Engine reuse between short-lived users (nec_context does this): acquire
+ * takes the device's pooled engine if there is one (else creates one);
+ * release returns an engine to the pool, one per device, keeping its
+ * streams, buffers and captured LU graph but none of its results, tables
+ * or statistics.  An engine whose settings were changed (stream, timing,
+ * refinement, pivoting, update format, tuning, resident inputs) or that ran
+ * a test, batch, matrix or allocation-free entry point is destroyed
+ * instead, as is one whose stream reports an error. */
+int necgpu_acquire(necgpu_engine** out, int device);
+int necgpu_release(necgpu_engine* e);
 const char* necgpu_last_error(const necgpu_engine* e);
 
 /* Use the given cudaStream_t (as void*) for all work; NULL = the engine's own
@@ -192,7 +202,7 @@ typedef struct necgpu_stats {
   double refine_residual;   /* final ||b - Z x|| / ||b|| (FP64) */
   double ms_fill, ms_factor, ms_solve, ms_pattern; /* last timings (0 if not timed) */
   int64_t launches;         /* kernels launched by the engine since create */
-  int64_t h2d_bytes, d2h_bytes; /* host<->device bytes copied since create */
+  int64_t h2d_bytes, d2h_bytes; /* host<->device bytes copied since create (or acquire) */
   /* per kernel class, accumulated while kernel timing is on: CUDA-event time
      of every launch (ms), launch count, algorithmic flops of the launches */
   double k_ms[NECGPU_K_COUNT];

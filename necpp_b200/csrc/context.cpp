@@ -27,7 +27,7 @@ void check(necgpu_engine* e, int st) {
 
 Context::Context() {}
 Context::~Context() {
-  if (eng_) necgpu_destroy(eng_);
+  if (eng_) necgpu_release(eng_);
 }
 
 necgpu_engine* Context::engine() {
@@ -35,7 +35,7 @@ necgpu_engine* Context::engine() {
     int dev = 0;
     if (const char* s = std::getenv("NECPP_B200_DEVICE")) dev = std::atoi(s);
     necgpu_engine* e = nullptr;
-    int st = necgpu_create(&e, dev);
+    int st = necgpu_acquire(&e, dev);
     if (st != NECGPU_OK) {
       std::string msg = e ? necgpu_last_error(e) : "no CUDA device";
       if (e) necgpu_destroy(e);

@@ -78,6 +78,9 @@ struct necgpu_engine {
   double2* Z64 = nullptr;
   float2* Z32 = nullptr;
   int factored = -1;  // precision of the factors held, -1 none
+  // a setting was changed or a test or batch entry point used since the
+  // engine was created: necgpu_release destroys it instead of pooling it
+  bool touched = false;
   bool filled = false;
   int* d_piv = nullptr;
   int* d_src = nullptr;  // block-pivoted LU: gather order of each diagonal block's rows
@@ -2165,8 +2168,60 @@ int necgpu_destroy(necgpu_engine* e) {
 
 const char* necgpu_last_error(const necgpu_engine* e) { return e ? e->err.c_str() : "null engine"; }
 
+// One idle engine per device, kept between contexts: its streams, events,
+// device buffers, tuned kernel attributes and captured LU graph serve the
+// next structure of the same size without being built again.
+namespace {
+constexpr int kPoolDevices = 16;
+std::mutex g_pool_mutex;
+necgpu_engine* g_pool[kPoolDevices] = {};
+}  // namespace
+
+int necgpu_acquire(necgpu_engine** out, int device) {
+  if (!out) return NECGPU_ERR_ARG;
+  *out = nullptr;
+  if (device >= 0 && device < kPoolDevices) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (g_pool[device]) {
+      *out = g_pool[device];
+      g_pool[device] = nullptr;
+      return NECGPU_OK;
+    }
+  }
+  return necgpu_create(out, device);
+}
+
+int necgpu_release(necgpu_engine* e) {
+  if (!e) return NECGPU_OK;
+  if (e->touched || e->device < 0 || e->device >= kPoolDevices || cudaSetDevice(e->device) != cudaSuccess ||
+      cudaStreamSynchronize(e->stream) != cudaSuccess)
+    return necgpu_destroy(e);
+  // forget what belonged to the context: its factors, solution, tables, the
+  // interpolation cache's state and the engine-life format choice; keep the
+  // buffers (the captured LU graph refers to them)
+  e->factored = -1;
+  e->have_solution = false;
+  e->filled = false;
+  e->somm_ready = false;
+  e->adj_ready = false;
+  e->tf32_demoted = false;
+  e->interp_key = InterpKey{kInterpFresh, 0, 0, 0};
+  e->stats = necgpu_stats{};
+  e->launches = 0;
+  e->err.clear();
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pool[e->device]) {
+      g_pool[e->device] = e;
+      return NECGPU_OK;
+    }
+  }
+  return necgpu_destroy(e);
+}
+
 int necgpu_set_stream(necgpu_engine* e, void* stream) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   CUDA_TRY(cudaSetDevice(e->device));
   if (e->stream) CUDA_TRY(cudaStreamSynchronize(e->stream));
   if (stream == nullptr) {
@@ -2184,6 +2239,7 @@ int necgpu_set_stream(necgpu_engine* e, void* stream) {
 
 int necgpu_enable_timing(necgpu_engine* e, int on) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   e->timing = on != 0;
   e->timing_level = on;
   return NECGPU_OK;
@@ -2210,6 +2266,7 @@ int necgpu_reset_kernel_stats(necgpu_engine* e) {
 
 int necgpu_reuse_last_inputs(necgpu_engine* e) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   if (!e->last_rhs) return fail(e, NECGPU_ERR_ARG, "reuse_last_inputs: no solve has run");
   e->res_rhs = true;
   e->res_ndir = e->last_ndir;
@@ -2218,6 +2275,7 @@ int necgpu_reuse_last_inputs(necgpu_engine* e) {
 
 int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter) {
   if (!e || !(tol > 0) || max_iter < 0) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   e->refine_tol = tol;
   e->refine_max = max_iter;
   return NECGPU_OK;
@@ -2225,12 +2283,14 @@ int necgpu_set_refinement(necgpu_engine* e, double tol, int max_iter) {
 
 int necgpu_set_pivoting(necgpu_engine* e, int mode) {
   if (!e || (mode != 0 && mode != 1)) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   e->prefer_blockpiv = (mode == 1);
   return NECGPU_OK;
 }
 
 int necgpu_set_update_format(necgpu_engine* e, int format) {
   if (!e || format < 0 || format > 2) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   e->tc_format = format;
   e->tf32_demoted = false;
   return NECGPU_OK;
@@ -2422,6 +2482,7 @@ int necgpu_pattern(necgpu_engine* e, int ndir, const double* theta, const double
 
 int necgpu_device_z(necgpu_engine* e, void** z, int64_t* ld) {
   if (!e || !z || !ld) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   *z = e->Z64;
   *ld = e->ld;
   return NECGPU_OK;
@@ -2440,6 +2501,7 @@ int necgpu_copy_z(necgpu_engine* e, double* out) {
 int necgpu_set_resident(necgpu_engine* e, const double* rhs, int ndir, const double* theta,
                         const double* phi) {
   if (!e || !rhs || ndir < 0) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaMemcpyAsync(e->d_b, rhs, e->n * sizeof(double2), cudaMemcpyHostToDevice, e->stream));
   if (ndir > 0) {
@@ -2458,6 +2520,7 @@ int necgpu_set_resident(necgpu_engine* e, const double* rhs, int ndir, const dou
 // factorisation and the refinement's residual norms (mixed precision).
 int necgpu_step_resident(necgpu_engine* e, int precision) {
   if (!e || !e->res_rhs) return e ? fail(e, NECGPU_ERR_ARG, "step: no resident inputs") : NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   CUDA_TRY(cudaSetDevice(e->device));
   tick(e);
   TRY(fill_checked(e, precision == NECGPU_MIXED));
@@ -2480,6 +2543,7 @@ int necgpu_step_resident(necgpu_engine* e, int precision) {
 int necgpu_check_tc_gemm(necgpu_engine* e, int m, int n, int kb, unsigned seed, double* max_abs_diff,
                          double* max_abs_ref) {
   if (!e || m < 1 || n < 1 || kb < 1 || kb > 1024 || !max_abs_diff || !max_abs_ref) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   CUDA_TRY(cudaSetDevice(e->device));
   // operands at a 64-aligned offset o: A = X[o.., 0..kb), B = X[0..kb, o..),
   // C = X[o.., o..); rows of ld (a multiple of 64) keep C 16-byte aligned
@@ -2551,6 +2615,7 @@ __global__ void lu_residual_kernel(const float2* A, const float2* F, const int* 
 int necgpu_matrix_solve(necgpu_engine* e, int64_t n, const double* z, const double* b, int precision, double* x,
                         double* residual) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   if (!z || !b || !x || n < 1 || n > 65536) return fail(e, NECGPU_ERR_ARG, "matrix_solve: bad arguments");
   if (precision != NECGPU_FP64 && precision != NECGPU_MIXED)
     return fail(e, NECGPU_ERR_ARG, "matrix_solve: unknown precision");
@@ -2594,6 +2659,7 @@ int necgpu_matrix_solve(necgpu_engine* e, int64_t n, const double* z, const doub
 
 int necgpu_set_tuning(necgpu_engine* e, const necgpu_tuning* t) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   if (!t) {
     e->tuning_explicit = false;
     return NECGPU_OK;
@@ -2624,6 +2690,7 @@ int necgpu_tuning_lookup(const char* path, int precision, int64_t n, necgpu_tuni
 
 int necgpu_measure_peak(necgpu_engine* e, int kind, double* tflops) {
   if (!e || !tflops || kind < 0 || kind > 1) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   CUDA_TRY(cudaSetDevice(e->device));
   const int ctas = 4 * e->nsm;
   double* sink = nullptr;
@@ -2662,6 +2729,7 @@ int necgpu_measure_peak(necgpu_engine* e, int kind, double* tflops) {
 int necgpu_check_block_lu(necgpu_engine* e, int n, unsigned seed, double* backward_err, double* max_abs,
                           int* interchanges) {
   if (!e || n < 1 || n > 4096 || !backward_err || !max_abs || !interchanges) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   if (e->n > 0) return fail(e, NECGPU_ERR_ARG, "check_block_lu: needs an engine without a structure");
   CUDA_TRY(cudaSetDevice(e->device));
   // the factorisation runs on the engine's own buffers, as for a structure
@@ -3064,6 +3132,7 @@ int necgpu_batch_solve(necgpu_engine* e, int nprob, const necgpu_structure* stru
                        const double* phi, double* cur, float* gain, double* eth, double* eph, int* status,
                        double* residual) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   if (nprob < 1 || nprob > 65535 || !structs || !rhs || !cur || !status || ndir < 0 ||
       (ndir > 0 && (!theta || !phi || (!eth) != (!eph))) || (gain && (!feed || !volt || !wavelength)))
     return fail(e, NECGPU_ERR_ARG, "batch_solve: bad arguments");
@@ -3557,6 +3626,7 @@ extern "C" {
 
 int necgpu_solve_noalloc(necgpu_engine* e, const double* rhs_dev, double* cur_dev, double* abc_dev) {
   if (!e) return NECGPU_ERR_ARG;
+  e->touched = true;  // a setting or use that a pooled engine must not carry over
   if (!rhs_dev || !cur_dev) return fail(e, NECGPU_ERR_ARG, "solve_noalloc: null argument");
   const int64_t n = e->n;
   if (n > kNoAllocMaxN)
