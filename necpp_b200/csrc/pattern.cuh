@@ -52,26 +52,37 @@ __device__ __forceinline__ void seg_term(const SegPat& g, double rox, double roy
   // one sincos per term: sin(el +- sill) from the segment's sin / cos of el
   double ssill, csill;
   sincos(sill, &ssill, &csill);
+  const double stop = g.sel * csill + g.cel * ssill, sbot = g.sel * csill - g.cel * ssill;
   double a, too, boo;
-  if (fabs(omega) >= 1.0e-7)
-    a = 2. * ssill / omega;
-  else
-    a = (2. - omega * omega * el * el / 3.) * el;
-  if (fabs(top) >= 1.0e-7)
-    too = (g.sel * csill + g.cel * ssill) / top;
-  else
-    too = 1. - top * top / 6.;
-  if (fabs(bot) >= 1.0e-7)
-    boo = (g.sel * csill - g.cel * ssill) / bot;
-  else
-    boo = 1. - bot * bot / 6.;
+  if (fabs(omega) >= 1.0e-7 && fabs(top) >= 1.0e-7 && fabs(bot) >= 1.0e-7) {
+    // the usual case: the three quotients from one reciprocal
+    const double ob = omega * bot, r = 1.0 / (ob * top);
+    a = 2. * ssill * (top * bot * r);
+    too = stop * (ob * r);
+    boo = sbot * (omega * top * r);
+  } else {
+    if (fabs(omega) >= 1.0e-7)
+      a = 2. * ssill / omega;
+    else
+      a = (2. - omega * omega * el * el / 3.) * el;
+    if (fabs(top) >= 1.0e-7)
+      too = stop / top;
+    else
+      too = 1. - top * top / 6.;
+    if (fabs(bot) >= 1.0e-7)
+      boo = sbot / bot;
+    else
+      boo = 1. - bot * bot / 6.;
+  }
   double b = el * (boo - too);
   double c = el * (boo + too);
   double rr = a * g.air + b * g.bii + c * g.cir;
   double ri = a * g.aii - b * g.bir + c * g.cii;
-  double arg = 2.0 * pi * (g.x * rox + g.y * roy + g.z * roz);
+  // the phase 2 pi r.r_i (pi the constant above) as sincospi of
+  // r.r_i * 2 pi / pi_exact: the reduction of a multiple of pi is exact
+  constexpr double kTwoPiOverPi = 2.0 * 3.1415926536 / 3.141592653589793;
   double sn, cs;
-  sincos(arg, &sn, &cs);
+  sincospi(kTwoPiOverPi * (g.x * rox + g.y * roy + g.z * roz), &sn, &cs);
   *exa = mk(cs, sn) * mk(rr, ri);
 }
 
