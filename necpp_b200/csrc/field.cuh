@@ -364,30 +364,42 @@ __device__ double efld_compute(const SrcSeg& J, double xij, double yij, double a
   double rhoy = yij - sabj * zp;
   double rhoz = zij - salpr * zp;
   double rh = sqrt(rhox * rhox + rhoy * rhoy + rhoz * rhoz + ai * ai);
+  double r = sqrt(zp * zp + rh * rh);
+  const bool far = r >= P.rkh;
+  // the FP64 divide is the costliest operation of a far pair: 1 / rh for
+  // the three components and, for a far pair, 1 / r come from one
+  // reciprocal of rh r
+  double rinv = 0.0;
   if (rh <= 1.e-10) {
     rhox = 0.0;
     rhoy = 0.0;
     rhoz = 0.0;
+    if (far) rinv = 1.0 / r;
   } else {
-    // one reciprocal for the three components (the FP64 divide is the
-    // costliest operation of a far pair)
-    const double rhinv = 1.0 / rh;
+    double rhinv;
+    if (far) {
+      const double q = 1.0 / (rh * r);
+      rhinv = r * q;
+      rinv = rh * q;
+    } else {
+      rhinv = 1.0 / rh;
+    }
     rhox *= rhinv;
     rhoy *= rhinv;
     rhoz *= rhinv;
   }
-  double r = sqrt(zp * zp + rh * rh);
-  if (r >= P.rkh) {
+  if (far) {
     // lumped current element, 2798-2819, with the divisions by r, rmag and
-    // py = 2 pi r^2 folded into two reciprocals
-    const double rinv = 1.0 / r;
+    // py = 2 pi r^2 folded into that reciprocal
     double rmag = kTwoPiD * r;
     double cth = zp * rinv;
     double px = rh * rinv;
+    // exp(-j rmag) as sincospi of r * 2 pi / pi_exact (exact reduction)
+    constexpr double kTwoPiOverPi = kTwoPiD / 3.141592653589793;
     double sn, cs;
-    sincos(rmag, &sn, &cs);
+    sincospi(kTwoPiOverPi * r, &sn, &cs);
     cplx e0 = mk(cs, -sn);
-    const double rminv = 1.0 / rmag;
+    const double rminv = rinv * (1.0 / kTwoPiD);
     const double pyinv = rminv * rinv;  // 1 / py
     cplx e1 = (P.eta * cth * pyinv) * e0 * mk(1.0, -rminv);
     cplx e2 = (0.5 * P.eta * px * pyinv) * e0 * mk(1.0, rmag - rminv);
