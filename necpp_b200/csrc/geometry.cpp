@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
+#include <tuple>
 #include <thread>
 #include <unordered_map>
 #include <cstdint>
@@ -367,8 +368,11 @@ void Geometry::build_connections(int ignd) {
   // inside their lambdas would give them their own, empty, instances).
   static thread_local FlatGrid tl_grid;
   FlatGrid& grid = tl_grid;
+  // cells of four times the search distance: a query box then meets one
+  // or two cells per axis (3.4 on average, against 8 with cells of twice
+  // the distance), and the sparse end points add few candidates per cell
   if (use_grid)
-    grid.build((size_t)(2 * n), 2.0 * max_slen, [&](size_t code) {
+    grid.build((size_t)(2 * n), 4.0 * max_slen, [&](size_t code) {
       const int64_t i = (int64_t)(code >> 1);
       return (code & 1) ? V3{x2[i], y2[i], z2[i]} : V3{x[i], y[i], z[i]};
     });
@@ -663,13 +667,15 @@ void Geometry::check_overlaps() {
   // candidate pair once, a < p; with the grid the items are split over
   // worker threads, each visiting the pairs of its own items.
   const int nworkers = host_workers(2 * n, 512);
-  auto grid_pairs = [&](size_t count, auto pos, double reach, int workers, auto visit) {
+  // cell_factor: cell edge over reach (>= 2; larger for sparse points, so
+  // that a query meets fewer cells)
+  auto grid_pairs = [&](size_t count, auto pos, double reach, double cell_factor, int workers, auto visit) {
     if (std::isfinite(reach) && reach > 0.0 && count > 256) {
       // reused by the two searches and by later structures; workers use the
       // reference, not the thread_local name
       static thread_local FlatGrid tl_pair_grid;
       FlatGrid& grid = tl_pair_grid;
-      const double cell = 2.0 * reach;
+      const double cell = cell_factor * reach;
       grid.build(count, cell, pos);
       const double r2 = reach * reach * 3.0;
       auto range = [&](int w, size_t i0, size_t i1) {
@@ -716,7 +722,7 @@ void Geometry::check_overlaps() {
   // node classes: pairs of ends in contact, collected per worker, then joined
   {
     std::vector<std::vector<std::pair<size_t, size_t>>> touch(nworkers);
-    grid_pairs(ends.size(), [&](size_t i) { return ends[i].p; }, thr_max, nworkers,
+    grid_pairs(ends.size(), [&](size_t i) { return ends[i].p; }, thr_max, 4.0, nworkers,
                [&](int w, size_t a, size_t p) {
                  double t = std::max(ends[a].thr, ends[p].thr);
                  if (norm_l1(sub(ends[a].p, ends[p].p)) <= t) touch[w].push_back({a, p});
@@ -751,14 +757,13 @@ void Geometry::check_overlaps() {
   double reach = 0.0;
   for (auto& v : views) reach = std::max(reach, 0.5 * norm3(sub(v.b, v.a)) + v.r);
   // a centre inside a segment lies within `reach` of that segment's centre;
-  // each worker keeps its first violation, the lowest (inside, container)
-  // segment pair is reported
+  // every violation is collected per worker
   struct Hit {
-    int64_t inside = -1, container = -1;
-    double d = 0;
+    int64_t inside, container;
+    double d;
   };
-  std::vector<Hit> hits(nworkers);
-  grid_pairs(views.size(), [&](size_t i) { return views[i].c; }, reach, nworkers, [&](int w, size_t a, size_t p) {
+  std::vector<std::vector<Hit>> hits(nworkers);
+  grid_pairs(views.size(), [&](size_t i) { return views[i].c; }, reach, 2.0, nworkers, [&](int w, size_t a, size_t p) {
     if (!overlap_fatal_ || one_node(views[a].idx, views[p].idx)) return;
     const View* pairs[2][2] = {{&views[a], &views[p]}, {&views[p], &views[a]}};
     for (auto& pr : pairs) {
@@ -766,26 +771,47 @@ void Geometry::check_overlaps() {
       const View& container = *pr[1];
       double d = axis_distance(container, inside.c);
       if (d > container.r) continue;
-      Hit& h = hits[w];
-      if (h.inside < 0 || std::make_pair(inside.idx, container.idx) < std::make_pair(h.inside, h.container))
-        h = Hit{inside.idx, container.idx, d};
+      hits[w].push_back(Hit{inside.idx, container.idx, d});
     }
   });
-  const Hit* first = nullptr;
-  for (auto& h : hits)
-    if (h.inside >= 0 && (!first || std::make_pair(h.inside, h.container) < std::make_pair(first->inside, first->container)))
-      first = &h;
-  if (first) {
-    const View& inside = views[first->inside];
-    const View& container = views[first->container];
-    char buf[256];
-    snprintf(buf, sizeof(buf),
-             "GEOMETRY DATA ERROR -- SEGMENT #%lld (TAG ID #%d) MIDPOINT LIES WITHIN "
-             "SEGMENT #%lld (TAG ID #%d) AT DISTANCE %.5f RADIUS %.5f",
-             (long long)(inside.idx + 1), inside.tag, (long long)(container.idx + 1), container.tag, first->d,
-             container.r);
-    throw nec_error(buf);
+  size_t nhits = 0;
+  for (auto& h : hits) nhits += h.size();
+  if (nhits == 0) return;
+  // The reported violation is the first of the reference's sweep
+  // (c_geometry.cpp:1608-1633): centres in a stable order along their
+  // widest axis, pairs by (anchor, probe) in that order, the anchor's centre
+  // tested against the probe first.  The order is needed only here.
+  V3 lo = views[0].c, hi = lo;
+  for (auto& v : views) {
+    lo = V3{std::min(lo.x, v.c.x), std::min(lo.y, v.c.y), std::min(lo.z, v.c.z)};
+    hi = V3{std::max(hi.x, v.c.x), std::max(hi.y, v.c.y), std::max(hi.z, v.c.z)};
   }
+  const double ext[3] = {hi.x - lo.x, hi.y - lo.y, hi.z - lo.z};
+  int ax = 0;
+  for (int k = 1; k < 3; k++)
+    if (ext[k] > ext[ax]) ax = k;
+  std::vector<int64_t> sorted(views.size()), rank(views.size());
+  std::iota(sorted.begin(), sorted.end(), 0);
+  std::stable_sort(sorted.begin(), sorted.end(),
+                   [&](int64_t l, int64_t r) { return coord(views[l].c, ax) < coord(views[r].c, ax); });
+  for (size_t q = 0; q < sorted.size(); q++) rank[views[sorted[q]].idx] = (int64_t)q;
+  auto key = [&](const Hit& h) {
+    const int64_t ri = rank[h.inside], rc = rank[h.container];
+    return std::make_tuple(std::min(ri, rc), std::max(ri, rc), ri < rc ? 0 : 1);
+  };
+  const Hit* first = nullptr;
+  for (auto& lst : hits)
+    for (auto& h : lst)
+      if (!first || key(h) < key(*first)) first = &h;
+  const View& inside = views[first->inside];
+  const View& container = views[first->container];
+  char buf[256];
+  snprintf(buf, sizeof(buf),
+           "GEOMETRY DATA ERROR -- SEGMENT #%lld (TAG ID #%d) MIDPOINT LIES WITHIN "
+           "SEGMENT #%lld (TAG ID #%d) AT DISTANCE %.5f RADIUS %.5f",
+           (long long)(inside.idx + 1), inside.tag, (long long)(container.idx + 1), container.tag, first->d,
+           container.r);
+  throw nec_error(buf);
 }
 
 // geometry_complete, c_geometry.cpp:454-612 (wire part).

@@ -163,3 +163,27 @@ def test_library_exports_every_declared_symbol(nb):
     assert len(names) > 60
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
+
+
+@pytest.mark.parametrize("along_x", [False, True])
+@pytest.mark.parametrize("nseg", [9, 200, 1500])
+@pytest.mark.parametrize("z0", [-1.0, 0.3])
+def test_overlap_check_matches_reference(nb, ref, nseg, z0, along_x):
+    """The segment-overlap check (a midpoint inside another segment) gives
+    the reference's message, segment pair and distance both below the grid
+    search's size (the scan) and above it (cell grids over the ends and the
+    centres, end cells of four times the contact distance).  With several
+    overlapping pairs the reported one is the first of the reference's
+    sweep along the widest axis (z, or x when the wires lie along x)."""
+    def p(u, v, w):  # (offset, offset, position along the wires)
+        return (w, u, v) if along_x else (u, v, w)
+    msgs = []
+    for api in (nb, ref):
+        ctx = api.nec_create()
+        api.nec_wire(ctx, 1, nseg, *p(0, 0, -1), *p(0, 0, 1), 1e-3, 1, 1)
+        api.nec_wire(ctx, 2, nseg, *p(0, 0.0005, z0), *p(0, 0.0005, 1 + (1 + z0)), 1e-3, 1, 1)
+        rc = api.nec_geometry_complete(ctx, 0)
+        msgs.append((rc, nb.nec_error_message() if api is nb else ref.error()))
+        api.nec_delete(ctx)
+    assert msgs[0][0] == 1 and "MIDPOINT LIES WITHIN" in msgs[0][1]
+    assert msgs[0] == msgs[1]
