@@ -700,7 +700,7 @@ def run_b200(args):
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_m_max, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64 LU + c128 fill/refinement", "data": "synthetic",
+        "vs_baseline": None, "dtype": "c64 LU (%s tensor-core update) + c128 fill/refinement" % update_format, "data": "synthetic",
         "config": workload_config(args, world), "precision": "mixed",
         "gpu_launches": int(launches_m / args.steps * args.steps),
         "clocks": clocks,
