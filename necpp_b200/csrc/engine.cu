@@ -1957,8 +1957,10 @@ int fill_checked(necgpu_engine* e, bool want32) {
 namespace {
 
 // Column-tile source lists of a structure's basis tables (fill.cuh): for
-// every tile of 32 basis columns, the distinct contributing source segments
-// (ascending) and their (column, a, b, c) entries.  ecoef = a | b | c.
+// every tile of kFillTB basis columns, the distinct contributing source
+// segments (ascending) and their (column, a, b, c) entries.  ecoef = a | b | c.
+// Built by a counting sort of the trio entries over tiles: each tile's
+// entries keep the (source, entry) order of the trio tables.
 struct TileLists {
   std::vector<int32_t> tile_ptr, tsrc, tsrc_eptr;
   std::vector<uint8_t> ecol;
@@ -1966,47 +1968,44 @@ struct TileLists {
 };
 void build_tile_lists(const necgpu_structure* s, int64_t n, int ntiles, TileLists& L) {
   const int32_t* tp = s->trio_ptr;
-  struct Ent {
-    int32_t j;
-    uint8_t col;
-    double a, b, c;
-  };
-  std::vector<std::vector<Ent>> tiles(ntiles);
-  for (int64_t j = 0; j < n; j++)
-    for (int32_t k = tp[j]; k < tp[j + 1]; k++) {
-      int32_t bas = s->trio_basis[k];
-      tiles[bas / kFillTB].push_back(
-          Ent{(int32_t)j, (uint8_t)(bas % kFillTB), s->trio_a[k], s->trio_b[k], s->trio_c[k]});
-    }
+  const int64_t ne = tp[n];
+  // entry k of the trio tables goes to position at[tile] of the tile-sorted order
+  std::vector<int64_t> at(ntiles + 1, 0);
+  for (int64_t k = 0; k < ne; k++) at[s->trio_basis[k] / kFillTB + 1]++;
+  for (int t = 0; t < ntiles; t++) at[t + 1] += at[t];
+  std::vector<int32_t> src(ne), ent(ne);  // per sorted position: source segment, trio entry
+  {
+    std::vector<int64_t> next(at.begin(), at.end() - 1);
+    for (int64_t j = 0; j < n; j++)
+      for (int32_t k = tp[j]; k < tp[j + 1]; k++) {
+        const int64_t q = next[s->trio_basis[k] / kFillTB]++;
+        src[q] = (int32_t)j;
+        ent[q] = k;
+      }
+  }
   L.tile_ptr.assign(ntiles + 1, 0);
   L.tsrc.clear();
   L.tsrc_eptr.clear();
-  L.ecol.clear();
-  std::vector<double> ea, eb, ec;
+  L.tsrc.reserve(ne);
+  L.tsrc_eptr.reserve(ne + 1);
+  L.ecol.resize(ne);
+  L.ecoef.assign(3 * std::max<int64_t>(ne, 1), 0.0);
   for (int t = 0; t < ntiles; t++) {
-    auto& v = tiles[t];  // pushed in ascending source order
     L.tile_ptr[t] = (int32_t)L.tsrc.size();
-    size_t k = 0;
-    while (k < v.size()) {
-      const int32_t j = v[k].j;
-      L.tsrc.push_back(j);
-      L.tsrc_eptr.push_back((int32_t)L.ecol.size());
-      while (k < v.size() && v[k].j == j) {
-        L.ecol.push_back(v[k].col);
-        ea.push_back(v[k].a);
-        eb.push_back(v[k].b);
-        ec.push_back(v[k].c);
-        k++;
+    for (int64_t q = at[t]; q < at[t + 1]; q++) {
+      if (q == at[t] || src[q] != src[q - 1]) {
+        L.tsrc.push_back(src[q]);
+        L.tsrc_eptr.push_back((int32_t)q);
       }
+      const int32_t k = ent[q];
+      L.ecol[q] = (uint8_t)(s->trio_basis[k] % kFillTB);
+      L.ecoef[q] = s->trio_a[k];
+      L.ecoef[ne + q] = s->trio_b[k];
+      L.ecoef[2 * ne + q] = s->trio_c[k];
     }
   }
   L.tile_ptr[ntiles] = (int32_t)L.tsrc.size();
-  L.tsrc_eptr.push_back((int32_t)L.ecol.size());
-  const size_t ne = L.ecol.size();
-  L.ecoef.assign(3 * std::max<size_t>(ne, 1), 0.0);
-  std::copy(ea.begin(), ea.end(), L.ecoef.begin());
-  std::copy(eb.begin(), eb.end(), L.ecoef.begin() + ne);
-  std::copy(ec.begin(), ec.end(), L.ecoef.begin() + 2 * ne);
+  L.tsrc_eptr.push_back((int32_t)ne);
 }
 
 // Per segment: the basis functions with support on it, ascending basis (the
@@ -2023,9 +2022,17 @@ void build_coef_lists(const necgpu_structure* s, int64_t n, CoefLists& C) {
   C.ccoef.assign(3 * std::max<int64_t>(ntrio, 1), 0.0);
   std::vector<int> order;
   for (int64_t j = 0; j < n; j++) {
+    // a segment has a few entries: a stable insertion sort by basis
     order.clear();
-    for (int32_t k = tp[j]; k < tp[j + 1]; k++) order.push_back(k);
-    std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return s->trio_basis[p] < s->trio_basis[q]; });
+    for (int32_t k = tp[j]; k < tp[j + 1]; k++) {
+      size_t q = order.size();
+      order.push_back(k);
+      while (q > 0 && s->trio_basis[order[q - 1]] > s->trio_basis[k]) {
+        order[q] = order[q - 1];
+        q--;
+      }
+      order[q] = k;
+    }
     C.cptr[j] = tp[j];
     for (size_t q = 0; q < order.size(); q++) {
       const int k = order[q];
